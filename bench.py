@@ -1,0 +1,388 @@
+"""Benchmark: FP64 finite-volume channel DNS cell-steps/s on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                    [--workload channel384_implicit|channel64_explicit]
+
+One "step" is one full RK3 time step (3 stages: momentum, semi-implicit
+wall-normal Crank-Nicolson, FFT/Thomas projection, lagged-pressure update)
+of the whole grid, preceded by its CFL reduction, as in the reference's
+solve! loop.  The default workload is the production channel: 384x256x384,
+domain 4pi x 2 x 4pi/3, tanh(1.5) stretching, nu = 1/395, body force 1,
+ydiffusion = :implicit, CFL 0.8, initial condition = a Reichardt mean
+profile (Re_tau = 395) plus seeded splitmix64 noise of amplitude 0.2.
+Synthetic data of that shape: the reference publishes no dataset.
+
+Prints ONE JSON line on rank 0.  Under torchrun (N > 1) each rank advances
+an independent replica (the single-GPU step does not shard without the
+multi-GPU transposes; weak scaling, no collective in the data path).
+--impl reference times the CPU oracle (a C/OpenMP restatement of the
+reference's Julia path; the Julia reference cannot run here) on the host
+cores, on rank 0 only.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+
+WORKLOADS = {
+    "channel384_implicit": dict(
+        n=(384, 256, 384), ydiffusion="implicit", visc=1 / 395, cfl=0.8, amp=0.2, retau=395.0,
+        bytes_per_cell_step=1080.0),
+    "channel64_explicit": dict(
+        n=(64, 64, 64), ydiffusion="explicit", visc=1 / 180, cfl=0.5, amp=0.1, retau=None,
+        bytes_per_cell_step=792.0),
+}
+COMMON = dict(lims=((0.0, 4 * math.pi), (-1.0, 1.0), (0.0, 4 * math.pi / 3)),
+              bc=("periodic", "wall", "periodic"), bodyforce=(1.0, 0.0, 0.0))
+
+# Algorithmic HBM passes (one FP64 field = nx*ny*nz*8 bytes) per launch of
+# each kernel kind on the default path; the half-spectrum counts
+# (nx/2+1)/(nx/2) of a real field.  Momentum reads q only from stage 2 on.
+def passes(kind, implicit, spec):
+    if kind == "momentum":
+        return (12 + 13 + 13) / 3 if implicit else (9 + 12 + 12) / 3
+    return {"cn_solve": 9.0, "div_rfft_x": 3 + spec, "fft_z": 2 * spec, "y_solve": 2 * spec,
+            "ifft_z": 2 * spec, "irfft_x": spec + 1, "grad_update": 9.0 if implicit else 7.0,
+            "other": 0.0}[kind]
+
+
+def tanhstretch(beta):
+    return lambda t: (math.tanh(beta * (2 * t - 1)) / math.tanh(beta) + 1) / 2
+
+
+def reichardt(y, retau):
+    """Reichardt mean profile in wall units (u_tau = 1, half height 1)."""
+    yp = (1 - np.abs(y)) * retau
+    k = 0.41
+    return (np.log1p(k * yp) / k + 7.8 * (1 - np.exp(-yp / 11) - (yp / 11) * np.exp(-yp / 3)))
+
+
+def mean_profile(wl):
+    if wl["retau"] is None:
+        return lambda x, y, z: 1.5 * (1 - y ** 2)
+    return lambda x, y, z: reichardt(y, wl["retau"]) + 0 * x
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_init():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+# ------------------------------------------------------------------ CPU arm
+
+def cpu_oracle_run(wl, nsteps, nwarm, dt=None):
+    """Advance the CPU oracle nwarm + nsteps steps; returns (seconds for
+    nsteps, threads, dt used)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    O.build()
+    threads = os.cpu_count() or 1
+    O.set_threads(threads)
+    s = O.Setup(wl["n"], lims=COMMON["lims"], bc=COMMON["bc"], stretch=tanhstretch(1.5),
+                visc=wl["visc"], bodyforce=COMMON["bodyforce"], ydiffusion=wl["ydiffusion"])
+    u = s.vectorfield()
+    prof = mean_profile(wl)
+    nx, ny, nz = s.n
+    s.interior(u["x"])[:] = np.broadcast_to(
+        prof(s.xf[None, None, :], s.yc[None, :, None], s.zc[:, None, None]), (nz, ny, nx))
+    for c in "xyz":
+        s.noise(u[c], c, 0, wl["amp"])
+    s.exchange_halo(u)
+    p = s.scalarfield()
+    q = s.vectorfield()
+    delta = s.scalarfield() if s.imexy else p
+    s.project(u, delta)
+    if dt is None:
+        dt = s.cfl_timestep(u, wl["cfl"])
+    for _ in range(nwarm):
+        s.step(u, p, q, delta, dt)
+    t0 = time.perf_counter()
+    for _ in range(nsteps):
+        s.step(u, p, q, delta, dt)
+    return time.perf_counter() - t0, threads, dt
+
+
+def reference_arm(args, wl, world, rank):
+    if rank != 0:
+        return
+    cells = math.prod(wl["n"])
+    secs, threads, _ = cpu_oracle_run(wl, args.steps, args.warmup)
+    value = cells * args.steps / secs
+    line = {
+        "metric": "DNS cell-steps/s (FP64)", "impl": "reference", "value": value,
+        "unit": "cell-steps/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * secs / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "grid": list(wl["n"]),
+                   "ydiffusion": wl["ydiffusion"], "parallelism": "host cores (OpenMP)"},
+        "cpu_baseline": {"value": value, "unit": "cell-steps/s", "cores": threads, "kind": "port",
+                         "sample": f"{args.steps} RK3 steps of the full grid after {args.warmup} "
+                                   "warm-up steps (C/OpenMP restatement of the Julia reference; "
+                                   "Julia is not available)"},
+        "e2e": {"value": value, "unit": "cell-steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------- GPU arm
+
+def b200_arm(args, wl, world, rank, local):
+    import ctypes
+
+    import torch
+
+    import distributednavierstokes_b200 as dns
+    from distributednavierstokes_b200 import _lib
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=dev)
+    lib = _lib.load()
+    s = dns.setup(n=wl["n"], stretch=tanhstretch(1.5), visc=wl["visc"],
+                  ydiffusion=wl["ydiffusion"], device=dev, **COMMON)
+    nx, ny, nz = s.n
+    cells = nx * ny * nz
+    G = s.shape[0] * s.shape[1] * s.shape[2]
+    u = dns.vectorfield(s)
+    dns.velocityfield(u, s, x=mean_profile(wl))
+    for c in "xyz":
+        dns.noise(u[c], c, s, 0, wl["amp"])
+    dns.exchange_halo(u, s)
+    host_ic = {c: u[c].cpu().pin_memory() for c in "xyz"}   # for the end-to-end leg
+    p = dns.scalarfield(s)
+    q = dns.vectorfield(s)
+    delta = dns.scalarfield(s) if s.imexy else p
+    dns.project(u, delta, s)
+    stream = torch.cuda.current_stream(dev)
+
+    def one_step(cached):
+        dt = dns.cfl_timestep(u, s, wl["cfl"], use_step_max=cached)
+        dns.step(u, p, q, delta, s, dt)
+        return dt
+
+    for i in range(args.warmup):
+        one_step(i > 0)
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize(dev)
+    ctx = s.ctx
+    lib.dnsb_profile(ctx, 1)
+    n0 = lib.dnsb_launch_count(ctx)
+    clocks = ClockSampler(local)
+    clocks.start()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for i in range(args.steps):
+        one_step(True)
+    ev1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms = ev0.elapsed_time(ev1)
+    clk = clocks.stop()
+    launches = lib.dnsb_launch_count(ctx) - n0
+    kinds = {}
+    for k, name in enumerate(_lib.KINDS):
+        t, n = ctypes.c_double(), ctypes.c_long()
+        lib.dnsb_profile_read(ctx, k, ctypes.byref(t), ctypes.byref(n))
+        kinds[name] = (t.value, n.value)
+    lib.dnsb_profile(ctx, 0)
+    if world > 1:
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+        torch.distributed.barrier()
+    assert dns.maxdiv(u, s) < 1e-10, "benchmark state lost incompressibility"
+    value = world * cells * args.steps / (ms / 1e3)
+
+    # roofline of the dominant kernel kind (by device time in the timed region)
+    peak, peak_kind = measured_peaks()
+    spec = (nx // 2 + 1) / (nx // 2)
+    dom = max((k for k in kinds if k != "other"), key=lambda k: kinds[k][0])
+    t_dom, n_dom = kinds[dom]
+    bytes_launch = passes(dom, s.imexy, spec) * cells * 8
+    achieved = bytes_launch / (t_dom / n_dom / 1e3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", f"traffic_{args.workload}.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            traffic = json.load(f).get(dom)
+    per_kernel = {}
+    for k, (t, n) in kinds.items():
+        if n == 0:
+            continue
+        b = passes(k, s.imexy, spec) * cells * 8
+        per_kernel[k] = {"launches": n, "ms_avg": t / n, "share": t / sum(v[0] for v in kinds.values()),
+                         "gbs": (b / (t / n / 1e3) / 1e9) if b else None}
+    step_bytes = wl["bytes_per_cell_step"] * cells
+    step_gbs = step_bytes / (ms / args.steps / 1e3) / 1e9
+
+    # end to end through the C ABI with host buffers (dnsb_solve_host):
+    # H2D of the initial velocity, initial projection, K CFL steps, D2H of u, p
+    hu = {c: host_ic[c].clone().pin_memory() for c in "xyz"}
+    hp = torch.zeros_like(hu["x"]).pin_memory()
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        torch.distributed.barrier()
+    t_out, n_out = ctypes.c_double(), ctypes.c_long()
+    t0 = time.perf_counter()
+    rc = lib.dnsb_solve_host(s.ctx, *(ctypes.c_void_p(h.data_ptr()) for h in
+                                      (hu["x"], hu["y"], hu["z"], hp)),
+                             0.0, 1e9, 0.0, wl["cfl"], args.steps, ctypes.byref(t_out),
+                             ctypes.byref(n_out))
+    e2e_s = time.perf_counter() - t0
+    _lib.check(rc, s._ctx)
+    if world > 1:
+        t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = world * cells * n_out.value / e2e_s
+    h2d = 3 * G * 8 / n_out.value
+    d2h = (4 * G * 8 + 24 * n_out.value) / n_out.value
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        secs, threads, _ = cpu_oracle_run(wl, args.cpu_steps, 1)
+        cpu = {"value": cells * args.cpu_steps / secs, "unit": "cell-steps/s", "cores": threads,
+               "kind": "port",
+               "sample": f"{args.cpu_steps} RK3 steps of the full {nx}x{ny}x{nz} grid after 1 "
+                         "warm-up step, CPU oracle (C/OpenMP restatement of the Julia "
+                         "reference) on all host threads"}
+
+    if rank == 0:
+        line = {
+            "metric": "DNS cell-steps/s (FP64)", "value": value, "unit": "cell-steps/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": args.workload, "grid": [nx, ny, nz],
+                       "ydiffusion": wl["ydiffusion"], "cfl": wl["cfl"],
+                       "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+                       "l2": "inputs larger than L2 (each field %.0f MB)" % (G * 8 / 1e6)},
+            "e2e": {"value": e2e, "unit": "cell-steps/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h,
+                    "note": "dnsb_solve_host: pinned host u in, initial projection, "
+                            f"{n_out.value} CFL steps, u and p out"},
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                         "peak_source": peak_kind,
+                         "algorithmic_bytes_per_launch": bytes_launch},
+            "step_roofline": {"bytes_per_cell_step": wl["bytes_per_cell_step"],
+                              "achieved": step_gbs, "peak": peak, "unit": "GB/s",
+                              "frac": step_gbs / peak},
+            "kernels": per_kernel,
+            "gpu_launches": launches,
+            "clocks": clk,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    s.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="channel384_implicit", choices=list(WORKLOADS))
+    ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3) if args.impl == "b200" else args.warmup
+    wl = WORKLOADS[args.workload]
+    world, rank, local = dist_init()
+    if args.impl == "reference":
+        reference_arm(args, wl, world, rank)
+    else:
+        b200_arm(args, wl, world, rank, local)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,13 @@
+"""distributednavierstokes_b200: the single-GPU finite-volume time step of
+DistributedNavierStokes as hand-written sm_100a CUDA kernels behind a C ABI
+(include/dnsb.h, libdnsb.so), with a host-side mirror of the reference's
+setup/solve API (api.py).
+"""
+from .api import (  # noqa: F401
+    RK3, State, VectorField, channelprofiles, channelstats, cfl_timestep, divergence,
+    energyspectrum, exchange_halo, imex_update, interior, kinetic_energy, logger, maxdiv,
+    momentum, noise, poisson, pressuregrad_component, pressuregrad_update, project,
+    scalarfield, setup, solve, spectrumstats, step, vectorfield, velocityfield,
+)
+
+__version__ = "0.1.0"

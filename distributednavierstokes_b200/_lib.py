@@ -1,0 +1,98 @@
+"""ctypes binding of libdnsb.so (the C ABI declared in include/dnsb.h).
+
+The shared library is built in-tree (see build.py) and loaded from this
+package directory.  There is no fallback: if the library is missing or a
+symbol is absent, importing the operators fails loudly.
+"""
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIBPATH = os.path.join(_HERE, "libdnsb.so")
+
+DNSB_OK = 0
+ERRORS = {1: "invalid argument", 2: "CUDA error", 3: "unsupported size", 4: "out of memory"}
+
+c_double = ctypes.c_double
+c_int = ctypes.c_int
+c_long = ctypes.c_long
+c_void_p = ctypes.c_void_p
+P = c_void_p
+
+
+class dnsb_grid(ctypes.Structure):
+    _fields_ = [
+        ("nx", c_int), ("ny", c_int), ("nz", c_int),
+        ("bc_y", c_int), ("ydiffusion", c_int),
+        ("dx", c_double), ("dz", c_double),
+        ("dy", P), ("dyu", P),
+        ("visc", c_double),
+        ("bodyforce", c_double * 3),
+    ]
+
+
+# name -> (restype, argtypes); every symbol declared in include/dnsb.h
+SIGNATURES = {
+    "dnsb_version": (c_int, []),
+    "dnsb_create": (c_int, [ctypes.POINTER(dnsb_grid), c_int, P, ctypes.POINTER(c_void_p)]),
+    "dnsb_destroy": (None, [P]),
+    "dnsb_last_error": (ctypes.c_char_p, [P]),
+    "dnsb_set_stream": (c_int, [P, P]),
+    "dnsb_sync": (c_int, [P]),
+    "dnsb_fill_ghosts": (c_int, [P, P, c_int]),
+    "dnsb_divergence": (c_int, [P, P, P, P, P]),
+    "dnsb_momentum": (c_int, [P, P, P, P, P, P, P, c_double, c_double]),
+    "dnsb_pressuregrad": (c_int, [P, P, P, c_int, c_double]),
+    "dnsb_poisson": (c_int, [P, P, P]),
+    "dnsb_project": (c_int, [P, P, P, P, P]),
+    "dnsb_imex_update": (c_int, [P, P, P, P, P, P, P, P, c_double, c_double, c_double]),
+    "dnsb_step": (c_int, [P, P, P, P, P, P, P, P, P, c_double]),
+    "dnsb_cfl": (c_int, [P, P, P, P, c_double, c_int, ctypes.POINTER(c_double)]),
+    "dnsb_solve": (c_int, [P, P, P, P, P, P, P, P, P, c_double, c_double, c_double, c_double,
+                           c_long, ctypes.POINTER(c_double), ctypes.POINTER(c_long)]),
+    "dnsb_solve_host": (c_int, [P, P, P, P, P, c_double, c_double, c_double, c_double, c_long,
+                                ctypes.POINTER(c_double), ctypes.POINTER(c_long)]),
+    "dnsb_maxdiv": (c_int, [P, P, P, P, ctypes.POINTER(c_double)]),
+    "dnsb_kinetic_energy": (c_int, [P, P, P, P, ctypes.POINTER(c_double)]),
+    "dnsb_channel_sample": (c_int, [P, P, P, P, P]),
+    "dnsb_spectrum_sample": (c_int, [P, P, P, P, P, c_int]),
+    "dnsb_noise": (c_int, [P, P, c_int, ctypes.c_ulonglong, c_double]),
+    "dnsb_profile": (c_int, [P, c_int]),
+    "dnsb_profile_read": (c_int, [P, c_int, ctypes.POINTER(c_double), ctypes.POINTER(c_long)]),
+    "dnsb_launch_count": (c_long, [P]),
+    "dnsb_kind_name": (ctypes.c_char_p, [c_int]),
+}
+
+KINDS = ["momentum", "cn_solve", "div_rfft_x", "fft_z", "y_solve", "ifft_z", "irfft_x",
+         "grad_update", "other"]
+
+_LIB = None
+
+
+def load():
+    """Load libdnsb.so and bind every entry point (raises if anything is missing)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(LIBPATH):
+        raise ImportError(
+            f"{LIBPATH} is missing: build it with `python -m distributednavierstokes_b200.build` "
+            "(nvcc, sm_100a); there is no CPU fallback")
+    lib = ctypes.CDLL(LIBPATH)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)  # AttributeError if the symbol is absent
+        fn.restype = res
+        fn.argtypes = args
+    _LIB = lib
+    return lib
+
+
+class DNSBError(RuntimeError):
+    pass
+
+
+def check(rc, ctx=None):
+    if rc != DNSB_OK:
+        msg = load().dnsb_last_error(ctx)
+        msg = msg.decode() if msg else ""
+        raise DNSBError(f"libdnsb: {ERRORS.get(rc, rc)}: {msg}")

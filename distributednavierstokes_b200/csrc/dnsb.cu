@@ -1,0 +1,987 @@
+// dnsb.cu -- context, plans and the C ABI of libdnsb.so (see include/dnsb.h).
+//
+// One RK3 stage (step!, src/timestep.jl:41-63) is, on the default path,
+//   explicit: k_momentum<EXPLICIT>  q, W = u + B q            (+ W halos)
+//             k_rfftx<DIVERGENCE>   S = rfft_x(div W)
+//             k_fftz                S = fft_z(S)
+//             k_thomas | k_yfourier solve in y
+//             k_fftz<inv>, k_irfftx psi (+ halos)
+//             k_grad<EXPLICIT>      u = W - grad psi          (+ u halos)
+//   implicit: k_momentum<IMPLICIT>  q, V = u + B q - a dt grad p
+//             k_cn                  u = (I - th Dy)^-1 (V + th Dy u)  (+ halos)
+//             Poisson as above      delta (+ halos)
+//             k_grad<IMPLICIT>      u -= grad delta, p += delta/(a dt) (+ halos)
+// so that no separate halo, copy or transpose kernel runs.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/dnsb.h"
+#include "common.cuh"
+#include "fft.cuh"
+#include "spectral.cuh"
+#include "stencil.cuh"
+
+using namespace dnsb;
+
+namespace {
+
+const double RK_A[3] = {0.0, -5.0 / 9.0, -153.0 / 128.0};
+const double RK_B[3] = {1.0 / 3.0, 15.0 / 16.0, 8.0 / 15.0};
+const double RK_AL[3] = {1.0 / 3.0, 5.0 / 12.0, 1.0 / 4.0};
+
+char g_create_err[512] = "";
+
+// exp(-2 pi i t / n) evaluated in long double and rounded once, with exact
+// values at the quarter turns.
+double2 unit_root(long t, long n) {
+  t %= n;
+  if (t < 0) t += n;
+  const long double pi = 3.141592653589793238462643383279502884L;
+  long double x = (long double)t / (long double)n;
+  long double c = cosl(2.0L * pi * x), s = sinl(2.0L * pi * x);
+  if (t == 0) { c = 1; s = 0; }
+  else if (4 * t == n) { c = 0; s = 1; }
+  else if (2 * t == n) { c = -1; s = 0; }
+  else if (4 * t == 3 * n) { c = 0; s = -1; }
+  return make_double2((double)c, -(double)s);
+}
+
+// modλ (src/poisson.jl:12): 2 (cospi(2(k-1)/n) - 1) / Δ^2, k = 1-based
+double modlam(int k1, int n, double d) {
+  const long double pi = 3.141592653589793238462643383279502884L;
+  double x = (double)(2 * (k1 - 1)) / (double)n;
+  double c = (double)cosl((long double)x * pi);
+  if (k1 - 1 == 0) c = 1.0;
+  else if (4 * (k1 - 1) == n || 4 * (k1 - 1) == 3 * n) c = 0.0;
+  else if (2 * (k1 - 1) == n) c = -1.0;
+  return 2 * (c - 1) / (d * d);
+}
+
+}  // namespace
+
+struct dnsb_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  Geo g{};
+  int implicit = 0;
+  double dymin = 0;
+  // device tables
+  double *dy = nullptr, *dyu = nullptr, *rdy = nullptr, *rdyu = nullptr;
+  double *lam1 = nullptr, *lam2 = nullptr, *lam3 = nullptr;
+  double *ay = nullptr, *by = nullptr, *cy = nullptr;
+  double *ycoef = nullptr;  // [at bt ct an bn cn] x ny
+  double *ytab = nullptr;   // [3 stages][2 sets][ta cp ib] x ny
+  double2 *twM = nullptr, *twN = nullptr, *twz = nullptr, *twy = nullptr;
+  FFTPlan pM{}, pz{}, py{};
+  int Lx = 1, Lz = 1, Ly = 1;
+  size_t smem_rx = 0, smem_ix = 0, smem_z = 0, smem_y = 0;
+  // scratch
+  double2 *S = nullptr;
+  double *work = nullptr;
+  double *r = nullptr;
+  double *W[3] = {nullptr, nullptr, nullptr};
+  double *V[3] = {nullptr, nullptr, nullptr};
+  unsigned long long *umax = nullptr;  // [3] max |u_c| of the last step; [3] scratch
+  double *partial = nullptr;           // reduction partials
+  double *hostred = nullptr;           // pinned, 8 doubles
+  const double *umax_for[3] = {nullptr, nullptr, nullptr};
+  // launch counting and per-kind CUDA-event timing (dnsb_profile)
+  long launches = 0;
+  bool prof_on = false;
+  std::vector<cudaEvent_t> evpool;
+  size_t evused = 0;
+  std::vector<std::pair<int, size_t>> recs;  // (kind, index of the start event)
+  double prof_ms[DNSB_NKINDS] = {};
+  long prof_n[DNSB_NKINDS] = {};
+  std::vector<void *> allocs;
+  std::string err;
+};
+
+namespace {
+
+constexpr int RED_BLOCKS = 1184;
+
+int fail(dnsb_ctx *c, int code, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  if (c) c->err = buf;
+  else snprintf(g_create_err, sizeof g_create_err, "%s", buf);
+  return code;
+}
+
+#define CK(ctx, call)                                                                        \
+  do {                                                                                       \
+    cudaError_t e_ = (call);                                                                 \
+    if (e_ != cudaSuccess)                                                                   \
+      return fail(ctx, DNSB_ECUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, \
+                  __LINE__);                                                                 \
+  } while (0)
+
+#define CKL(ctx) CK(ctx, cudaGetLastError())
+
+const char *KIND_NAMES[DNSB_NKINDS] = {"momentum", "cn_solve", "div_rfft_x", "fft_z", "y_solve",
+                                       "ifft_z", "irfft_x", "grad_update", "other"};
+
+int prof_harvest(dnsb_ctx *c) {
+  if (c->recs.empty()) { c->evused = 0; return 0; }
+  CK(c, cudaEventSynchronize(c->evpool[c->recs.back().second + 1]));
+  for (auto &r : c->recs) {
+    float ms = 0;
+    CK(c, cudaEventElapsedTime(&ms, c->evpool[r.second], c->evpool[r.second + 1]));
+    c->prof_ms[r.first] += ms;
+    c->prof_n[r.first] += 1;
+  }
+  c->recs.clear();
+  c->evused = 0;
+  return 0;
+}
+
+int prof_begin(dnsb_ctx *c, int kind) {
+  (void)kind;
+  c->launches++;
+  if (!c->prof_on) return 0;
+  if (c->evused + 2 > c->evpool.size()) {
+    int rc = prof_harvest(c);
+    if (rc) return rc;
+  }
+  CK(c, cudaEventRecord(c->evpool[c->evused], c->stream));
+  return 0;
+}
+
+int prof_end(dnsb_ctx *c, int kind) {
+  if (!c->prof_on) return 0;
+  CK(c, cudaEventRecord(c->evpool[c->evused + 1], c->stream));
+  c->recs.push_back({kind, c->evused});
+  c->evused += 2;
+  return 0;
+}
+
+// Launch with counting and (when enabled) event timing of its kind.
+#define LAUNCH(ctx, kind, ...)                       \
+  do {                                               \
+    int rc_ = prof_begin(ctx, kind);                 \
+    if (rc_) return rc_;                             \
+    __VA_ARGS__;                                     \
+    CKL(ctx);                                        \
+    rc_ = prof_end(ctx, kind);                       \
+    if (rc_) return rc_;                             \
+  } while (0)
+
+template <class T>
+int dalloc(dnsb_ctx *c, T **p, size_t n) {
+  void *v = nullptr;
+  cudaError_t e = cudaMalloc(&v, n * sizeof(T) > 0 ? n * sizeof(T) : 16);
+  if (e != cudaSuccess)
+    return fail(c, DNSB_ENOMEM, "cudaMalloc(%zu bytes): %s", n * sizeof(T), cudaGetErrorString(e));
+  c->allocs.push_back(v);
+  *p = (T *)v;
+  return 0;
+}
+
+template <class T>
+int upload(dnsb_ctx *c, T **p, const std::vector<T> &h) {
+  int rc = dalloc(c, p, h.size());
+  if (rc) return rc;
+  CK(c, cudaMemcpy(*p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+  return 0;
+}
+
+dim3 cell_grid(const Geo &g) { return dim3((g.nx + 31) / 32, (g.ny + 7) / 8, g.nz); }
+const dim3 cell_block(32, 8, 1);
+
+CFields3 cf(const double *x, const double *y, const double *z) { return CFields3{x, y, z}; }
+Fields3 ff(double *x, double *y, double *z) { return Fields3{x, y, z}; }
+
+template <class K>
+int allow_smem(dnsb_ctx *c, K kernel, size_t bytes) {
+  if (bytes > 48 * 1024)
+    CK(c, cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  return 0;
+}
+
+// ----------------------------------------------------------- reductions --
+
+__global__ void k_maxabs3(Geo g, CFields3 u, unsigned long long *out) {
+  double m[3] = {0, 0, 0};
+  const long long n = (long long)g.nx * g.ny * g.nz;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int I = (int)(t % g.nx) + 1;
+    const long long r = t / g.nx;
+    const int J = (int)(r % g.ny) + 1, K = (int)(r / g.ny) + 1;
+    const long long c0 = gidx(g, I, J, K);
+    m[0] = fmax(m[0], fabs(u.x[c0]));
+    m[1] = fmax(m[1], fabs(u.y[c0]));
+    m[2] = fmax(m[2], fabs(u.z[c0]));
+  }
+  for (int c = 0; c < 3; c++) {
+    double v = m[c];
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out + c, dbits(v));
+  }
+}
+
+__global__ void k_maxdiv(Geo g, CFields3 u, unsigned long long *out) {
+  double m = 0;
+  const long long n = (long long)g.nx * g.ny * g.nz;
+  const long long sy = g.NX, sz = (long long)g.NX * g.NY;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int I = (int)(t % g.nx) + 1;
+    const long long r = t / g.nx;
+    const int J = (int)(r % g.ny) + 1, K = (int)(r / g.ny) + 1;
+    const long long c0 = gidx(g, I, J, K);
+    const double d = (u.x[c0] - u.x[c0 - 1]) * g.rdx + (u.y[c0] - u.y[c0 - sy]) * g.rdy[J] +
+                     (u.z[c0] - u.z[c0 - sz]) * g.rdz;
+    m = fmax(m, fabs(d));
+  }
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, dbits(m));
+}
+
+__device__ double block_sum(double v) {
+  __shared__ double sh[32];
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) sh[w] = v;
+  __syncthreads();
+  v = 0;
+  if (w == 0) {
+    const int nw = (blockDim.x + 31) >> 5;
+    v = l < nw ? sh[l] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  }
+  return v;  // valid in thread 0
+}
+
+// kinetic energy partials: sum of u_c^2 dx D2[J] dz / 2 over ranges[c]
+__global__ void k_ke_partial(Geo g, CFields3 u, double *partial) {
+  double s = 0;
+  const long long n = (long long)g.nx * g.ny * g.nz;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int I = (int)(t % g.nx) + 1;
+    const long long r = t / g.nx;
+    const int J = (int)(r % g.ny) + 1, K = (int)(r / g.ny) + 1;
+    const long long c0 = gidx(g, I, J, K);
+    const double vx = u.x[c0], vz = u.z[c0];
+    s += vx * vx * g.dx * g.dy[J] * g.dz / 2;
+    s += vz * vz * g.dx * g.dy[J] * g.dz / 2;
+    if (J <= g.jymax) {
+      const double vy = u.y[c0];
+      s += vy * vy * g.dx * g.dyu[J] * g.dz / 2;
+    }
+  }
+  s = block_sum(s);
+  if (threadIdx.x == 0) partial[blockIdx.x] = s;
+}
+
+__global__ void k_sum_final(const double *partial, int n, double *out) {
+  double s = 0;
+  for (int t = threadIdx.x; t < n; t += blockDim.x) s += partial[t];
+  s = block_sum(s);
+  if (threadIdx.x == 0) *out = s;
+}
+
+// channel plane sums (sample_channelstats!, src/stats.jl:39-58): one block
+// per y row; rows 0..ny-1 cell quantities, rows ny..ny+nf-1 face quantities
+__global__ void k_channel(Geo g, CFields3 u, double *acc, int nf) {
+  const int row = blockIdx.x;
+  const bool face = row >= g.ny;
+  const int J = (face ? row - g.ny : row) + 1;
+  double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+  const long long n = (long long)g.nx * g.nz;
+  const long long sy = g.NX;
+  for (long long t = threadIdx.x; t < n; t += blockDim.x) {
+    const int I = (int)(t % g.nx) + 1, K = (int)(t / g.nx) + 1;
+    const long long c0 = gidx(g, I, J, K);
+    if (!face) {
+      const double x = u.x[c0], z = u.z[c0];
+      s0 += x; s1 += z; s2 += x * x; s3 += z * z;
+    } else {
+      const double v = u.y[c0];
+      const double uf = (u.x[c0] + u.x[c0 + sy]) / 2;
+      const double vf = (u.y[c0] + u.y[c0 + 1]) / 2;
+      s0 += v; s1 += v * v; s2 += uf; s3 += uf * vf;
+    }
+  }
+  s0 = block_sum(s0);
+  s1 = block_sum(s1);
+  s2 = block_sum(s2);
+  s3 = block_sum(s3);
+  if (threadIdx.x == 0) {
+    if (!face) {
+      const int j = J - 1;
+      acc[j] += s0; acc[g.ny + j] += s1; acc[2 * g.ny + j] += s2; acc[3 * g.ny + j] += s3;
+    } else {
+      double *f = acc + 4 * g.ny;
+      const int j = J - 1;
+      f[j] += s0; f[nf + j] += s1; f[2 * nf + j] += s2; f[3 * nf + j] += s3;
+    }
+  }
+}
+
+// binshells! (src/stats.jl:143-157): 1/2 |u_hat|^2 / N^2 into integer
+// shells round(|k|), conjugate modes 0 < kx < nx/2 counted twice
+__global__ void k_binshells(Geo g, const double2 *S, double *E, int nbins) {
+  const long long n = (long long)g.nkx * g.ny * g.nz;
+  const double N = (double)g.nx * g.ny * g.nz;
+  const double N2 = N * N;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int kz0 = (int)(t % g.nz);
+    const long long r = t / g.nz;
+    const int j = (int)(r % g.ny), kx = (int)(r / g.ny);
+    const int ky = j > g.ny / 2 ? j - g.ny : j;
+    const int kz = kz0 > g.nz / 2 ? kz0 - g.nz : kz0;
+    const int kap = (int)llrint(sqrt((double)(kx * kx + ky * ky + kz * kz)));
+    const double wgt = (0 < kx && 2 * kx < g.nx) ? 2.0 : 1.0;
+    const double2 a = S[t];
+    const double a2 = a.x * a.x + a.y * a.y;
+    if (kap < nbins) atomicAdd(E + kap, wgt * a2 / 2 / N2);
+  }
+}
+
+__device__ __forceinline__ unsigned long long splitmix64(unsigned long long x) {
+  unsigned long long z = x + 0x9e3779b97f4a7c15ULL;
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+  return z ^ (z >> 31);
+}
+
+__global__ void k_noise(Geo g, double *phi, int c, unsigned long long seed, double amp) {
+  const int I = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int J = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  const int K = blockIdx.z + 1;
+  const int jh = c == STAG_Y ? g.jymax : g.ny;
+  if (I > g.nx || J > jh) return;
+  const unsigned long long key =
+      (((unsigned long long)c * g.nz + (K - 1)) * g.ny + (J - 1)) * g.nx + (I - 1);
+  const unsigned long long rr = splitmix64(seed + key);
+  const double U = ((double)(rr >> 11) + 0.5) * 0x1p-53;
+  const long long c0 = gidx(g, I, J, K);
+  phi[c0] += amp * (2 * U - 1);
+}
+
+// ------------------------------------------------------------- pipeline --
+
+int ensure_device(dnsb_ctx *c) {
+  CK(c, cudaSetDevice(c->device));
+  return 0;
+}
+
+// rfft_x of the divergence of (a, b, cc) (mode RIN_DIVERGENCE), of the
+// ghost-free real a (RIN_REAL) or of the interior of field a (RIN_FIELD)
+int launch_rfftx(dnsb_ctx *c, int mode, const double *a, const double *b, const double *cc) {
+  const Geo &g = c->g;
+  dim3 grid(g.ny * ((g.nz + c->Lx - 1) / c->Lx));
+  if (mode == RIN_DIVERGENCE)
+    LAUNCH(c, DNSB_KIND_RFFTX, k_rfftx<RIN_DIVERGENCE><<<grid, SPEC_THREADS, c->smem_rx, c->stream>>>(g, c->S, a, b, cc, c->pM, c->Lx, c->twM, c->twN));
+  else if (mode == RIN_REAL)
+    LAUNCH(c, DNSB_KIND_RFFTX, k_rfftx<RIN_REAL><<<grid, SPEC_THREADS, c->smem_rx, c->stream>>>(g, c->S, a, b, cc, c->pM, c->Lx, c->twM, c->twN));
+  else
+    LAUNCH(c, DNSB_KIND_RFFTX, k_rfftx<RIN_FIELD><<<grid, SPEC_THREADS, c->smem_rx, c->stream>>>(g, c->S, a, b, cc, c->pM, c->Lx, c->twM, c->twN));
+  return 0;
+}
+
+int launch_fftz(dnsb_ctx *c, bool inv) {
+  const Geo &g = c->g;
+  long long nlines = (long long)g.ny * g.nkx;
+  dim3 grid((unsigned)((nlines + c->Lz - 1) / c->Lz));
+  if (inv) LAUNCH(c, DNSB_KIND_IFFTZ, k_fftz<true><<<grid, SPEC_THREADS, c->smem_z, c->stream>>>(g, c->S, c->pz, c->Lz, c->twz));
+  else LAUNCH(c, DNSB_KIND_FFTZ, k_fftz<false><<<grid, SPEC_THREADS, c->smem_z, c->stream>>>(g, c->S, c->pz, c->Lz, c->twz));
+  return 0;
+}
+
+int launch_ysolve(dnsb_ctx *c) {
+  const Geo &g = c->g;
+  if (g.wall) {
+    long long n = (long long)g.nkx * g.nz;
+    LAUNCH(c, DNSB_KIND_YSOLVE, k_thomas<<<(unsigned)((n + 127) / 128), 128, 0, c->stream>>>(g, c->S, c->work, c->ay, c->by, c->cy, c->lam1, c->lam3));
+  } else {
+    dim3 grid(g.nkx * ((g.nz + c->Ly - 1) / c->Ly));
+    LAUNCH(c, DNSB_KIND_YSOLVE, k_yfourier<false><<<grid, SPEC_THREADS, c->smem_y, c->stream>>>(g, c->S, c->py, c->Ly, c->twy, c->lam1, c->lam2, c->lam3));
+  }
+  return 0;
+}
+
+int launch_irfftx(dnsb_ctx *c, int mode, double *out) {
+  const Geo &g = c->g;
+  dim3 grid(g.ny * ((g.nz + c->Lx - 1) / c->Lx));
+  if (mode == ROUT_INTERIOR)
+    LAUNCH(c, DNSB_KIND_IRFFTX, k_irfftx<ROUT_INTERIOR><<<grid, SPEC_THREADS, c->smem_ix, c->stream>>>(g, c->S, out, c->pM, c->Lx, c->twM, c->twN));
+  else if (mode == ROUT_IMAGES)
+    LAUNCH(c, DNSB_KIND_IRFFTX, k_irfftx<ROUT_IMAGES><<<grid, SPEC_THREADS, c->smem_ix, c->stream>>>(g, c->S, out, c->pM, c->Lx, c->twM, c->twN));
+  else
+    LAUNCH(c, DNSB_KIND_IRFFTX, k_irfftx<ROUT_REAL><<<grid, SPEC_THREADS, c->smem_ix, c->stream>>>(g, c->S, out, c->pM, c->Lx, c->twM, c->twN));
+  return 0;
+}
+
+// S already holds rfft_x(rhs): finish the Poisson solve into out
+int poisson_from_spectrum(dnsb_ctx *c, int outmode, double *out) {
+  int rc;
+  if ((rc = launch_fftz(c, false))) return rc;
+  if ((rc = launch_ysolve(c))) return rc;
+  if ((rc = launch_fftz(c, true))) return rc;
+  return launch_irfftx(c, outmode, out);
+}
+
+int do_step(dnsb_ctx *c, double *ux, double *uy, double *uz, double *p, double *qx, double *qy,
+            double *qz, double *delta, double dt) {
+  const Geo &g = c->g;
+  int rc;
+  CK(c, cudaMemsetAsync(c->umax, 0, 3 * sizeof(unsigned long long), c->stream));
+  if (c->implicit)
+    LAUNCH(c, DNSB_KIND_OTHER,
+           k_cn_tables<<<1, 32, 0, c->stream>>>(g.ny, c->ycoef, c->ytab, dt, g.visc, RK_AL[0],
+                                                RK_AL[1], RK_AL[2]));
+  for (int s = 0; s < 3; s++) {
+    const double A = RK_A[s], B = RK_B[s], al = RK_AL[s];
+    const int readq = A != 0.0;
+    unsigned long long *um = s == 2 ? c->umax : nullptr;
+    if (!c->implicit) {
+      LAUNCH(c, DNSB_KIND_MOMENTUM,
+             k_momentum<MOM_EXPLICIT><<<cell_grid(g), cell_block, 0, c->stream>>>(
+                 g, ff(qx, qy, qz), cf(ux, uy, uz), ff(c->W[0], c->W[1], c->W[2]), nullptr, A, dt,
+                 B, 0.0, readq));
+      if ((rc = launch_rfftx(c, RIN_DIVERGENCE, c->W[0], c->W[1], c->W[2]))) return rc;
+      if ((rc = poisson_from_spectrum(c, ROUT_IMAGES, p))) return rc;
+      LAUNCH(c, DNSB_KIND_GRAD,
+             k_grad<GRAD_EXPLICIT><<<cell_grid(g), cell_block, 0, c->stream>>>(
+                 g, ff(ux, uy, uz), cf(c->W[0], c->W[1], c->W[2]), p, nullptr, 0.0, um));
+    } else {
+      const double adt = al * dt;
+      LAUNCH(c, DNSB_KIND_MOMENTUM,
+             k_momentum<MOM_IMPLICIT><<<cell_grid(g), cell_block, 0, c->stream>>>(
+                 g, ff(qx, qy, qz), cf(ux, uy, uz), ff(c->V[0], c->V[1], c->V[2]), p, A, dt, B,
+                 adt, readq));
+      const double th = al * dt * g.visc / 2;
+      LAUNCH(c, DNSB_KIND_CN,
+             k_cn<<<dim3((g.nx + 63) / 64, g.nz, 3), 64, 0, c->stream>>>(
+                 g, ff(ux, uy, uz), cf(c->V[0], c->V[1], c->V[2]), cf(ux, uy, uz), c->ycoef,
+                 c->ytab + (long long)s * 6 * g.ny, th));
+      if ((rc = launch_rfftx(c, RIN_DIVERGENCE, ux, uy, uz))) return rc;
+      if ((rc = poisson_from_spectrum(c, ROUT_IMAGES, delta))) return rc;
+      LAUNCH(c, DNSB_KIND_GRAD,
+             k_grad<GRAD_IMPLICIT><<<cell_grid(g), cell_block, 0, c->stream>>>(
+                 g, ff(ux, uy, uz), cf(ux, uy, uz), delta, p, 1.0 / adt, um));
+    }
+  }
+  c->umax_for[0] = ux;
+  c->umax_for[1] = uy;
+  c->umax_for[2] = uz;
+  return 0;
+}
+
+int do_project(dnsb_ctx *c, double *ux, double *uy, double *uz, double *psi) {
+  const Geo &g = c->g;
+  int rc;
+  if ((rc = launch_rfftx(c, RIN_DIVERGENCE, ux, uy, uz))) return rc;
+  if ((rc = poisson_from_spectrum(c, ROUT_IMAGES, psi))) return rc;
+  LAUNCH(c, DNSB_KIND_GRAD,
+         k_grad<GRAD_EXPLICIT><<<cell_grid(g), cell_block, 0, c->stream>>>(
+             g, ff(ux, uy, uz), cf(ux, uy, uz), psi, nullptr, 0.0, nullptr));
+  c->umax_for[0] = c->umax_for[1] = c->umax_for[2] = nullptr;
+  return 0;
+}
+
+int fill3(dnsb_ctx *c, double *ux, double *uy, double *uz) {
+  const Geo &g = c->g;
+  double *f[3] = {ux, uy, uz};
+  for (int s = 0; s < 3; s++) {
+    k_fill_ghosts<<<4 * 148, 256, 0, c->stream>>>(g, f[s], s);
+    CKL(c);
+  }
+  return 0;
+}
+
+int cfl_from_max(dnsb_ctx *c, double cfl, const unsigned long long *bits, double *dt_out) {
+  const Geo &g = c->g;
+  const double eps = 2.220446049250313e-16;
+  double mx[3];
+  for (int i = 0; i < 3; i++) {
+    long long b = (long long)bits[i];
+    memcpy(&mx[i], &b, sizeof(double));
+  }
+  const double c1 = g.dx / (mx[0] + eps), c2 = c->dymin / (mx[1] + eps), c3 = g.dz / (mx[2] + eps);
+  const double conv = std::fmin(std::fmin(c1, c2), c3);
+  const double invdy2 = c->implicit ? 0.0 : 1 / (c->dymin * c->dymin);
+  const double diff = 1 / (2 * g.visc * (1 / (g.dx * g.dx) + invdy2 + 1 / (g.dz * g.dz)) + eps);
+  *dt_out = std::fmin(cfl * conv, cfl * diff);
+  return 0;
+}
+
+}  // namespace
+
+// ================================================================== C ABI ==
+
+extern "C" {
+
+int dnsb_version(void) { return DNSB_VERSION; }
+
+const char *dnsb_last_error(const dnsb_ctx *ctx) { return ctx ? ctx->err.c_str() : g_create_err; }
+
+int dnsb_create(const dnsb_grid *gr, int device, void *stream, dnsb_ctx **out) {
+  if (!gr || !out) return fail(nullptr, DNSB_EINVAL, "null argument");
+  *out = nullptr;
+  const int nx = gr->nx, ny = gr->ny, nz = gr->nz;
+  if (nx < 2 || ny < 2 || nz < 1 || nx % 2)
+    return fail(nullptr, DNSB_EINVAL, "need nx >= 2 even, ny >= 2, nz >= 1 (got %d %d %d)", nx, ny, nz);
+  if (gr->bc_y != DNSB_BC_PERIODIC && gr->bc_y != DNSB_BC_WALL)
+    return fail(nullptr, DNSB_EINVAL, "bc[2] must be :periodic or :wall");
+  if (gr->ydiffusion != DNSB_YDIFF_EXPLICIT && gr->ydiffusion != DNSB_YDIFF_IMPLICIT)
+    return fail(nullptr, DNSB_EINVAL, "ydiffusion must be :explicit or :implicit");
+  if (gr->ydiffusion == DNSB_YDIFF_IMPLICIT && gr->bc_y != DNSB_BC_WALL)
+    return fail(nullptr, DNSB_EINVAL, "implicit y-diffusion requires bc[2] == :wall");
+  if (!gr->dy || !gr->dyu) return fail(nullptr, DNSB_EINVAL, "dy/dyu missing");
+  const int M = nx / 2;
+  if (M > 4096 || nz > 4096 || ny > 4096)
+    return fail(nullptr, DNSB_EUNSUP, "FFT lengths above 4096 are not supported");
+  dnsb_ctx *c = new dnsb_ctx();
+  c->device = device;
+  c->stream = (cudaStream_t)stream;
+  c->implicit = gr->ydiffusion == DNSB_YDIFF_IMPLICIT;
+  auto bail = [&](int rc) {
+    g_create_err[0] = 0;
+    snprintf(g_create_err, sizeof g_create_err, "%s", c->err.c_str());
+    dnsb_destroy(c);
+    return rc;
+  };
+  if (cudaSetDevice(device) != cudaSuccess) {
+    fail(c, DNSB_ECUDA, "cudaSetDevice(%d) failed", device);
+    return bail(DNSB_ECUDA);
+  }
+  if (!make_fft_plan(M, c->pM) || !make_fft_plan(nz, c->pz) ||
+      (gr->bc_y == DNSB_BC_PERIODIC && !make_fft_plan(ny, c->py))) {
+    fail(c, DNSB_EUNSUP, "FFT lengths nx/2=%d, nz=%d%s must factor into 2, 3, 5", M, nz,
+         gr->bc_y == DNSB_BC_PERIODIC ? ", ny" : "");
+    return bail(DNSB_EUNSUP);
+  }
+  Geo &g = c->g;
+  g.nx = nx; g.ny = ny; g.nz = nz;
+  g.NX = nx + 2; g.NY = ny + 2; g.NZ = nz + 2;
+  g.wall = gr->bc_y == DNSB_BC_WALL;
+  g.jymax = g.wall ? ny - 1 : ny;
+  g.nkx = M + 1;
+  g.dx = gr->dx; g.dz = gr->dz;
+  g.rdx = 1.0 / g.dx; g.rdz = 1.0 / g.dz;
+  g.rdx2 = 1.0 / (g.dx * g.dx); g.rdz2 = 1.0 / (g.dz * g.dz);
+  g.visc = gr->visc;
+  g.fx = gr->bodyforce[0]; g.fy = gr->bodyforce[1]; g.fz = gr->bodyforce[2];
+  g.epsy = c->implicit ? 0.0 : 1.0;  // src/setup.jl:108
+
+  std::vector<double> dy(gr->dy, gr->dy + ny + 2), dyu(gr->dyu, gr->dyu + ny + 2);
+  std::vector<double> rdy(ny + 2), rdyu(ny + 2);
+  for (int J = 0; J < ny + 2; J++) { rdy[J] = 1.0 / dy[J]; rdyu[J] = 1.0 / dyu[J]; }
+  c->dymin = dy[1];
+  for (int J = 1; J <= ny; J++) c->dymin = std::fmin(c->dymin, dy[J]);
+  int rc;
+  if ((rc = upload(c, &c->dy, dy)) || (rc = upload(c, &c->dyu, dyu)) ||
+      (rc = upload(c, &c->rdy, rdy)) || (rc = upload(c, &c->rdyu, rdyu)))
+    return bail(rc);
+  g.dy = c->dy; g.dyu = c->dyu; g.rdy = c->rdy; g.rdyu = c->rdyu;
+
+  // plan_poisson (src/poisson.jl:56-120), w = 1: Julia's Δye[j+w] is dy[j]
+  std::vector<double> lam1(g.nkx), lam3(nz), lam2(ny);
+  for (int k = 1; k <= g.nkx; k++) lam1[k - 1] = modlam(k, nx, g.dx);
+  for (int k = 1; k <= nz; k++) lam3[k - 1] = modlam(k, nz, g.dz);
+  for (int k = 1; k <= ny; k++) lam2[k - 1] = modlam(k, ny, dy[1]);
+  std::vector<double> ay(ny, 0.0), by(ny, 0.0), cy(ny, 0.0);
+  if (g.wall) {
+    for (int j = 1; j <= ny; j++) {
+      double a = j == 1 ? 0.0 : 1 / (dy[j] * dyu[j - 1]);
+      double cc = j == ny ? 0.0 : 1 / (dy[j] * dyu[j]);
+      ay[j - 1] = a; cy[j - 1] = cc; by[j - 1] = -(a + cc);
+    }
+  } else {
+    double mx = dy[1], mn = dy[1];
+    for (int J = 1; J <= ny; J++) { mx = std::fmax(mx, dy[J]); mn = std::fmin(mn, dy[J]); }
+    if (!(mx - mn < 1e-12 * mx)) {
+      fail(c, DNSB_EINVAL, "periodic y requires a uniform grid (stretch = identity)");
+      return bail(DNSB_EINVAL);
+    }
+  }
+  // ydiffusion_coefficients (src/ydiffusion.jl:31-51)
+  std::vector<double> yc(6 * (size_t)ny, 0.0);
+  double *at = yc.data(), *bt = at + ny, *ct = bt + ny, *an = ct + ny, *bn = an + ny, *cn = bn + ny;
+  for (int j = 1; j <= ny; j++) {
+    double a = 1 / (dy[j] * dyu[j - 1]);
+    double cc = 1 / (dy[j] * dyu[j]);
+    at[j - 1] = j == 1 ? 0.0 : a;
+    ct[j - 1] = j == ny ? 0.0 : cc;
+    bt[j - 1] = j == 1 ? -(cc + 2 * a) : j == ny ? -(a + 2 * cc) : -(a + cc);
+  }
+  for (int j = 1; j <= ny - 1; j++) {
+    double a = 1 / (dyu[j] * dy[j]);
+    double cc = 1 / (dyu[j] * dy[j + 1]);
+    an[j - 1] = j == 1 ? 0.0 : a;
+    cn[j - 1] = j == ny - 1 ? 0.0 : cc;
+    bn[j - 1] = -(a + cc);
+  }
+  std::vector<double2> twM(M), twN(M + 1), twz(nz), twy(ny);
+  for (int t = 0; t < M; t++) twM[t] = unit_root(t, M);
+  for (int t = 0; t <= M; t++) twN[t] = unit_root(t, nx);
+  for (int t = 0; t < nz; t++) twz[t] = unit_root(t, nz);
+  for (int t = 0; t < ny; t++) twy[t] = unit_root(t, ny);
+  if ((rc = upload(c, &c->lam1, lam1)) || (rc = upload(c, &c->lam2, lam2)) ||
+      (rc = upload(c, &c->lam3, lam3)) || (rc = upload(c, &c->ay, ay)) ||
+      (rc = upload(c, &c->by, by)) || (rc = upload(c, &c->cy, cy)) ||
+      (rc = upload(c, &c->ycoef, yc)) || (rc = upload(c, &c->twM, twM)) ||
+      (rc = upload(c, &c->twN, twN)) || (rc = upload(c, &c->twz, twz)) ||
+      (rc = upload(c, &c->twy, twy)))
+    return bail(rc);
+  if ((rc = dalloc(c, &c->ytab, 18 * (size_t)ny))) return bail(rc);
+
+  // launch shapes: L lines per CTA, two line buffers each within ~100 KB
+  auto pow2floor = [](int v) { int p = 1; while (2 * p <= v) p *= 2; return p; };
+  const int budget = 100 * 1024 / (2 * (int)sizeof(double2));  // complex per buffer
+  c->Lx = pow2floor(std::max(1, std::min({8, nz, budget / (M + 2)})));
+  c->Lz = std::max(1, std::min(8, budget / (nz + 1)));
+  c->Ly = pow2floor(std::max(1, std::min({8, nz, budget / ny})));
+  c->smem_rx = sizeof(double2) * (2 * (size_t)c->Lx * (M + 1) + M + (M + 1));
+  c->smem_ix = sizeof(double2) * (2 * (size_t)c->Lx * (M + 2) + M + (M + 1));
+  c->smem_z = sizeof(double2) * (2 * (size_t)c->Lz * (nz + 1) + nz);
+  c->smem_y = sizeof(double2) * (2 * (size_t)c->Ly * ny + ny);
+  if ((rc = allow_smem(c, k_rfftx<RIN_DIVERGENCE>, c->smem_rx)) ||
+      (rc = allow_smem(c, k_rfftx<RIN_REAL>, c->smem_rx)) ||
+      (rc = allow_smem(c, k_rfftx<RIN_FIELD>, c->smem_rx)) ||
+      (rc = allow_smem(c, k_irfftx<ROUT_INTERIOR>, c->smem_ix)) ||
+      (rc = allow_smem(c, k_irfftx<ROUT_IMAGES>, c->smem_ix)) ||
+      (rc = allow_smem(c, k_irfftx<ROUT_REAL>, c->smem_ix)) ||
+      (rc = allow_smem(c, k_fftz<false>, c->smem_z)) ||
+      (rc = allow_smem(c, k_fftz<true>, c->smem_z)) ||
+      (rc = allow_smem(c, k_yfourier<false>, c->smem_y)) ||
+      (rc = allow_smem(c, k_yfourier<true>, c->smem_y)))
+    return bail(rc);
+
+  // scratch
+  const size_t G = (size_t)g.NX * g.NY * g.NZ;
+  const size_t nspec = (size_t)g.nkx * ny * nz;
+  if ((rc = dalloc(c, &c->S, nspec)) || (rc = dalloc(c, &c->r, (size_t)nx * ny * nz)) ||
+      (rc = dalloc(c, &c->umax, 8)) || (rc = dalloc(c, &c->partial, RED_BLOCKS + 8)))
+    return bail(rc);
+  if (g.wall && (rc = dalloc(c, &c->work, nspec))) return bail(rc);
+  for (int i = 0; i < 3; i++) {
+    if (!c->implicit) {
+      if ((rc = dalloc(c, &c->W[i], G))) return bail(rc);
+      if (cudaMemset(c->W[i], 0, G * sizeof(double)) != cudaSuccess) {
+        fail(c, DNSB_ECUDA, "cudaMemset failed");
+        return bail(DNSB_ECUDA);
+      }
+    } else {
+      if ((rc = dalloc(c, &c->V[i], G))) return bail(rc);
+    }
+  }
+  if (cudaMallocHost(&c->hostred, 8 * sizeof(double)) != cudaSuccess) {
+    fail(c, DNSB_ENOMEM, "cudaMallocHost failed");
+    return bail(DNSB_ENOMEM);
+  }
+  if (cudaDeviceSynchronize() != cudaSuccess) {
+    fail(c, DNSB_ECUDA, "device synchronisation after setup failed");
+    return bail(DNSB_ECUDA);
+  }
+  *out = c;
+  return DNSB_OK;
+}
+
+void dnsb_destroy(dnsb_ctx *c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  else cudaDeviceSynchronize();
+  for (auto &e : c->evpool) cudaEventDestroy(e);
+  for (void *p : c->allocs) cudaFree(p);
+  if (c->hostred) cudaFreeHost(c->hostred);
+  delete c;
+}
+
+int dnsb_set_stream(dnsb_ctx *c, void *stream) {
+  if (!c) return DNSB_EINVAL;
+  c->stream = (cudaStream_t)stream;
+  return 0;
+}
+
+int dnsb_sync(dnsb_ctx *c) {
+  if (!c) return DNSB_EINVAL;
+  if (ensure_device(c)) return DNSB_ECUDA;
+  CK(c, cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int dnsb_fill_ghosts(dnsb_ctx *c, double *phi, int stag) {
+  if (!c || !phi || stag < 0 || stag > 3) return c ? fail(c, DNSB_EINVAL, "bad argument") : DNSB_EINVAL;
+  if (ensure_device(c)) return DNSB_ECUDA;
+  k_fill_ghosts<<<4 * 148, 256, 0, c->stream>>>(c->g, phi, stag);
+  CKL(c);
+  c->umax_for[0] = c->umax_for[1] = c->umax_for[2] = nullptr;
+  return 0;
+}
+
+int dnsb_divergence(dnsb_ctx *c, double *r, const double *ux, const double *uy, const double *uz) {
+  if (!c || !r || !ux || !uy || !uz) return c ? fail(c, DNSB_EINVAL, "null field") : DNSB_EINVAL;
+  if (ensure_device(c)) return DNSB_ECUDA;
+  k_divergence<<<cell_grid(c->g), cell_block, 0, c->stream>>>(c->g, r, cf(ux, uy, uz));
+  CKL(c);
+  return 0;
+}
+
+int dnsb_momentum(dnsb_ctx *c, double *qx, double *qy, double *qz, const double *ux,
+                  const double *uy, const double *uz, double A, double dt) {
+  if (!c || !qx || !qy || !qz || !ux || !uy || !uz)
+    return c ? fail(c, DNSB_EINVAL, "null field") : DNSB_EINVAL;
+  if (ensure_device(c)) return DNSB_ECUDA;
+  k_momentum<MOM_ONLY><<<cell_grid(c->g), cell_block, 0, c->stream>>>(
+      c->g, ff(qx, qy, qz), cf(ux, uy, uz), ff(nullptr, nullptr, nullptr), nullptr, A, dt, 0.0,
+      0.0, 1);
+  CKL(c);
+  return 0;
+}
+
+int dnsb_pressuregrad(dnsb_ctx *c, double *phi, const double *p, int comp, double s) {
+  if (!c || !phi || !p || comp < 0 || comp > 2)
+    return c ? fail(c, DNSB_EINVAL, "bad argument") : DNSB_EINVAL;
+  if (ensure_device(c)) return DNSB_ECUDA;
+  k_pgrad<<<cell_grid(c->g), cell_block, 0, c->stream>>>(c->g, phi, p, comp, s);
+  CKL(c);
+  c->umax_for[0] = c->umax_for[1] = c->umax_for[2] = nullptr;
+  return 0;
+}
+
+int dnsb_poisson(dnsb_ctx *c, const double *r, double *p) {
+  if (!c || !r || !p) return c ? fail(c, DNSB_EINVAL, "null field") : DNSB_EINVAL;
+  if (ensure_device(c)) return DNSB_ECUDA;
+  int rc;
+  if ((rc = launch_rfftx(c, RIN_REAL, r, nullptr, nullptr))) return rc;
+  return poisson_from_spectrum(c, ROUT_INTERIOR, p);
+}
+
+int dnsb_project(dnsb_ctx *c, double *ux, double *uy, double *uz, double *psi) {
+  if (!c || !ux || !uy || !uz || !psi) return c ? fail(c, DNSB_EINVAL, "null field") : DNSB_EINVAL;
+  if (ensure_device(c)) return DNSB_ECUDA;
+  return do_project(c, ux, uy, uz, psi);
+}
+
+int dnsb_imex_update(dnsb_ctx *c, double *ux, double *uy, double *uz, const double *qx,
+                     const double *qy, const double *qz, const double *p, double B, double alpha,
+                     double dt) {
+  if (!c) return DNSB_EINVAL;
+  if (!c->implicit) return fail(c, DNSB_EINVAL, "implicit y-diffusion requires ydiffusion = :implicit");
+  if (!ux || !uy || !uz || !qx || !qy || !qz || !p) return fail(c, DNSB_EINVAL, "null field");
+  if (ensure_device(c)) return DNSB_ECUDA;
+  const Geo &g = c->g;
+  const double adt = alpha * dt;
+  k_vupdate<<<cell_grid(g), cell_block, 0, c->stream>>>(
+      g, ff(c->V[0], c->V[1], c->V[2]), cf(ux, uy, uz), cf(qx, qy, qz), p, B, adt);
+  CKL(c);
+  // tables for this alpha in stage slot 0
+  k_cn_tables<<<1, 32, 0, c->stream>>>(g.ny, c->ycoef, c->ytab, dt, g.visc, alpha, alpha, alpha);
+  CKL(c);
+  const double th = alpha * dt * g.visc / 2;
+  k_cn<<<dim3((g.nx + 63) / 64, g.nz, 3), 64, 0, c->stream>>>(
+      g, ff(ux, uy, uz), cf(c->V[0], c->V[1], c->V[2]), cf(ux, uy, uz), c->ycoef, c->ytab, th);
+  CKL(c);
+  c->umax_for[0] = c->umax_for[1] = c->umax_for[2] = nullptr;
+  return 0;
+}
+
+int dnsb_step(dnsb_ctx *c, double *ux, double *uy, double *uz, double *p, double *qx, double *qy,
+              double *qz, double *delta, double dt) {
+  if (!c || !ux || !uy || !uz || !p || !qx || !qy || !qz)
+    return c ? fail(c, DNSB_EINVAL, "null field") : DNSB_EINVAL;
+  if (c->implicit && (!delta || delta == p))
+    return fail(c, DNSB_EINVAL, "semi-implicit mode needs a separate delta field");
+  if (!(dt > 0) || !std::isfinite(dt)) return fail(c, DNSB_EINVAL, "dt must be positive and finite");
+  if (ensure_device(c)) return DNSB_ECUDA;
+  return do_step(c, ux, uy, uz, p, qx, qy, qz, delta, dt);
+}
+
+int dnsb_cfl(dnsb_ctx *c, const double *ux, const double *uy, const double *uz, double cfl,
+             int use_step_max, double *dt_out) {
+  if (!c || !ux || !uy || !uz || !dt_out) return c ? fail(c, DNSB_EINVAL, "null argument") : DNSB_EINVAL;
+  if (ensure_device(c)) return DNSB_ECUDA;
+  const bool cached = use_step_max && c->umax_for[0] == ux && c->umax_for[1] == uy && c->umax_for[2] == uz;
+  if (!cached) {
+    CK(c, cudaMemsetAsync(c->umax + 3, 0, 3 * sizeof(unsigned long long), c->stream));
+    k_maxabs3<<<RED_BLOCKS, 256, 0, c->stream>>>(c->g, cf(ux, uy, uz), c->umax + 3);
+    CKL(c);
+  }
+  CK(c, cudaMemcpyAsync(c->hostred, c->umax + (cached ? 0 : 3), 3 * sizeof(unsigned long long),
+                        cudaMemcpyDeviceToHost, c->stream));
+  CK(c, cudaStreamSynchronize(c->stream));
+  return cfl_from_max(c, cfl, reinterpret_cast<const unsigned long long *>(c->hostred), dt_out);
+}
+
+int dnsb_maxdiv(dnsb_ctx *c, const double *ux, const double *uy, const double *uz, double *out) {
+  if (!c || !ux || !uy || !uz || !out) return c ? fail(c, DNSB_EINVAL, "null argument") : DNSB_EINVAL;
+  if (ensure_device(c)) return DNSB_ECUDA;
+  CK(c, cudaMemsetAsync(c->umax + 3, 0, sizeof(unsigned long long), c->stream));
+  k_maxdiv<<<RED_BLOCKS, 256, 0, c->stream>>>(c->g, cf(ux, uy, uz), c->umax + 3);
+  CKL(c);
+  CK(c, cudaMemcpyAsync(c->hostred, c->umax + 3, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(c, cudaStreamSynchronize(c->stream));
+  *out = c->hostred[0];
+  return 0;
+}
+
+int dnsb_kinetic_energy(dnsb_ctx *c, const double *ux, const double *uy, const double *uz, double *out) {
+  if (!c || !ux || !uy || !uz || !out) return c ? fail(c, DNSB_EINVAL, "null argument") : DNSB_EINVAL;
+  if (ensure_device(c)) return DNSB_ECUDA;
+  k_ke_partial<<<RED_BLOCKS, 256, 0, c->stream>>>(c->g, cf(ux, uy, uz), c->partial);
+  CKL(c);
+  k_sum_final<<<1, 1024, 0, c->stream>>>(c->partial, RED_BLOCKS, c->partial + RED_BLOCKS);
+  CKL(c);
+  CK(c, cudaMemcpyAsync(c->hostred, c->partial + RED_BLOCKS, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(c, cudaStreamSynchronize(c->stream));
+  *out = c->hostred[0];
+  return 0;
+}
+
+int dnsb_channel_sample(dnsb_ctx *c, const double *ux, const double *uy, const double *uz, double *acc) {
+  if (!c || !ux || !uy || !uz || !acc) return c ? fail(c, DNSB_EINVAL, "null argument") : DNSB_EINVAL;
+  if (ensure_device(c)) return DNSB_ECUDA;
+  const int nf = c->g.wall ? c->g.ny - 1 : c->g.ny;
+  k_channel<<<c->g.ny + nf, 256, 0, c->stream>>>(c->g, cf(ux, uy, uz), acc, nf);
+  CKL(c);
+  return 0;
+}
+
+int dnsb_spectrum_sample(dnsb_ctx *c, const double *ux, const double *uy, const double *uz, double *E,
+                         int nbins) {
+  if (!c || !ux || !uy || !uz || !E || nbins < 1) return c ? fail(c, DNSB_EINVAL, "bad argument") : DNSB_EINVAL;
+  if (c->g.wall) return fail(c, DNSB_EINVAL, "spectra require a fully periodic box");
+  if (ensure_device(c)) return DNSB_ECUDA;
+  const Geo &g = c->g;
+  const double *u[3] = {ux, uy, uz};
+  int rc;
+  for (int comp = 0; comp < 3; comp++) {
+    if ((rc = launch_rfftx(c, RIN_FIELD, u[comp], nullptr, nullptr))) return rc;
+    if ((rc = launch_fftz(c, false))) return rc;
+    dim3 grid(g.nkx * ((g.nz + c->Ly - 1) / c->Ly));
+    k_yfourier<true><<<grid, SPEC_THREADS, c->smem_y, c->stream>>>(g, c->S, c->py, c->Ly, c->twy,
+                                                                  c->lam1, c->lam2, c->lam3);
+    CKL(c);
+    k_binshells<<<RED_BLOCKS, 256, 0, c->stream>>>(g, c->S, E, nbins);
+    CKL(c);
+  }
+  return 0;
+}
+
+int dnsb_noise(dnsb_ctx *c, double *phi, int comp, unsigned long long seed, double amp) {
+  if (!c || !phi || comp < 0 || comp > 2) return c ? fail(c, DNSB_EINVAL, "bad argument") : DNSB_EINVAL;
+  if (ensure_device(c)) return DNSB_ECUDA;
+  k_noise<<<cell_grid(c->g), cell_block, 0, c->stream>>>(c->g, phi, comp, seed, amp);
+  CKL(c);
+  c->umax_for[0] = c->umax_for[1] = c->umax_for[2] = nullptr;
+  return 0;
+}
+
+int dnsb_profile(dnsb_ctx *c, int enable) {
+  if (!c) return DNSB_EINVAL;
+  if (ensure_device(c)) return DNSB_ECUDA;
+  if (enable && c->evpool.empty()) {
+    c->evpool.resize(4096);
+    for (auto &e : c->evpool) CK(c, cudaEventCreate(&e));
+  }
+  int rc = prof_harvest(c);
+  if (rc) return rc;
+  for (int k = 0; k < DNSB_NKINDS; k++) { c->prof_ms[k] = 0; c->prof_n[k] = 0; }
+  c->prof_on = enable != 0;
+  return 0;
+}
+
+int dnsb_profile_read(dnsb_ctx *c, int kind, double *ms, long *launches) {
+  if (!c || kind < 0 || kind >= DNSB_NKINDS) return c ? fail(c, DNSB_EINVAL, "bad kind") : DNSB_EINVAL;
+  if (ensure_device(c)) return DNSB_ECUDA;
+  int rc = prof_harvest(c);
+  if (rc) return rc;
+  if (ms) *ms = c->prof_ms[kind];
+  if (launches) *launches = c->prof_n[kind];
+  return 0;
+}
+
+long dnsb_launch_count(const dnsb_ctx *c) { return c ? c->launches : -1; }
+
+const char *dnsb_kind_name(int kind) {
+  return (kind >= 0 && kind < DNSB_NKINDS) ? KIND_NAMES[kind] : "";
+}
+
+int dnsb_solve(dnsb_ctx *c, double *ux, double *uy, double *uz, double *p, double *qx, double *qy,
+               double *qz, double *delta, double t0, double t1, double dt, double cfl,
+               long max_steps, double *t_out, long *n_out) {
+  if (!c || !ux || !uy || !uz || !p || !qx || !qy || !qz)
+    return c ? fail(c, DNSB_EINVAL, "null field") : DNSB_EINVAL;
+  if (c->implicit && (!delta || delta == p))
+    return fail(c, DNSB_EINVAL, "semi-implicit mode needs a separate delta field");
+  if (ensure_device(c)) return DNSB_ECUDA;
+  double *d = c->implicit ? delta : p;
+  int rc;
+  // solve! (src/timestep.jl:92-111): halo, projection, then the loop
+  if ((rc = fill3(c, ux, uy, uz))) return rc;
+  if ((rc = do_project(c, ux, uy, uz, d))) return rc;
+  double t = t0;
+  long n = 0;
+  bool have_max = false;
+  while (t < t1 - 1e-10 * (std::fabs(t1) + 1)) {
+    if (max_steps >= 0 && n >= max_steps) break;
+    double dtn = dt;
+    if (!(dt > 0)) {
+      if ((rc = dnsb_cfl(c, ux, uy, uz, cfl, have_max ? 1 : 0, &dtn))) return rc;
+    }
+    dtn = std::fmin(dtn, t1 - t);
+    if ((rc = do_step(c, ux, uy, uz, p, qx, qy, qz, d, dtn))) return rc;
+    have_max = true;
+    t += dtn;
+    n++;
+  }
+  CK(c, cudaStreamSynchronize(c->stream));
+  if (t_out) *t_out = t;
+  if (n_out) *n_out = n;
+  return 0;
+}
+
+int dnsb_solve_host(dnsb_ctx *c, double *ux, double *uy, double *uz, double *p, double t0, double t1,
+                    double dt, double cfl, long max_steps, double *t_out, long *n_out) {
+  if (!c || !ux || !uy || !uz) return c ? fail(c, DNSB_EINVAL, "null field") : DNSB_EINVAL;
+  if (ensure_device(c)) return DNSB_ECUDA;
+  const Geo &g = c->g;
+  const size_t G = (size_t)g.NX * g.NY * g.NZ;
+  double *buf = nullptr;
+  const int nf = c->implicit ? 8 : 7;
+  CK(c, cudaMallocAsync((void **)&buf, nf * G * sizeof(double), c->stream));
+  double *f[8];
+  for (int i = 0; i < nf; i++) f[i] = buf + i * G;
+  int rc = 0;
+  do {
+    if (cudaMemsetAsync(buf, 0, nf * G * sizeof(double), c->stream) != cudaSuccess) { rc = fail(c, DNSB_ECUDA, "memset failed"); break; }
+    double *hu[3] = {ux, uy, uz};
+    for (int i = 0; i < 3 && !rc; i++)
+      if (cudaMemcpyAsync(f[i], hu[i], G * sizeof(double), cudaMemcpyHostToDevice, c->stream) != cudaSuccess)
+        rc = fail(c, DNSB_ECUDA, "host to device copy failed");
+    if (rc) break;
+    rc = dnsb_solve(c, f[0], f[1], f[2], f[3], f[4], f[5], f[6], c->implicit ? f[7] : nullptr, t0, t1,
+                    dt, cfl, max_steps, t_out, n_out);
+    if (rc) break;
+    for (int i = 0; i < 3 && !rc; i++)
+      if (cudaMemcpyAsync(hu[i], f[i], G * sizeof(double), cudaMemcpyDeviceToHost, c->stream) != cudaSuccess)
+        rc = fail(c, DNSB_ECUDA, "device to host copy failed");
+    if (!rc && p && cudaMemcpyAsync(p, f[3], G * sizeof(double), cudaMemcpyDeviceToHost, c->stream) != cudaSuccess)
+      rc = fail(c, DNSB_ECUDA, "device to host copy failed");
+  } while (0);
+  cudaFreeAsync(buf, c->stream);
+  cudaError_t e = cudaStreamSynchronize(c->stream);
+  if (!rc && e != cudaSuccess) rc = fail(c, DNSB_ECUDA, "%s", cudaGetErrorString(e));
+  return rc;
+}
+
+}  // extern "C"

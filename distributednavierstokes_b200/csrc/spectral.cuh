@@ -1,0 +1,378 @@
+// spectral.cuh -- pressure Poisson pipeline and the wall-normal solves.
+//
+// poisson! (src/poisson.jl:147-161) on one GPU: every transpose! of the
+// reference is an identity copy on a single rank (src/transpose.jl:96-102),
+// so the stages address one spectrum buffer S in the layout of sidx()
+// (kz fastest, y, kx slowest) and no copy kernel exists:
+//   k_rfftx  : [divergence of W] -> real FFT along x -> S       (x lines)
+//   k_fftz   : complex FFT along z, in place                    (z lines)
+//   k_thomas : Thomas along y per (kx, kz) (walls)              (y lines)
+//   k_yfourier: FFT along y, divide by lambda, inverse (periodic y)
+//   k_fftz<inv>, then k_irfftx: inverse real FFT -> psi (+ ghost images)
+// and the semi-implicit wall-normal Crank-Nicolson solve (k_cn).
+#pragma once
+#include "common.cuh"
+#include "fft.cuh"
+
+namespace dnsb {
+
+constexpr int SPEC_THREADS = 256;
+
+enum RInMode { RIN_DIVERGENCE = 0, RIN_REAL = 1, RIN_FIELD = 2 };
+enum ROutMode { ROUT_INTERIOR = 0, ROUT_IMAGES = 1, ROUT_REAL = 2 };
+
+// Real forward FFT along x of L lines (j fixed, kz = k0..k0+L-1) through
+// the half-length complex transform: z[m] = r[2m] + i r[2m+1],
+// X[k] = E[k] + w^k O[k] with E = (Z[k] + conj Z[M-k])/2,
+// O = (Z[k] - conj Z[M-k])/(2i), w = exp(-2 pi i/nx), k = 0..M.
+// RIN_DIVERGENCE: r is the divergence of (in0, in1, in2) (operators.jl:10-26).
+// RIN_REAL: r is the ghost-free array in0.  RIN_FIELD: the interior of the
+// ghosted field in0.
+// Shared memory: 2*L*(M+1) complex (ping-pong lines) + M + (M+1) twiddles.
+template <int INMODE>
+__global__ void __launch_bounds__(SPEC_THREADS) k_rfftx(Geo g, double2 *__restrict__ S,
+                                                       const double *__restrict__ in0,
+                                                       const double *__restrict__ in1,
+                                                       const double *__restrict__ in2,
+                                                       FFTPlan plan, int L,
+                                                       const double2 *__restrict__ twM,
+                                                       const double2 *__restrict__ twN) {
+  extern __shared__ double2 smem[];
+  const int M = g.nx / 2;
+  const int ls = M + 1;
+  double2 *buf = smem;
+  double2 *buf2 = smem + L * ls;
+  double2 *tw = buf2 + L * ls;
+  double2 *tn = tw + M;
+  const int ngrp = (g.nz + L - 1) / L;
+  const int grp = blockIdx.x % ngrp;
+  const int j = blockIdx.x / ngrp;  // 0-based row
+  const int k0 = grp * L;
+  for (int t = threadIdx.x; t < M; t += blockDim.x) tw[t] = twM[t];
+  for (int t = threadIdx.x; t <= M; t += blockDim.x) tn[t] = twN[t];
+  const long long sy = g.NX, sz = (long long)g.NX * g.NY;
+  const int J = j + 1;
+  const double rdyJ = __ldg(g.rdy + J);
+  for (int t = threadIdx.x; t < L * M; t += blockDim.x) {
+    const int l = t / M, m = t - l * M;
+    const int k = k0 + l;
+    double2 z = make_double2(0.0, 0.0);
+    if (k < g.nz) {
+      if (INMODE == RIN_REAL) {
+        const double *row = in0 + (long long)g.nx * (j + (long long)g.ny * k);
+        z = *reinterpret_cast<const double2 *>(row + 2 * m);
+      } else {
+        const long long c0 = gidx(g, 2 * m + 1, J, k + 1);
+        if (INMODE == RIN_FIELD) {
+          z = make_double2(in0[c0], in0[c0 + 1]);
+        } else {
+          const double a0 = in0[c0 - 1], a1 = in0[c0], a2 = in0[c0 + 1];
+          const double r0 = (a1 - a0) * g.rdx + (in1[c0] - in1[c0 - sy]) * rdyJ +
+                            (in2[c0] - in2[c0 - sz]) * g.rdz;
+          const double r1 = (a2 - a1) * g.rdx + (in1[c0 + 1] - in1[c0 + 1 - sy]) * rdyJ +
+                            (in2[c0 + 1] - in2[c0 + 1 - sz]) * g.rdz;
+          z = make_double2(r0, r1);
+        }
+      }
+    }
+    buf[l * ls + m] = z;
+  }
+  __syncthreads();
+  const double2 *res = fft_lines<false>(buf, buf2, plan, L, 1, ls, true, tw);
+  // post-process and store S(kx, j, k0 + l), l fastest (coalesced in kz)
+  const int Lv = min(L, g.nz - k0);
+  for (int t = threadIdx.x; t < Lv * (M + 1); t += blockDim.x) {
+    const int kx = t / Lv, l = t - kx * Lv;
+    const double2 zk = res[l * ls + (kx == M ? 0 : kx)];
+    const double2 zc = cconj(res[l * ls + (kx == 0 ? 0 : M - kx)]);
+    const double2 e = make_double2(0.5 * (zk.x + zc.x), 0.5 * (zk.y + zc.y));
+    // o = -i/2 (zk - zc)
+    const double2 d = csub(zk, zc);
+    const double2 o = make_double2(0.5 * d.y, -0.5 * d.x);
+    S[sidx(g, kx, j, k0 + l)] = cadd(e, cmul(tn[kx], o));
+  }
+}
+
+// Complex FFT along z of L contiguous lines of S; INV scales by 1/nz.
+template <bool INV>
+__global__ void __launch_bounds__(SPEC_THREADS) k_fftz(Geo g, double2 *__restrict__ S,
+                                                      FFTPlan plan, int L,
+                                                      const double2 *__restrict__ twz) {
+  extern __shared__ double2 smem[];
+  const int n = g.nz;
+  const int ls = n + 1;
+  double2 *buf = smem;
+  double2 *buf2 = smem + L * ls;
+  double2 *tw = buf2 + L * ls;
+  const long long nlines = (long long)g.ny * g.nkx;
+  const long long l0 = (long long)blockIdx.x * L;
+  const int Lv = (int)min((long long)L, nlines - l0);
+  for (int t = threadIdx.x; t < n; t += blockDim.x) tw[t] = twz[t];
+  double2 *src = S + l0 * n;
+  for (int t = threadIdx.x; t < L * n; t += blockDim.x) {
+    const int l = t / n, e = t - l * n;
+    buf[l * ls + e] = l < Lv ? src[t] : make_double2(0.0, 0.0);
+  }
+  __syncthreads();
+  const double2 *res = fft_lines<INV>(buf, buf2, plan, L, 1, ls, true, tw);
+  const double sc = 1.0 / n;
+  for (int t = threadIdx.x; t < Lv * n; t += blockDim.x) {
+    const int l = t / n, e = t - l * n;
+    const double2 v = res[l * ls + e];
+    src[t] = INV ? cscale(v, sc) : v;
+  }
+}
+
+// thomas_kernel! (src/poisson.jl:14-41): one thread per (kx, kz) line, in
+// place on S, c' in the work array (same layout as S).  The mean mode
+// (lambda == 0) is pinned by replacing its first row with x_1 = 0.
+__global__ void k_thomas(Geo g, double2 *__restrict__ S, double *__restrict__ work,
+                         const double *__restrict__ ay, const double *__restrict__ by,
+                         const double *__restrict__ cy, const double *__restrict__ lam1,
+                         const double *__restrict__ lam3) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)g.nz * g.nkx) return;
+  const int kz = (int)(t % g.nz), kx = (int)(t / g.nz);
+  const double lam = lam1[kx] + lam3[kz];
+  const long long st = g.nz;
+  double2 *x = S + sidx(g, kx, 0, kz);
+  double *cp = work + sidx(g, kx, 0, kz);
+  const bool pin = lam == 0.0;
+  double beta = pin ? 1.0 : by[0] + lam;
+  double cprev = (pin ? 0.0 : cy[0]) / beta;
+  cp[0] = cprev;
+  double2 xprev = pin ? make_double2(0.0, 0.0) : x[0];
+  xprev = make_double2(xprev.x / beta, xprev.y / beta);
+  x[0] = xprev;
+  for (int j = 1; j < g.ny; j++) {
+    const double a = ay[j];
+    beta = (by[j] + lam) - a * cprev;
+    cprev = cy[j] / beta;
+    cp[j * st] = cprev;
+    const double2 xj = x[j * st];
+    xprev = make_double2((xj.x - a * xprev.x) / beta, (xj.y - a * xprev.y) / beta);
+    x[j * st] = xprev;
+  }
+  double2 xn = xprev;
+  for (int j = g.ny - 2; j >= 0; j--) {
+    const double c = cp[j * st];
+    double2 xj = x[j * st];
+    xj = make_double2(xj.x - c * xn.x, xj.y - c * xn.y);
+    x[j * st] = xj;
+    xn = xj;
+  }
+}
+
+// Periodic y (src/poisson.jl:106-118,135-138, modedivide_kernel! :43-49):
+// per CTA a tile of L consecutive kz for one kx with all ny rows: FFT along
+// y, divide by lambda1+lambda2+lambda3 (0 for the mean), inverse, 1/ny.
+// SPECTRUM_ONLY leaves the forward transform in S (for energy spectra).
+template <bool SPECTRUM_ONLY>
+__global__ void __launch_bounds__(SPEC_THREADS) k_yfourier(Geo g, double2 *__restrict__ S,
+                                                          FFTPlan plan, int L,
+                                                          const double2 *__restrict__ twy,
+                                                          const double *__restrict__ lam1,
+                                                          const double *__restrict__ lam2,
+                                                          const double *__restrict__ lam3) {
+  extern __shared__ double2 smem[];
+  const int n = g.ny;
+  double2 *buf = smem;  // buf[j*L + l]
+  double2 *buf2 = smem + L * n;
+  double2 *tw = buf2 + L * n;
+  const int ngrp = (g.nz + L - 1) / L;
+  const int grp = blockIdx.x % ngrp;
+  const int kx = blockIdx.x / ngrp;
+  const int k0 = grp * L;
+  const int Lv = min(L, g.nz - k0);
+  for (int t = threadIdx.x; t < n; t += blockDim.x) tw[t] = twy[t];
+  for (int t = threadIdx.x; t < L * n; t += blockDim.x) {
+    const int j = t / L, l = t - j * L;
+    buf[t] = l < Lv ? S[sidx(g, kx, j, k0 + l)] : make_double2(0.0, 0.0);
+  }
+  __syncthreads();
+  double2 *res = fft_lines<false>(buf, buf2, plan, L, L, 1, false, tw);
+  if (!SPECTRUM_ONLY) {
+    const double l1 = lam1[kx];
+    for (int t = threadIdx.x; t < L * n; t += blockDim.x) {
+      const int j = t / L, l = t - j * L;
+      const int kz = min(k0 + l, g.nz - 1);
+      const double lam = (l1 + lam2[j]) + lam3[kz];
+      const double2 v = res[t];
+      res[t] = lam == 0.0 ? make_double2(0.0, 0.0) : make_double2(v.x / lam, v.y / lam);
+    }
+    __syncthreads();
+    res = fft_lines<true>(res, res == buf ? buf2 : buf, plan, L, L, 1, false, tw);
+  }
+  const double sc = SPECTRUM_ONLY ? 1.0 : 1.0 / n;
+  for (int t = threadIdx.x; t < Lv * n; t += blockDim.x) {
+    const int j = t / Lv, l = t - j * Lv;
+    const double2 v = res[j * L + l];
+    S[sidx(g, kx, j, k0 + l)] = SPECTRUM_ONLY ? v : cscale(v, sc);
+  }
+}
+
+// Inverse real FFT along x (normalised 1/nx, imaginary parts of the kx = 0
+// and kx = nx/2 inputs ignored as in FFTW c2r) of L lines, written to
+//   ROUT_INTERIOR: the interior of the ghosted psi (poisson!, no halo),
+//   ROUT_IMAGES:   the interior plus pressure ghost images,
+//   ROUT_REAL:     the ghost-free array out.
+template <int OUTMODE>
+__global__ void __launch_bounds__(SPEC_THREADS) k_irfftx(Geo g, const double2 *__restrict__ S,
+                                                        double *__restrict__ out, FFTPlan plan,
+                                                        int L, const double2 *__restrict__ twM,
+                                                        const double2 *__restrict__ twN) {
+  extern __shared__ double2 smem[];
+  const int M = g.nx / 2;
+  const int ls = M + 2;
+  double2 *buf = smem;
+  double2 *buf2 = smem + L * ls;
+  double2 *tw = buf2 + L * ls;
+  double2 *tn = tw + M;
+  const int ngrp = (g.nz + L - 1) / L;
+  const int grp = blockIdx.x % ngrp;
+  const int j = blockIdx.x / ngrp;
+  const int k0 = grp * L;
+  const int Lv = min(L, g.nz - k0);
+  for (int t = threadIdx.x; t < M; t += blockDim.x) tw[t] = twM[t];
+  for (int t = threadIdx.x; t <= M; t += blockDim.x) tn[t] = twN[t];
+  for (int t = threadIdx.x; t < L * (M + 1); t += blockDim.x) {
+    const int kx = t / L, l = t - kx * L;
+    buf[l * ls + kx] = l < Lv ? S[sidx(g, kx, j, k0 + l)] : make_double2(0.0, 0.0);
+  }
+  __syncthreads();
+  // Z[k] = E[k] + i O[k], E = (X[k] + conj X[M-k])/2,
+  // O = (X[k] - conj X[M-k]) conj(w^k)/2; one thread per pair (k, M-k).
+  const int half = M / 2 + 1;
+  for (int t = threadIdx.x; t < L * half; t += blockDim.x) {
+    const int l = t / half, k = t - l * half;
+    double2 *X = buf + l * ls;
+    if (k == 0) {
+      const double a = X[0].x, b = X[M].x;
+      const double e = 0.5 * (a + b), o = 0.5 * (a - b);
+      X[0] = make_double2(e, o);
+    } else if (2 * k <= M) {
+      const int k2 = M - k;
+      const double2 a = X[k], b = X[k2];
+      {
+        const double2 bc = cconj(b);
+        const double2 e = cscale(cadd(a, bc), 0.5);
+        const double2 o = cmul(cscale(csub(a, bc), 0.5), cconj(tn[k]));
+        X[k] = make_double2(e.x - o.y, e.y + o.x);
+      }
+      if (k2 != k) {
+        const double2 ac = cconj(a);
+        const double2 e = cscale(cadd(b, ac), 0.5);
+        const double2 o = cmul(cscale(csub(b, ac), 0.5), cconj(tn[k2]));
+        X[k2] = make_double2(e.x - o.y, e.y + o.x);
+      }
+    }
+  }
+  __syncthreads();
+  const double2 *res = fft_lines<true>(buf, buf2, plan, L, 1, ls, true, tw);
+  const double sc = 1.0 / M;
+  const int J = j + 1;
+  for (int t = threadIdx.x; t < Lv * M; t += blockDim.x) {
+    const int l = t / M, m = t - l * M;
+    const double2 z = res[l * ls + m];
+    const double x0 = z.x * sc, x1 = z.y * sc;
+    const int K = k0 + l + 1;
+    if (OUTMODE == ROUT_REAL) {
+      double *row = out + (long long)g.nx * (j + (long long)g.ny * (K - 1));
+      *reinterpret_cast<double2 *>(row + 2 * m) = make_double2(x0, x1);
+    } else if (OUTMODE == ROUT_INTERIOR) {
+      const long long c0 = gidx(g, 2 * m + 1, J, K);
+      out[c0] = x0;
+      out[c0 + 1] = x1;
+    } else {
+      store_img(out, g, 2 * m + 1, J, K, x0, STAG_P);
+      store_img(out, g, 2 * m + 2, J, K, x1, STAG_P);
+    }
+  }
+}
+
+// Per-step Crank-Nicolson tables (imexsolve_kernel!, src/ydiffusion.jl:94-109):
+// the Thomas coefficients of (I - theta Dy) depend on y only, so
+// beta_j, c'_j = -theta c_j / beta_j and theta a_j are computed once per
+// stage and set instead of once per line.  tab layout per (stage, set):
+// [ta(ny) | cp(ny) | ib(ny)], ib = 1/beta; set 0 tangential, 1 normal.
+// coef: [at bt ct an bn cn], ny each.  One thread per (stage, set).
+__global__ void k_cn_tables(int ny, const double *__restrict__ coef, double *__restrict__ tab,
+                            double dt, double visc, double al0, double al1, double al2) {
+  const int t = threadIdx.x;
+  if (t >= 6) return;
+  const int st = t / 2, set = t % 2;
+  const double al = st == 0 ? al0 : st == 1 ? al1 : al2;
+  const double th = al * dt * visc / 2;
+  const double *a = coef + (set ? 3 : 0) * ny;
+  const double *b = a + ny, *c = b + ny;
+  double *ta = tab + (long long)(st * 2 + set) * 3 * ny;
+  double *cp = ta + ny, *ib = cp + ny;
+  double beta = 1 - th * b[0];
+  double cprev = -th * c[0] / beta;
+  ta[0] = th * a[0];
+  cp[0] = cprev;
+  ib[0] = 1.0 / beta;
+  for (int j = 1; j < ny; j++) {
+    beta = (1 - th * b[j]) + th * a[j] * cprev;
+    cprev = -th * c[j] / beta;
+    ta[j] = th * a[j];
+    cp[j] = cprev;
+    ib[j] = 1.0 / beta;
+  }
+}
+
+// imexrhs_kernel! + imexsolve_kernel! (src/ydiffusion.jl:71-109) fused: one
+// thread per (I, K) y-line of component c = blockIdx.z; rhs = v + theta Dy u^n
+// with the walls folded into the rows, then the Thomas sweeps with the
+// per-stage tables.  The forward-swept values go to out (which may alias
+// the u^n field, each line being owned by one thread); the backward sweep
+// writes the result with ghost images.
+__global__ void __launch_bounds__(128) k_cn(Geo g, Fields3 out, CFields3 V, CFields3 un,
+                                           const double *__restrict__ coef,
+                                           const double *__restrict__ tab, double theta) {
+  const int I = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int K = blockIdx.y + 1;
+  const int c = blockIdx.z;
+  if (I > g.nx) return;
+  const int ny = g.ny;
+  const int set = c == STAG_Y ? 1 : 0;
+  const double *a = coef + set * 3 * ny, *b = a + ny, *cc = b + ny;
+  const double *ta = tab + set * 3 * ny, *cp = ta + ny, *ib = cp + ny;
+  const double *v = c == 0 ? V.x : c == 1 ? V.y : V.z;
+  const double *u = c == 0 ? un.x : c == 1 ? un.y : un.z;
+  double *o = c == 0 ? out.x : c == 1 ? out.y : out.z;
+  const long long sy = g.NX;
+  const long long base = gidx(g, I, 1, K);
+  // forward sweep
+  double um = 0.0, u0 = u[base], up = ny > 1 ? u[base + sy] : 0.0;
+  double xprev = 0.0;
+  for (int j = 0; j < ny; j++) {
+    const long long cj = base + j * sy;
+    double s;
+    if (j == 0) s = b[0] * u0 + (ny > 1 ? cc[0] * up : 0.0);
+    else if (j == ny - 1) s = a[j] * um + b[j] * u0;
+    else s = (a[j] * um + b[j] * u0) + cc[j] * up;
+    const double rhs = v[cj] + theta * s;
+    const double x = j == 0 ? rhs * ib[0] : (rhs + ta[j] * xprev) * ib[j];
+    o[cj] = x;
+    xprev = x;
+    um = u0;
+    u0 = up;
+    if (j + 2 < ny) up = u[cj + 2 * sy];
+  }
+  // backward sweep + images
+  double xn = xprev;
+  const int stag = c;
+  const bool normal_wall = g.wall && c == STAG_Y;
+  // the inactive wall face J = ny of the normal component keeps its zero
+  // (row ny of the normal operator is zero) and gets no images of its own
+  if (!normal_wall) store_img(o, g, I, ny, K, xn, stag);
+  for (int j = ny - 2; j >= 0; j--) {
+    const long long cj = base + j * sy;
+    const double x = o[cj] - cp[j] * xn;
+    store_img(o, g, I, j + 1, K, x, stag);
+    xn = x;
+  }
+}
+
+}  // namespace dnsb

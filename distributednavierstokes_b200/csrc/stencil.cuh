@@ -1,0 +1,236 @@
+// stencil.cuh -- staggered finite-volume stencils on ghosted fields.
+//
+// Restates src/operators.jl (divergence, momentum, pressure gradient) and
+// the pointwise parts of src/timestep.jl / src/ydiffusion.jl, fused per RK
+// stage: the momentum kernel also applies the explicit register update
+// (timestep.jl:54-58) or forms the semi-implicit explicit increment
+// v = u + B q - alpha dt grad p (ydiffusion.jl:133-135); the gradient kernel
+// also updates the lagged pressure (timestep.jl:49-51), writes ghost images
+// (replacing exchange_halo!) and reduces max|u| for the next CFL step.
+// Divisions by grid metrics use precomputed reciprocals (<= 1 ulp apart from
+// the reference's divisions); halving uses *0.5 (exact).
+#pragma once
+#include "common.cuh"
+
+namespace dnsb {
+
+enum MomMode { MOM_ONLY = 0, MOM_EXPLICIT = 1, MOM_IMPLICIT = 2 };
+
+#define LDG(p, o) __ldg((p) + (o))
+
+// momentum_kernel! (src/operators.jl:44-145), one thread per interior cell.
+// MODE_ONLY: q <- A q + dt F(u).
+// MOM_EXPLICIT: also W_c = u_c + B q_c on active DOFs, with ghost images.
+// MOM_IMPLICIT: also V_c = u_c + B q_c - adt * d_c p on active DOFs.
+template <int MODE>
+__global__ void __launch_bounds__(256) k_momentum(Geo g, Fields3 q, CFields3 u, Fields3 out,
+                                                  const double *__restrict__ p, double A, double dt,
+                                                  double B, double adt, int readq) {
+  const int I = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int J = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  const int K = blockIdx.z + 1;
+  if (I > g.nx || J > g.ny) return;
+  const long long sy = g.NX, sz = (long long)g.NX * g.NY;
+  const long long c0 = gidx(g, I, J, K);
+  const double *ux = u.x, *uy = u.y, *uz = u.z;
+
+  const double ux0 = LDG(ux, c0), uxE = LDG(ux, c0 + 1), uxW = LDG(ux, c0 - 1);
+  const double uxN = LDG(ux, c0 + sy), uxS = LDG(ux, c0 - sy);
+  const double uxT = LDG(ux, c0 + sz), uxB = LDG(ux, c0 - sz);
+  const double uxWN = LDG(ux, c0 - 1 + sy), uxWT = LDG(ux, c0 - 1 + sz);
+  const double uy0 = LDG(uy, c0), uyE = LDG(uy, c0 + 1), uyW = LDG(uy, c0 - 1);
+  const double uyN = LDG(uy, c0 + sy), uyS = LDG(uy, c0 - sy);
+  const double uyT = LDG(uy, c0 + sz), uyB = LDG(uy, c0 - sz);
+  const double uySE = LDG(uy, c0 + 1 - sy), uyST = LDG(uy, c0 - sy + sz);
+  const double uz0 = LDG(uz, c0), uzE = LDG(uz, c0 + 1), uzW = LDG(uz, c0 - 1);
+  const double uzN = LDG(uz, c0 + sy), uzS = LDG(uz, c0 - sy);
+  const double uzT = LDG(uz, c0 + sz), uzB = LDG(uz, c0 - sz);
+  const double uzEB = LDG(uz, c0 + 1 - sz), uzNB = LDG(uz, c0 + sy - sz);
+
+  const double dyJ = __ldg(g.dy + J), dyJ1 = __ldg(g.dy + J + 1);
+  const double rdyJ = __ldg(g.rdy + J), rdyJ1 = __ldg(g.rdy + J + 1);
+  const double rdyuJ = __ldg(g.rdyu + J), rdyuJm = __ldg(g.rdyu + J - 1);
+  const double ey = g.epsy, nu = g.visc;
+
+  // x momentum, at the right x-face of cell (I, J, K)
+  double qxn, qyn, qzn;
+  {
+    const double uce = 0.5 * (ux0 + uxE), ucw = 0.5 * (uxW + ux0);
+    const double vn = 0.5 * (uy0 + uyE), un = 0.5 * (ux0 + uxN);
+    const double vs = 0.5 * (uyS + uySE), us = 0.5 * (uxS + ux0);
+    const double wt = 0.5 * (uz0 + uzE), ut = 0.5 * (ux0 + uxT);
+    const double wb = 0.5 * (uzB + uzEB), ub = 0.5 * (uxB + ux0);
+    const double conv = (uce * uce - ucw * ucw) * g.rdx + (vn * un - vs * us) * rdyJ +
+                        (wt * ut - wb * ub) * g.rdz;
+    const double diff = (uxE - 2 * ux0 + uxW) * g.rdx2 +
+                        ey * ((uxN - ux0) * rdyuJ - (ux0 - uxS) * rdyuJm) * rdyJ +
+                        (uxT - 2 * ux0 + uxB) * g.rdz2;
+    const double f = dt * (-conv + nu * diff + g.fx);
+    qxn = readq ? A * q.x[c0] + f : f;
+  }
+  // y momentum, at the top y-face; Delta-y weighted transporters
+  {
+    const double h = 0.5 * rdyuJ;
+    const double ue = (ux0 * dyJ + uxN * dyJ1) * h, ve = 0.5 * (uy0 + uyE);
+    const double uw = (uxW * dyJ + uxWN * dyJ1) * h, vw = 0.5 * (uyW + uy0);
+    const double vcn = 0.5 * (uy0 + uyN), vcs = 0.5 * (uyS + uy0);
+    const double wtv = (uz0 * dyJ + uzN * dyJ1) * h, vt = 0.5 * (uy0 + uyT);
+    const double wbv = (uzB * dyJ + uzNB * dyJ1) * h, vb = 0.5 * (uyB + uy0);
+    const double conv = (ue * ve - uw * vw) * g.rdx + (vcn * vcn - vcs * vcs) * rdyuJ +
+                        (wtv * vt - wbv * vb) * g.rdz;
+    const double diff = (uyE - 2 * uy0 + uyW) * g.rdx2 +
+                        ey * ((uyN - uy0) * rdyJ1 - (uy0 - uyS) * rdyJ) * rdyuJ +
+                        (uyT - 2 * uy0 + uyB) * g.rdz2;
+    const double f = dt * (-conv + nu * diff + g.fy);
+    qyn = readq ? A * q.y[c0] + f : f;
+  }
+  // z momentum, at the back z-face
+  {
+    const double ue = 0.5 * (ux0 + uxT), we = 0.5 * (uz0 + uzE);
+    const double uw = 0.5 * (uxW + uxWT), ww = 0.5 * (uzW + uz0);
+    const double vnw = 0.5 * (uy0 + uyT), wn = 0.5 * (uz0 + uzN);
+    const double vsw = 0.5 * (uyS + uyST), ws = 0.5 * (uzS + uz0);
+    const double wct = 0.5 * (uz0 + uzT), wcb = 0.5 * (uzB + uz0);
+    const double conv = (ue * we - uw * ww) * g.rdx + (vnw * wn - vsw * ws) * rdyJ +
+                        (wct * wct - wcb * wcb) * g.rdz;
+    const double diff = (uzE - 2 * uz0 + uzW) * g.rdx2 +
+                        ey * ((uzN - uz0) * rdyuJ - (uz0 - uzS) * rdyuJm) * rdyJ +
+                        (uzT - 2 * uz0 + uzB) * g.rdz2;
+    const double f = dt * (-conv + nu * diff + g.fz);
+    qzn = readq ? A * q.z[c0] + f : f;
+  }
+  const bool yact = J <= g.jymax;
+  q.x[c0] = qxn;
+  if (yact) q.y[c0] = qyn;
+  q.z[c0] = qzn;
+
+  if (MODE == MOM_EXPLICIT) {
+    // u <- u + B q on ranges[c] (timestep.jl:54-58), halo via images
+    store_img(out.x, g, I, J, K, ux0 + B * qxn, STAG_X);
+    if (yact) store_img(out.y, g, I, J, K, uy0 + B * qyn, STAG_Y);
+    store_img(out.z, g, I, J, K, uz0 + B * qzn, STAG_Z);
+  } else if (MODE == MOM_IMPLICIT) {
+    // v = u + B q - alpha dt grad p (ydiffusion.jl:133-135), interior only
+    const double p0 = __ldg(p + c0);
+    out.x[c0] = (ux0 + B * qxn) - adt * (__ldg(p + c0 + 1) - p0) * g.rdx;
+    out.y[c0] = yact ? (uy0 + B * qyn) - adt * (__ldg(p + c0 + sy) - p0) * rdyuJ : uy0;
+    out.z[c0] = (uz0 + B * qzn) - adt * (__ldg(p + c0 + sz) - p0) * g.rdz;
+  }
+}
+
+enum GradMode { GRAD_EXPLICIT = 0, GRAD_IMPLICIT = 1 };
+
+__device__ __forceinline__ unsigned long long dbits(double v) {
+  return (unsigned long long)__double_as_longlong(v);
+}
+
+// Projection update u = W - grad(psi) on active DOFs with ghost images
+// (pressuregrad_update! + exchange_halo!, src/operators.jl:180-220,
+// src/timestep.jl:28-30).  GRAD_IMPLICIT additionally does
+// p += delta/(alpha dt) with images (src/timestep.jl:49-52).  W may alias u.
+// If umax != nullptr, the block maxima of |u_c| over the interior are
+// folded into umax[c] (as ordered bit patterns of non-negative doubles).
+template <int MODE>
+__global__ void __launch_bounds__(256) k_grad(Geo g, Fields3 u, CFields3 W,
+                                              const double *__restrict__ psi, double *p,
+                                              double radt, unsigned long long *umax) {
+  const int I = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int J = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  const int K = blockIdx.z + 1;
+  double m0 = 0, m1 = 0, m2 = 0;
+  if (I <= g.nx && J <= g.ny) {
+    const long long sy = g.NX, sz = (long long)g.NX * g.NY;
+    const long long c0 = gidx(g, I, J, K);
+    const double s0 = psi[c0];
+    const double vx = W.x[c0] - (psi[c0 + 1] - s0) * g.rdx;
+    const double vz = W.z[c0] - (psi[c0 + sz] - s0) * g.rdz;
+    store_img(u.x, g, I, J, K, vx, STAG_X);
+    store_img(u.z, g, I, J, K, vz, STAG_Z);
+    m0 = fabs(vx);
+    m2 = fabs(vz);
+    if (J <= g.jymax) {
+      const double vy = W.y[c0] - (psi[c0 + sy] - s0) * __ldg(g.rdyu + J);
+      store_img(u.y, g, I, J, K, vy, STAG_Y);
+      m1 = fabs(vy);
+    }
+    if (MODE == GRAD_IMPLICIT) store_img(p, g, I, J, K, p[c0] + s0 * radt, STAG_P);
+  }
+  if (umax) {
+    for (int o = 16; o > 0; o >>= 1) {
+      m0 = fmax(m0, __shfl_xor_sync(0xffffffffu, m0, o));
+      m1 = fmax(m1, __shfl_xor_sync(0xffffffffu, m1, o));
+      m2 = fmax(m2, __shfl_xor_sync(0xffffffffu, m2, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+      atomicMax(umax + 0, dbits(m0));
+      atomicMax(umax + 1, dbits(m1));
+      atomicMax(umax + 2, dbits(m2));
+    }
+  }
+}
+
+// pgrad{x,y,z}_kernel! (src/operators.jl:180-196): phi -= s * d_c p on
+// ranges[c]; no halo update (as in the reference).
+__global__ void k_pgrad(Geo g, double *phi, const double *__restrict__ p, int c, double s) {
+  const int I = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int J = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  const int K = blockIdx.z + 1;
+  const int jh = (c == STAG_Y) ? g.jymax : g.ny;
+  if (I > g.nx || J > jh) return;
+  const long long c0 = gidx(g, I, J, K);
+  const long long off = c == 0 ? 1 : c == 1 ? (long long)g.NX : (long long)g.NX * g.NY;
+  const double r = c == 0 ? g.rdx : c == 1 ? __ldg(g.rdyu + J) : g.rdz;
+  phi[c0] = phi[c0] - s * (p[c0 + off] - p[c0]) * r;
+}
+
+// ranges-wise register update u_c += B q_c then u_c -= s d_c p (the first
+// half of imex_update!, src/ydiffusion.jl:133-135), writing v into V.
+__global__ void k_vupdate(Geo g, Fields3 V, CFields3 u, CFields3 q, const double *__restrict__ p,
+                          double B, double adt) {
+  const int I = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int J = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  const int K = blockIdx.z + 1;
+  if (I > g.nx || J > g.ny) return;
+  const long long sy = g.NX, sz = (long long)g.NX * g.NY;
+  const long long c0 = gidx(g, I, J, K);
+  const double p0 = p[c0];
+  V.x[c0] = (u.x[c0] + B * q.x[c0]) - adt * (p[c0 + 1] - p0) * g.rdx;
+  V.y[c0] = J <= g.jymax ? (u.y[c0] + B * q.y[c0]) - adt * (p[c0 + sy] - p0) * __ldg(g.rdyu + J)
+                         : u.y[c0];
+  V.z[c0] = (u.z[c0] + B * q.z[c0]) - adt * (p[c0 + sz] - p0) * g.rdz;
+}
+
+// divergence_kernel! (src/operators.jl:10-26) into the ghost-free r.
+__global__ void k_divergence(Geo g, double *r, CFields3 u) {
+  const int I = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int J = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  const int K = blockIdx.z + 1;
+  if (I > g.nx || J > g.ny) return;
+  const long long sy = g.NX, sz = (long long)g.NX * g.NY;
+  const long long c0 = gidx(g, I, J, K);
+  r[(I - 1) + (long long)g.nx * ((J - 1) + (long long)g.ny * (K - 1))] =
+      (u.x[c0] - u.x[c0 - 1]) * g.rdx + (u.y[c0] - u.y[c0 - sy]) * __ldg(g.rdy + J) +
+      (u.z[c0] - u.z[c0 - sz]) * g.rdz;
+}
+
+// exchange_halo! on one rank: every ghost cell (and, for the wall-normal
+// component, the wall faces) from its interior source.
+__global__ void k_fill_ghosts(Geo g, double *phi, int stag) {
+  long long n = (long long)g.NX * g.NY * g.NZ;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+       t += (long long)gridDim.x * blockDim.x) {
+    int I = (int)(t % g.NX);
+    long long r = t / g.NX;
+    int J = (int)(r % g.NY);
+    int K = (int)(r / g.NY);
+    bool ghost = I == 0 || I == g.nx + 1 || J == 0 || J == g.ny + 1 || K == 0 || K == g.nz + 1 ||
+                 (g.wall && stag == STAG_Y && J == g.ny);
+    if (!ghost) continue;
+    int Is = I, Js = J, Ks = K;
+    double s;
+    bool nz = ghost_src(g, stag, Is, Js, Ks, s);
+    phi[t] = nz ? s * phi[gidx(g, Is, Js, Ks)] : 0.0;
+  }
+}
+
+}  // namespace dnsb

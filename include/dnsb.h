@@ -1,0 +1,173 @@
+/*
+ * dnsb.h -- C ABI of libdnsb.so, the B200 (sm_100a) finite-volume time step.
+ *
+ * Drop-in for the single-GPU hot path of DistributedNavierStokes
+ * (Julia): the functions below replace, one for one, the reference's
+ * operator API for that path.  Each entry point cites the reference
+ * function it stands in for (file:line in the reference repository).
+ *
+ * Fields are borrowed DEVICE pointers to the caller's ghosted arrays,
+ * exactly the reference's `scalarfield` layout (src/fields.jl:4-5):
+ * (nx+2) x (ny+2) x (nz+2) doubles, column-major (x fastest), ghost width 1.
+ * A CuArray{Float64,3} from `scalarfield(setup)` can be passed as-is
+ * (pointer(u.x)).  The library never frees them.  Scratch (spectrum, FFT
+ * twiddles, coefficient tables, y-solve work) belongs to the context.
+ *
+ * Every call returns 0 on success or a DNSB_E* code; dnsb_last_error()
+ * gives the message.  Work is enqueued on the context's stream; calls that
+ * return a host scalar (dnsb_cfl, dnsb_maxdiv, dnsb_kinetic_energy)
+ * synchronise that stream, as the reference's reductions do.  A context is
+ * not re-entrant: one context per GPU and host thread.
+ */
+#ifndef DNSB_H
+#define DNSB_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DNSB_VERSION 1
+
+enum {
+  DNSB_OK = 0,
+  DNSB_EINVAL = 1,   /* bad configuration or argument */
+  DNSB_ECUDA = 2,    /* CUDA runtime error */
+  DNSB_EUNSUP = 3,   /* size the kernels do not support (e.g. FFT length) */
+  DNSB_ENOMEM = 4
+};
+
+enum { DNSB_STAG_X = 0, DNSB_STAG_Y = 1, DNSB_STAG_Z = 2, DNSB_STAG_P = 3 };
+enum { DNSB_BC_PERIODIC = 0, DNSB_BC_WALL = 1 };
+enum { DNSB_YDIFF_EXPLICIT = 0, DNSB_YDIFF_IMPLICIT = 1 };
+
+/* The problem description that setup() builds (src/setup.jl:34-113) and
+ * that griddata() computes (src/setup.jl:148-193), single rank, w = 1.
+ * dy/dyu are copied at create time. */
+typedef struct {
+  int nx, ny, nz;        /* cells; nx even; FFT lengths nx/2, nz (and ny when
+                            periodic) must factor into 2, 3, 5 */
+  int bc_y;              /* DNSB_BC_PERIODIC or DNSB_BC_WALL (bc[2]) */
+  int ydiffusion;        /* DNSB_YDIFF_* (setup keyword ydiffusion) */
+  double dx, dz;         /* grid.Δx, grid.Δz */
+  const double *dy;      /* grid.Δy: ny+2 cell widths, ghosted index 0..ny+1 */
+  const double *dyu;     /* grid.Δyu: ny+2 centre distances */
+  double visc;           /* setup.visc */
+  double bodyforce[3];   /* setup.bodyforce */
+} dnsb_grid;
+
+typedef struct dnsb_ctx dnsb_ctx;
+
+/* Library version (DNSB_VERSION). */
+int dnsb_version(void);
+
+/* setup(; ...) plans: plan_poisson (src/poisson.jl:56-120) and
+ * plan_ydiffusion (src/ydiffusion.jl:54-68).  `stream` is a cudaStream_t
+ * (NULL = legacy default stream) on device `device`. */
+int dnsb_create(const dnsb_grid *grid, int device, void *stream, dnsb_ctx **out);
+void dnsb_destroy(dnsb_ctx *ctx);
+/* Message of the last failed call on ctx (or of the last failed create when
+ * ctx is NULL). */
+const char *dnsb_last_error(const dnsb_ctx *ctx);
+int dnsb_set_stream(dnsb_ctx *ctx, void *stream);
+int dnsb_sync(dnsb_ctx *ctx);
+
+/* exchange_halo!(φ, stag, setup), single rank (src/halo.jl:81-126). */
+int dnsb_fill_ghosts(dnsb_ctx *ctx, double *phi, int stag);
+
+/* divergence!(r, u, setup) (src/operators.jl:29-42); r ghost-free
+ * nx*ny*nz, x fastest. */
+int dnsb_divergence(dnsb_ctx *ctx, double *r, const double *ux, const double *uy,
+                    const double *uz);
+
+/* momentum!(q, u, A, Δt, setup) (src/operators.jl:155-178). */
+int dnsb_momentum(dnsb_ctx *ctx, double *qx, double *qy, double *qz, const double *ux,
+                  const double *uy, const double *uz, double A, double dt);
+
+/* pressuregrad_component!(φ, p, c, s, setup) (src/operators.jl:204-216). */
+int dnsb_pressuregrad(dnsb_ctx *ctx, double *phi, const double *p, int c, double s);
+
+/* poisson!(p, setup) (src/poisson.jl:147-161) with the right-hand side r
+ * (the reference's setup.poisson.r): writes the interior of p, no halos. */
+int dnsb_poisson(dnsb_ctx *ctx, const double *r, double *p);
+
+/* project!(u, ψ, setup) (src/timestep.jl:25-31): u and ψ leave with valid
+ * halos. */
+int dnsb_project(dnsb_ctx *ctx, double *ux, double *uy, double *uz, double *psi);
+
+/* imex_update!(u, q, p, B, α, Δt, setup) (src/ydiffusion.jl:119-154). */
+int dnsb_imex_update(dnsb_ctx *ctx, double *ux, double *uy, double *uz, const double *qx,
+                     const double *qy, const double *qz, const double *p, double B,
+                     double alpha, double dt);
+
+/* step!(u, p, q, δ, setup, Δt) (src/timestep.jl:41-63).  δ is scratch in
+ * explicit mode (the reference aliases it to p there); pass p or NULL. */
+int dnsb_step(dnsb_ctx *ctx, double *ux, double *uy, double *uz, double *p, double *qx,
+              double *qy, double *qz, double *delta, double dt);
+
+/* cfl_timestep(u, setup; cfl) (src/timestep.jl:69-80).  With
+ * use_step_max != 0 the velocity maxima reduced by the last dnsb_step on
+ * these same fields are reused (valid only if u was not modified since). */
+int dnsb_cfl(dnsb_ctx *ctx, const double *ux, const double *uy, const double *uz, double cfl,
+             int use_step_max, double *dt_out);
+
+/* solve!(; u, setup, tlims, Δt, cfl) (src/timestep.jl:92-111) without
+ * processors: initial halo + projection, then steps until t1 (or until
+ * max_steps).  dt > 0 fixes the step, dt <= 0 is CFL-adaptive.  p, q and
+ * delta are caller scratch fields (delta may be NULL in explicit mode).
+ * Reports the final time and the number of steps. */
+int dnsb_solve(dnsb_ctx *ctx, double *ux, double *uy, double *uz, double *p, double *qx,
+               double *qy, double *qz, double *delta, double t0, double t1, double dt,
+               double cfl, long max_steps, double *t_out, long *n_out);
+
+/* The same with HOST arrays for u (in/out) and p (out): the velocity is
+ * copied to the device, solved, and u, p copied back (for callers without
+ * device arrays; pinned host memory makes the copies faster). */
+int dnsb_solve_host(dnsb_ctx *ctx, double *ux, double *uy, double *uz, double *p, double t0,
+                    double t1, double dt, double cfl, long max_steps, double *t_out,
+                    long *n_out);
+
+/* maxdiv(u, setup) (src/fields.jl:38-42). */
+int dnsb_maxdiv(dnsb_ctx *ctx, const double *ux, const double *uy, const double *uz,
+                double *out);
+
+/* kinetic_energy(u, setup) (src/fields.jl:45-60). */
+int dnsb_kinetic_energy(dnsb_ctx *ctx, const double *ux, const double *uy, const double *uz,
+                        double *out);
+
+/* sample_channelstats! (src/stats.jl:39-58): adds the (x, z) plane sums of
+ * (U, W, uu, ww) on the ny cell rows and (V, vv, Uf, uv) on the nf active
+ * face rows (nf = ny-1 with walls) to the DEVICE accumulator acc
+ * (4*ny + 4*nf doubles, in that order). */
+int dnsb_channel_sample(dnsb_ctx *ctx, const double *ux, const double *uy, const double *uz,
+                        double *acc);
+
+/* sample_spectrum! + binshells! (src/stats.jl:120-157): adds the shell
+ * energies of u to the DEVICE array E (nbins doubles); periodic boxes only. */
+int dnsb_spectrum_sample(dnsb_ctx *ctx, const double *ux, const double *uy, const double *uz,
+                         double *E, int nbins);
+
+/* Counter-based noise on the active DOFs of component c (a channel initial
+ * condition; hash after src/spectral/ic.jl:31-45): φ += amp*(2U-1) with
+ * U = ((splitmix64(seed + key) >> 11) + 0.5) * 2^-53 and
+ * key = ((c*nz + K-1)*ny + J-1)*nx + I-1. */
+int dnsb_noise(dnsb_ctx *ctx, double *phi, int c, unsigned long long seed, double amp);
+
+/* Instrumentation (no counterpart in the reference, which has no profiling
+ * for the FV path): launches are counted always; with dnsb_profile(ctx, 1)
+ * every launch of the step path is bracketed by CUDA events on the context's
+ * stream and its device time is accumulated per kernel kind.  Enabling
+ * resets the accumulators; dnsb_profile_read synchronises. */
+enum {
+  DNSB_KIND_MOMENTUM = 0, DNSB_KIND_CN = 1, DNSB_KIND_RFFTX = 2, DNSB_KIND_FFTZ = 3,
+  DNSB_KIND_YSOLVE = 4, DNSB_KIND_IFFTZ = 5, DNSB_KIND_IRFFTX = 6, DNSB_KIND_GRAD = 7,
+  DNSB_KIND_OTHER = 8, DNSB_NKINDS = 9
+};
+int dnsb_profile(dnsb_ctx *ctx, int enable);
+int dnsb_profile_read(dnsb_ctx *ctx, int kind, double *ms, long *launches);
+long dnsb_launch_count(const dnsb_ctx *ctx);
+const char *dnsb_kind_name(int kind);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
