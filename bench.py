@@ -37,6 +37,9 @@ WORKLOADS = {
     "channel384_implicit": dict(
         n=(384, 256, 384), ydiffusion="implicit", visc=1 / 395, cfl=0.8, amp=0.2, retau=395.0,
         bytes_per_cell_step=1080.0),
+    "channel256_implicit": dict(
+        n=(256, 192, 256), ydiffusion="implicit", visc=1 / 395, cfl=0.8, amp=0.2, retau=395.0,
+        bytes_per_cell_step=1080.0),
     "channel64_explicit": dict(
         n=(64, 64, 64), ydiffusion="explicit", visc=1 / 180, cfl=0.5, amp=0.1, retau=None,
         bytes_per_cell_step=792.0),
@@ -301,6 +304,55 @@ def b200_arm(args, wl, world, rank, local):
     step_bytes = wl["bytes_per_cell_step"] * cells
     step_gbs = step_bytes / (ms / args.steps / 1e3) / 1e9
 
+    e2e_line = None
+    if not args.no_e2e:
+        e2e_line = e2e_leg(lib, s, host_ic, wl, args, world, dev, cells, G)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        secs, threads, _ = cpu_oracle_run(wl, args.cpu_steps, 1)
+        cpu = {"value": cells * args.cpu_steps / secs, "unit": "cell-steps/s", "cores": threads,
+               "kind": "port",
+               "sample": f"{args.cpu_steps} RK3 steps of the full {nx}x{ny}x{nz} grid after 1 "
+                         "warm-up step, CPU oracle (C/OpenMP restatement of the Julia "
+                         "reference) on all host threads"}
+
+    if rank == 0:
+        line = {
+            "metric": "DNS cell-steps/s (FP64)", "value": value, "unit": "cell-steps/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": args.workload, "grid": [nx, ny, nz],
+                       "ydiffusion": wl["ydiffusion"], "cfl": wl["cfl"],
+                       "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+                       "l2": "inputs larger than L2 (each field %.0f MB)" % (G * 8 / 1e6)},
+            "e2e": e2e_line,
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                         "peak_source": peak_kind,
+                         "algorithmic_bytes_per_launch": bytes_launch},
+            "step_roofline": {"bytes_per_cell_step": wl["bytes_per_cell_step"],
+                              "achieved": step_gbs, "peak": peak, "unit": "GB/s",
+                              "frac": step_gbs / peak},
+            "kernels": per_kernel,
+            "gpu_launches": launches,
+            "clocks": clk,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    s.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+def e2e_leg(lib, s, host_ic, wl, args, world, dev, cells, G):
+    """End to end through the C ABI with host buffers (dnsb_solve_host)."""
+    import ctypes
+
+    import torch
+
+    from distributednavierstokes_b200 import _lib
+
     # end to end through the C ABI with host buffers (dnsb_solve_host):
     # H2D of the initial velocity, initial projection, K CFL steps, D2H of u, p
     hu = {c: host_ic[c].clone().pin_memory() for c in "xyz"}
@@ -323,46 +375,10 @@ def b200_arm(args, wl, world, rank, local):
     e2e = world * cells * n_out.value / e2e_s
     h2d = 3 * G * 8 / n_out.value
     d2h = (4 * G * 8 + 24 * n_out.value) / n_out.value
-
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu:
-        secs, threads, _ = cpu_oracle_run(wl, args.cpu_steps, 1)
-        cpu = {"value": cells * args.cpu_steps / secs, "unit": "cell-steps/s", "cores": threads,
-               "kind": "port",
-               "sample": f"{args.cpu_steps} RK3 steps of the full {nx}x{ny}x{nz} grid after 1 "
-                         "warm-up step, CPU oracle (C/OpenMP restatement of the Julia "
-                         "reference) on all host threads"}
-
-    if rank == 0:
-        line = {
-            "metric": "DNS cell-steps/s (FP64)", "value": value, "unit": "cell-steps/s",
-            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": args.workload, "grid": [nx, ny, nz],
-                       "ydiffusion": wl["ydiffusion"], "cfl": wl["cfl"],
-                       "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
-                       "l2": "inputs larger than L2 (each field %.0f MB)" % (G * 8 / 1e6)},
-            "e2e": {"value": e2e, "unit": "cell-steps/s", "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h,
-                    "note": "dnsb_solve_host: pinned host u in, initial projection, "
-                            f"{n_out.value} CFL steps, u and p out"},
-            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
-                         "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
-                         "peak_source": peak_kind,
-                         "algorithmic_bytes_per_launch": bytes_launch},
-            "step_roofline": {"bytes_per_cell_step": wl["bytes_per_cell_step"],
-                              "achieved": step_gbs, "peak": peak, "unit": "GB/s",
-                              "frac": step_gbs / peak},
-            "kernels": per_kernel,
-            "gpu_launches": launches,
-            "clocks": clk,
-            "cpu_baseline": cpu,
-        }
-        print(json.dumps(line), flush=True)
-    s.close()
-    if world > 1:
-        torch.distributed.destroy_process_group()
+    return {"value": e2e, "unit": "cell-steps/s", "h2d_bytes_per_step": h2d,
+            "d2h_bytes_per_step": d2h,
+            "note": "dnsb_solve_host: pinned host u in, initial projection, "
+                    f"{n_out.value} CFL steps, u and p out"}
 
 
 def main():
@@ -374,6 +390,7 @@ def main():
     ap.add_argument("--workload", default="channel384_implicit", choices=list(WORKLOADS))
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "b200" else args.warmup
     wl = WORKLOADS[args.workload]

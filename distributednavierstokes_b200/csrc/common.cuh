@@ -83,22 +83,29 @@ __device__ __forceinline__ void img_y(Img &m, const Geo &g, int J, int stag) {
   }
 }
 
-// Store v at interior (I, J, K) and at all its ghost images.
-__device__ __forceinline__ void store_img(double *__restrict__ f, const Geo &g, int I, int J,
-                                          int K, double v, int stag) {
+// Ghost images only (not the interior cell itself); the slow path of
+// store_img, kept out of line so that interior threads carry no image
+// bookkeeping.
+__device__ __noinline__ void store_images_only(double *__restrict__ f, const Geo &g, int I, int J,
+                                               int K, double v, int stag) {
   Img mx, my, mz;
   img_periodic(mx, I, g.nx);
   img_y(my, g, J, stag);
   img_periodic(mz, K, g.nz);
-  if (mx.n == 1 && my.n == 1 && mz.n == 1) {
-    f[gidx(g, I, J, K)] = v;
-    return;
-  }
   for (int c = 0; c < mz.n; c++)
     for (int b = 0; b < my.n; b++) {
       double vv = my.sgn[b] == 0.0 ? 0.0 : my.sgn[b] * v;
-      for (int a = 0; a < mx.n; a++) f[gidx(g, mx.pos[a], my.pos[b], mz.pos[c])] = vv;
+      for (int a = 0; a < mx.n; a++)
+        if (a | b | c) f[gidx(g, mx.pos[a], my.pos[b], mz.pos[c])] = vv;
     }
+}
+
+// Store v at interior (I, J, K) and at all its ghost images.
+__device__ __forceinline__ void store_img(double *__restrict__ f, const Geo &g, int I, int J,
+                                          int K, double v, int stag) {
+  f[gidx(g, I, J, K)] = v;
+  const bool edge = (I == 1) | (I == g.nx) | (K == 1) | (K == g.nz) | (J == 1) | (J >= g.ny - 1);
+  if (edge) store_images_only(f, g, I, J, K, v, stag);
 }
 
 // Interior source of a ghost cell (inverse of the image map); returns false

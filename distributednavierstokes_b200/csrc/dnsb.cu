@@ -18,6 +18,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -81,7 +82,8 @@ struct dnsb_ctx {
   double2 *twM = nullptr, *twN = nullptr, *twz = nullptr, *twy = nullptr;
   FFTPlan pM{}, pz{}, py{};
   int Lx = 1, Lz = 1, Ly = 1;
-  size_t smem_rx = 0, smem_ix = 0, smem_z = 0, smem_y = 0;
+  size_t smem_rx = 0, smem_ix = 0, smem_z = 0, smem_y = 0, smem_cn = 0;
+  dim3 cgrid, cblock;  // launch shape of the per-cell step kernels
   // scratch
   double2 *S = nullptr;
   double *work = nullptr;
@@ -197,6 +199,7 @@ int upload(dnsb_ctx *c, T **p, const std::vector<T> &h) {
 }
 
 dim3 cell_grid(const Geo &g) { return dim3((g.nx + 31) / 32, (g.ny + 7) / 8, g.nz); }
+dim3 cn_grid(const Geo &g) { return dim3((g.nx + CN_LINES - 1) / CN_LINES, g.nz, 3); }
 const dim3 cell_block(32, 8, 1);
 
 CFields3 cf(const double *x, const double *y, const double *z) { return CFields3{x, y, z}; }
@@ -371,7 +374,9 @@ __global__ void k_noise(Geo g, double *phi, int c, unsigned long long seed, doub
   const unsigned long long rr = splitmix64(seed + key);
   const double U = ((double)(rr >> 11) + 0.5) * 0x1p-53;
   const long long c0 = gidx(g, I, J, K);
-  phi[c0] += amp * (2 * U - 1);
+  // explicit roundings (no FMA contraction) so that the field is bit-identical
+  // to a host evaluation of phi + amp*(2U - 1)
+  phi[c0] = __dadd_rn(phi[c0], __dmul_rn(amp, __dsub_rn(2 * U, 1.0)));
 }
 
 // ------------------------------------------------------------- pipeline --
@@ -452,29 +457,29 @@ int do_step(dnsb_ctx *c, double *ux, double *uy, double *uz, double *p, double *
     unsigned long long *um = s == 2 ? c->umax : nullptr;
     if (!c->implicit) {
       LAUNCH(c, DNSB_KIND_MOMENTUM,
-             k_momentum<MOM_EXPLICIT><<<cell_grid(g), cell_block, 0, c->stream>>>(
+             k_momentum<MOM_EXPLICIT><<<c->cgrid, c->cblock, 0, c->stream>>>(
                  g, ff(qx, qy, qz), cf(ux, uy, uz), ff(c->W[0], c->W[1], c->W[2]), nullptr, A, dt,
                  B, 0.0, readq));
       if ((rc = launch_rfftx(c, RIN_DIVERGENCE, c->W[0], c->W[1], c->W[2]))) return rc;
       if ((rc = poisson_from_spectrum(c, ROUT_IMAGES, p))) return rc;
       LAUNCH(c, DNSB_KIND_GRAD,
-             k_grad<GRAD_EXPLICIT><<<cell_grid(g), cell_block, 0, c->stream>>>(
+             k_grad<GRAD_EXPLICIT><<<c->cgrid, c->cblock, 0, c->stream>>>(
                  g, ff(ux, uy, uz), cf(c->W[0], c->W[1], c->W[2]), p, nullptr, 0.0, um));
     } else {
       const double adt = al * dt;
       LAUNCH(c, DNSB_KIND_MOMENTUM,
-             k_momentum<MOM_IMPLICIT><<<cell_grid(g), cell_block, 0, c->stream>>>(
+             k_momentum<MOM_IMPLICIT><<<c->cgrid, c->cblock, 0, c->stream>>>(
                  g, ff(qx, qy, qz), cf(ux, uy, uz), ff(c->V[0], c->V[1], c->V[2]), p, A, dt, B,
                  adt, readq));
       const double th = al * dt * g.visc / 2;
       LAUNCH(c, DNSB_KIND_CN,
-             k_cn<<<dim3((g.nx + 63) / 64, g.nz, 3), 64, 0, c->stream>>>(
+             k_cn<<<cn_grid(g), dim3(CN_LINES, CN_CHUNKS), c->smem_cn, c->stream>>>(
                  g, ff(ux, uy, uz), cf(c->V[0], c->V[1], c->V[2]), cf(ux, uy, uz), c->ycoef,
-                 c->ytab + (long long)s * 6 * g.ny, th));
+                 c->ytab + (long long)s * 2 * cn_tab_stride(g.ny), th));
       if ((rc = launch_rfftx(c, RIN_DIVERGENCE, ux, uy, uz))) return rc;
       if ((rc = poisson_from_spectrum(c, ROUT_IMAGES, delta))) return rc;
       LAUNCH(c, DNSB_KIND_GRAD,
-             k_grad<GRAD_IMPLICIT><<<cell_grid(g), cell_block, 0, c->stream>>>(
+             k_grad<GRAD_IMPLICIT><<<c->cgrid, c->cblock, 0, c->stream>>>(
                  g, ff(ux, uy, uz), cf(ux, uy, uz), delta, p, 1.0 / adt, um));
     }
   }
@@ -490,7 +495,7 @@ int do_project(dnsb_ctx *c, double *ux, double *uy, double *uz, double *psi) {
   if ((rc = launch_rfftx(c, RIN_DIVERGENCE, ux, uy, uz))) return rc;
   if ((rc = poisson_from_spectrum(c, ROUT_IMAGES, psi))) return rc;
   LAUNCH(c, DNSB_KIND_GRAD,
-         k_grad<GRAD_EXPLICIT><<<cell_grid(g), cell_block, 0, c->stream>>>(
+         k_grad<GRAD_EXPLICIT><<<c->cgrid, c->cblock, 0, c->stream>>>(
              g, ff(ux, uy, uz), cf(ux, uy, uz), psi, nullptr, 0.0, nullptr));
   c->umax_for[0] = c->umax_for[1] = c->umax_for[2] = nullptr;
   return 0;
@@ -641,14 +646,33 @@ int dnsb_create(const dnsb_grid *gr, int device, void *stream, dnsb_ctx **out) {
       (rc = upload(c, &c->twN, twN)) || (rc = upload(c, &c->twz, twz)) ||
       (rc = upload(c, &c->twy, twy)))
     return bail(rc);
-  if ((rc = dalloc(c, &c->ytab, 18 * (size_t)ny))) return bail(rc);
+  if ((rc = dalloc(c, &c->ytab, 6 * (size_t)cn_tab_stride(ny)))) return bail(rc);
+  c->smem_cn = sizeof(double) * ((size_t)ny * CN_LINES + 2 * CN_CHUNKS * CN_LINES);
+  if (c->implicit && c->smem_cn > 200 * 1024) {
+    fail(c, DNSB_EUNSUP, "semi-implicit y-diffusion supports ny <= %d", (200 * 1024 / 8 - 2 * CN_CHUNKS * CN_LINES) / CN_LINES);
+    return bail(DNSB_EUNSUP);
+  }
+  if ((rc = allow_smem(c, k_cn, c->smem_cn))) return bail(rc);
 
-  // launch shapes: L lines per CTA, two line buffers each within ~100 KB
+  // launch shapes: L lines per CTA, two line buffers each within ~100 KB;
+  // DNSB_LX / DNSB_LZ / DNSB_LY / DNSB_CELL_BLOCK ("32x8") override them
   auto pow2floor = [](int v) { int p = 1; while (2 * p <= v) p *= 2; return p; };
+  auto envint = [](const char *name, int dflt) {
+    const char *e = getenv(name);
+    return (e && atoi(e) > 0) ? atoi(e) : dflt;
+  };
   const int budget = 100 * 1024 / (2 * (int)sizeof(double2));  // complex per buffer
-  c->Lx = pow2floor(std::max(1, std::min({8, nz, budget / (M + 2)})));
-  c->Lz = std::max(1, std::min(8, budget / (nz + 1)));
-  c->Ly = pow2floor(std::max(1, std::min({8, nz, budget / ny})));
+  c->Lx = pow2floor(std::max(1, std::min({envint("DNSB_LX", 8), nz, budget / (M + 2)})));
+  c->Lz = std::max(1, std::min(envint("DNSB_LZ", 8), budget / (nz + 1)));
+  c->Ly = pow2floor(std::max(1, std::min({envint("DNSB_LY", 8), nz, budget / ny})));
+  {
+    int bx = 32, by = 8;
+    const char *e = getenv("DNSB_CELL_BLOCK");
+    if (e && sscanf(e, "%dx%d", &bx, &by) == 2 && bx > 0 && by > 0 && bx * by <= 256 && bx % 32 == 0) {
+    } else { bx = 32; by = 8; }
+    c->cblock = dim3(bx, by, 1);
+    c->cgrid = dim3((nx + bx - 1) / bx, (ny + by - 1) / by, nz);
+  }
   c->smem_rx = sizeof(double2) * (2 * (size_t)c->Lx * (M + 1) + M + (M + 1));
   c->smem_ix = sizeof(double2) * (2 * (size_t)c->Lx * (M + 2) + M + (M + 1));
   c->smem_z = sizeof(double2) * (2 * (size_t)c->Lz * (nz + 1) + nz);
@@ -788,7 +812,7 @@ int dnsb_imex_update(dnsb_ctx *c, double *ux, double *uy, double *uz, const doub
   k_cn_tables<<<1, 32, 0, c->stream>>>(g.ny, c->ycoef, c->ytab, dt, g.visc, alpha, alpha, alpha);
   CKL(c);
   const double th = alpha * dt * g.visc / 2;
-  k_cn<<<dim3((g.nx + 63) / 64, g.nz, 3), 64, 0, c->stream>>>(
+  k_cn<<<cn_grid(g), dim3(CN_LINES, CN_CHUNKS), c->smem_cn, c->stream>>>(
       g, ff(ux, uy, uz), cf(c->V[0], c->V[1], c->V[2]), cf(ux, uy, uz), c->ycoef, c->ytab, th);
   CKL(c);
   c->umax_for[0] = c->umax_for[1] = c->umax_for[2] = nullptr;

@@ -290,12 +290,21 @@ __global__ void __launch_bounds__(SPEC_THREADS) k_irfftx(Geo g, const double2 *_
   }
 }
 
-// Per-step Crank-Nicolson tables (imexsolve_kernel!, src/ydiffusion.jl:94-109):
-// the Thomas coefficients of (I - theta Dy) depend on y only, so
-// beta_j, c'_j = -theta c_j / beta_j and theta a_j are computed once per
-// stage and set instead of once per line.  tab layout per (stage, set):
-// [ta(ny) | cp(ny) | ib(ny)], ib = 1/beta; set 0 tangential, 1 normal.
-// coef: [at bt ct an bn cn], ny each.  One thread per (stage, set).
+// Per-stage Crank-Nicolson tables (imexsolve_kernel!, src/ydiffusion.jl:94-109).
+// The Thomas coefficients of (I - theta Dy) depend on y only, so they are
+// computed once per stage and set instead of once per line: beta_j,
+// c'_j = -theta c_j / beta_j, theta a_j.  For the chunked sweeps of k_cn the
+// forward multipliers f_j = theta a_j / beta_j and backward multipliers
+// -c'_j are also accumulated per chunk of CN_CHUNKS rows:
+//   g_j = prod_{i=s..j} f_i (s = chunk start), h_j = prod_{i=j..e} (-c'_i)
+// (e = chunk end), G_k = g at the end of chunk k, H_k = h at its start.
+// tab layout per (stage, set): [ta | cp | ib | g | h](ny each), [G | H](CN_CHUNKS
+// each); ib = 1/beta; set 0 tangential, 1 normal.  coef: [at bt ct an bn cn].
+constexpr int CN_CHUNKS = 8;
+constexpr int CN_LINES = 32;
+
+__host__ __device__ constexpr long long cn_tab_stride(int ny) { return 5LL * ny + 2 * CN_CHUNKS; }
+
 __global__ void k_cn_tables(int ny, const double *__restrict__ coef, double *__restrict__ tab,
                             double dt, double visc, double al0, double al1, double al2) {
   const int t = threadIdx.x;
@@ -305,8 +314,9 @@ __global__ void k_cn_tables(int ny, const double *__restrict__ coef, double *__r
   const double th = al * dt * visc / 2;
   const double *a = coef + (set ? 3 : 0) * ny;
   const double *b = a + ny, *c = b + ny;
-  double *ta = tab + (long long)(st * 2 + set) * 3 * ny;
-  double *cp = ta + ny, *ib = cp + ny;
+  double *ta = tab + (long long)(st * 2 + set) * cn_tab_stride(ny);
+  double *cp = ta + ny, *ib = cp + ny, *gf = ib + ny, *hb = gf + ny;
+  double *G = hb + ny, *H = G + CN_CHUNKS;
   double beta = 1 - th * b[0];
   double cprev = -th * c[0] / beta;
   ta[0] = th * a[0];
@@ -319,59 +329,102 @@ __global__ void k_cn_tables(int ny, const double *__restrict__ coef, double *__r
     cp[j] = cprev;
     ib[j] = 1.0 / beta;
   }
+  const int m = (ny + CN_CHUNKS - 1) / CN_CHUNKS;
+  for (int k = 0; k < CN_CHUNKS; k++) {
+    const int s0 = k * m, e0 = min(ny, s0 + m) - 1;
+    G[k] = 1.0;
+    H[k] = 1.0;
+    if (s0 > e0) continue;
+    double acc = 1.0;
+    for (int j = s0; j <= e0; j++) { acc *= ta[j] * ib[j]; gf[j] = acc; }
+    G[k] = acc;
+    acc = 1.0;
+    for (int j = e0; j >= s0; j--) { acc *= -cp[j]; hb[j] = acc; }
+    H[k] = acc;
+  }
 }
 
-// imexrhs_kernel! + imexsolve_kernel! (src/ydiffusion.jl:71-109) fused: one
-// thread per (I, K) y-line of component c = blockIdx.z; rhs = v + theta Dy u^n
-// with the walls folded into the rows, then the Thomas sweeps with the
-// per-stage tables.  The forward-swept values go to out (which may alias
-// the u^n field, each line being owned by one thread); the backward sweep
-// writes the result with ghost images.
-__global__ void __launch_bounds__(128) k_cn(Geo g, Fields3 out, CFields3 V, CFields3 un,
-                                           const double *__restrict__ coef,
-                                           const double *__restrict__ tab, double theta) {
-  const int I = blockIdx.x * blockDim.x + threadIdx.x + 1;
+// imexrhs_kernel! + imexsolve_kernel! (src/ydiffusion.jl:71-109) fused.
+// A block owns CN_LINES consecutive x-lines (I) at one K for component
+// c = blockIdx.z and splits every y-line into CN_CHUNKS chunks, one thread
+// per (line, chunk).  Each thread forms rhs = v + theta Dy u^n on its rows
+// (walls folded into the rows), runs the Thomas forward sweep from a zero
+// carry, the chunks exchange their end values through shared memory and
+// add the carried-in part with the per-chunk multiplier products (g, G);
+// the backward sweep is split the same way (h, H).  Algebraically this is
+// the reference's Thomas algorithm; every element is read from and written
+// to HBM once.  out may alias u^n: all reads precede the first write.
+__global__ void __launch_bounds__(CN_LINES *CN_CHUNKS) k_cn(Geo g, Fields3 out, CFields3 V, CFields3 un,
+                                                           const double *__restrict__ coef,
+                                                           const double *__restrict__ tab,
+                                                           double theta) {
+  extern __shared__ double cs[];  // [ny][CN_LINES] line columns, then exchange slots
+  const int i = threadIdx.x, ck = threadIdx.y;
+  const int I = blockIdx.x * CN_LINES + i + 1;
   const int K = blockIdx.y + 1;
   const int c = blockIdx.z;
-  if (I > g.nx) return;
   const int ny = g.ny;
+  double *col = cs;
+  double *xa = cs + (long long)ny * CN_LINES;  // [CN_CHUNKS][CN_LINES]
+  double *xb = xa + CN_CHUNKS * CN_LINES;
   const int set = c == STAG_Y ? 1 : 0;
   const double *a = coef + set * 3 * ny, *b = a + ny, *cc = b + ny;
-  const double *ta = tab + set * 3 * ny, *cp = ta + ny, *ib = cp + ny;
+  const double *ta = tab + set * cn_tab_stride(ny), *cp = ta + ny, *ib = cp + ny, *gf = ib + ny,
+               *hb = gf + ny, *G = hb + ny, *H = G + CN_CHUNKS;
   const double *v = c == 0 ? V.x : c == 1 ? V.y : V.z;
   const double *u = c == 0 ? un.x : c == 1 ? un.y : un.z;
   double *o = c == 0 ? out.x : c == 1 ? out.y : out.z;
+  const bool active = I <= g.nx;
+  const int m = (ny + CN_CHUNKS - 1) / CN_CHUNKS;
+  const int s0 = ck * m, e0 = min(ny, s0 + m) - 1;
   const long long sy = g.NX;
-  const long long base = gidx(g, I, 1, K);
-  // forward sweep
-  double um = 0.0, u0 = u[base], up = ny > 1 ? u[base + sy] : 0.0;
-  double xprev = 0.0;
-  for (int j = 0; j < ny; j++) {
-    const long long cj = base + j * sy;
-    double s;
-    if (j == 0) s = b[0] * u0 + (ny > 1 ? cc[0] * up : 0.0);
-    else if (j == ny - 1) s = a[j] * um + b[j] * u0;
-    else s = (a[j] * um + b[j] * u0) + cc[j] * up;
-    const double rhs = v[cj] + theta * s;
-    const double x = j == 0 ? rhs * ib[0] : (rhs + ta[j] * xprev) * ib[j];
-    o[cj] = x;
-    xprev = x;
-    um = u0;
-    u0 = up;
-    if (j + 2 < ny) up = u[cj + 2 * sy];
+  const long long base = gidx(g, active ? I : 1, 1, K);
+  // 1. rhs and local forward sweep (zero carry)
+  double z = 0.0;
+  if (active && s0 <= e0) {
+    double um = s0 > 0 ? u[base + (s0 - 1) * sy] : 0.0;
+    double u0 = u[base + s0 * sy];
+    for (int j = s0; j <= e0; j++) {
+      const long long cj = base + j * sy;
+      const double up = j + 1 < ny ? u[cj + sy] : 0.0;
+      double sum;
+      if (j == 0) sum = b[0] * u0 + (ny > 1 ? cc[0] * up : 0.0);
+      else if (j == ny - 1) sum = a[j] * um + b[j] * u0;
+      else sum = (a[j] * um + b[j] * u0) + cc[j] * up;
+      const double rhs = v[cj] + theta * sum;
+      z = j == s0 ? rhs * ib[j] : (rhs + ta[j] * z) * ib[j];
+      col[j * CN_LINES + i] = z;
+      um = u0;
+      u0 = up;
+    }
   }
-  // backward sweep + images
-  double xn = xprev;
-  const int stag = c;
-  const bool normal_wall = g.wall && c == STAG_Y;
-  // the inactive wall face J = ny of the normal component keeps its zero
-  // (row ny of the normal operator is zero) and gets no images of its own
-  if (!normal_wall) store_img(o, g, I, ny, K, xn, stag);
-  for (int j = ny - 2; j >= 0; j--) {
-    const long long cj = base + j * sy;
-    const double x = o[cj] - cp[j] * xn;
-    store_img(o, g, I, j + 1, K, x, stag);
-    xn = x;
+  xa[ck * CN_LINES + i] = z;
+  __syncthreads();
+  // 2. carry into this chunk: x'_{s-1} = sum over earlier chunks
+  double cin = 0.0;
+  for (int k = 0; k < ck; k++) cin = xa[k * CN_LINES + i] + G[k] * cin;
+  // 3. forward values and local backward sweep (zero carry)
+  double bnext = 0.0;
+  if (active && s0 <= e0) {
+    for (int j = e0; j >= s0; j--) {
+      const double xp = col[j * CN_LINES + i] + gf[j] * cin;
+      bnext = xp - cp[j] * bnext;
+      col[j * CN_LINES + i] = bnext;
+    }
+  }
+  xb[ck * CN_LINES + i] = bnext;  // first row of the chunk (b_s)
+  __syncthreads();
+  // 4. carry from later chunks: x_{e+1}
+  double cout = 0.0;
+  for (int k = CN_CHUNKS - 1; k > ck; k--) cout = xb[k * CN_LINES + i] + H[k] * cout;
+  // 5. final values with ghost images
+  if (active && s0 <= e0) {
+    const bool normal_wall = g.wall && c == STAG_Y;
+    for (int j = s0; j <= e0; j++) {
+      const double x = col[j * CN_LINES + i] + hb[j] * cout;
+      if (normal_wall && j == ny - 1) o[base + j * sy] = x;
+      else store_img(o, g, I, j + 1, K, x, c);
+    }
   }
 }
 
