@@ -50,62 +50,70 @@ __host__ __device__ __forceinline__ long long sidx(const Geo &g, int kx, int j, 
 // Writing v to every image after writing the interior keeps the halo of a
 // field valid without a separate exchange pass; the x, y and z fills of the
 // reference compose into exactly this product of per-axis images.
-struct Img {
-  int n;
-  int pos[3];
-  double sgn[3];
-};
-
-__device__ __forceinline__ void img_periodic(Img &m, int I, int n) {
-  m.n = 1;
-  m.pos[0] = I;
-  m.sgn[0] = 1.0;
-  if (I == 1) { m.pos[m.n] = n + 1; m.sgn[m.n++] = 1.0; }
-  if (I == n) { m.pos[m.n] = 0; m.sgn[m.n++] = 1.0; }
-}
-
-// y images; a sign of 0 marks a wall face that receives an exact zero
-__device__ __forceinline__ void img_y(Img &m, const Geo &g, int J, int stag) {
-  if (!g.wall) { img_periodic(m, J, g.ny); return; }
-  m.n = 1;
-  m.pos[0] = J;
-  m.sgn[0] = 1.0;
-  if (stag == STAG_Y) {
-    if (J == 1) { m.pos[m.n] = 0; m.sgn[m.n++] = 0.0; }
-    if (J == g.ny - 1) {
-      m.pos[m.n] = g.ny; m.sgn[m.n++] = 0.0;
-      m.pos[m.n] = g.ny + 1; m.sgn[m.n++] = -1.0;
-    }
-  } else {
-    double s = stag == STAG_P ? 1.0 : -1.0;
-    if (J == 1) { m.pos[m.n] = 0; m.sgn[m.n++] = s; }
-    if (J == g.ny) { m.pos[m.n] = g.ny + 1; m.sgn[m.n++] = s; }
-  }
-}
-
-// Ghost images only (not the interior cell itself); the slow path of
-// store_img, kept out of line so that interior threads carry no image
-// bookkeeping.
-__device__ __noinline__ void store_images_only(double *__restrict__ f, const Geo &g, int I, int J,
-                                               int K, double v, int stag) {
-  Img mx, my, mz;
-  img_periodic(mx, I, g.nx);
-  img_y(my, g, J, stag);
-  img_periodic(mz, K, g.nz);
-  for (int c = 0; c < mz.n; c++)
-    for (int b = 0; b < my.n; b++) {
-      double vv = my.sgn[b] == 0.0 ? 0.0 : my.sgn[b] * v;
-      for (int a = 0; a < mx.n; a++)
-        if (a | b | c) f[gidx(g, mx.pos[a], my.pos[b], mz.pos[c])] = vv;
-    }
-}
-
-// Store v at interior (I, J, K) and at all its ghost images.
+// Interior threads only test the edge predicate; edge threads run
+// straight-line predicated stores (no local memory).
 __device__ __forceinline__ void store_img(double *__restrict__ f, const Geo &g, int I, int J,
                                           int K, double v, int stag) {
   f[gidx(g, I, J, K)] = v;
   const bool edge = (I == 1) | (I == g.nx) | (K == 1) | (K == g.nz) | (J == 1) | (J >= g.ny - 1);
-  if (edge) store_images_only(f, g, I, J, K, v, stag);
+  if (!edge) return;
+  const int Ia = (I == 1) ? g.nx + 1 : (I == g.nx) ? 0 : -1;  // nx >= 2: at most one
+  const int Ka = (K == 1) ? g.nz + 1 : (K == g.nz) ? 0 : -1;
+  const int Kb = (K == 1 && K == g.nz) ? 0 : -1;               // nz == 1
+  int Ja = -1, Jb = -1, Jc = -1;
+  double fa = 0.0, fb = 0.0, fc = 0.0;
+  if (!g.wall) {
+    Ja = (J == 1) ? g.ny + 1 : (J == g.ny) ? 0 : -1;
+    fa = 1.0;
+  } else if (stag == STAG_Y) {
+    if (J == 1) { Ja = 0; fa = 0.0; }
+    if (J == g.ny - 1) { Jb = g.ny; fb = 0.0; Jc = g.ny + 1; fc = -1.0; }
+  } else {
+    const double s = stag == STAG_P ? 1.0 : -1.0;
+    if (J == 1) { Ja = 0; fa = s; }
+    if (J == g.ny) { Jb = g.ny + 1; fb = s; }
+  }
+#pragma unroll
+  for (int zc = 0; zc < 3; zc++) {
+    const int Kz = zc == 0 ? K : zc == 1 ? Ka : Kb;
+    if (Kz < 0) continue;
+#pragma unroll
+    for (int yc = 0; yc < 4; yc++) {
+      const int Jy = yc == 0 ? J : yc == 1 ? Ja : yc == 2 ? Jb : Jc;
+      if (Jy < 0) continue;
+      const double fy = yc == 0 ? 1.0 : yc == 1 ? fa : yc == 2 ? fb : fc;
+      const double vv = fy == 0.0 ? 0.0 : fy * v;
+#pragma unroll
+      for (int xc = 0; xc < 2; xc++) {
+        const int Ix = xc == 0 ? I : Ia;
+        if (Ix < 0 || (xc == 0 && yc == 0 && zc == 0)) continue;
+        f[gidx(g, Ix, Jy, Kz)] = vv;
+      }
+    }
+  }
+}
+
+// Cooperative copy loop with B loads in flight per thread: element t of
+// [0, total) is read with ld(t) and written with st(t, value).  All B loads
+// of a batch are issued before the first store, so a thread keeps B
+// requests outstanding instead of one.
+template <int B, class Ld, class St>
+__device__ __forceinline__ void batched_copy(int total, Ld ld, St st) {
+  const int nth = blockDim.x * blockDim.y;
+  const int tid = threadIdx.x + blockDim.x * threadIdx.y;
+  for (int base = tid; base < total; base += B * nth) {
+    decltype(ld(0)) r[B];
+#pragma unroll
+    for (int u = 0; u < B; u++) {
+      const int t = base + u * nth;
+      if (t < total) r[u] = ld(t);
+    }
+#pragma unroll
+    for (int u = 0; u < B; u++) {
+      const int t = base + u * nth;
+      if (t < total) st(t, r[u]);
+    }
+  }
 }
 
 // Interior source of a ghost cell (inverse of the image map); returns false

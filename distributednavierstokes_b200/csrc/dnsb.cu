@@ -647,9 +647,9 @@ int dnsb_create(const dnsb_grid *gr, int device, void *stream, dnsb_ctx **out) {
       (rc = upload(c, &c->twy, twy)))
     return bail(rc);
   if ((rc = dalloc(c, &c->ytab, 6 * (size_t)cn_tab_stride(ny)))) return bail(rc);
-  c->smem_cn = sizeof(double) * ((size_t)ny * CN_LINES + 2 * CN_CHUNKS * CN_LINES);
+  c->smem_cn = sizeof(double) * (2 * (size_t)ny * CN_LINES + 2 * CN_CHUNKS * CN_LINES);
   if (c->implicit && c->smem_cn > 200 * 1024) {
-    fail(c, DNSB_EUNSUP, "semi-implicit y-diffusion supports ny <= %d", (200 * 1024 / 8 - 2 * CN_CHUNKS * CN_LINES) / CN_LINES);
+    fail(c, DNSB_EUNSUP, "semi-implicit y-diffusion supports ny <= %d", (200 * 1024 / 8 - 2 * CN_CHUNKS * CN_LINES) / (2 * CN_LINES));
     return bail(DNSB_EUNSUP);
   }
   if ((rc = allow_smem(c, k_cn, c->smem_cn))) return bail(rc);

@@ -163,6 +163,84 @@ __device__ double2 *fft_lines(double2 *a, double2 *b, const FFTPlan &p, int L, i
   return a;
 }
 
+// Stages that read their inputs from, or write their outputs to, global
+// memory through functors, so that the first stage loads straight into
+// registers (R independent loads in flight per butterfly, no staging copy)
+// and the last stage stores straight from registers.
+// ld(l, e) returns element e of line l; st(l, e, v) stores it.
+template <int R, bool INV, class Ld, class St>
+__device__ __forceinline__ void fft_stage_io(Ld ld, const double2 *__restrict__ in,
+                                             double2 *__restrict__ out, St st, bool gin,
+                                             bool gout, int n, int Ns, int L, int es, int ls,
+                                             bool jfast, const double2 *__restrict__ tw) {
+  const int nb = n / R;
+  const int total = nb * L;
+  const int stride_tw = n / (Ns * R);
+  for (int b = threadIdx.x; b < total; b += blockDim.x) {
+    int l, j;
+    if (jfast) { l = b / nb; j = b - l * nb; }
+    else { j = b / L; l = b - j * L; }
+    const int k = j % Ns;
+    double2 v[R];
+#pragma unroll
+    for (int r = 0; r < R; r++) v[r] = gin ? ld(l, j + r * nb) : in[l * ls + (j + r * nb) * es];
+    if (k != 0) {
+#pragma unroll
+      for (int r = 1; r < R; r++) {
+        double2 w = tw[k * r * stride_tw];
+        if (INV) w = cconj(w);
+        v[r] = cmul(v[r], w);
+      }
+    }
+    dft_small<R, INV>(v);
+    const int base = (j - k) * R + k;
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+      if (gout) st(l, base + r * Ns, v[r]);
+      else out[l * ls + (base + r * Ns) * es] = v[r];
+    }
+  }
+  __syncthreads();
+}
+
+template <bool INV, class Ld, class St>
+__device__ __forceinline__ void fft_stage_io_any(int R, Ld ld, const double2 *in, double2 *out,
+                                                 St st, bool gin, bool gout, int n, int Ns, int L,
+                                                 int es, int ls, bool jfast,
+                                                 const double2 *__restrict__ tw) {
+  switch (R) {
+    case 2: fft_stage_io<2, INV>(ld, in, out, st, gin, gout, n, Ns, L, es, ls, jfast, tw); break;
+    case 3: fft_stage_io<3, INV>(ld, in, out, st, gin, gout, n, Ns, L, es, ls, jfast, tw); break;
+    case 4: fft_stage_io<4, INV>(ld, in, out, st, gin, gout, n, Ns, L, es, ls, jfast, tw); break;
+    case 5: fft_stage_io<5, INV>(ld, in, out, st, gin, gout, n, Ns, L, es, ls, jfast, tw); break;
+    case 8: fft_stage_io<8, INV>(ld, in, out, st, gin, gout, n, Ns, L, es, ls, jfast, tw); break;
+    default: break;
+  }
+}
+
+// Transform of L lines in which the first stage reads with ld (when
+// load_global, else from a) and the last stage writes with st (when
+// store_global, else to shared memory); the stages between ping-pong in
+// shared memory (a, b with layout es/ls).  Returns the shared buffer that
+// holds the result when !store_global.  The twiddle table must be in place
+// (and synchronised) before the call.
+template <bool INV, class Ld, class St>
+__device__ double2 *fft_lines_io(Ld ld, St st, double2 *a, double2 *b, const FFTPlan &p, int L,
+                                 int es, int ls, bool jfast, const double2 *__restrict__ tw,
+                                 bool load_global, bool store_global) {
+  int Ns = 1;
+  for (int s = 0; s < p.nst; s++) {
+    const int R = p.radix[s];
+    const bool gin = load_global && s == 0, gout = store_global && s == p.nst - 1;
+    fft_stage_io_any<INV>(R, ld, a, b, st, gin, gout, p.n, Ns, L, es, ls, jfast, tw);
+    Ns *= R;
+    double2 *t = a;
+    a = b;
+    b = t;
+  }
+  return a;
+}
+
 // Host-side plan: radices 8 first, then 4, 2, 3, 5.  Returns false
 // when n has another prime factor.
 inline bool make_fft_plan(int n, FFTPlan &p) {

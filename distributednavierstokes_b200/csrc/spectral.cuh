@@ -53,32 +53,34 @@ __global__ void __launch_bounds__(SPEC_THREADS) k_rfftx(Geo g, double2 *__restri
   const long long sy = g.NX, sz = (long long)g.NX * g.NY;
   const int J = j + 1;
   const double rdyJ = __ldg(g.rdy + J);
-  for (int t = threadIdx.x; t < L * M; t += blockDim.x) {
-    const int l = t / M, m = t - l * M;
+  __syncthreads();
+  auto ld = [&](int l, int m) {
     const int k = k0 + l;
     double2 z = make_double2(0.0, 0.0);
     if (k < g.nz) {
       if (INMODE == RIN_REAL) {
         const double *row = in0 + (long long)g.nx * (j + (long long)g.ny * k);
-        z = *reinterpret_cast<const double2 *>(row + 2 * m);
+        z = __ldg(reinterpret_cast<const double2 *>(row + 2 * m));
       } else {
         const long long c0 = gidx(g, 2 * m + 1, J, k + 1);
         if (INMODE == RIN_FIELD) {
-          z = make_double2(in0[c0], in0[c0 + 1]);
+          z = make_double2(__ldg(in0 + c0), __ldg(in0 + c0 + 1));
         } else {
-          const double a0 = in0[c0 - 1], a1 = in0[c0], a2 = in0[c0 + 1];
-          const double r0 = (a1 - a0) * g.rdx + (in1[c0] - in1[c0 - sy]) * rdyJ +
-                            (in2[c0] - in2[c0 - sz]) * g.rdz;
-          const double r1 = (a2 - a1) * g.rdx + (in1[c0 + 1] - in1[c0 + 1 - sy]) * rdyJ +
-                            (in2[c0 + 1] - in2[c0 + 1 - sz]) * g.rdz;
+          const double a0 = __ldg(in0 + c0 - 1), a1 = __ldg(in0 + c0), a2 = __ldg(in0 + c0 + 1);
+          const double b0 = __ldg(in1 + c0), b1 = __ldg(in1 + c0 - sy);
+          const double b2 = __ldg(in1 + c0 + 1), b3 = __ldg(in1 + c0 + 1 - sy);
+          const double d0 = __ldg(in2 + c0), d1 = __ldg(in2 + c0 - sz);
+          const double d2 = __ldg(in2 + c0 + 1), d3 = __ldg(in2 + c0 + 1 - sz);
+          const double r0 = (a1 - a0) * g.rdx + (b0 - b1) * rdyJ + (d0 - d1) * g.rdz;
+          const double r1 = (a2 - a1) * g.rdx + (b2 - b3) * rdyJ + (d2 - d3) * g.rdz;
           z = make_double2(r0, r1);
         }
       }
     }
-    buf[l * ls + m] = z;
-  }
-  __syncthreads();
-  const double2 *res = fft_lines<false>(buf, buf2, plan, L, 1, ls, true, tw);
+    return z;
+  };
+  auto nost = [](int, int, double2) {};
+  const double2 *res = fft_lines_io<false>(ld, nost, buf, buf2, plan, L, 1, ls, true, tw, true, false);
   // post-process and store S(kx, j, k0 + l), l fastest (coalesced in kz)
   const int Lv = min(L, g.nz - k0);
   for (int t = threadIdx.x; t < Lv * (M + 1); t += blockDim.x) {
@@ -93,7 +95,8 @@ __global__ void __launch_bounds__(SPEC_THREADS) k_rfftx(Geo g, double2 *__restri
   }
 }
 
-// Complex FFT along z of L contiguous lines of S; INV scales by 1/nz.
+// Complex FFT along z of L contiguous lines of S; INV scales by 1/nz.  The
+// first stage loads from HBM into registers, the last stores from registers.
 template <bool INV>
 __global__ void __launch_bounds__(SPEC_THREADS) k_fftz(Geo g, double2 *__restrict__ S,
                                                       FFTPlan plan, int L,
@@ -108,33 +111,36 @@ __global__ void __launch_bounds__(SPEC_THREADS) k_fftz(Geo g, double2 *__restric
   const long long l0 = (long long)blockIdx.x * L;
   const int Lv = (int)min((long long)L, nlines - l0);
   for (int t = threadIdx.x; t < n; t += blockDim.x) tw[t] = twz[t];
-  double2 *src = S + l0 * n;
-  for (int t = threadIdx.x; t < L * n; t += blockDim.x) {
-    const int l = t / n, e = t - l * n;
-    buf[l * ls + e] = l < Lv ? src[t] : make_double2(0.0, 0.0);
-  }
   __syncthreads();
-  const double2 *res = fft_lines<INV>(buf, buf2, plan, L, 1, ls, true, tw);
+  double2 *src = S + l0 * n;
   const double sc = 1.0 / n;
-  for (int t = threadIdx.x; t < Lv * n; t += blockDim.x) {
-    const int l = t / n, e = t - l * n;
-    const double2 v = res[l * ls + e];
-    src[t] = INV ? cscale(v, sc) : v;
-  }
+  fft_lines_io<INV>(
+      [&](int l, int e) { return l < Lv ? src[l * n + e] : make_double2(0.0, 0.0); },
+      [&](int l, int e, double2 v) {
+        if (l < Lv) src[l * n + e] = INV ? cscale(v, sc) : v;
+      },
+      buf, buf2, plan, L, 1, ls, true, tw, true, true);
 }
 
 // thomas_kernel! (src/poisson.jl:14-41): one thread per (kx, kz) line, in
 // place on S, c' in the work array (same layout as S).  The mean mode
-// (lambda == 0) is pinned by replacing its first row with x_1 = 0.
-__global__ void k_thomas(Geo g, double2 *__restrict__ S, double *__restrict__ work,
-                         const double *__restrict__ ay, const double *__restrict__ by,
-                         const double *__restrict__ cy, const double *__restrict__ lam1,
-                         const double *__restrict__ lam3) {
+// (lambda == 0) is pinned by replacing its first row with x_1 = 0.  Rows are
+// processed in groups of TP whose loads are issued together, so a thread
+// keeps TP rows in flight while its recurrence runs.
+constexpr int TP = 8;
+__global__ void __launch_bounds__(128) k_thomas(Geo g, double2 *__restrict__ S,
+                                                double *__restrict__ work,
+                                                const double *__restrict__ ay,
+                                                const double *__restrict__ by,
+                                                const double *__restrict__ cy,
+                                                const double *__restrict__ lam1,
+                                                const double *__restrict__ lam3) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (long long)g.nz * g.nkx) return;
   const int kz = (int)(t % g.nz), kx = (int)(t / g.nz);
   const double lam = lam1[kx] + lam3[kz];
   const long long st = g.nz;
+  const int ny = g.ny;
   double2 *x = S + sidx(g, kx, 0, kz);
   double *cp = work + sidx(g, kx, 0, kz);
   const bool pin = lam == 0.0;
@@ -144,22 +150,43 @@ __global__ void k_thomas(Geo g, double2 *__restrict__ S, double *__restrict__ wo
   double2 xprev = pin ? make_double2(0.0, 0.0) : x[0];
   xprev = make_double2(xprev.x / beta, xprev.y / beta);
   x[0] = xprev;
-  for (int j = 1; j < g.ny; j++) {
-    const double a = ay[j];
-    beta = (by[j] + lam) - a * cprev;
-    cprev = cy[j] / beta;
-    cp[j * st] = cprev;
-    const double2 xj = x[j * st];
-    xprev = make_double2((xj.x - a * xprev.x) / beta, (xj.y - a * xprev.y) / beta);
-    x[j * st] = xprev;
+  for (int j0 = 1; j0 < ny; j0 += TP) {
+    double2 xr[TP];
+#pragma unroll
+    for (int q = 0; q < TP; q++)
+      if (j0 + q < ny) xr[q] = x[(j0 + q) * st];
+#pragma unroll
+    for (int q = 0; q < TP; q++) {
+      const int j = j0 + q;
+      if (j < ny) {
+        const double a = __ldg(ay + j);
+        beta = (__ldg(by + j) + lam) - a * cprev;
+        cprev = __ldg(cy + j) / beta;
+        cp[j * st] = cprev;
+        xprev = make_double2((xr[q].x - a * xprev.x) / beta, (xr[q].y - a * xprev.y) / beta);
+        x[j * st] = xprev;
+      }
+    }
   }
   double2 xn = xprev;
-  for (int j = g.ny - 2; j >= 0; j--) {
-    const double c = cp[j * st];
-    double2 xj = x[j * st];
-    xj = make_double2(xj.x - c * xn.x, xj.y - c * xn.y);
-    x[j * st] = xj;
-    xn = xj;
+  for (int j0 = ny - 2; j0 >= 0; j0 -= TP) {
+    double2 xr[TP];
+    double cr[TP];
+#pragma unroll
+    for (int q = 0; q < TP; q++)
+      if (j0 - q >= 0) {
+        xr[q] = x[(j0 - q) * st];
+        cr[q] = cp[(j0 - q) * st];
+      }
+#pragma unroll
+    for (int q = 0; q < TP; q++) {
+      const int j = j0 - q;
+      if (j >= 0) {
+        const double2 xj = make_double2(xr[q].x - cr[q] * xn.x, xr[q].y - cr[q] * xn.y);
+        x[j * st] = xj;
+        xn = xj;
+      }
+    }
   }
 }
 
@@ -185,30 +212,29 @@ __global__ void __launch_bounds__(SPEC_THREADS) k_yfourier(Geo g, double2 *__res
   const int k0 = grp * L;
   const int Lv = min(L, g.nz - k0);
   for (int t = threadIdx.x; t < n; t += blockDim.x) tw[t] = twy[t];
+  __syncthreads();
+  auto ld = [&](int l, int e) {
+    return l < Lv ? S[sidx(g, kx, e, k0 + l)] : make_double2(0.0, 0.0);
+  };
+  const double sc = SPECTRUM_ONLY ? 1.0 : 1.0 / n;
+  auto st = [&](int l, int e, double2 v) {
+    if (l < Lv) S[sidx(g, kx, e, k0 + l)] = SPECTRUM_ONLY ? v : cscale(v, sc);
+  };
+  if (SPECTRUM_ONLY) {
+    fft_lines_io<false>(ld, st, buf, buf2, plan, L, L, 1, false, tw, true, true);
+    return;
+  }
+  double2 *res = fft_lines_io<false>(ld, st, buf, buf2, plan, L, L, 1, false, tw, true, false);
+  const double l1 = lam1[kx];
   for (int t = threadIdx.x; t < L * n; t += blockDim.x) {
     const int j = t / L, l = t - j * L;
-    buf[t] = l < Lv ? S[sidx(g, kx, j, k0 + l)] : make_double2(0.0, 0.0);
+    const int kz = min(k0 + l, g.nz - 1);
+    const double lam = (l1 + lam2[j]) + lam3[kz];
+    const double2 v = res[t];
+    res[t] = lam == 0.0 ? make_double2(0.0, 0.0) : make_double2(v.x / lam, v.y / lam);
   }
   __syncthreads();
-  double2 *res = fft_lines<false>(buf, buf2, plan, L, L, 1, false, tw);
-  if (!SPECTRUM_ONLY) {
-    const double l1 = lam1[kx];
-    for (int t = threadIdx.x; t < L * n; t += blockDim.x) {
-      const int j = t / L, l = t - j * L;
-      const int kz = min(k0 + l, g.nz - 1);
-      const double lam = (l1 + lam2[j]) + lam3[kz];
-      const double2 v = res[t];
-      res[t] = lam == 0.0 ? make_double2(0.0, 0.0) : make_double2(v.x / lam, v.y / lam);
-    }
-    __syncthreads();
-    res = fft_lines<true>(res, res == buf ? buf2 : buf, plan, L, L, 1, false, tw);
-  }
-  const double sc = SPECTRUM_ONLY ? 1.0 : 1.0 / n;
-  for (int t = threadIdx.x; t < Lv * n; t += blockDim.x) {
-    const int j = t / Lv, l = t - j * Lv;
-    const double2 v = res[j * L + l];
-    S[sidx(g, kx, j, k0 + l)] = SPECTRUM_ONLY ? v : cscale(v, sc);
-  }
+  fft_lines_io<true>(ld, st, res, res == buf ? buf2 : buf, plan, L, L, 1, false, tw, false, true);
 }
 
 // Inverse real FFT along x (normalised 1/nx, imaginary parts of the kx = 0
@@ -235,10 +261,16 @@ __global__ void __launch_bounds__(SPEC_THREADS) k_irfftx(Geo g, const double2 *_
   const int Lv = min(L, g.nz - k0);
   for (int t = threadIdx.x; t < M; t += blockDim.x) tw[t] = twM[t];
   for (int t = threadIdx.x; t <= M; t += blockDim.x) tn[t] = twN[t];
-  for (int t = threadIdx.x; t < L * (M + 1); t += blockDim.x) {
-    const int kx = t / L, l = t - kx * L;
-    buf[l * ls + kx] = l < Lv ? S[sidx(g, kx, j, k0 + l)] : make_double2(0.0, 0.0);
-  }
+  batched_copy<8>(
+      L * (M + 1),
+      [&](int t) {
+        const int kx = t / L, l = t - kx * L;
+        return l < Lv ? S[sidx(g, kx, j, k0 + l)] : make_double2(0.0, 0.0);
+      },
+      [&](int t, double2 v) {
+        const int kx = t / L, l = t - kx * L;
+        buf[l * ls + kx] = v;
+      });
   __syncthreads();
   // Z[k] = E[k] + i O[k], E = (X[k] + conj X[M-k])/2,
   // O = (X[k] - conj X[M-k]) conj(w^k)/2; one thread per pair (k, M-k).
@@ -268,12 +300,11 @@ __global__ void __launch_bounds__(SPEC_THREADS) k_irfftx(Geo g, const double2 *_
     }
   }
   __syncthreads();
-  const double2 *res = fft_lines<true>(buf, buf2, plan, L, 1, ls, true, tw);
   const double sc = 1.0 / M;
   const int J = j + 1;
-  for (int t = threadIdx.x; t < Lv * M; t += blockDim.x) {
-    const int l = t / M, m = t - l * M;
-    const double2 z = res[l * ls + m];
+  auto noload = [](int, int) { return make_double2(0.0, 0.0); };
+  auto st = [&](int l, int m, double2 z) {
+    if (l >= Lv) return;
     const double x0 = z.x * sc, x1 = z.y * sc;
     const int K = k0 + l + 1;
     if (OUTMODE == ROUT_REAL) {
@@ -287,7 +318,8 @@ __global__ void __launch_bounds__(SPEC_THREADS) k_irfftx(Geo g, const double2 *_
       store_img(out, g, 2 * m + 1, J, K, x0, STAG_P);
       store_img(out, g, 2 * m + 2, J, K, x1, STAG_P);
     }
-  }
+  };
+  fft_lines_io<true>(noload, st, buf, buf2, plan, L, 1, ls, true, tw, false, true);
 }
 
 // Per-stage Crank-Nicolson tables (imexsolve_kernel!, src/ydiffusion.jl:94-109).
@@ -300,8 +332,8 @@ __global__ void __launch_bounds__(SPEC_THREADS) k_irfftx(Geo g, const double2 *_
 // (e = chunk end), G_k = g at the end of chunk k, H_k = h at its start.
 // tab layout per (stage, set): [ta | cp | ib | g | h](ny each), [G | H](CN_CHUNKS
 // each); ib = 1/beta; set 0 tangential, 1 normal.  coef: [at bt ct an bn cn].
-constexpr int CN_CHUNKS = 8;
-constexpr int CN_LINES = 32;
+constexpr int CN_CHUNKS = 16;
+constexpr int CN_LINES = 16;
 
 __host__ __device__ constexpr long long cn_tab_stride(int ny) { return 5LL * ny + 2 * CN_CHUNKS; }
 
@@ -346,26 +378,30 @@ __global__ void k_cn_tables(int ny, const double *__restrict__ coef, double *__r
 
 // imexrhs_kernel! + imexsolve_kernel! (src/ydiffusion.jl:71-109) fused.
 // A block owns CN_LINES consecutive x-lines (I) at one K for component
-// c = blockIdx.z and splits every y-line into CN_CHUNKS chunks, one thread
-// per (line, chunk).  Each thread forms rhs = v + theta Dy u^n on its rows
-// (walls folded into the rows), runs the Thomas forward sweep from a zero
-// carry, the chunks exchange their end values through shared memory and
-// add the carried-in part with the per-chunk multiplier products (g, G);
-// the backward sweep is split the same way (h, H).  Algebraically this is
-// the reference's Thomas algorithm; every element is read from and written
-// to HBM once.  out may alias u^n: all reads precede the first write.
+// c = blockIdx.z.  The block first stages the y-columns of v and u^n of its
+// lines in shared memory (coalesced rows, many loads in flight), then splits
+// every y-line into CN_CHUNKS chunks, one thread per (line, chunk).  Each
+// thread forms rhs = v + theta Dy u^n on its rows (walls folded into the
+// rows), runs the Thomas forward sweep from a zero carry, the chunks
+// exchange their end values through shared memory and add the carried-in
+// part with the per-chunk multiplier products (g, G); the backward sweep is
+// split the same way (h, H).  Algebraically this is the reference's Thomas
+// algorithm; every element is read from and written to HBM once.  out may
+// alias u^n: all reads precede the first write.
 __global__ void __launch_bounds__(CN_LINES *CN_CHUNKS) k_cn(Geo g, Fields3 out, CFields3 V, CFields3 un,
                                                            const double *__restrict__ coef,
                                                            const double *__restrict__ tab,
                                                            double theta) {
-  extern __shared__ double cs[];  // [ny][CN_LINES] line columns, then exchange slots
+  extern __shared__ double cs[];  // vcol[ny][CN_LINES], ucol[ny][CN_LINES], exchange
   const int i = threadIdx.x, ck = threadIdx.y;
-  const int I = blockIdx.x * CN_LINES + i + 1;
+  const int I0 = blockIdx.x * CN_LINES + 1;
+  const int I = I0 + i;
   const int K = blockIdx.y + 1;
   const int c = blockIdx.z;
   const int ny = g.ny;
   double *col = cs;
-  double *xa = cs + (long long)ny * CN_LINES;  // [CN_CHUNKS][CN_LINES]
+  double *ucol = cs + (long long)ny * CN_LINES;
+  double *xa = ucol + (long long)ny * CN_LINES;  // [CN_CHUNKS][CN_LINES]
   double *xb = xa + CN_CHUNKS * CN_LINES;
   const int set = c == STAG_Y ? 1 : 0;
   const double *a = coef + set * 3 * ny, *b = a + ny, *cc = b + ny;
@@ -374,55 +410,79 @@ __global__ void __launch_bounds__(CN_LINES *CN_CHUNKS) k_cn(Geo g, Fields3 out, 
   const double *v = c == 0 ? V.x : c == 1 ? V.y : V.z;
   const double *u = c == 0 ? un.x : c == 1 ? un.y : un.z;
   double *o = c == 0 ? out.x : c == 1 ? out.y : out.z;
-  const bool active = I <= g.nx;
+  const long long sy = g.NX;
+  const long long base0 = gidx(g, I0, 1, K);
+  const int nl = min(CN_LINES, g.nx - I0 + 1);
+  // 0. stage v and u^n columns (rows J = 1..ny)
+  batched_copy<4>(
+      ny * CN_LINES,
+      [&](int t) {
+        const int row = t / CN_LINES, l = t - row * CN_LINES;
+        const long long off = base0 + row * sy + l;
+        return l < nl ? make_double2(v[off], u[off]) : make_double2(0.0, 0.0);
+      },
+      [&](int t, double2 w) {
+        col[t] = w.x;
+        ucol[t] = w.y;
+      });
+  __syncthreads();
+  // 1. rhs = v + theta Dy u^n for every staged element (independent)
+  batched_copy<4>(
+      ny * CN_LINES,
+      [&](int t) {
+        const int j = t / CN_LINES;
+        const double u0 = ucol[t];
+        const double um = j > 0 ? ucol[t - CN_LINES] : 0.0;
+        const double up = j + 1 < ny ? ucol[t + CN_LINES] : 0.0;
+        double sum;
+        if (j == 0) sum = __ldg(b) * u0 + (ny > 1 ? __ldg(cc) * up : 0.0);
+        else if (j == ny - 1) sum = __ldg(a + j) * um + __ldg(b + j) * u0;
+        else sum = (__ldg(a + j) * um + __ldg(b + j) * u0) + __ldg(cc + j) * up;
+        return col[t] + theta * sum;
+      },
+      [&](int t, double r) { col[t] = r; });
+  __syncthreads();
+  const bool active = i < nl;
   const int m = (ny + CN_CHUNKS - 1) / CN_CHUNKS;
   const int s0 = ck * m, e0 = min(ny, s0 + m) - 1;
-  const long long sy = g.NX;
-  const long long base = gidx(g, active ? I : 1, 1, K);
-  // 1. rhs and local forward sweep (zero carry)
+  // 2. local forward sweep (zero carry)
   double z = 0.0;
   if (active && s0 <= e0) {
-    double um = s0 > 0 ? u[base + (s0 - 1) * sy] : 0.0;
-    double u0 = u[base + s0 * sy];
-    for (int j = s0; j <= e0; j++) {
-      const long long cj = base + j * sy;
-      const double up = j + 1 < ny ? u[cj + sy] : 0.0;
-      double sum;
-      if (j == 0) sum = b[0] * u0 + (ny > 1 ? cc[0] * up : 0.0);
-      else if (j == ny - 1) sum = a[j] * um + b[j] * u0;
-      else sum = (a[j] * um + b[j] * u0) + cc[j] * up;
-      const double rhs = v[cj] + theta * sum;
-      z = j == s0 ? rhs * ib[j] : (rhs + ta[j] * z) * ib[j];
+    z = col[s0 * CN_LINES + i] * __ldg(ib + s0);
+    col[s0 * CN_LINES + i] = z;
+#pragma unroll 4
+    for (int j = s0 + 1; j <= e0; j++) {
+      z = fma(__ldg(ta + j), z, col[j * CN_LINES + i]) * __ldg(ib + j);
       col[j * CN_LINES + i] = z;
-      um = u0;
-      u0 = up;
     }
   }
   xa[ck * CN_LINES + i] = z;
   __syncthreads();
-  // 2. carry into this chunk: x'_{s-1} = sum over earlier chunks
+  // 2. carry into this chunk: x'_{s-1} from the earlier chunks
   double cin = 0.0;
   for (int k = 0; k < ck; k++) cin = xa[k * CN_LINES + i] + G[k] * cin;
   // 3. forward values and local backward sweep (zero carry)
   double bnext = 0.0;
   if (active && s0 <= e0) {
+#pragma unroll 4
     for (int j = e0; j >= s0; j--) {
-      const double xp = col[j * CN_LINES + i] + gf[j] * cin;
-      bnext = xp - cp[j] * bnext;
+      const double xp = fma(__ldg(gf + j), cin, col[j * CN_LINES + i]);
+      bnext = fma(-__ldg(cp + j), bnext, xp);
       col[j * CN_LINES + i] = bnext;
     }
   }
   xb[ck * CN_LINES + i] = bnext;  // first row of the chunk (b_s)
   __syncthreads();
-  // 4. carry from later chunks: x_{e+1}
+  // 4. carry from the later chunks: x_{e+1}
   double cout = 0.0;
   for (int k = CN_CHUNKS - 1; k > ck; k--) cout = xb[k * CN_LINES + i] + H[k] * cout;
   // 5. final values with ghost images
   if (active && s0 <= e0) {
     const bool normal_wall = g.wall && c == STAG_Y;
+#pragma unroll 4
     for (int j = s0; j <= e0; j++) {
-      const double x = col[j * CN_LINES + i] + hb[j] * cout;
-      if (normal_wall && j == ny - 1) o[base + j * sy] = x;
+      const double x = fma(__ldg(hb + j), cout, col[j * CN_LINES + i]);
+      if (normal_wall && j == ny - 1) o[base0 + i + j * sy] = x;
       else store_img(o, g, I, j + 1, K, x, c);
     }
   }

@@ -23,7 +23,7 @@ enum MomMode { MOM_ONLY = 0, MOM_EXPLICIT = 1, MOM_IMPLICIT = 2 };
 // MOM_EXPLICIT: also W_c = u_c + B q_c on active DOFs, with ghost images.
 // MOM_IMPLICIT: also V_c = u_c + B q_c - adt * d_c p on active DOFs.
 template <int MODE>
-__global__ void __launch_bounds__(256) k_momentum(Geo g, Fields3 q, CFields3 u, Fields3 out,
+__global__ void __launch_bounds__(256, 4) k_momentum(Geo g, Fields3 q, CFields3 u, Fields3 out,
                                                   const double *__restrict__ p, double A, double dt,
                                                   double B, double adt, int readq) {
   const int I = blockIdx.x * blockDim.x + threadIdx.x + 1;
@@ -47,6 +47,15 @@ __global__ void __launch_bounds__(256) k_momentum(Geo g, Fields3 q, CFields3 u, 
   const double uzT = LDG(uz, c0 + sz), uzB = LDG(uz, c0 - sz);
   const double uzEB = LDG(uz, c0 + 1 - sz), uzNB = LDG(uz, c0 + sy - sz);
 
+  const double qx0 = readq ? q.x[c0] : 0.0, qy0 = readq ? q.y[c0] : 0.0;
+  const double qz0 = readq ? q.z[c0] : 0.0;
+  double pE = 0.0, pN = 0.0, pT = 0.0, p0 = 0.0;
+  if (MODE == MOM_IMPLICIT) {
+    p0 = __ldg(p + c0);
+    pE = __ldg(p + c0 + 1);
+    pN = __ldg(p + c0 + sy);
+    pT = __ldg(p + c0 + sz);
+  }
   const double dyJ = __ldg(g.dy + J), dyJ1 = __ldg(g.dy + J + 1);
   const double rdyJ = __ldg(g.rdy + J), rdyJ1 = __ldg(g.rdy + J + 1);
   const double rdyuJ = __ldg(g.rdyu + J), rdyuJm = __ldg(g.rdyu + J - 1);
@@ -66,7 +75,7 @@ __global__ void __launch_bounds__(256) k_momentum(Geo g, Fields3 q, CFields3 u, 
                         ey * ((uxN - ux0) * rdyuJ - (ux0 - uxS) * rdyuJm) * rdyJ +
                         (uxT - 2 * ux0 + uxB) * g.rdz2;
     const double f = dt * (-conv + nu * diff + g.fx);
-    qxn = readq ? A * q.x[c0] + f : f;
+    qxn = readq ? A * qx0 + f : f;
   }
   // y momentum, at the top y-face; Delta-y weighted transporters
   {
@@ -82,7 +91,7 @@ __global__ void __launch_bounds__(256) k_momentum(Geo g, Fields3 q, CFields3 u, 
                         ey * ((uyN - uy0) * rdyJ1 - (uy0 - uyS) * rdyJ) * rdyuJ +
                         (uyT - 2 * uy0 + uyB) * g.rdz2;
     const double f = dt * (-conv + nu * diff + g.fy);
-    qyn = readq ? A * q.y[c0] + f : f;
+    qyn = readq ? A * qy0 + f : f;
   }
   // z momentum, at the back z-face
   {
@@ -97,7 +106,7 @@ __global__ void __launch_bounds__(256) k_momentum(Geo g, Fields3 q, CFields3 u, 
                         ey * ((uzN - uz0) * rdyuJ - (uz0 - uzS) * rdyuJm) * rdyJ +
                         (uzT - 2 * uz0 + uzB) * g.rdz2;
     const double f = dt * (-conv + nu * diff + g.fz);
-    qzn = readq ? A * q.z[c0] + f : f;
+    qzn = readq ? A * qz0 + f : f;
   }
   const bool yact = J <= g.jymax;
   q.x[c0] = qxn;
@@ -111,10 +120,9 @@ __global__ void __launch_bounds__(256) k_momentum(Geo g, Fields3 q, CFields3 u, 
     store_img(out.z, g, I, J, K, uz0 + B * qzn, STAG_Z);
   } else if (MODE == MOM_IMPLICIT) {
     // v = u + B q - alpha dt grad p (ydiffusion.jl:133-135), interior only
-    const double p0 = __ldg(p + c0);
-    out.x[c0] = (ux0 + B * qxn) - adt * (__ldg(p + c0 + 1) - p0) * g.rdx;
-    out.y[c0] = yact ? (uy0 + B * qyn) - adt * (__ldg(p + c0 + sy) - p0) * rdyuJ : uy0;
-    out.z[c0] = (uz0 + B * qzn) - adt * (__ldg(p + c0 + sz) - p0) * g.rdz;
+    out.x[c0] = (ux0 + B * qxn) - adt * (pE - p0) * g.rdx;
+    out.y[c0] = yact ? (uy0 + B * qyn) - adt * (pN - p0) * rdyuJ : uy0;
+    out.z[c0] = (uz0 + B * qzn) - adt * (pT - p0) * g.rdz;
   }
 }
 
@@ -141,19 +149,22 @@ __global__ void __launch_bounds__(256) k_grad(Geo g, Fields3 u, CFields3 W,
   if (I <= g.nx && J <= g.ny) {
     const long long sy = g.NX, sz = (long long)g.NX * g.NY;
     const long long c0 = gidx(g, I, J, K);
-    const double s0 = psi[c0];
-    const double vx = W.x[c0] - (psi[c0 + 1] - s0) * g.rdx;
-    const double vz = W.z[c0] - (psi[c0 + sz] - s0) * g.rdz;
+    const bool yact = J <= g.jymax;
+    // every load before the first store (u may alias W)
+    const double s0 = psi[c0], sE = psi[c0 + 1], sN = psi[c0 + sy], sT = psi[c0 + sz];
+    const double wx = W.x[c0], wy = W.y[c0], wz = W.z[c0];
+    const double p0 = MODE == GRAD_IMPLICIT ? p[c0] : 0.0;
+    const double ry = __ldg(g.rdyu + J);
+    const double vx = wx - (sE - s0) * g.rdx;
+    const double vy = wy - (sN - s0) * ry;
+    const double vz = wz - (sT - s0) * g.rdz;
     store_img(u.x, g, I, J, K, vx, STAG_X);
     store_img(u.z, g, I, J, K, vz, STAG_Z);
+    if (yact) store_img(u.y, g, I, J, K, vy, STAG_Y);
+    if (MODE == GRAD_IMPLICIT) store_img(p, g, I, J, K, p0 + s0 * radt, STAG_P);
     m0 = fabs(vx);
+    m1 = yact ? fabs(vy) : 0.0;
     m2 = fabs(vz);
-    if (J <= g.jymax) {
-      const double vy = W.y[c0] - (psi[c0 + sy] - s0) * __ldg(g.rdyu + J);
-      store_img(u.y, g, I, J, K, vy, STAG_Y);
-      m1 = fabs(vy);
-    }
-    if (MODE == GRAD_IMPLICIT) store_img(p, g, I, J, K, p[c0] + s0 * radt, STAG_P);
   }
   if (umax) {
     for (int o = 16; o > 0; o >>= 1) {
