@@ -83,6 +83,7 @@ struct dnsb_ctx {
   FFTPlan pM{}, pz{}, py{};
   int Lx = 1, Lz = 1, Ly = 1;
   size_t smem_rx = 0, smem_ix = 0, smem_z = 0, smem_y = 0, smem_cn = 0;
+  int cn_mr = 1;      // rows per chunk of the CN solve
   dim3 cgrid, cblock;  // launch shape of the per-cell step kernels
   // scratch
   double2 *S = nullptr;
@@ -93,6 +94,7 @@ struct dnsb_ctx {
   unsigned long long *umax = nullptr;  // [3] max |u_c| of the last step; [3] scratch
   double *partial = nullptr;           // reduction partials
   double *hostred = nullptr;           // pinned, 8 doubles
+  unsigned long long *hostumax = nullptr;  // pinned, 3 * UMAX_SLOTS
   const double *umax_for[3] = {nullptr, nullptr, nullptr};
   // launch counting and per-kind CUDA-event timing (dnsb_profile)
   long launches = 0;
@@ -442,15 +444,28 @@ int poisson_from_spectrum(dnsb_ctx *c, int outmode, double *out) {
   return launch_irfftx(c, outmode, out);
 }
 
+void launch_cn(dnsb_ctx *c, Fields3 out, CFields3 V, CFields3 un, const double *tab, double th) {
+  const Geo &g = c->g;
+  const dim3 grid = cn_grid(g), block(CN_LINES, CN_CHUNKS);
+  switch (c->cn_mr) {
+    case 1: k_cn<1><<<grid, block, c->smem_cn, c->stream>>>(g, out, V, un, c->ycoef, tab, th); break;
+    case 2: k_cn<2><<<grid, block, c->smem_cn, c->stream>>>(g, out, V, un, c->ycoef, tab, th); break;
+    case 4: k_cn<4><<<grid, block, c->smem_cn, c->stream>>>(g, out, V, un, c->ycoef, tab, th); break;
+    case 8: k_cn<8><<<grid, block, c->smem_cn, c->stream>>>(g, out, V, un, c->ycoef, tab, th); break;
+    case 16: k_cn<16><<<grid, block, c->smem_cn, c->stream>>>(g, out, V, un, c->ycoef, tab, th); break;
+    default: k_cn<32><<<grid, block, c->smem_cn, c->stream>>>(g, out, V, un, c->ycoef, tab, th); break;
+  }
+}
+
 int do_step(dnsb_ctx *c, double *ux, double *uy, double *uz, double *p, double *qx, double *qy,
             double *qz, double *delta, double dt) {
   const Geo &g = c->g;
   int rc;
-  CK(c, cudaMemsetAsync(c->umax, 0, 3 * sizeof(unsigned long long), c->stream));
+  CK(c, cudaMemsetAsync(c->umax, 0, 3 * UMAX_SLOTS * sizeof(unsigned long long), c->stream));
   if (c->implicit)
     LAUNCH(c, DNSB_KIND_OTHER,
-           k_cn_tables<<<1, 32, 0, c->stream>>>(g.ny, c->ycoef, c->ytab, dt, g.visc, RK_AL[0],
-                                                RK_AL[1], RK_AL[2]));
+           k_cn_tables<<<1, 32, 0, c->stream>>>(g.ny, c->cn_mr, c->ycoef, c->ytab, dt, g.visc,
+                                                RK_AL[0], RK_AL[1], RK_AL[2]));
   for (int s = 0; s < 3; s++) {
     const double A = RK_A[s], B = RK_B[s], al = RK_AL[s];
     const int readq = A != 0.0;
@@ -473,9 +488,8 @@ int do_step(dnsb_ctx *c, double *ux, double *uy, double *uz, double *p, double *
                  adt, readq));
       const double th = al * dt * g.visc / 2;
       LAUNCH(c, DNSB_KIND_CN,
-             k_cn<<<cn_grid(g), dim3(CN_LINES, CN_CHUNKS), c->smem_cn, c->stream>>>(
-                 g, ff(ux, uy, uz), cf(c->V[0], c->V[1], c->V[2]), cf(ux, uy, uz), c->ycoef,
-                 c->ytab + (long long)s * 2 * cn_tab_stride(g.ny), th));
+             launch_cn(c, ff(ux, uy, uz), cf(c->V[0], c->V[1], c->V[2]), cf(ux, uy, uz),
+                       c->ytab + (long long)s * 2 * cn_tab_stride(g.ny), th));
       if ((rc = launch_rfftx(c, RIN_DIVERGENCE, ux, uy, uz))) return rc;
       if ((rc = poisson_from_spectrum(c, ROUT_IMAGES, delta))) return rc;
       LAUNCH(c, DNSB_KIND_GRAD,
@@ -647,12 +661,17 @@ int dnsb_create(const dnsb_grid *gr, int device, void *stream, dnsb_ctx **out) {
       (rc = upload(c, &c->twy, twy)))
     return bail(rc);
   if ((rc = dalloc(c, &c->ytab, 6 * (size_t)cn_tab_stride(ny)))) return bail(rc);
-  c->smem_cn = sizeof(double) * (2 * (size_t)ny * CN_LINES + 2 * CN_CHUNKS * CN_LINES);
-  if (c->implicit && c->smem_cn > 200 * 1024) {
-    fail(c, DNSB_EUNSUP, "semi-implicit y-diffusion supports ny <= %d", (200 * 1024 / 8 - 2 * CN_CHUNKS * CN_LINES) / (2 * CN_LINES));
+  c->cn_mr = 1;
+  while (c->cn_mr * CN_CHUNKS < ny) c->cn_mr *= 2;
+  c->smem_cn = sizeof(double) * (8 * (size_t)ny + 2 * CN_CHUNKS + 2 * CN_CHUNKS * CN_LINES);
+  if (c->implicit && c->cn_mr > 32) {
+    fail(c, DNSB_EUNSUP, "semi-implicit y-diffusion supports ny <= %d", 32 * CN_CHUNKS);
     return bail(DNSB_EUNSUP);
   }
-  if ((rc = allow_smem(c, k_cn, c->smem_cn))) return bail(rc);
+  if ((rc = allow_smem(c, k_cn<1>, c->smem_cn)) || (rc = allow_smem(c, k_cn<2>, c->smem_cn)) ||
+      (rc = allow_smem(c, k_cn<4>, c->smem_cn)) || (rc = allow_smem(c, k_cn<8>, c->smem_cn)) ||
+      (rc = allow_smem(c, k_cn<16>, c->smem_cn)) || (rc = allow_smem(c, k_cn<32>, c->smem_cn)))
+    return bail(rc);
 
   // launch shapes: L lines per CTA, two line buffers each within ~100 KB;
   // DNSB_LX / DNSB_LZ / DNSB_LY / DNSB_CELL_BLOCK ("32x8") override them
@@ -663,13 +682,13 @@ int dnsb_create(const dnsb_grid *gr, int device, void *stream, dnsb_ctx **out) {
   };
   const int budget = 100 * 1024 / (2 * (int)sizeof(double2));  // complex per buffer
   c->Lx = pow2floor(std::max(1, std::min({envint("DNSB_LX", 8), nz, budget / (M + 2)})));
-  c->Lz = std::max(1, std::min(envint("DNSB_LZ", 8), budget / (nz + 1)));
+  c->Lz = std::max(1, std::min(envint("DNSB_LZ", 4), budget / (nz + 1)));
   c->Ly = pow2floor(std::max(1, std::min({envint("DNSB_LY", 8), nz, budget / ny})));
   {
-    int bx = 32, by = 8;
+    int bx = 64, by = 2;
     const char *e = getenv("DNSB_CELL_BLOCK");
     if (e && sscanf(e, "%dx%d", &bx, &by) == 2 && bx > 0 && by > 0 && bx * by <= 256 && bx % 32 == 0) {
-    } else { bx = 32; by = 8; }
+    } else { bx = 64; by = 2; }
     c->cblock = dim3(bx, by, 1);
     c->cgrid = dim3((nx + bx - 1) / bx, (ny + by - 1) / by, nz);
   }
@@ -693,7 +712,7 @@ int dnsb_create(const dnsb_grid *gr, int device, void *stream, dnsb_ctx **out) {
   const size_t G = (size_t)g.NX * g.NY * g.NZ;
   const size_t nspec = (size_t)g.nkx * ny * nz;
   if ((rc = dalloc(c, &c->S, nspec)) || (rc = dalloc(c, &c->r, (size_t)nx * ny * nz)) ||
-      (rc = dalloc(c, &c->umax, 8)) || (rc = dalloc(c, &c->partial, RED_BLOCKS + 8)))
+      (rc = dalloc(c, &c->umax, 3 * UMAX_SLOTS + 8)) || (rc = dalloc(c, &c->partial, RED_BLOCKS + 8)))
     return bail(rc);
   if (g.wall && (rc = dalloc(c, &c->work, nspec))) return bail(rc);
   for (int i = 0; i < 3; i++) {
@@ -707,7 +726,8 @@ int dnsb_create(const dnsb_grid *gr, int device, void *stream, dnsb_ctx **out) {
       if ((rc = dalloc(c, &c->V[i], G))) return bail(rc);
     }
   }
-  if (cudaMallocHost(&c->hostred, 8 * sizeof(double)) != cudaSuccess) {
+  if (cudaMallocHost(&c->hostred, 8 * sizeof(double)) != cudaSuccess ||
+      cudaMallocHost(&c->hostumax, 3 * UMAX_SLOTS * sizeof(unsigned long long)) != cudaSuccess) {
     fail(c, DNSB_ENOMEM, "cudaMallocHost failed");
     return bail(DNSB_ENOMEM);
   }
@@ -727,6 +747,7 @@ void dnsb_destroy(dnsb_ctx *c) {
   for (auto &e : c->evpool) cudaEventDestroy(e);
   for (void *p : c->allocs) cudaFree(p);
   if (c->hostred) cudaFreeHost(c->hostred);
+  if (c->hostumax) cudaFreeHost(c->hostumax);
   delete c;
 }
 
@@ -809,11 +830,10 @@ int dnsb_imex_update(dnsb_ctx *c, double *ux, double *uy, double *uz, const doub
       g, ff(c->V[0], c->V[1], c->V[2]), cf(ux, uy, uz), cf(qx, qy, qz), p, B, adt);
   CKL(c);
   // tables for this alpha in stage slot 0
-  k_cn_tables<<<1, 32, 0, c->stream>>>(g.ny, c->ycoef, c->ytab, dt, g.visc, alpha, alpha, alpha);
+  k_cn_tables<<<1, 32, 0, c->stream>>>(g.ny, c->cn_mr, c->ycoef, c->ytab, dt, g.visc, alpha, alpha, alpha);
   CKL(c);
   const double th = alpha * dt * g.visc / 2;
-  k_cn<<<cn_grid(g), dim3(CN_LINES, CN_CHUNKS), c->smem_cn, c->stream>>>(
-      g, ff(ux, uy, uz), cf(c->V[0], c->V[1], c->V[2]), cf(ux, uy, uz), c->ycoef, c->ytab, th);
+  launch_cn(c, ff(ux, uy, uz), cf(c->V[0], c->V[1], c->V[2]), cf(ux, uy, uz), c->ytab, th);
   CKL(c);
   c->umax_for[0] = c->umax_for[1] = c->umax_for[2] = nullptr;
   return 0;
@@ -835,24 +855,33 @@ int dnsb_cfl(dnsb_ctx *c, const double *ux, const double *uy, const double *uz, 
   if (!c || !ux || !uy || !uz || !dt_out) return c ? fail(c, DNSB_EINVAL, "null argument") : DNSB_EINVAL;
   if (ensure_device(c)) return DNSB_ECUDA;
   const bool cached = use_step_max && c->umax_for[0] == ux && c->umax_for[1] == uy && c->umax_for[2] == uz;
+  unsigned long long bits[3] = {0, 0, 0};
+  unsigned long long *scratch = c->umax + 3 * UMAX_SLOTS;
   if (!cached) {
-    CK(c, cudaMemsetAsync(c->umax + 3, 0, 3 * sizeof(unsigned long long), c->stream));
-    k_maxabs3<<<RED_BLOCKS, 256, 0, c->stream>>>(c->g, cf(ux, uy, uz), c->umax + 3);
+    CK(c, cudaMemsetAsync(scratch, 0, 3 * sizeof(unsigned long long), c->stream));
+    k_maxabs3<<<RED_BLOCKS, 256, 0, c->stream>>>(c->g, cf(ux, uy, uz), scratch);
     CKL(c);
+    CK(c, cudaMemcpyAsync(c->hostred, scratch, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    memcpy(bits, c->hostred, sizeof bits);
+  } else {
+    CK(c, cudaMemcpyAsync(c->hostumax, c->umax, 3 * UMAX_SLOTS * sizeof(unsigned long long),
+                          cudaMemcpyDeviceToHost, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    for (int k = 0; k < 3; k++)
+      for (int s = 0; s < UMAX_SLOTS; s++) bits[k] = std::max(bits[k], c->hostumax[k * UMAX_SLOTS + s]);
   }
-  CK(c, cudaMemcpyAsync(c->hostred, c->umax + (cached ? 0 : 3), 3 * sizeof(unsigned long long),
-                        cudaMemcpyDeviceToHost, c->stream));
-  CK(c, cudaStreamSynchronize(c->stream));
-  return cfl_from_max(c, cfl, reinterpret_cast<const unsigned long long *>(c->hostred), dt_out);
+  return cfl_from_max(c, cfl, bits, dt_out);
 }
 
 int dnsb_maxdiv(dnsb_ctx *c, const double *ux, const double *uy, const double *uz, double *out) {
   if (!c || !ux || !uy || !uz || !out) return c ? fail(c, DNSB_EINVAL, "null argument") : DNSB_EINVAL;
   if (ensure_device(c)) return DNSB_ECUDA;
-  CK(c, cudaMemsetAsync(c->umax + 3, 0, sizeof(unsigned long long), c->stream));
-  k_maxdiv<<<RED_BLOCKS, 256, 0, c->stream>>>(c->g, cf(ux, uy, uz), c->umax + 3);
+  unsigned long long *scratch = c->umax + 3 * UMAX_SLOTS;
+  CK(c, cudaMemsetAsync(scratch, 0, sizeof(unsigned long long), c->stream));
+  k_maxdiv<<<RED_BLOCKS, 256, 0, c->stream>>>(c->g, cf(ux, uy, uz), scratch);
   CKL(c);
-  CK(c, cudaMemcpyAsync(c->hostred, c->umax + 3, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(c, cudaMemcpyAsync(c->hostred, scratch, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   CK(c, cudaStreamSynchronize(c->stream));
   *out = c->hostred[0];
   return 0;

@@ -30,7 +30,7 @@ enum ROutMode { ROUT_INTERIOR = 0, ROUT_IMAGES = 1, ROUT_REAL = 2 };
 // ghosted field in0.
 // Shared memory: 2*L*(M+1) complex (ping-pong lines) + M + (M+1) twiddles.
 template <int INMODE>
-__global__ void __launch_bounds__(SPEC_THREADS) k_rfftx(Geo g, double2 *__restrict__ S,
+__global__ void __launch_bounds__(SPEC_THREADS, 3) k_rfftx(Geo g, double2 *__restrict__ S,
                                                        const double *__restrict__ in0,
                                                        const double *__restrict__ in1,
                                                        const double *__restrict__ in2,
@@ -98,7 +98,7 @@ __global__ void __launch_bounds__(SPEC_THREADS) k_rfftx(Geo g, double2 *__restri
 // Complex FFT along z of L contiguous lines of S; INV scales by 1/nz.  The
 // first stage loads from HBM into registers, the last stores from registers.
 template <bool INV>
-__global__ void __launch_bounds__(SPEC_THREADS) k_fftz(Geo g, double2 *__restrict__ S,
+__global__ void __launch_bounds__(SPEC_THREADS, 3) k_fftz(Geo g, double2 *__restrict__ S,
                                                       FFTPlan plan, int L,
                                                       const double2 *__restrict__ twz) {
   extern __shared__ double2 smem[];
@@ -195,7 +195,7 @@ __global__ void __launch_bounds__(128) k_thomas(Geo g, double2 *__restrict__ S,
 // y, divide by lambda1+lambda2+lambda3 (0 for the mean), inverse, 1/ny.
 // SPECTRUM_ONLY leaves the forward transform in S (for energy spectra).
 template <bool SPECTRUM_ONLY>
-__global__ void __launch_bounds__(SPEC_THREADS) k_yfourier(Geo g, double2 *__restrict__ S,
+__global__ void __launch_bounds__(SPEC_THREADS, 3) k_yfourier(Geo g, double2 *__restrict__ S,
                                                           FFTPlan plan, int L,
                                                           const double2 *__restrict__ twy,
                                                           const double *__restrict__ lam1,
@@ -243,7 +243,7 @@ __global__ void __launch_bounds__(SPEC_THREADS) k_yfourier(Geo g, double2 *__res
 //   ROUT_IMAGES:   the interior plus pressure ghost images,
 //   ROUT_REAL:     the ghost-free array out.
 template <int OUTMODE>
-__global__ void __launch_bounds__(SPEC_THREADS) k_irfftx(Geo g, const double2 *__restrict__ S,
+__global__ void __launch_bounds__(SPEC_THREADS, 3) k_irfftx(Geo g, const double2 *__restrict__ S,
                                                         double *__restrict__ out, FFTPlan plan,
                                                         int L, const double2 *__restrict__ twM,
                                                         const double2 *__restrict__ twN) {
@@ -332,12 +332,13 @@ __global__ void __launch_bounds__(SPEC_THREADS) k_irfftx(Geo g, const double2 *_
 // (e = chunk end), G_k = g at the end of chunk k, H_k = h at its start.
 // tab layout per (stage, set): [ta | cp | ib | g | h](ny each), [G | H](CN_CHUNKS
 // each); ib = 1/beta; set 0 tangential, 1 normal.  coef: [at bt ct an bn cn].
+// m is the number of rows per chunk (a power of two, CN_CHUNKS * m >= ny).
 constexpr int CN_CHUNKS = 16;
 constexpr int CN_LINES = 16;
 
 __host__ __device__ constexpr long long cn_tab_stride(int ny) { return 5LL * ny + 2 * CN_CHUNKS; }
 
-__global__ void k_cn_tables(int ny, const double *__restrict__ coef, double *__restrict__ tab,
+__global__ void k_cn_tables(int ny, int m, const double *__restrict__ coef, double *__restrict__ tab,
                             double dt, double visc, double al0, double al1, double al2) {
   const int t = threadIdx.x;
   if (t >= 6) return;
@@ -361,7 +362,6 @@ __global__ void k_cn_tables(int ny, const double *__restrict__ coef, double *__r
     cp[j] = cprev;
     ib[j] = 1.0 / beta;
   }
-  const int m = (ny + CN_CHUNKS - 1) / CN_CHUNKS;
   for (int k = 0; k < CN_CHUNKS; k++) {
     const int s0 = k * m, e0 = min(ny, s0 + m) - 1;
     G[k] = 1.0;
@@ -378,112 +378,116 @@ __global__ void k_cn_tables(int ny, const double *__restrict__ coef, double *__r
 
 // imexrhs_kernel! + imexsolve_kernel! (src/ydiffusion.jl:71-109) fused.
 // A block owns CN_LINES consecutive x-lines (I) at one K for component
-// c = blockIdx.z.  The block first stages the y-columns of v and u^n of its
-// lines in shared memory (coalesced rows, many loads in flight), then splits
-// every y-line into CN_CHUNKS chunks, one thread per (line, chunk).  Each
-// thread forms rhs = v + theta Dy u^n on its rows (walls folded into the
-// rows), runs the Thomas forward sweep from a zero carry, the chunks
-// exchange their end values through shared memory and add the carried-in
-// part with the per-chunk multiplier products (g, G); the backward sweep is
-// split the same way (h, H).  Algebraically this is the reference's Thomas
-// algorithm; every element is read from and written to HBM once.  out may
-// alias u^n: all reads precede the first write.
-__global__ void __launch_bounds__(CN_LINES *CN_CHUNKS) k_cn(Geo g, Fields3 out, CFields3 V, CFields3 un,
-                                                           const double *__restrict__ coef,
-                                                           const double *__restrict__ tab,
-                                                           double theta) {
-  extern __shared__ double cs[];  // vcol[ny][CN_LINES], ucol[ny][CN_LINES], exchange
+// c = blockIdx.z and splits every y-line into CN_CHUNKS chunks of MR rows,
+// one thread per (line, chunk).  A thread loads the v and u^n values of its
+// rows straight into registers (all loads issued together), forms
+// rhs = v + theta Dy u^n (walls folded into the rows), runs the Thomas
+// forward sweep from a zero carry; the chunks exchange their end values
+// through shared memory and add the carried-in part with the per-chunk
+// multiplier products (g, G); the backward sweep is split the same way
+// (h, H).  Algebraically this is the reference's Thomas algorithm; every
+// element is read from and written to HBM once.  The line-independent
+// coefficient tables sit in shared memory.  out may alias u^n: all reads
+// precede the first write (a barrier separates them).
+template <int MR>
+__global__ void __launch_bounds__(CN_LINES *CN_CHUNKS, 2) k_cn(Geo g, Fields3 out, CFields3 V,
+                                                              CFields3 un,
+                                                              const double *__restrict__ coef,
+                                                              const double *__restrict__ tab,
+                                                              double theta) {
+  extern __shared__ double cs[];  // a b c ta cp ib gf hb (ny each), G H, exchange
   const int i = threadIdx.x, ck = threadIdx.y;
+  const int tid = i + CN_LINES * ck;
   const int I0 = blockIdx.x * CN_LINES + 1;
   const int I = I0 + i;
   const int K = blockIdx.y + 1;
   const int c = blockIdx.z;
   const int ny = g.ny;
-  double *col = cs;
-  double *ucol = cs + (long long)ny * CN_LINES;
-  double *xa = ucol + (long long)ny * CN_LINES;  // [CN_CHUNKS][CN_LINES]
-  double *xb = xa + CN_CHUNKS * CN_LINES;
   const int set = c == STAG_Y ? 1 : 0;
-  const double *a = coef + set * 3 * ny, *b = a + ny, *cc = b + ny;
-  const double *ta = tab + set * cn_tab_stride(ny), *cp = ta + ny, *ib = cp + ny, *gf = ib + ny,
-               *hb = gf + ny, *G = hb + ny, *H = G + CN_CHUNKS;
   const double *v = c == 0 ? V.x : c == 1 ? V.y : V.z;
   const double *u = c == 0 ? un.x : c == 1 ? un.y : un.z;
   double *o = c == 0 ? out.x : c == 1 ? out.y : out.z;
   const long long sy = g.NX;
-  const long long base0 = gidx(g, I0, 1, K);
-  const int nl = min(CN_LINES, g.nx - I0 + 1);
-  // 0. stage v and u^n columns (rows J = 1..ny)
-  batched_copy<4>(
-      ny * CN_LINES,
-      [&](int t) {
-        const int row = t / CN_LINES, l = t - row * CN_LINES;
-        const long long off = base0 + row * sy + l;
-        return l < nl ? make_double2(v[off], u[off]) : make_double2(0.0, 0.0);
-      },
-      [&](int t, double2 w) {
-        col[t] = w.x;
-        ucol[t] = w.y;
-      });
+  const bool active = I <= g.nx;
+  const long long base = gidx(g, active ? I : I0, 1, K);
+  const int s0 = ck * MR;
+  // 1. this thread's rows of v and u^n (u with one row either side)
+  double x[MR], uu[MR + 2];
+#pragma unroll
+  for (int r = 0; r < MR; r++) {
+    const int j = s0 + r;
+    const bool ok = active && j < ny;
+    x[r] = ok ? v[base + j * sy] : 0.0;
+    uu[r + 1] = ok ? u[base + j * sy] : 0.0;
+  }
+  uu[0] = (active && s0 > 0 && s0 - 1 < ny) ? u[base + (s0 - 1) * sy] : 0.0;
+  uu[MR + 1] = (active && s0 + MR < ny) ? u[base + (s0 + MR) * sy] : 0.0;
+  // 2. stage the tables (line-independent) while the loads are in flight
+  double *ta_ = cs, *ib_ = cs + ny, *cp_ = cs + 2 * ny, *gf_ = cs + 3 * ny, *hb_ = cs + 4 * ny;
+  double *a_ = cs + 5 * ny, *b_ = cs + 6 * ny, *c_ = cs + 7 * ny;
+  double *G_ = cs + 8 * ny, *H_ = G_ + CN_CHUNKS;
+  double *xa = H_ + CN_CHUNKS, *xb = xa + CN_CHUNKS * CN_LINES;
+  {
+    const double *ts = tab + set * cn_tab_stride(ny);  // [ta cp ib gf hb] G H
+    const double *cf3 = coef + set * 3 * ny;           // [a b c]
+    for (int t = tid; t < ny; t += CN_LINES * CN_CHUNKS) {
+      ta_[t] = ts[t];
+      cp_[t] = ts[ny + t];
+      ib_[t] = ts[2 * ny + t];
+      gf_[t] = ts[3 * ny + t];
+      hb_[t] = ts[4 * ny + t];
+      a_[t] = cf3[t];
+      b_[t] = cf3[ny + t];
+      c_[t] = cf3[2 * ny + t];
+    }
+    if (tid < 2 * CN_CHUNKS) G_[tid] = ts[5 * ny + tid];  // G then H are contiguous
+  }
   __syncthreads();
-  // 1. rhs = v + theta Dy u^n for every staged element (independent)
-  batched_copy<4>(
-      ny * CN_LINES,
-      [&](int t) {
-        const int j = t / CN_LINES;
-        const double u0 = ucol[t];
-        const double um = j > 0 ? ucol[t - CN_LINES] : 0.0;
-        const double up = j + 1 < ny ? ucol[t + CN_LINES] : 0.0;
-        double sum;
-        if (j == 0) sum = __ldg(b) * u0 + (ny > 1 ? __ldg(cc) * up : 0.0);
-        else if (j == ny - 1) sum = __ldg(a + j) * um + __ldg(b + j) * u0;
-        else sum = (__ldg(a + j) * um + __ldg(b + j) * u0) + __ldg(cc + j) * up;
-        return col[t] + theta * sum;
-      },
-      [&](int t, double r) { col[t] = r; });
-  __syncthreads();
-  const bool active = i < nl;
-  const int m = (ny + CN_CHUNKS - 1) / CN_CHUNKS;
-  const int s0 = ck * m, e0 = min(ny, s0 + m) - 1;
-  // 2. local forward sweep (zero carry)
+  // 3. rhs and local forward sweep (zero carry)
   double z = 0.0;
-  if (active && s0 <= e0) {
-    z = col[s0 * CN_LINES + i] * __ldg(ib + s0);
-    col[s0 * CN_LINES + i] = z;
-#pragma unroll 4
-    for (int j = s0 + 1; j <= e0; j++) {
-      z = fma(__ldg(ta + j), z, col[j * CN_LINES + i]) * __ldg(ib + j);
-      col[j * CN_LINES + i] = z;
+#pragma unroll
+  for (int r = 0; r < MR; r++) {
+    const int j = s0 + r;
+    if (j < ny) {
+      double sum;
+      if (j == 0) sum = b_[0] * uu[r + 1] + (ny > 1 ? c_[0] * uu[r + 2] : 0.0);
+      else if (j == ny - 1) sum = a_[j] * uu[r] + b_[j] * uu[r + 1];
+      else sum = (a_[j] * uu[r] + b_[j] * uu[r + 1]) + c_[j] * uu[r + 2];
+      const double rhs = x[r] + theta * sum;
+      z = r == 0 ? rhs * ib_[j] : fma(ta_[j], z, rhs) * ib_[j];
+      x[r] = z;
     }
   }
   xa[ck * CN_LINES + i] = z;
   __syncthreads();
-  // 2. carry into this chunk: x'_{s-1} from the earlier chunks
+  // 4. carry into this chunk from the earlier chunks, then backward sweep
   double cin = 0.0;
-  for (int k = 0; k < ck; k++) cin = xa[k * CN_LINES + i] + G[k] * cin;
-  // 3. forward values and local backward sweep (zero carry)
+  for (int k = 0; k < ck; k++) cin = xa[k * CN_LINES + i] + G_[k] * cin;
   double bnext = 0.0;
-  if (active && s0 <= e0) {
-#pragma unroll 4
-    for (int j = e0; j >= s0; j--) {
-      const double xp = fma(__ldg(gf + j), cin, col[j * CN_LINES + i]);
-      bnext = fma(-__ldg(cp + j), bnext, xp);
-      col[j * CN_LINES + i] = bnext;
+#pragma unroll
+  for (int r = MR - 1; r >= 0; r--) {
+    const int j = s0 + r;
+    if (j < ny) {
+      const double xp = fma(gf_[j], cin, x[r]);
+      bnext = fma(-cp_[j], bnext, xp);
+      x[r] = bnext;
     }
   }
-  xb[ck * CN_LINES + i] = bnext;  // first row of the chunk (b_s)
+  xb[ck * CN_LINES + i] = s0 < ny ? bnext : 0.0;
   __syncthreads();
-  // 4. carry from the later chunks: x_{e+1}
+  // 5. carry from the later chunks, final values with ghost images
   double cout = 0.0;
-  for (int k = CN_CHUNKS - 1; k > ck; k--) cout = xb[k * CN_LINES + i] + H[k] * cout;
-  // 5. final values with ghost images
-  if (active && s0 <= e0) {
+  for (int k = CN_CHUNKS - 1; k > ck; k--) cout = xb[k * CN_LINES + i] + H_[k] * cout;
+  if (active) {
     const bool normal_wall = g.wall && c == STAG_Y;
-#pragma unroll 4
-    for (int j = s0; j <= e0; j++) {
-      const double x = fma(__ldg(hb + j), cout, col[j * CN_LINES + i]);
-      if (normal_wall && j == ny - 1) o[base0 + i + j * sy] = x;
-      else store_img(o, g, I, j + 1, K, x, c);
+#pragma unroll
+    for (int r = 0; r < MR; r++) {
+      const int j = s0 + r;
+      if (j < ny) {
+        const double xv = fma(hb_[j], cout, x[r]);
+        if (normal_wall && j == ny - 1) o[base + j * sy] = xv;
+        else store_img(o, g, I, j + 1, K, xv, c);
+      }
     }
   }
 }

@@ -127,6 +127,7 @@ __global__ void __launch_bounds__(256, 4) k_momentum(Geo g, Fields3 q, CFields3 
 }
 
 enum GradMode { GRAD_EXPLICIT = 0, GRAD_IMPLICIT = 1 };
+constexpr int UMAX_SLOTS = 128;
 
 __device__ __forceinline__ unsigned long long dbits(double v) {
   return (unsigned long long)__double_as_longlong(v);
@@ -167,15 +168,23 @@ __global__ void __launch_bounds__(256) k_grad(Geo g, Fields3 u, CFields3 W,
     m2 = fabs(vz);
   }
   if (umax) {
+    // block maximum, then one atomic per block into one of UMAX_SLOTS slots
+    // per component (spreads the contention; the host reduces the slots)
+    __shared__ double red[3][8];
     for (int o = 16; o > 0; o >>= 1) {
       m0 = fmax(m0, __shfl_xor_sync(0xffffffffu, m0, o));
       m1 = fmax(m1, __shfl_xor_sync(0xffffffffu, m1, o));
       m2 = fmax(m2, __shfl_xor_sync(0xffffffffu, m2, o));
     }
-    if ((threadIdx.x & 31) == 0) {
-      atomicMax(umax + 0, dbits(m0));
-      atomicMax(umax + 1, dbits(m1));
-      atomicMax(umax + 2, dbits(m2));
+    const int tid = threadIdx.x + blockDim.x * threadIdx.y;
+    const int w = tid >> 5, nw = (blockDim.x * blockDim.y + 31) >> 5;
+    if ((tid & 31) == 0) { red[0][w] = m0; red[1][w] = m1; red[2][w] = m2; }
+    __syncthreads();
+    if (tid < 3) {
+      double m = 0.0;
+      for (int k = 0; k < nw; k++) m = fmax(m, red[tid][k]);
+      const unsigned slot = (blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)) % UMAX_SLOTS;
+      atomicMax(umax + tid * UMAX_SLOTS + slot, dbits(m));
     }
   }
 }
