@@ -93,6 +93,13 @@ __device__ __forceinline__ void store_img(double *__restrict__ f, const Geo &g, 
   }
 }
 
+// Out-of-line variant for callers that write the interior value themselves
+// and only need the ghost images of edge cells (keeps unrolled loops small).
+__device__ __noinline__ void store_images_of(double *__restrict__ f, const Geo &g, int I, int J,
+                                             int K, double v, int stag) {
+  store_img(f, g, I, J, K, v, stag);
+}
+
 // Cooperative copy loop with B loads in flight per thread: element t of
 // [0, total) is read with ld(t) and written with st(t, value).  All B loads
 // of a batch are issued before the first store, so a thread keeps B

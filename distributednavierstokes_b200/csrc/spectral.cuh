@@ -480,13 +480,17 @@ __global__ void __launch_bounds__(CN_LINES *CN_CHUNKS, 2) k_cn(Geo g, Fields3 ou
   for (int k = CN_CHUNKS - 1; k > ck; k--) cout = xb[k * CN_LINES + i] + H_[k] * cout;
   if (active) {
     const bool normal_wall = g.wall && c == STAG_Y;
+    const bool line_edge = (I == 1) | (I == g.nx) | (K == 1) | (K == g.nz);
 #pragma unroll
     for (int r = 0; r < MR; r++) {
       const int j = s0 + r;
       if (j < ny) {
         const double xv = fma(hb_[j], cout, x[r]);
-        if (normal_wall && j == ny - 1) o[base + j * sy] = xv;
-        else store_img(o, g, I, j + 1, K, xv, c);
+        o[base + j * sy] = xv;
+        // ghost images of edge lines and of the first/last rows (the
+        // inactive wall face of the normal component has none)
+        if ((line_edge || j == 0 || j >= ny - 2) && !(normal_wall && j == ny - 1))
+          store_images_of(o, g, I, j + 1, K, xv, c);
       }
     }
   }
