@@ -93,6 +93,10 @@ struct dnsb_ctx {
   double *V[3] = {nullptr, nullptr, nullptr};
   unsigned long long *umax = nullptr;  // [3] max |u_c| of the last step; [3] scratch
   double *partial = nullptr;           // reduction partials
+  int *deverr = nullptr;               // device-side error word (bounded waits)
+  int use_tma = 1;                     // persistent TMA-pipelined z-FFT
+  int nsm = 148;
+  size_t smem_zt = 0;
   double *hostred = nullptr;           // pinned, 8 doubles
   unsigned long long *hostumax = nullptr;  // pinned, 3 * UMAX_SLOTS
   const double *umax_for[3] = {nullptr, nullptr, nullptr};
@@ -405,6 +409,13 @@ int launch_rfftx(dnsb_ctx *c, int mode, const double *a, const double *b, const 
 int launch_fftz(dnsb_ctx *c, bool inv) {
   const Geo &g = c->g;
   long long nlines = (long long)g.ny * g.nkx;
+  if (c->use_tma) {
+    const long long ngroups = (nlines + c->Lz - 1) / c->Lz;
+    dim3 grid((unsigned)std::min<long long>(ngroups, 2LL * c->nsm));
+    if (inv) LAUNCH(c, DNSB_KIND_IFFTZ, k_fftz_tma<true><<<grid, SPEC_THREADS, c->smem_zt, c->stream>>>(g, c->S, c->pz, c->Lz, c->twz, c->deverr));
+    else LAUNCH(c, DNSB_KIND_FFTZ, k_fftz_tma<false><<<grid, SPEC_THREADS, c->smem_zt, c->stream>>>(g, c->S, c->pz, c->Lz, c->twz, c->deverr));
+    return 0;
+  }
   dim3 grid((unsigned)((nlines + c->Lz - 1) / c->Lz));
   if (inv) LAUNCH(c, DNSB_KIND_IFFTZ, k_fftz<true><<<grid, SPEC_THREADS, c->smem_z, c->stream>>>(g, c->S, c->pz, c->Lz, c->twz));
   else LAUNCH(c, DNSB_KIND_FFTZ, k_fftz<false><<<grid, SPEC_THREADS, c->smem_z, c->stream>>>(g, c->S, c->pz, c->Lz, c->twz));
@@ -521,6 +532,18 @@ int fill3(dnsb_ctx *c, double *ux, double *uy, double *uz) {
   for (int s = 0; s < 3; s++) {
     k_fill_ghosts<<<4 * 148, 256, 0, c->stream>>>(g, f[s], s);
     CKL(c);
+  }
+  return 0;
+}
+
+// reads the device error word (set by a kernel whose bounded wait ran out);
+// the caller has synchronised the stream
+int check_deverr(dnsb_ctx *c) {
+  int e = 0;
+  CK(c, cudaMemcpy(&e, c->deverr, sizeof(int), cudaMemcpyDeviceToHost));
+  if (e != 0) {
+    cudaMemset(c->deverr, 0, sizeof(int));
+    return fail(c, DNSB_ECUDA, "a device-side wait ran out of its iteration limit (code %d)", e);
   }
   return 0;
 }
@@ -678,12 +701,12 @@ int dnsb_create(const dnsb_grid *gr, int device, void *stream, dnsb_ctx **out) {
   auto pow2floor = [](int v) { int p = 1; while (2 * p <= v) p *= 2; return p; };
   auto envint = [](const char *name, int dflt) {
     const char *e = getenv(name);
-    return (e && atoi(e) > 0) ? atoi(e) : dflt;
+    return (e && *e) ? atoi(e) : dflt;
   };
   const int budget = 100 * 1024 / (2 * (int)sizeof(double2));  // complex per buffer
-  c->Lx = pow2floor(std::max(1, std::min({envint("DNSB_LX", 8), nz, budget / (M + 2)})));
-  c->Lz = std::max(1, std::min(envint("DNSB_LZ", 4), budget / (nz + 1)));
-  c->Ly = pow2floor(std::max(1, std::min({envint("DNSB_LY", 8), nz, budget / ny})));
+  c->Lx = pow2floor(std::max(1, std::min({std::max(1, envint("DNSB_LX", 8)), nz, budget / (M + 2)})));
+  c->Lz = std::max(1, std::min(std::max(1, envint("DNSB_LZ", 4)), budget / (nz + 1)));
+  c->Ly = pow2floor(std::max(1, std::min({std::max(1, envint("DNSB_LY", 8)), nz, budget / ny})));
   {
     int bx = 64, by = 2;
     const char *e = getenv("DNSB_CELL_BLOCK");
@@ -696,6 +719,14 @@ int dnsb_create(const dnsb_grid *gr, int device, void *stream, dnsb_ctx **out) {
   c->smem_ix = sizeof(double2) * (2 * (size_t)c->Lx * (M + 2) + M + (M + 1));
   c->smem_z = sizeof(double2) * (2 * (size_t)c->Lz * (nz + 1) + nz);
   c->smem_y = sizeof(double2) * (2 * (size_t)c->Ly * ny + ny);
+  c->smem_zt = sizeof(double2) * (2 * (size_t)c->Lz * nz + 2 * (size_t)c->Lz * (nz + 1) + nz) + 16;
+  c->use_tma = envint("DNSB_TMA", 1) != 0 && c->smem_zt <= 200 * 1024;
+  {
+    int dev = 0, nsm = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && nsm > 0)
+      c->nsm = nsm;
+  }
   if ((rc = allow_smem(c, k_rfftx<RIN_DIVERGENCE>, c->smem_rx)) ||
       (rc = allow_smem(c, k_rfftx<RIN_REAL>, c->smem_rx)) ||
       (rc = allow_smem(c, k_rfftx<RIN_FIELD>, c->smem_rx)) ||
@@ -704,6 +735,8 @@ int dnsb_create(const dnsb_grid *gr, int device, void *stream, dnsb_ctx **out) {
       (rc = allow_smem(c, k_irfftx<ROUT_REAL>, c->smem_ix)) ||
       (rc = allow_smem(c, k_fftz<false>, c->smem_z)) ||
       (rc = allow_smem(c, k_fftz<true>, c->smem_z)) ||
+      (rc = allow_smem(c, k_fftz_tma<false>, c->smem_zt)) ||
+      (rc = allow_smem(c, k_fftz_tma<true>, c->smem_zt)) ||
       (rc = allow_smem(c, k_yfourier<false>, c->smem_y)) ||
       (rc = allow_smem(c, k_yfourier<true>, c->smem_y)))
     return bail(rc);
@@ -712,7 +745,8 @@ int dnsb_create(const dnsb_grid *gr, int device, void *stream, dnsb_ctx **out) {
   const size_t G = (size_t)g.NX * g.NY * g.NZ;
   const size_t nspec = (size_t)g.nkx * ny * nz;
   if ((rc = dalloc(c, &c->S, nspec)) || (rc = dalloc(c, &c->r, (size_t)nx * ny * nz)) ||
-      (rc = dalloc(c, &c->umax, 3 * UMAX_SLOTS + 8)) || (rc = dalloc(c, &c->partial, RED_BLOCKS + 8)))
+      (rc = dalloc(c, &c->umax, 3 * UMAX_SLOTS + 8)) || (rc = dalloc(c, &c->partial, RED_BLOCKS + 8)) ||
+      (rc = dalloc(c, &c->deverr, 4)))
     return bail(rc);
   if (g.wall && (rc = dalloc(c, &c->work, nspec))) return bail(rc);
   for (int i = 0; i < 3; i++) {
@@ -725,6 +759,10 @@ int dnsb_create(const dnsb_grid *gr, int device, void *stream, dnsb_ctx **out) {
     } else {
       if ((rc = dalloc(c, &c->V[i], G))) return bail(rc);
     }
+  }
+  if (cudaMemset(c->deverr, 0, 4 * sizeof(int)) != cudaSuccess) {
+    fail(c, DNSB_ECUDA, "cudaMemset failed");
+    return bail(DNSB_ECUDA);
   }
   if (cudaMallocHost(&c->hostred, 8 * sizeof(double)) != cudaSuccess ||
       cudaMallocHost(&c->hostumax, 3 * UMAX_SLOTS * sizeof(unsigned long long)) != cudaSuccess) {
@@ -761,7 +799,7 @@ int dnsb_sync(dnsb_ctx *c) {
   if (!c) return DNSB_EINVAL;
   if (ensure_device(c)) return DNSB_ECUDA;
   CK(c, cudaStreamSynchronize(c->stream));
-  return 0;
+  return check_deverr(c);
 }
 
 int dnsb_fill_ghosts(dnsb_ctx *c, double *phi, int stag) {
@@ -871,6 +909,8 @@ int dnsb_cfl(dnsb_ctx *c, const double *ux, const double *uy, const double *uz, 
     for (int k = 0; k < 3; k++)
       for (int s = 0; s < UMAX_SLOTS; s++) bits[k] = std::max(bits[k], c->hostumax[k * UMAX_SLOTS + s]);
   }
+  int rc = check_deverr(c);
+  if (rc) return rc;
   return cfl_from_max(c, cfl, bits, dt_out);
 }
 
@@ -998,6 +1038,7 @@ int dnsb_solve(dnsb_ctx *c, double *ux, double *uy, double *uz, double *p, doubl
     n++;
   }
   CK(c, cudaStreamSynchronize(c->stream));
+  if ((rc = check_deverr(c))) return rc;
   if (t_out) *t_out = t;
   if (n_out) *n_out = n;
   return 0;

@@ -13,6 +13,7 @@
 #pragma once
 #include "common.cuh"
 #include "fft.cuh"
+#include "tma.cuh"
 
 namespace dnsb {
 
@@ -120,6 +121,69 @@ __global__ void __launch_bounds__(SPEC_THREADS, 3) k_fftz(Geo g, double2 *__rest
         if (l < Lv) src[l * n + e] = INV ? cscale(v, sc) : v;
       },
       buf, buf2, plan, L, 1, ls, true, tw, true, true);
+}
+
+// Persistent z-FFT: each CTA walks tiles of L contiguous z-lines; the next
+// tile is fetched with one bulk asynchronous copy (TMA engine) into the other
+// half of a double-buffered staging area while the current tile is
+// transformed.  The first radix stage reads the staging buffer, the middle
+// stages ping-pong in shared memory, the last stage writes HBM directly.
+// On a (bounded) wait timeout the kernel records err and stops after its
+// in-flight copy has landed.
+template <bool INV>
+__global__ void __launch_bounds__(SPEC_THREADS, 2) k_fftz_tma(Geo g, double2 *__restrict__ S,
+                                                             FFTPlan plan, int L,
+                                                             const double2 *__restrict__ twz,
+                                                             int *err) {
+  extern __shared__ __align__(128) double2 smem[];
+  const int n = g.nz;
+  const int ls = n + 1;
+  double2 *stage0 = smem;
+  double2 *stage1 = smem + L * n;
+  double2 *A = stage1 + L * n;
+  double2 *B = A + L * ls;
+  double2 *tw = B + L * ls;
+  uint64_t *bar = reinterpret_cast<uint64_t *>(tw + n);
+  const long long nlines = (long long)g.ny * g.nkx;
+  const long long ngroups = (nlines + L - 1) / L;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    fence_mbar_init();
+  }
+  for (int t = threadIdx.x; t < n; t += blockDim.x) tw[t] = twz[t];
+  __syncthreads();
+  auto issue = [&](long long grp, int b) {
+    const long long l0 = grp * L;
+    const uint32_t bytes = (uint32_t)(min((long long)L, nlines - l0) * n * sizeof(double2));
+    mbar_expect_tx(&bar[b], bytes);
+    bulk_g2s(b ? stage1 : stage0, S + l0 * n, bytes, &bar[b]);
+  };
+  long long grp = blockIdx.x;
+  if (grp < ngroups && threadIdx.x == 0) issue(grp, 0);
+  const double sc = 1.0 / n;
+  for (int it = 0; grp < ngroups; grp += gridDim.x, it++) {
+    const int cur = it & 1;
+    const long long nxt = grp + gridDim.x;
+    if (nxt < ngroups && threadIdx.x == 0) {
+      fence_proxy_async_smem();  // the previous readers of this buffer are past a barrier
+      issue(nxt, cur ^ 1);
+    }
+    if (!mbar_wait(&bar[cur], (it >> 1) & 1, err)) {
+      if (nxt < ngroups) mbar_wait(&bar[cur ^ 1], ((it + 1) >> 1) & 1, nullptr);
+      return;
+    }
+    const double2 *st = cur ? stage1 : stage0;
+    const long long l0 = grp * L;
+    const int Lv = (int)min((long long)L, nlines - l0);
+    double2 *dst = S + l0 * n;
+    fft_lines_io<INV>(
+        [&](int l, int e) { return l < Lv ? st[l * n + e] : make_double2(0.0, 0.0); },
+        [&](int l, int e, double2 v) {
+          if (l < Lv) dst[l * n + e] = INV ? cscale(v, sc) : v;
+        },
+        A, B, plan, L, 1, ls, true, tw, true, true);
+  }
 }
 
 // thomas_kernel! (src/poisson.jl:14-41): one thread per (kx, kz) line, in
