@@ -61,6 +61,7 @@ SIGNATURES = {
     "dnsb_profile_read": (c_int, [P, c_int, ctypes.POINTER(c_double), ctypes.POINTER(c_long)]),
     "dnsb_launch_count": (c_long, [P]),
     "dnsb_kind_name": (ctypes.c_char_p, [c_int]),
+    "dnsb_poisson_noalloc": (c_int, [ctypes.POINTER(dnsb_grid), P, P, P]),
 }
 
 KINDS = ["momentum", "cn_solve", "div_rfft_x", "fft_z", "y_solve", "ifft_z", "irfft_x",

@@ -1079,3 +1079,180 @@ int dnsb_solve_host(dnsb_ctx *c, double *ux, double *uy, double *uz, double *p, 
 }
 
 }  // extern "C"
+
+// ====================================================== allocation-free ==
+//
+// dnsb_poisson_noalloc: the Poisson solve of dnsb_poisson for callers that
+// cannot allocate device memory.  Typical such callers hand all device
+// memory to a pooling allocator with a hard cap (CUDA.jl's memory pool, a
+// framework caching allocator), so a foreign cudaMalloc can fail or force a
+// pool flush, or run timed loops in which the implicit device-wide
+// synchronisation of cudaMalloc/cudaFree is not acceptable.  They cannot
+// create a dnsb_ctx either (dnsb_create allocates), so this entry point
+// needs none: the spectrum, the y-solve work array and every coefficient
+// and twiddle table live in one file-scope device array of fixed size
+// (kNoAllocBytes, held by every GPU that loads the library until exit).
+// Inputs and outputs are still the caller's device arrays.
+namespace {
+
+constexpr long long kNoAllocMaxSpec = 1LL << 20;  // (nx/2+1)*ny*nz complex values
+constexpr int kNoAllocMaxN = 4096;                // nx, ny, nz
+// layout in doubles: S (2*spec) | work (spec) | dy dyu rdy rdyu (4*(N+2)) |
+// lam1 lam2 lam3 ay by cy (6*N) | twM twN twz twy (2*(N/2 + N/2+1 + N + N))
+constexpr long long kNoAllocDoubles = 3 * kNoAllocMaxSpec + 4LL * (kNoAllocMaxN + 2) +
+                                      6LL * kNoAllocMaxN + 2LL * (3 * kNoAllocMaxN + 1);
+constexpr long long kNoAllocBytes = kNoAllocDoubles * (long long)sizeof(double);
+static_assert(kNoAllocBytes < (28LL << 20), "the fixed scratch stays modest (about 26 MB)");
+
+__device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
+
+// host staging for the per-call tables (static: the entry point allocates
+// nothing, host or device; overlapping calls race anyway)
+double h_tab[4 * (kNoAllocMaxN + 2) + 6 * kNoAllocMaxN];
+double2 h_tw[3 * kNoAllocMaxN + 1];
+
+constexpr int kMaxDevices = 64;
+double *g_noalloc_ptr[kMaxDevices] = {};
+
+// once per device, with that device current: the device address of the
+// scratch array (in host code the symbol is only a stand-in) and the
+// shared-memory limits of the kernels used
+int noalloc_setup(int dev, double **out) {
+  if (dev < 0 || dev >= kMaxDevices) return fail(nullptr, DNSB_EUNSUP, "device index %d out of range", dev);
+  if (!g_noalloc_ptr[dev]) {
+    void *ptr = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+    if (e != cudaSuccess || !ptr)
+      return fail(nullptr, DNSB_ECUDA, "cudaGetSymbolAddress(scratch): %s", cudaGetErrorString(e));
+    const int big = 200 * 1024;
+    cudaError_t a = cudaSuccess;
+    a = a != cudaSuccess ? a : cudaFuncSetAttribute(k_rfftx<RIN_REAL>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+    a = a != cudaSuccess ? a : cudaFuncSetAttribute(k_fftz<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+    a = a != cudaSuccess ? a : cudaFuncSetAttribute(k_fftz<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+    a = a != cudaSuccess ? a : cudaFuncSetAttribute(k_yfourier<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+    a = a != cudaSuccess ? a : cudaFuncSetAttribute(k_irfftx<ROUT_INTERIOR>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+    if (a != cudaSuccess)
+      return fail(nullptr, DNSB_ECUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(a));
+    g_noalloc_ptr[dev] = (double *)ptr;
+  }
+  *out = g_noalloc_ptr[dev];
+  return 0;
+}
+
+}  // namespace
+
+extern "C" int dnsb_poisson_noalloc(const dnsb_grid *gr, const double *r, double *p, void *stream) {
+  if (!gr || !r || !p) return fail(nullptr, DNSB_EINVAL, "null argument");
+  const int nx = gr->nx, ny = gr->ny, nz = gr->nz;
+  if (nx < 2 || ny < 2 || nz < 1 || nx % 2)
+    return fail(nullptr, DNSB_EINVAL, "need nx >= 2 even, ny >= 2, nz >= 1 (got %d %d %d)", nx, ny, nz);
+  if (gr->bc_y != DNSB_BC_PERIODIC && gr->bc_y != DNSB_BC_WALL)
+    return fail(nullptr, DNSB_EINVAL, "bc[2] must be :periodic or :wall");
+  if (!gr->dy || !gr->dyu) return fail(nullptr, DNSB_EINVAL, "dy/dyu missing");
+  const int M = nx / 2;
+  const long long spec = (long long)(M + 1) * ny * nz;
+  if (nx > kNoAllocMaxN || ny > kNoAllocMaxN || nz > kNoAllocMaxN || spec > kNoAllocMaxSpec)
+    return fail(nullptr, DNSB_EUNSUP,
+                "dnsb_poisson_noalloc: grid %dx%dx%d exceeds its fixed scratch "
+                "((nx/2+1)*ny*nz <= %lld, nx, ny, nz <= %d)", nx, ny, nz, kNoAllocMaxSpec, kNoAllocMaxN);
+  FFTPlan pM{}, pz{}, py{};
+  const bool wall = gr->bc_y == DNSB_BC_WALL;
+  if (!make_fft_plan(M, pM) || !make_fft_plan(nz, pz) || (!wall && !make_fft_plan(ny, py)))
+    return fail(nullptr, DNSB_EUNSUP, "FFT lengths nx/2=%d, nz=%d%s must factor into 2, 3, 5", M, nz,
+                wall ? "" : ", ny");
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return fail(nullptr, DNSB_ECUDA, "cudaGetDevice failed");
+  double *base = nullptr;
+  int rc = noalloc_setup(dev, &base);
+  if (rc) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+
+  // carve the scratch array
+  double2 *S = reinterpret_cast<double2 *>(base);
+  double *work = base + 2 * kNoAllocMaxSpec;
+  double *tabs = work + kNoAllocMaxSpec;  // 4*(N+2) + 6*N doubles, then twiddles
+  double2 *tws = reinterpret_cast<double2 *>(tabs + 4 * (kNoAllocMaxN + 2) + 6 * kNoAllocMaxN);
+
+  // tables, computed exactly as in dnsb_create (plan_poisson, griddata)
+  double *dy = h_tab, *dyu = dy + (ny + 2), *rdy = dyu + (ny + 2), *rdyu = rdy + (ny + 2);
+  double *lam1 = rdyu + (ny + 2), *lam2 = lam1 + (M + 1), *lam3 = lam2 + ny;
+  double *ay = lam3 + nz, *by = ay + ny, *cy = by + ny;
+  const long long ntab = (cy + ny) - h_tab;
+  for (int J = 0; J < ny + 2; J++) {
+    dy[J] = gr->dy[J];
+    dyu[J] = gr->dyu[J];
+    rdy[J] = 1.0 / dy[J];
+    rdyu[J] = 1.0 / dyu[J];
+  }
+  for (int k = 1; k <= M + 1; k++) lam1[k - 1] = modlam(k, nx, gr->dx);
+  for (int k = 1; k <= nz; k++) lam3[k - 1] = modlam(k, nz, gr->dz);
+  for (int k = 1; k <= ny; k++) lam2[k - 1] = modlam(k, ny, dy[1]);
+  for (int j = 1; j <= ny; j++) {
+    double a = 0.0, cc = 0.0;
+    if (wall) {
+      a = j == 1 ? 0.0 : 1 / (dy[j] * dyu[j - 1]);
+      cc = j == ny ? 0.0 : 1 / (dy[j] * dyu[j]);
+    }
+    ay[j - 1] = a;
+    cy[j - 1] = cc;
+    by[j - 1] = -(a + cc);
+  }
+  double2 *twM = h_tw, *twN = twM + M, *twz = twN + (M + 1), *twy = twz + nz;
+  const long long ntw = (twy + ny) - h_tw;
+  for (int t = 0; t < M; t++) twM[t] = unit_root(t, M);
+  for (int t = 0; t <= M; t++) twN[t] = unit_root(t, nx);
+  for (int t = 0; t < nz; t++) twz[t] = unit_root(t, nz);
+  for (int t = 0; t < ny; t++) twy[t] = unit_root(t, ny);
+  cudaError_t e = cudaMemcpyAsync(tabs, h_tab, ntab * sizeof(double), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(tws, h_tw, ntw * sizeof(double2), cudaMemcpyHostToDevice, st);
+  if (e != cudaSuccess) return fail(nullptr, DNSB_ECUDA, "table upload: %s", cudaGetErrorString(e));
+  // the static host staging is reused by the next call: wait for the copies
+  if ((e = cudaStreamSynchronize(st)) != cudaSuccess)
+    return fail(nullptr, DNSB_ECUDA, "%s", cudaGetErrorString(e));
+
+  Geo g{};
+  g.nx = nx; g.ny = ny; g.nz = nz;
+  g.NX = nx + 2; g.NY = ny + 2; g.NZ = nz + 2;
+  g.wall = wall;
+  g.jymax = wall ? ny - 1 : ny;
+  g.nkx = M + 1;
+  g.dx = gr->dx; g.dz = gr->dz;
+  g.rdx = 1.0 / g.dx; g.rdz = 1.0 / g.dz;
+  g.rdx2 = 1.0 / (g.dx * g.dx); g.rdz2 = 1.0 / (g.dz * g.dz);
+  g.visc = gr->visc;
+  g.dy = tabs;
+  g.dyu = tabs + (ny + 2);
+  g.rdy = tabs + 2 * (ny + 2);
+  g.rdyu = tabs + 3 * (ny + 2);
+  const double *d_lam1 = tabs + 4 * (ny + 2), *d_lam2 = d_lam1 + (M + 1), *d_lam3 = d_lam2 + ny;
+  const double *d_ay = d_lam3 + nz, *d_by = d_ay + ny, *d_cy = d_by + ny;
+  const double2 *d_twM = tws, *d_twN = d_twM + M, *d_twz = d_twN + (M + 1), *d_twy = d_twz + nz;
+
+  // launch shapes as chosen by dnsb_create
+  auto pow2floor = [](int v) { int q = 1; while (2 * q <= v) q *= 2; return q; };
+  const int budget = 100 * 1024 / (2 * (int)sizeof(double2));
+  const int Lx = pow2floor(std::max(1, std::min({8, nz, budget / (M + 2)})));
+  const int Lz = std::max(1, std::min(4, budget / (nz + 1)));
+  const int Ly = pow2floor(std::max(1, std::min({8, nz, budget / ny})));
+  const size_t smem_rx = sizeof(double2) * (2 * (size_t)Lx * (M + 1) + M + (M + 1));
+  const size_t smem_ix = sizeof(double2) * (2 * (size_t)Lx * (M + 2) + M + (M + 1));
+  const size_t smem_z = sizeof(double2) * (2 * (size_t)Lz * (nz + 1) + nz);
+  const size_t smem_y = sizeof(double2) * (2 * (size_t)Ly * ny + ny);
+  const long long nlines = (long long)ny * g.nkx;
+  const dim3 gx(ny * ((nz + Lx - 1) / Lx)), gz((unsigned)((nlines + Lz - 1) / Lz));
+  k_rfftx<RIN_REAL><<<gx, SPEC_THREADS, smem_rx, st>>>(g, S, r, nullptr, nullptr, pM, Lx, d_twM, d_twN);
+  k_fftz<false><<<gz, SPEC_THREADS, smem_z, st>>>(g, S, pz, Lz, d_twz);
+  if (wall) {
+    const long long nl = (long long)g.nkx * nz;
+    k_thomas<<<(unsigned)((nl + 127) / 128), 128, 0, st>>>(g, S, work, d_ay, d_by, d_cy, d_lam1, d_lam3);
+  } else {
+    k_yfourier<false><<<dim3(g.nkx * ((nz + Ly - 1) / Ly)), SPEC_THREADS, smem_y, st>>>(
+        g, S, py, Ly, d_twy, d_lam1, d_lam2, d_lam3);
+  }
+  k_fftz<true><<<gz, SPEC_THREADS, smem_z, st>>>(g, S, pz, Lz, d_twz);
+  k_irfftx<ROUT_INTERIOR><<<gx, SPEC_THREADS, smem_ix, st>>>(g, S, p, pM, Lx, d_twM, d_twN);
+  if ((e = cudaGetLastError()) != cudaSuccess)
+    return fail(nullptr, DNSB_ECUDA, "launch: %s", cudaGetErrorString(e));
+  return 0;
+}

@@ -152,6 +152,27 @@ int dnsb_spectrum_sample(dnsb_ctx *ctx, const double *ux, const double *uy, cons
  * key = ((c*nz + K-1)*ny + J-1)*nx + I-1. */
 int dnsb_noise(dnsb_ctx *ctx, double *phi, int c, unsigned long long seed, double amp);
 
+/* Allocation-free Poisson solve (no counterpart in the reference): the same
+ * computation as dnsb_poisson(ctx, r, p) for callers that cannot allocate
+ * device memory -- e.g. callers whose device memory is held by a pooling
+ * allocator with a hard cap (a foreign cudaMalloc may fail or force a pool
+ * flush), or timed loops that cannot afford the implicit synchronisation of
+ * cudaMalloc/cudaFree -- and that therefore cannot create a context.  It
+ * needs no dnsb_ctx: the spectrum, the y-solve work array and all tables
+ * live in one fixed file-scope device array (about 26 MB, held by every GPU
+ * that loads the library until the process exits).  Limits: nx, ny, nz <=
+ * 4096 and (nx/2+1)*ny*nz <= 1048576 (e.g. 96^3 or 128x128x64); larger
+ * grids are rejected with DNSB_EUNSUP.  r (ghost-free nx*ny*nz) and p
+ * (ghosted; its interior is written, no halos) are the caller's device
+ * arrays on the current device; work is enqueued on `stream`.  The first
+ * call on a device resolves the scratch array's device address
+ * (cudaGetSymbolAddress) and sets kernel attributes, so make that first call
+ * before any stream capture.  Every call reuses the same scratch (nothing in
+ * it needs to start at zero; each call rewrites what it reads): calls that
+ * overlap on the GPU (other streams, other host threads) race.  Errors are
+ * reported by dnsb_last_error(NULL). */
+int dnsb_poisson_noalloc(const dnsb_grid *grid, const double *r, double *p, void *stream);
+
 /* Instrumentation (no counterpart in the reference, which has no profiling
  * for the FV path): launches are counted always; with dnsb_profile(ctx, 1)
  * every launch of the step path is bracketed by CUDA events on the context's
