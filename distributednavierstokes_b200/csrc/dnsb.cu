@@ -84,6 +84,7 @@ struct dnsb_ctx {
   int Lx = 1, Lz = 1, Ly = 1;
   size_t smem_rx = 0, smem_ix = 0, smem_z = 0, smem_y = 0, smem_cn = 0;
   int cn_mr = 1;      // rows per chunk of the CN solve
+
   dim3 cgrid, cblock;  // launch shape of the per-cell step kernels
   // scratch
   double2 *S = nullptr;
@@ -115,6 +116,12 @@ struct dnsb_ctx {
 namespace {
 
 constexpr int RED_BLOCKS = 1184;
+
+// integer knob from the environment (launch-shape tuning), default if unset
+int envint(const char *name, int dflt) {
+  const char *e = getenv(name);
+  return (e && *e) ? atoi(e) : dflt;
+}
 
 int fail(dnsb_ctx *c, int code, const char *fmt, ...) {
   char buf[512];
@@ -211,10 +218,11 @@ const dim3 cell_block(32, 8, 1);
 CFields3 cf(const double *x, const double *y, const double *z) { return CFields3{x, y, z}; }
 Fields3 ff(double *x, double *y, double *z) { return Fields3{x, y, z}; }
 
+// opt in to the dynamic shared memory a kernel launches with (needed whenever
+// static + dynamic shared memory exceeds 48 KB; set unconditionally)
 template <class K>
 int allow_smem(dnsb_ctx *c, K kernel, size_t bytes) {
-  if (bytes > 48 * 1024)
-    CK(c, cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  CK(c, cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
   return 0;
 }
 
@@ -475,8 +483,8 @@ int do_step(dnsb_ctx *c, double *ux, double *uy, double *uz, double *p, double *
   CK(c, cudaMemsetAsync(c->umax, 0, 3 * UMAX_SLOTS * sizeof(unsigned long long), c->stream));
   if (c->implicit)
     LAUNCH(c, DNSB_KIND_OTHER,
-           k_cn_tables<<<1, 32, 0, c->stream>>>(g.ny, c->cn_mr, c->ycoef, c->ytab, dt, g.visc,
-                                                RK_AL[0], RK_AL[1], RK_AL[2]));
+           k_cn_tables<<<1, 32, 0, c->stream>>>(g.ny, c->cn_mr, CN_CHUNKS, c->ycoef, c->ytab, dt,
+                                                g.visc, RK_AL[0], RK_AL[1], RK_AL[2]));
   for (int s = 0; s < 3; s++) {
     const double A = RK_A[s], B = RK_B[s], al = RK_AL[s];
     const int readq = A != 0.0;
@@ -493,11 +501,11 @@ int do_step(dnsb_ctx *c, double *ux, double *uy, double *uz, double *p, double *
                  g, ff(ux, uy, uz), cf(c->W[0], c->W[1], c->W[2]), p, nullptr, 0.0, um));
     } else {
       const double adt = al * dt;
+      const double th = al * dt * g.visc / 2;
       LAUNCH(c, DNSB_KIND_MOMENTUM,
              k_momentum<MOM_IMPLICIT><<<c->cgrid, c->cblock, 0, c->stream>>>(
                  g, ff(qx, qy, qz), cf(ux, uy, uz), ff(c->V[0], c->V[1], c->V[2]), p, A, dt, B,
                  adt, readq));
-      const double th = al * dt * g.visc / 2;
       LAUNCH(c, DNSB_KIND_CN,
              launch_cn(c, ff(ux, uy, uz), cf(c->V[0], c->V[1], c->V[2]), cf(ux, uy, uz),
                        c->ytab + (long long)s * 2 * cn_tab_stride(g.ny), th));
@@ -699,10 +707,6 @@ int dnsb_create(const dnsb_grid *gr, int device, void *stream, dnsb_ctx **out) {
   // launch shapes: L lines per CTA, two line buffers each within ~100 KB;
   // DNSB_LX / DNSB_LZ / DNSB_LY / DNSB_CELL_BLOCK ("32x8") override them
   auto pow2floor = [](int v) { int p = 1; while (2 * p <= v) p *= 2; return p; };
-  auto envint = [](const char *name, int dflt) {
-    const char *e = getenv(name);
-    return (e && *e) ? atoi(e) : dflt;
-  };
   const int budget = 100 * 1024 / (2 * (int)sizeof(double2));  // complex per buffer
   c->Lx = pow2floor(std::max(1, std::min({std::max(1, envint("DNSB_LX", 8)), nz, budget / (M + 2)})));
   c->Lz = std::max(1, std::min(std::max(1, envint("DNSB_LZ", 4)), budget / (nz + 1)));
@@ -720,7 +724,10 @@ int dnsb_create(const dnsb_grid *gr, int device, void *stream, dnsb_ctx **out) {
   c->smem_z = sizeof(double2) * (2 * (size_t)c->Lz * (nz + 1) + nz);
   c->smem_y = sizeof(double2) * (2 * (size_t)c->Ly * ny + ny);
   c->smem_zt = sizeof(double2) * (2 * (size_t)c->Lz * nz + 2 * (size_t)c->Lz * (nz + 1) + nz) + 16;
-  c->use_tma = envint("DNSB_TMA", 1) != 0 && c->smem_zt <= 200 * 1024;
+  // the persistent TMA-pipelined z-FFT is opt-in: at the production size the
+  // non-persistent kernel with more CTAs per SM is faster (the transform is
+  // shared-memory bound)
+  c->use_tma = envint("DNSB_TMA", 0) != 0 && c->smem_zt <= 200 * 1024;
   {
     int dev = 0, nsm = 0;
     cudaGetDevice(&dev);
@@ -756,7 +763,8 @@ int dnsb_create(const dnsb_grid *gr, int device, void *stream, dnsb_ctx **out) {
         fail(c, DNSB_ECUDA, "cudaMemset failed");
         return bail(DNSB_ECUDA);
       }
-    } else {
+    }
+    if (c->implicit) {
       if ((rc = dalloc(c, &c->V[i], G))) return bail(rc);
     }
   }
@@ -868,7 +876,8 @@ int dnsb_imex_update(dnsb_ctx *c, double *ux, double *uy, double *uz, const doub
       g, ff(c->V[0], c->V[1], c->V[2]), cf(ux, uy, uz), cf(qx, qy, qz), p, B, adt);
   CKL(c);
   // tables for this alpha in stage slot 0
-  k_cn_tables<<<1, 32, 0, c->stream>>>(g.ny, c->cn_mr, c->ycoef, c->ytab, dt, g.visc, alpha, alpha, alpha);
+  k_cn_tables<<<1, 32, 0, c->stream>>>(g.ny, c->cn_mr, CN_CHUNKS, c->ycoef, c->ytab, dt, g.visc,
+                                       alpha, alpha, alpha);
   CKL(c);
   const double th = alpha * dt * g.visc / 2;
   launch_cn(c, ff(ux, uy, uz), cf(c->V[0], c->V[1], c->V[2]), cf(ux, uy, uz), c->ytab, th);

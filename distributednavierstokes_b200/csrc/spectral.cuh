@@ -400,10 +400,12 @@ __global__ void __launch_bounds__(SPEC_THREADS, 3) k_irfftx(Geo g, const double2
 constexpr int CN_CHUNKS = 16;
 constexpr int CN_LINES = 16;
 
-__host__ __device__ constexpr long long cn_tab_stride(int ny) { return 5LL * ny + 2 * CN_CHUNKS; }
+constexpr int CN_MAXCHUNKS = 32;
+__host__ __device__ constexpr long long cn_tab_stride(int ny) { return 5LL * ny + 2 * CN_MAXCHUNKS; }
 
-__global__ void k_cn_tables(int ny, int m, const double *__restrict__ coef, double *__restrict__ tab,
-                            double dt, double visc, double al0, double al1, double al2) {
+__global__ void k_cn_tables(int ny, int m, int nchunks, const double *__restrict__ coef,
+                            double *__restrict__ tab, double dt, double visc, double al0,
+                            double al1, double al2) {
   const int t = threadIdx.x;
   if (t >= 6) return;
   const int st = t / 2, set = t % 2;
@@ -413,7 +415,7 @@ __global__ void k_cn_tables(int ny, int m, const double *__restrict__ coef, doub
   const double *b = a + ny, *c = b + ny;
   double *ta = tab + (long long)(st * 2 + set) * cn_tab_stride(ny);
   double *cp = ta + ny, *ib = cp + ny, *gf = ib + ny, *hb = gf + ny;
-  double *G = hb + ny, *H = G + CN_CHUNKS;
+  double *G = hb + ny, *H = G + CN_MAXCHUNKS;
   double beta = 1 - th * b[0];
   double cprev = -th * c[0] / beta;
   ta[0] = th * a[0];
@@ -426,7 +428,7 @@ __global__ void k_cn_tables(int ny, int m, const double *__restrict__ coef, doub
     cp[j] = cprev;
     ib[j] = 1.0 / beta;
   }
-  for (int k = 0; k < CN_CHUNKS; k++) {
+  for (int k = 0; k < nchunks; k++) {
     const int s0 = k * m, e0 = min(ny, s0 + m) - 1;
     G[k] = 1.0;
     H[k] = 1.0;
@@ -489,7 +491,7 @@ __global__ void __launch_bounds__(CN_LINES *CN_CHUNKS, 2) k_cn(Geo g, Fields3 ou
   // 2. stage the tables (line-independent) while the loads are in flight
   double *ta_ = cs, *ib_ = cs + ny, *cp_ = cs + 2 * ny, *gf_ = cs + 3 * ny, *hb_ = cs + 4 * ny;
   double *a_ = cs + 5 * ny, *b_ = cs + 6 * ny, *c_ = cs + 7 * ny;
-  double *G_ = cs + 8 * ny, *H_ = G_ + CN_CHUNKS;
+  double *G_ = cs + 8 * ny, *H_ = G_ + CN_CHUNKS;  // copies of G[0..CN_CHUNKS), H[...]
   double *xa = H_ + CN_CHUNKS, *xb = xa + CN_CHUNKS * CN_LINES;
   {
     const double *ts = tab + set * cn_tab_stride(ny);  // [ta cp ib gf hb] G H
@@ -504,7 +506,10 @@ __global__ void __launch_bounds__(CN_LINES *CN_CHUNKS, 2) k_cn(Geo g, Fields3 ou
       b_[t] = cf3[ny + t];
       c_[t] = cf3[2 * ny + t];
     }
-    if (tid < 2 * CN_CHUNKS) G_[tid] = ts[5 * ny + tid];  // G then H are contiguous
+    if (tid < CN_CHUNKS) {
+      G_[tid] = ts[5 * ny + tid];
+      H_[tid] = ts[5 * ny + CN_MAXCHUNKS + tid];
+    }
   }
   __syncthreads();
   // 3. rhs and local forward sweep (zero carry)

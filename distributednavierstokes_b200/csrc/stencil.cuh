@@ -18,18 +18,24 @@ enum MomMode { MOM_ONLY = 0, MOM_EXPLICIT = 1, MOM_IMPLICIT = 2 };
 
 #define LDG(p, o) __ldg((p) + (o))
 
-// momentum_kernel! (src/operators.jl:44-145), one thread per interior cell.
-// MODE_ONLY: q <- A q + dt F(u).
-// MOM_EXPLICIT: also W_c = u_c + B q_c on active DOFs, with ghost images.
-// MOM_IMPLICIT: also V_c = u_c + B q_c - adt * d_c p on active DOFs.
+// momentum_kernel! (src/operators.jl:44-145) at one interior cell: loads
+// the 3x3x3 staggered neighbourhood (27 values) plus q and p, returns the
+// new RK registers q, the stage increment v (MOM_EXPLICIT: u + B q,
+// MOM_IMPLICIT: u + B q - adt grad p on active DOFs) and the wall-normal
+// neighbours of u that the Crank-Nicolson right-hand side needs.
+struct MomCell {
+  double qx, qy, qz;     // new registers
+  double vx, vy, vz;     // stage increments
+  double uxS, ux0, uxN;  // u^n at J-1, J, J+1 (x, y, z components)
+  double uyS, uy0, uyN;
+  double uzS, uz0, uzN;
+};
+
 template <int MODE>
-__global__ void __launch_bounds__(256, 4) k_momentum(Geo g, Fields3 q, CFields3 u, Fields3 out,
-                                                  const double *__restrict__ p, double A, double dt,
-                                                  double B, double adt, int readq) {
-  const int I = blockIdx.x * blockDim.x + threadIdx.x + 1;
-  const int J = blockIdx.y * blockDim.y + threadIdx.y + 1;
-  const int K = blockIdx.z + 1;
-  if (I > g.nx || J > g.ny) return;
+__device__ __forceinline__ MomCell momentum_cell(const Geo &g, int I, int J, int K, const Fields3 &q,
+                                                 const CFields3 &u, const double *__restrict__ p,
+                                                 double A, double dt, double B, double adt,
+                                                 int readq) {
   const long long sy = g.NX, sz = (long long)g.NX * g.NY;
   const long long c0 = gidx(g, I, J, K);
   const double *ux = u.x, *uy = u.y, *uz = u.z;
@@ -61,8 +67,8 @@ __global__ void __launch_bounds__(256, 4) k_momentum(Geo g, Fields3 q, CFields3 
   const double rdyuJ = __ldg(g.rdyu + J), rdyuJm = __ldg(g.rdyu + J - 1);
   const double ey = g.epsy, nu = g.visc;
 
+  MomCell m;
   // x momentum, at the right x-face of cell (I, J, K)
-  double qxn, qyn, qzn;
   {
     const double uce = 0.5 * (ux0 + uxE), ucw = 0.5 * (uxW + ux0);
     const double vn = 0.5 * (uy0 + uyE), un = 0.5 * (ux0 + uxN);
@@ -75,7 +81,7 @@ __global__ void __launch_bounds__(256, 4) k_momentum(Geo g, Fields3 q, CFields3 
                         ey * ((uxN - ux0) * rdyuJ - (ux0 - uxS) * rdyuJm) * rdyJ +
                         (uxT - 2 * ux0 + uxB) * g.rdz2;
     const double f = dt * (-conv + nu * diff + g.fx);
-    qxn = readq ? A * qx0 + f : f;
+    m.qx = readq ? A * qx0 + f : f;
   }
   // y momentum, at the top y-face; Delta-y weighted transporters
   {
@@ -91,7 +97,7 @@ __global__ void __launch_bounds__(256, 4) k_momentum(Geo g, Fields3 q, CFields3 
                         ey * ((uyN - uy0) * rdyJ1 - (uy0 - uyS) * rdyJ) * rdyuJ +
                         (uyT - 2 * uy0 + uyB) * g.rdz2;
     const double f = dt * (-conv + nu * diff + g.fy);
-    qyn = readq ? A * qy0 + f : f;
+    m.qy = readq ? A * qy0 + f : f;
   }
   // z momentum, at the back z-face
   {
@@ -106,23 +112,53 @@ __global__ void __launch_bounds__(256, 4) k_momentum(Geo g, Fields3 q, CFields3 
                         ey * ((uzN - uz0) * rdyuJ - (uz0 - uzS) * rdyuJm) * rdyJ +
                         (uzT - 2 * uz0 + uzB) * g.rdz2;
     const double f = dt * (-conv + nu * diff + g.fz);
-    qzn = readq ? A * qz0 + f : f;
+    m.qz = readq ? A * qz0 + f : f;
   }
   const bool yact = J <= g.jymax;
-  q.x[c0] = qxn;
-  if (yact) q.y[c0] = qyn;
-  q.z[c0] = qzn;
-
   if (MODE == MOM_EXPLICIT) {
-    // u <- u + B q on ranges[c] (timestep.jl:54-58), halo via images
-    store_img(out.x, g, I, J, K, ux0 + B * qxn, STAG_X);
-    if (yact) store_img(out.y, g, I, J, K, uy0 + B * qyn, STAG_Y);
-    store_img(out.z, g, I, J, K, uz0 + B * qzn, STAG_Z);
+    // u <- u + B q on ranges[c] (timestep.jl:54-58)
+    m.vx = ux0 + B * m.qx;
+    m.vy = yact ? uy0 + B * m.qy : uy0;
+    m.vz = uz0 + B * m.qz;
+  } else {
+    // v = u + B q - alpha dt grad p (ydiffusion.jl:133-135)
+    m.vx = (ux0 + B * m.qx) - adt * (pE - p0) * g.rdx;
+    m.vy = yact ? (uy0 + B * m.qy) - adt * (pN - p0) * rdyuJ : uy0;
+    m.vz = (uz0 + B * m.qz) - adt * (pT - p0) * g.rdz;
+  }
+  m.uxS = uxS; m.ux0 = ux0; m.uxN = uxN;
+  m.uyS = uyS; m.uy0 = uy0; m.uyN = uyN;
+  m.uzS = uzS; m.uz0 = uz0; m.uzN = uzN;
+  return m;
+}
+
+// momentum_kernel! (src/operators.jl:44-145), one thread per interior cell.
+// MOM_ONLY: q <- A q + dt F(u).
+// MOM_EXPLICIT: also W_c = u_c + B q_c on active DOFs, with ghost images.
+// MOM_IMPLICIT: also V_c = u_c + B q_c - adt * d_c p on active DOFs.
+template <int MODE>
+__global__ void __launch_bounds__(256, 4) k_momentum(Geo g, Fields3 q, CFields3 u, Fields3 out,
+                                                  const double *__restrict__ p, double A, double dt,
+                                                  double B, double adt, int readq) {
+  const int I = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int J = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  const int K = blockIdx.z + 1;
+  if (I > g.nx || J > g.ny) return;
+  const long long c0 = gidx(g, I, J, K);
+  const MomCell m = momentum_cell<MODE == MOM_ONLY ? MOM_EXPLICIT : MODE>(g, I, J, K, q, u, p, A,
+                                                                          dt, B, adt, readq);
+  const bool yact = J <= g.jymax;
+  q.x[c0] = m.qx;
+  if (yact) q.y[c0] = m.qy;
+  q.z[c0] = m.qz;
+  if (MODE == MOM_EXPLICIT) {
+    store_img(out.x, g, I, J, K, m.vx, STAG_X);
+    if (yact) store_img(out.y, g, I, J, K, m.vy, STAG_Y);
+    store_img(out.z, g, I, J, K, m.vz, STAG_Z);
   } else if (MODE == MOM_IMPLICIT) {
-    // v = u + B q - alpha dt grad p (ydiffusion.jl:133-135), interior only
-    out.x[c0] = (ux0 + B * qxn) - adt * (pE - p0) * g.rdx;
-    out.y[c0] = yact ? (uy0 + B * qyn) - adt * (pN - p0) * rdyuJ : uy0;
-    out.z[c0] = (uz0 + B * qzn) - adt * (pT - p0) * g.rdz;
+    out.x[c0] = m.vx;
+    out.y[c0] = m.vy;
+    out.z[c0] = m.vz;
   }
 }
 
