@@ -14,7 +14,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libdnsb.so")
 SOURCES = ["dnsb.cu"]
-HEADERS = ["common.cuh", "fft.cuh", "spectral.cuh", "stencil.cuh"]
+HEADERS = ["common.cuh", "fft.cuh", "fft4.cuh", "spectral.cuh", "spectral4.cuh", "stencil.cuh",
+           "tma.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -27,6 +27,7 @@
 #include "common.cuh"
 #include "fft.cuh"
 #include "spectral.cuh"
+#include "spectral4.cuh"
 #include "stencil.cuh"
 
 using namespace dnsb;
@@ -96,6 +97,9 @@ struct dnsb_ctx {
   double *partial = nullptr;           // reduction partials
   int *deverr = nullptr;               // device-side error word (bounded waits)
   int use_tma = 1;                     // persistent TMA-pipelined z-FFT
+  int x1 = 0, x2 = 0, z1 = 0, z2 = 0;  // four-step splits of nx/2 and nz (0: generic kernels)
+  int L4x = 16, L4r = 8, L4z = 8;      // lines per CTA: irfft-x, rfft-x, z-FFT
+  size_t smem_rx4 = 0, smem_ix4 = 0, smem_z4 = 0;
   int nsm = 148;
   size_t smem_zt = 0;
   double *hostred = nullptr;           // pinned, 8 doubles
@@ -400,10 +404,89 @@ int ensure_device(dnsb_ctx *c) {
   return 0;
 }
 
+#define FFT4_SPLITS(X) X(16, 24) X(16, 16) X(16, 12) X(16, 8) X(8, 12) X(8, 8) X(8, 6) X(8, 4)
+
+// four-step kernel launches for the split chosen at create time
+int launch_rfftx4(dnsb_ctx *c, int mode, const double *a, const double *b, const double *cc) {
+  const Geo &g = c->g;
+  dim3 grid(g.ny * ((g.nz + c->L4r - 1) / c->L4r));
+#define RF4(A, B)                                                                                  \
+  if (c->x1 == A && c->x2 == B) {                                                                  \
+    if (mode == RIN_DIVERGENCE)                                                                    \
+      LAUNCH(c, DNSB_KIND_RFFTX, k_rfftx4<A, B, RIN_DIVERGENCE><<<grid, F4_THREADS, c->smem_rx4, c->stream>>>(g, c->S, a, b, cc, c->L4r, c->twM, c->twN)); \
+    else if (mode == RIN_REAL)                                                                     \
+      LAUNCH(c, DNSB_KIND_RFFTX, k_rfftx4<A, B, RIN_REAL><<<grid, F4_THREADS, c->smem_rx4, c->stream>>>(g, c->S, a, b, cc, c->L4r, c->twM, c->twN)); \
+    else                                                                                           \
+      LAUNCH(c, DNSB_KIND_RFFTX, k_rfftx4<A, B, RIN_FIELD><<<grid, F4_THREADS, c->smem_rx4, c->stream>>>(g, c->S, a, b, cc, c->L4r, c->twM, c->twN)); \
+    return 0;                                                                                      \
+  }
+  FFT4_SPLITS(RF4)
+#undef RF4
+  return fail(c, DNSB_EUNSUP, "no four-step x kernel for %d x %d", c->x1, c->x2);
+}
+
+int launch_irfftx4(dnsb_ctx *c, int mode, double *out) {
+  const Geo &g = c->g;
+  dim3 grid(g.ny * ((g.nz + c->L4x - 1) / c->L4x));
+#define IF4(A, B)                                                                                  \
+  if (c->x1 == A && c->x2 == B) {                                                                  \
+    if (mode == ROUT_INTERIOR)                                                                     \
+      LAUNCH(c, DNSB_KIND_IRFFTX, k_irfftx4<A, B, ROUT_INTERIOR><<<grid, F4_THREADS, c->smem_ix4, c->stream>>>(g, c->S, out, c->L4x, c->twM, c->twN)); \
+    else if (mode == ROUT_IMAGES)                                                                  \
+      LAUNCH(c, DNSB_KIND_IRFFTX, k_irfftx4<A, B, ROUT_IMAGES><<<grid, F4_THREADS, c->smem_ix4, c->stream>>>(g, c->S, out, c->L4x, c->twM, c->twN)); \
+    else                                                                                           \
+      LAUNCH(c, DNSB_KIND_IRFFTX, k_irfftx4<A, B, ROUT_REAL><<<grid, F4_THREADS, c->smem_ix4, c->stream>>>(g, c->S, out, c->L4x, c->twM, c->twN)); \
+    return 0;                                                                                      \
+  }
+  FFT4_SPLITS(IF4)
+#undef IF4
+  return fail(c, DNSB_EUNSUP, "no four-step x kernel for %d x %d", c->x1, c->x2);
+}
+
+int launch_fftz4(dnsb_ctx *c, bool inv) {
+  const Geo &g = c->g;
+  const long long nlines = (long long)g.ny * g.nkx;
+  dim3 grid((unsigned)((nlines + c->L4z - 1) / c->L4z));
+#define ZF4(A, B)                                                                                  \
+  if (c->z1 == A && c->z2 == B) {                                                                  \
+    if (inv) LAUNCH(c, DNSB_KIND_IFFTZ, k_fftz4<A, B, true><<<grid, F4_THREADS, c->smem_z4, c->stream>>>(g, c->S, c->L4z, c->twz)); \
+    else LAUNCH(c, DNSB_KIND_FFTZ, k_fftz4<A, B, false><<<grid, F4_THREADS, c->smem_z4, c->stream>>>(g, c->S, c->L4z, c->twz)); \
+    return 0;                                                                                      \
+  }
+  FFT4_SPLITS(ZF4)
+#undef ZF4
+  return fail(c, DNSB_EUNSUP, "no four-step z kernel for %d x %d", c->z1, c->z2);
+}
+
+// shared-memory opt-in of the four-step kernels of one split
+template <int A, int B>
+int allow_fft4(dnsb_ctx *c) {
+  int rc;
+  if ((rc = allow_smem(c, k_rfftx4<A, B, RIN_DIVERGENCE>, c->smem_rx4)) ||
+      (rc = allow_smem(c, k_rfftx4<A, B, RIN_REAL>, c->smem_rx4)) ||
+      (rc = allow_smem(c, k_rfftx4<A, B, RIN_FIELD>, c->smem_rx4)) ||
+      (rc = allow_smem(c, k_irfftx4<A, B, ROUT_INTERIOR>, c->smem_ix4)) ||
+      (rc = allow_smem(c, k_irfftx4<A, B, ROUT_IMAGES>, c->smem_ix4)) ||
+      (rc = allow_smem(c, k_irfftx4<A, B, ROUT_REAL>, c->smem_ix4)) ||
+      (rc = allow_smem(c, k_fftz4<A, B, false>, c->smem_z4)) ||
+      (rc = allow_smem(c, k_fftz4<A, B, true>, c->smem_z4)))
+    return rc;
+  return 0;
+}
+
+int allow_fft4_split(dnsb_ctx *c, int a, int b) {
+#define AF4(A, B) \
+  if (a == A && b == B) return allow_fft4<A, B>(c);
+  FFT4_SPLITS(AF4)
+#undef AF4
+  return 0;
+}
+
 // rfft_x of the divergence of (a, b, cc) (mode RIN_DIVERGENCE), of the
 // ghost-free real a (RIN_REAL) or of the interior of field a (RIN_FIELD)
 int launch_rfftx(dnsb_ctx *c, int mode, const double *a, const double *b, const double *cc) {
   const Geo &g = c->g;
+  if (c->x1) return launch_rfftx4(c, mode, a, b, cc);
   dim3 grid(g.ny * ((g.nz + c->Lx - 1) / c->Lx));
   if (mode == RIN_DIVERGENCE)
     LAUNCH(c, DNSB_KIND_RFFTX, k_rfftx<RIN_DIVERGENCE><<<grid, SPEC_THREADS, c->smem_rx, c->stream>>>(g, c->S, a, b, cc, c->pM, c->Lx, c->twM, c->twN));
@@ -416,6 +499,7 @@ int launch_rfftx(dnsb_ctx *c, int mode, const double *a, const double *b, const 
 
 int launch_fftz(dnsb_ctx *c, bool inv) {
   const Geo &g = c->g;
+  if (c->z1 && !c->use_tma) return launch_fftz4(c, inv);
   long long nlines = (long long)g.ny * g.nkx;
   if (c->use_tma) {
     const long long ngroups = (nlines + c->Lz - 1) / c->Lz;
@@ -444,6 +528,7 @@ int launch_ysolve(dnsb_ctx *c) {
 
 int launch_irfftx(dnsb_ctx *c, int mode, double *out) {
   const Geo &g = c->g;
+  if (c->x1) return launch_irfftx4(c, mode, out);
   dim3 grid(g.ny * ((g.nz + c->Lx - 1) / c->Lx));
   if (mode == ROUT_INTERIOR)
     LAUNCH(c, DNSB_KIND_IRFFTX, k_irfftx<ROUT_INTERIOR><<<grid, SPEC_THREADS, c->smem_ix, c->stream>>>(g, c->S, out, c->pM, c->Lx, c->twM, c->twN));
@@ -724,6 +809,25 @@ int dnsb_create(const dnsb_grid *gr, int device, void *stream, dnsb_ctx **out) {
   c->smem_z = sizeof(double2) * (2 * (size_t)c->Lz * (nz + 1) + nz);
   c->smem_y = sizeof(double2) * (2 * (size_t)c->Ly * ny + ny);
   c->smem_zt = sizeof(double2) * (2 * (size_t)c->Lz * nz + 2 * (size_t)c->Lz * (nz + 1) + nz) + 16;
+  // four-step kernels for the lengths with a register split (DNSB_FFT4=0: off)
+  if (envint("DNSB_FFT4", 1) != 0) {
+    int a = 0, b = 0;
+    c->L4x = std::max(1, std::min(envint("DNSB_L4X", 16), nz));
+    c->L4r = std::max(1, std::min(envint("DNSB_L4R", 8), nz));
+    c->L4z = std::max(1, envint("DNSB_L4Z", 8));
+    if (fft4_split(M, a, b)) {
+      c->x1 = a;
+      c->x2 = b;
+      const size_t pitch = b % 2 == 0 ? b + 1 : b;
+      c->smem_rx4 = sizeof(double2) * ((size_t)c->L4r * a * pitch + (size_t)c->L4r * (M + 1) + M + (M + 1));
+      c->smem_ix4 = sizeof(double2) * ((size_t)c->L4x * (M + 2) + (size_t)c->L4x * a * pitch + M + (M + 1));
+    }
+    if (fft4_split(nz, a, b)) {
+      c->z1 = a;
+      c->z2 = b;
+      c->smem_z4 = sizeof(double2) * ((size_t)c->L4z * a * (b % 2 == 0 ? b + 1 : b) + nz);
+    }
+  }
   // the persistent TMA-pipelined z-FFT is opt-in: at the production size the
   // non-persistent kernel with more CTAs per SM is faster (the transform is
   // shared-memory bound)
@@ -734,6 +838,9 @@ int dnsb_create(const dnsb_grid *gr, int device, void *stream, dnsb_ctx **out) {
     if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && nsm > 0)
       c->nsm = nsm;
   }
+  if ((c->x1 && (rc = allow_fft4_split(c, c->x1, c->x2))) ||
+      (c->z1 && (rc = allow_fft4_split(c, c->z1, c->z2))))
+    return bail(rc);
   if ((rc = allow_smem(c, k_rfftx<RIN_DIVERGENCE>, c->smem_rx)) ||
       (rc = allow_smem(c, k_rfftx<RIN_REAL>, c->smem_rx)) ||
       (rc = allow_smem(c, k_rfftx<RIN_FIELD>, c->smem_rx)) ||

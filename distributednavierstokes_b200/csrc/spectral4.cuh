@@ -1,0 +1,199 @@
+// spectral4.cuh -- the Poisson transform kernels on the four-step engine.
+//
+// Same contracts as k_fftz / k_rfftx / k_irfftx in spectral.cuh (which
+// remain the path for lengths without a specialised split), with the
+// transforms of fft4.cuh: every element crosses shared memory once per
+// transform, so these kernels stay bound by HBM traffic.
+#pragma once
+#include "fft4.cuh"
+#include "spectral.cuh"
+
+namespace dnsb {
+
+constexpr int F4_THREADS = 256;
+
+// Complex FFT along z of L contiguous lines of S (n = N1*N2 = nz); INV
+// scales by 1/nz.  Shared memory: transpose buffer + n twiddles.
+template <int N1, int N2, bool INV>
+__global__ void __launch_bounds__(F4_THREADS, 2) k_fftz4(Geo g, double2 *__restrict__ S, int L,
+                                                         const double2 *__restrict__ twz) {
+  constexpr int n = N1 * N2;
+  extern __shared__ double2 smem[];
+  double2 *buf = smem;
+  double2 *tw = smem + fft4_buf<N1, N2>(L);
+  const long long nlines = (long long)g.ny * g.nkx;
+  const long long l0 = (long long)blockIdx.x * L;
+  const int Lv = (int)min((long long)L, nlines - l0);
+  for (int t = threadIdx.x; t < n; t += blockDim.x) tw[t] = twz[t];
+  __syncthreads();
+  double2 *src = S + l0 * n;
+  const double sc = 1.0 / n;
+  fft4_lines<N1, N2, INV>(
+      [&](int l, int e) { return l < Lv ? src[l * n + e] : make_double2(0.0, 0.0); },
+      [&](int l, int e, double2 v) {
+        if (l < Lv) src[l * n + e] = INV ? cscale(v, sc) : v;
+      },
+      buf, L, tw);
+}
+
+// Real forward FFT along x of L lines (j fixed, kz = k0..k0+L-1) through the
+// half-length complex transform (see k_rfftx).  The packed input
+// z[m] = r[2m] + i r[2m+1] (r = divergence of in0..in2, a ghost-free real
+// array, or a field's interior) is first staged in shared memory by all
+// threads with batched loads, then transformed.  M = N1*N2 = nx/2.
+template <int N1, int N2, int INMODE>
+__global__ void __launch_bounds__(F4_THREADS, 2) k_rfftx4(Geo g, double2 *__restrict__ S,
+                                                          const double *__restrict__ in0,
+                                                          const double *__restrict__ in1,
+                                                          const double *__restrict__ in2, int L,
+                                                          const double2 *__restrict__ twM,
+                                                          const double2 *__restrict__ twN) {
+  constexpr int M = N1 * N2;
+  constexpr int ls = M + 1;
+  extern __shared__ double2 smem[];
+  double2 *buf = smem;
+  double2 *res = buf + fft4_buf<N1, N2>(L);
+  double2 *tw = res + L * ls;
+  double2 *tn = tw + M;
+  const int ngrp = (g.nz + L - 1) / L;
+  const int grp = blockIdx.x % ngrp;
+  const int j = blockIdx.x / ngrp;
+  const int k0 = grp * L;
+  for (int t = threadIdx.x; t < M; t += blockDim.x) tw[t] = twM[t];
+  for (int t = threadIdx.x; t <= M; t += blockDim.x) tn[t] = twN[t];
+  const long long sy = g.NX, sz = (long long)g.NX * g.NY;
+  const int J = j + 1;
+  const double rdyJ = __ldg(g.rdy + J);
+  batched_copy<4>(
+      L * M,
+      [&](int t) {
+        const int l = t / M, m = t - l * M;
+        const int k = k0 + l;
+        double2 z = make_double2(0.0, 0.0);
+        if (k < g.nz) {
+          if (INMODE == RIN_REAL) {
+            const double *row = in0 + (long long)g.nx * (j + (long long)g.ny * k);
+            z = __ldg(reinterpret_cast<const double2 *>(row + 2 * m));
+          } else {
+            const long long c0 = gidx(g, 2 * m + 1, J, k + 1);
+            if (INMODE == RIN_FIELD) {
+              z = make_double2(__ldg(in0 + c0), __ldg(in0 + c0 + 1));
+            } else {
+              const double a0 = __ldg(in0 + c0 - 1), a1 = __ldg(in0 + c0), a2 = __ldg(in0 + c0 + 1);
+              const double b0 = __ldg(in1 + c0), b1 = __ldg(in1 + c0 - sy);
+              const double b2 = __ldg(in1 + c0 + 1), b3 = __ldg(in1 + c0 + 1 - sy);
+              const double d0 = __ldg(in2 + c0), d1 = __ldg(in2 + c0 - sz);
+              const double d2 = __ldg(in2 + c0 + 1), d3 = __ldg(in2 + c0 + 1 - sz);
+              const double r0 = (a1 - a0) * g.rdx + (b0 - b1) * rdyJ + (d0 - d1) * g.rdz;
+              const double r1 = (a2 - a1) * g.rdx + (b2 - b3) * rdyJ + (d2 - d3) * g.rdz;
+              z = make_double2(r0, r1);
+            }
+          }
+        }
+        return z;
+      },
+      [&](int t, double2 z) {
+        const int l = t / M, m = t - l * M;
+        res[l * ls + m] = z;
+      });
+  __syncthreads();
+  // step 1 reads res, step 2 (after the barrier inside) overwrites it
+  fft4_lines<N1, N2, false>([&](int l, int m) { return res[l * ls + m]; },
+                            [&](int l, int e, double2 v) { res[l * ls + e] = v; }, buf, L, tw);
+  // post-process (X = E + w^k O) and store S(kx, j, k0 + l), l fastest
+  const int Lv = min(L, g.nz - k0);
+  for (int t = threadIdx.x; t < Lv * (M + 1); t += blockDim.x) {
+    const int kx = t / Lv, l = t - kx * Lv;
+    const double2 zk = res[l * ls + (kx == M ? 0 : kx)];
+    const double2 zc = cconj(res[l * ls + (kx == 0 ? 0 : M - kx)]);
+    const double2 e = make_double2(0.5 * (zk.x + zc.x), 0.5 * (zk.y + zc.y));
+    const double2 d = csub(zk, zc);
+    const double2 o = make_double2(0.5 * d.y, -0.5 * d.x);
+    S[sidx(g, kx, j, k0 + l)] = cadd(e, cmul(tn[kx], o));
+  }
+}
+
+// Inverse real FFT along x (see k_irfftx): pre-processing of the pairs
+// (k, M-k) in shared memory, then the four-step inverse whose step 2 writes
+// the field (OUTMODE as in k_irfftx).
+template <int N1, int N2, int OUTMODE>
+__global__ void __launch_bounds__(F4_THREADS, 2) k_irfftx4(Geo g, const double2 *__restrict__ S,
+                                                           double *__restrict__ out, int L,
+                                                           const double2 *__restrict__ twM,
+                                                           const double2 *__restrict__ twN) {
+  constexpr int M = N1 * N2;
+  constexpr int ls = M + 2;
+  extern __shared__ double2 smem[];
+  double2 *zb = smem;
+  double2 *buf = zb + L * ls;
+  double2 *tw = buf + fft4_buf<N1, N2>(L);
+  double2 *tn = tw + M;
+  const int ngrp = (g.nz + L - 1) / L;
+  const int grp = blockIdx.x % ngrp;
+  const int j = blockIdx.x / ngrp;
+  const int k0 = grp * L;
+  const int Lv = min(L, g.nz - k0);
+  for (int t = threadIdx.x; t < M; t += blockDim.x) tw[t] = twM[t];
+  for (int t = threadIdx.x; t <= M; t += blockDim.x) tn[t] = twN[t];
+  batched_copy<8>(
+      L * (M + 1),
+      [&](int t) {
+        const int kx = t / L, l = t - kx * L;
+        return l < Lv ? S[sidx(g, kx, j, k0 + l)] : make_double2(0.0, 0.0);
+      },
+      [&](int t, double2 v) {
+        const int kx = t / L, l = t - kx * L;
+        zb[l * ls + kx] = v;
+      });
+  __syncthreads();
+  // Z[k] = E[k] + i O[k], E = (X[k] + conj X[M-k])/2,
+  // O = (X[k] - conj X[M-k]) conj(w^k)/2; one thread per pair (k, M-k)
+  constexpr int half = M / 2 + 1;
+  for (int t = threadIdx.x; t < L * half; t += blockDim.x) {
+    const int l = t / half, k = t - l * half;
+    double2 *X = zb + l * ls;
+    if (k == 0) {
+      const double a = X[0].x, b = X[M].x;
+      X[0] = make_double2(0.5 * (a + b), 0.5 * (a - b));
+    } else if (2 * k <= M) {
+      const int k2 = M - k;
+      const double2 a = X[k], b = X[k2];
+      {
+        const double2 bc = cconj(b);
+        const double2 e = cscale(cadd(a, bc), 0.5);
+        const double2 o = cmul(cscale(csub(a, bc), 0.5), cconj(tn[k]));
+        X[k] = make_double2(e.x - o.y, e.y + o.x);
+      }
+      if (k2 != k) {
+        const double2 ac = cconj(a);
+        const double2 e = cscale(cadd(b, ac), 0.5);
+        const double2 o = cmul(cscale(csub(b, ac), 0.5), cconj(tn[k2]));
+        X[k2] = make_double2(e.x - o.y, e.y + o.x);
+      }
+    }
+  }
+  __syncthreads();
+  const double sc = 1.0 / M;
+  const int J = j + 1;
+  fft4_lines<N1, N2, true>(
+      [&](int l, int e) { return zb[l * ls + e]; },
+      [&](int l, int m, double2 z) {
+        if (l >= Lv) return;
+        const double x0 = z.x * sc, x1 = z.y * sc;
+        const int K = k0 + l + 1;
+        if (OUTMODE == ROUT_REAL) {
+          double *row = out + (long long)g.nx * (j + (long long)g.ny * (K - 1));
+          *reinterpret_cast<double2 *>(row + 2 * m) = make_double2(x0, x1);
+        } else if (OUTMODE == ROUT_INTERIOR) {
+          const long long c0 = gidx(g, 2 * m + 1, J, K);
+          out[c0] = x0;
+          out[c0 + 1] = x1;
+        } else {
+          store_img(out, g, 2 * m + 1, J, K, x0, STAG_P);
+          store_img(out, g, 2 * m + 2, J, K, x1, STAG_P);
+        }
+      },
+      buf, L, tw);
+}
+
+}  // namespace dnsb
