@@ -53,7 +53,7 @@ COMMON = dict(lims=((0.0, 4 * math.pi), (-1.0, 1.0), (0.0, 4 * math.pi / 3)),
 def passes(kind, implicit, spec):
     if kind == "momentum":
         return (12 + 13 + 13) / 3 if implicit else (9 + 12 + 12) / 3
-    return {"cn_solve": 9.0, "div_rfft_x": 3 + spec, "fft_z": 2 * spec, "y_solve": 2 * spec,
+    return {"cn_solve": 6.0, "div_rfft_x": 3 + spec, "fft_z": 2 * spec, "y_solve": 2 * spec,
             "ifft_z": 2 * spec, "irfft_x": spec + 1, "grad_update": 9.0 if implicit else 7.0,
             "other": 0.0}[kind]
 

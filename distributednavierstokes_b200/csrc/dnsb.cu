@@ -7,8 +7,8 @@
 //             k_thomas | k_yfourier solve in y
 //             k_fftz<inv>, k_irfftx psi (+ halos)
 //             k_grad<EXPLICIT>      u = W - grad psi          (+ u halos)
-//   implicit: k_momentum<IMPLICIT>  q, V = u + B q - a dt grad p
-//             k_cn                  u = (I - th Dy)^-1 (V + th Dy u)  (+ halos)
+//   implicit: k_momentum<IMPLICIT>  q, V = u + B q - a dt grad p + th Dy u
+//             k_cn                  u = (I - th Dy)^-1 V      (+ halos)
 //             Poisson as above      delta (+ halos)
 //             k_grad<IMPLICIT>      u -= grad delta, p += delta/(a dt) (+ halos)
 // so that no separate halo, copy or transpose kernel runs.
@@ -548,16 +548,16 @@ int poisson_from_spectrum(dnsb_ctx *c, int outmode, double *out) {
   return launch_irfftx(c, outmode, out);
 }
 
-void launch_cn(dnsb_ctx *c, Fields3 out, CFields3 V, CFields3 un, const double *tab, double th) {
+void launch_cn(dnsb_ctx *c, Fields3 out, CFields3 V, const double *tab) {
   const Geo &g = c->g;
   const dim3 grid = cn_grid(g), block(CN_LINES, CN_CHUNKS);
   switch (c->cn_mr) {
-    case 1: k_cn<1><<<grid, block, c->smem_cn, c->stream>>>(g, out, V, un, c->ycoef, tab, th); break;
-    case 2: k_cn<2><<<grid, block, c->smem_cn, c->stream>>>(g, out, V, un, c->ycoef, tab, th); break;
-    case 4: k_cn<4><<<grid, block, c->smem_cn, c->stream>>>(g, out, V, un, c->ycoef, tab, th); break;
-    case 8: k_cn<8><<<grid, block, c->smem_cn, c->stream>>>(g, out, V, un, c->ycoef, tab, th); break;
-    case 16: k_cn<16><<<grid, block, c->smem_cn, c->stream>>>(g, out, V, un, c->ycoef, tab, th); break;
-    default: k_cn<32><<<grid, block, c->smem_cn, c->stream>>>(g, out, V, un, c->ycoef, tab, th); break;
+    case 1: k_cn<1><<<grid, block, c->smem_cn, c->stream>>>(g, out, V, tab); break;
+    case 2: k_cn<2><<<grid, block, c->smem_cn, c->stream>>>(g, out, V, tab); break;
+    case 4: k_cn<4><<<grid, block, c->smem_cn, c->stream>>>(g, out, V, tab); break;
+    case 8: k_cn<8><<<grid, block, c->smem_cn, c->stream>>>(g, out, V, tab); break;
+    case 16: k_cn<16><<<grid, block, c->smem_cn, c->stream>>>(g, out, V, tab); break;
+    default: k_cn<32><<<grid, block, c->smem_cn, c->stream>>>(g, out, V, tab); break;
   }
 }
 
@@ -578,7 +578,7 @@ int do_step(dnsb_ctx *c, double *ux, double *uy, double *uz, double *p, double *
       LAUNCH(c, DNSB_KIND_MOMENTUM,
              k_momentum<MOM_EXPLICIT><<<c->cgrid, c->cblock, 0, c->stream>>>(
                  g, ff(qx, qy, qz), cf(ux, uy, uz), ff(c->W[0], c->W[1], c->W[2]), nullptr, A, dt,
-                 B, 0.0, readq));
+                 B, 0.0, readq, nullptr, 0.0));
       if ((rc = launch_rfftx(c, RIN_DIVERGENCE, c->W[0], c->W[1], c->W[2]))) return rc;
       if ((rc = poisson_from_spectrum(c, ROUT_IMAGES, p))) return rc;
       LAUNCH(c, DNSB_KIND_GRAD,
@@ -590,10 +590,10 @@ int do_step(dnsb_ctx *c, double *ux, double *uy, double *uz, double *p, double *
       LAUNCH(c, DNSB_KIND_MOMENTUM,
              k_momentum<MOM_IMPLICIT><<<c->cgrid, c->cblock, 0, c->stream>>>(
                  g, ff(qx, qy, qz), cf(ux, uy, uz), ff(c->V[0], c->V[1], c->V[2]), p, A, dt, B,
-                 adt, readq));
+                 adt, readq, c->ycoef, th));
       LAUNCH(c, DNSB_KIND_CN,
-             launch_cn(c, ff(ux, uy, uz), cf(c->V[0], c->V[1], c->V[2]), cf(ux, uy, uz),
-                       c->ytab + (long long)s * 2 * cn_tab_stride(g.ny), th));
+             launch_cn(c, ff(ux, uy, uz), cf(c->V[0], c->V[1], c->V[2]),
+                       c->ytab + (long long)s * 2 * cn_tab_stride(g.ny)));
       if ((rc = launch_rfftx(c, RIN_DIVERGENCE, ux, uy, uz))) return rc;
       if ((rc = poisson_from_spectrum(c, ROUT_IMAGES, delta))) return rc;
       LAUNCH(c, DNSB_KIND_GRAD,
@@ -779,7 +779,7 @@ int dnsb_create(const dnsb_grid *gr, int device, void *stream, dnsb_ctx **out) {
   if ((rc = dalloc(c, &c->ytab, 6 * (size_t)cn_tab_stride(ny)))) return bail(rc);
   c->cn_mr = 1;
   while (c->cn_mr * CN_CHUNKS < ny) c->cn_mr *= 2;
-  c->smem_cn = sizeof(double) * (8 * (size_t)ny + 2 * CN_CHUNKS + 2 * CN_CHUNKS * CN_LINES);
+  c->smem_cn = sizeof(double) * (5 * (size_t)ny + 2 * CN_CHUNKS + 2 * CN_CHUNKS * CN_LINES);
   if (c->implicit && c->cn_mr > 32) {
     fail(c, DNSB_EUNSUP, "semi-implicit y-diffusion supports ny <= %d", 32 * CN_CHUNKS);
     return bail(DNSB_EUNSUP);
@@ -941,7 +941,7 @@ int dnsb_momentum(dnsb_ctx *c, double *qx, double *qy, double *qz, const double 
   if (ensure_device(c)) return DNSB_ECUDA;
   k_momentum<MOM_ONLY><<<cell_grid(c->g), cell_block, 0, c->stream>>>(
       c->g, ff(qx, qy, qz), cf(ux, uy, uz), ff(nullptr, nullptr, nullptr), nullptr, A, dt, 0.0,
-      0.0, 1);
+      0.0, 1, nullptr, 0.0);
   CKL(c);
   return 0;
 }
@@ -979,15 +979,15 @@ int dnsb_imex_update(dnsb_ctx *c, double *ux, double *uy, double *uz, const doub
   if (ensure_device(c)) return DNSB_ECUDA;
   const Geo &g = c->g;
   const double adt = alpha * dt;
+  const double th = alpha * dt * g.visc / 2;
   k_vupdate<<<cell_grid(g), cell_block, 0, c->stream>>>(
-      g, ff(c->V[0], c->V[1], c->V[2]), cf(ux, uy, uz), cf(qx, qy, qz), p, B, adt);
+      g, ff(c->V[0], c->V[1], c->V[2]), cf(ux, uy, uz), cf(qx, qy, qz), p, B, adt, c->ycoef, th);
   CKL(c);
   // tables for this alpha in stage slot 0
   k_cn_tables<<<1, 32, 0, c->stream>>>(g.ny, c->cn_mr, CN_CHUNKS, c->ycoef, c->ytab, dt, g.visc,
                                        alpha, alpha, alpha);
   CKL(c);
-  const double th = alpha * dt * g.visc / 2;
-  launch_cn(c, ff(ux, uy, uz), cf(c->V[0], c->V[1], c->V[2]), cf(ux, uy, uz), c->ytab, th);
+  launch_cn(c, ff(ux, uy, uz), cf(c->V[0], c->V[1], c->V[2]), c->ytab);
   CKL(c);
   c->umax_for[0] = c->umax_for[1] = c->umax_for[2] = nullptr;
   return 0;

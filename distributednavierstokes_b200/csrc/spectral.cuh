@@ -442,26 +442,22 @@ __global__ void k_cn_tables(int ny, int m, int nchunks, const double *__restrict
   }
 }
 
-// imexrhs_kernel! + imexsolve_kernel! (src/ydiffusion.jl:71-109) fused.
+// imexsolve_kernel! (src/ydiffusion.jl:94-109) on right-hand sides that the
+// producer (k_momentum<IMPLICIT> or k_vupdate) has already formed.
 // A block owns CN_LINES consecutive x-lines (I) at one K for component
 // c = blockIdx.z and splits every y-line into CN_CHUNKS chunks of MR rows,
-// one thread per (line, chunk).  A thread loads the v and u^n values of its
-// rows straight into registers (all loads issued together), forms
-// rhs = v + theta Dy u^n (walls folded into the rows), runs the Thomas
-// forward sweep from a zero carry; the chunks exchange their end values
-// through shared memory and add the carried-in part with the per-chunk
-// multiplier products (g, G); the backward sweep is split the same way
-// (h, H).  Algebraically this is the reference's Thomas algorithm; every
-// element is read from and written to HBM once.  The line-independent
-// coefficient tables sit in shared memory.  out may alias u^n: all reads
-// precede the first write (a barrier separates them).
+// one thread per (line, chunk).  A thread loads its rows of V straight into
+// registers (all loads issued together), runs the Thomas forward sweep from
+// a zero carry; the chunks exchange their end values through shared memory
+// and add the carried-in part with the per-chunk multiplier products
+// (g, G); the backward sweep is split the same way (h, H).  Algebraically
+// this is the reference's Thomas algorithm; every element is read from and
+// written to HBM once.  The line-independent coefficient tables sit in
+// shared memory.
 template <int MR>
-__global__ void __launch_bounds__(CN_LINES *CN_CHUNKS, 2) k_cn(Geo g, Fields3 out, CFields3 V,
-                                                              CFields3 un,
-                                                              const double *__restrict__ coef,
-                                                              const double *__restrict__ tab,
-                                                              double theta) {
-  extern __shared__ double cs[];  // a b c ta cp ib gf hb (ny each), G H, exchange
+__global__ void __launch_bounds__(CN_LINES *CN_CHUNKS, 3) k_cn(Geo g, Fields3 out, CFields3 V,
+                                                              const double *__restrict__ tab) {
+  extern __shared__ double cs[];  // ta cp ib gf hb (ny each), G H, exchange
   const int i = threadIdx.x, ck = threadIdx.y;
   const int tid = i + CN_LINES * ck;
   const int I0 = blockIdx.x * CN_LINES + 1;
@@ -471,40 +467,30 @@ __global__ void __launch_bounds__(CN_LINES *CN_CHUNKS, 2) k_cn(Geo g, Fields3 ou
   const int ny = g.ny;
   const int set = c == STAG_Y ? 1 : 0;
   const double *v = c == 0 ? V.x : c == 1 ? V.y : V.z;
-  const double *u = c == 0 ? un.x : c == 1 ? un.y : un.z;
   double *o = c == 0 ? out.x : c == 1 ? out.y : out.z;
   const long long sy = g.NX;
   const bool active = I <= g.nx;
   const long long base = gidx(g, active ? I : I0, 1, K);
   const int s0 = ck * MR;
-  // 1. this thread's rows of v and u^n (u with one row either side)
-  double x[MR], uu[MR + 2];
+  // 1. this thread's rows of the right-hand side
+  double x[MR];
 #pragma unroll
   for (int r = 0; r < MR; r++) {
     const int j = s0 + r;
-    const bool ok = active && j < ny;
-    x[r] = ok ? v[base + j * sy] : 0.0;
-    uu[r + 1] = ok ? u[base + j * sy] : 0.0;
+    x[r] = (active && j < ny) ? v[base + j * sy] : 0.0;
   }
-  uu[0] = (active && s0 > 0 && s0 - 1 < ny) ? u[base + (s0 - 1) * sy] : 0.0;
-  uu[MR + 1] = (active && s0 + MR < ny) ? u[base + (s0 + MR) * sy] : 0.0;
   // 2. stage the tables (line-independent) while the loads are in flight
   double *ta_ = cs, *ib_ = cs + ny, *cp_ = cs + 2 * ny, *gf_ = cs + 3 * ny, *hb_ = cs + 4 * ny;
-  double *a_ = cs + 5 * ny, *b_ = cs + 6 * ny, *c_ = cs + 7 * ny;
-  double *G_ = cs + 8 * ny, *H_ = G_ + CN_CHUNKS;  // copies of G[0..CN_CHUNKS), H[...]
+  double *G_ = cs + 5 * ny, *H_ = G_ + CN_CHUNKS;  // copies of G[0..CN_CHUNKS), H[...]
   double *xa = H_ + CN_CHUNKS, *xb = xa + CN_CHUNKS * CN_LINES;
   {
     const double *ts = tab + set * cn_tab_stride(ny);  // [ta cp ib gf hb] G H
-    const double *cf3 = coef + set * 3 * ny;           // [a b c]
     for (int t = tid; t < ny; t += CN_LINES * CN_CHUNKS) {
       ta_[t] = ts[t];
       cp_[t] = ts[ny + t];
       ib_[t] = ts[2 * ny + t];
       gf_[t] = ts[3 * ny + t];
       hb_[t] = ts[4 * ny + t];
-      a_[t] = cf3[t];
-      b_[t] = cf3[ny + t];
-      c_[t] = cf3[2 * ny + t];
     }
     if (tid < CN_CHUNKS) {
       G_[tid] = ts[5 * ny + tid];
@@ -512,18 +498,13 @@ __global__ void __launch_bounds__(CN_LINES *CN_CHUNKS, 2) k_cn(Geo g, Fields3 ou
     }
   }
   __syncthreads();
-  // 3. rhs and local forward sweep (zero carry)
+  // 3. local forward sweep (zero carry)
   double z = 0.0;
 #pragma unroll
   for (int r = 0; r < MR; r++) {
     const int j = s0 + r;
     if (j < ny) {
-      double sum;
-      if (j == 0) sum = b_[0] * uu[r + 1] + (ny > 1 ? c_[0] * uu[r + 2] : 0.0);
-      else if (j == ny - 1) sum = a_[j] * uu[r] + b_[j] * uu[r + 1];
-      else sum = (a_[j] * uu[r] + b_[j] * uu[r + 1]) + c_[j] * uu[r + 2];
-      const double rhs = x[r] + theta * sum;
-      z = r == 0 ? rhs * ib_[j] : fma(ta_[j], z, rhs) * ib_[j];
+      z = r == 0 ? x[r] * ib_[j] : fma(ta_[j], z, x[r]) * ib_[j];
       x[r] = z;
     }
   }

@@ -18,24 +18,37 @@ enum MomMode { MOM_ONLY = 0, MOM_EXPLICIT = 1, MOM_IMPLICIT = 2 };
 
 #define LDG(p, o) __ldg((p) + (o))
 
+// Right-hand side of the Crank-Nicolson row j = J-1 of one component
+// (imexrhs_kernel!, src/ydiffusion.jl:71-91): v + theta (a u_S + b u_0 +
+// c u_N) with the wall rows folded into the coefficients (a_0 = 0,
+// c_{ny-1} = 0); abc points at the component set's [a | b | c] rows.
+__device__ __forceinline__ double cn_rhs(const double *__restrict__ abc, int ny, int j, double v,
+                                         double theta, double uS, double u0, double uN) {
+  const double a = __ldg(abc + j), b = __ldg(abc + ny + j), c = __ldg(abc + 2 * ny + j);
+  double sum;
+  if (j == 0) sum = b * u0 + (ny > 1 ? c * uN : 0.0);
+  else if (j == ny - 1) sum = a * uS + b * u0;
+  else sum = (a * uS + b * u0) + c * uN;
+  return v + theta * sum;
+}
+
 // momentum_kernel! (src/operators.jl:44-145) at one interior cell: loads
 // the 3x3x3 staggered neighbourhood (27 values) plus q and p, returns the
-// new RK registers q, the stage increment v (MOM_EXPLICIT: u + B q,
-// MOM_IMPLICIT: u + B q - adt grad p on active DOFs) and the wall-normal
-// neighbours of u that the Crank-Nicolson right-hand side needs.
+// new RK registers q and the stage increment v (MOM_EXPLICIT: u + B q;
+// MOM_IMPLICIT: u + B q - adt grad p on active DOFs, plus theta Dy u^n:
+// the Crank-Nicolson right-hand side).  Each component's v is finished
+// right after its q so that its wall-normal neighbours die early.
 struct MomCell {
-  double qx, qy, qz;     // new registers
-  double vx, vy, vz;     // stage increments
-  double uxS, ux0, uxN;  // u^n at J-1, J, J+1 (x, y, z components)
-  double uyS, uy0, uyN;
-  double uzS, uz0, uzN;
+  double qx, qy, qz;  // new registers
+  double vx, vy, vz;  // stage increments
 };
 
 template <int MODE>
 __device__ __forceinline__ MomCell momentum_cell(const Geo &g, int I, int J, int K, const Fields3 &q,
                                                  const CFields3 &u, const double *__restrict__ p,
                                                  double A, double dt, double B, double adt,
-                                                 int readq) {
+                                                 int readq, const double *__restrict__ coef,
+                                                 double theta) {
   const long long sy = g.NX, sz = (long long)g.NX * g.NY;
   const long long c0 = gidx(g, I, J, K);
   const double *ux = u.x, *uy = u.y, *uz = u.z;
@@ -82,6 +95,13 @@ __device__ __forceinline__ MomCell momentum_cell(const Geo &g, int I, int J, int
                         (uxT - 2 * ux0 + uxB) * g.rdz2;
     const double f = dt * (-conv + nu * diff + g.fx);
     m.qx = readq ? A * qx0 + f : f;
+    if (MODE == MOM_EXPLICIT) {
+      m.vx = ux0 + B * m.qx;  // u <- u + B q on ranges[c] (timestep.jl:54-58)
+    } else {
+      // v = u + B q - alpha dt grad p (ydiffusion.jl:133-135)
+      m.vx = cn_rhs(coef, g.ny, J - 1, (ux0 + B * m.qx) - adt * (pE - p0) * g.rdx, theta, uxS,
+                    ux0, uxN);
+    }
   }
   // y momentum, at the top y-face; Delta-y weighted transporters
   {
@@ -98,6 +118,13 @@ __device__ __forceinline__ MomCell momentum_cell(const Geo &g, int I, int J, int
                         (uyT - 2 * uy0 + uyB) * g.rdz2;
     const double f = dt * (-conv + nu * diff + g.fy);
     m.qy = readq ? A * qy0 + f : f;
+    const bool yact = J <= g.jymax;
+    if (MODE == MOM_EXPLICIT) {
+      m.vy = yact ? uy0 + B * m.qy : uy0;
+    } else {
+      const double v = yact ? (uy0 + B * m.qy) - adt * (pN - p0) * rdyuJ : uy0;
+      m.vy = cn_rhs(coef + 3 * g.ny, g.ny, J - 1, v, theta, uyS, uy0, uyN);
+    }
   }
   // z momentum, at the back z-face
   {
@@ -113,40 +140,36 @@ __device__ __forceinline__ MomCell momentum_cell(const Geo &g, int I, int J, int
                         (uzT - 2 * uz0 + uzB) * g.rdz2;
     const double f = dt * (-conv + nu * diff + g.fz);
     m.qz = readq ? A * qz0 + f : f;
+    if (MODE == MOM_EXPLICIT) {
+      m.vz = uz0 + B * m.qz;
+    } else {
+      m.vz = cn_rhs(coef, g.ny, J - 1, (uz0 + B * m.qz) - adt * (pT - p0) * g.rdz, theta, uzS,
+                    uz0, uzN);
+    }
   }
-  const bool yact = J <= g.jymax;
-  if (MODE == MOM_EXPLICIT) {
-    // u <- u + B q on ranges[c] (timestep.jl:54-58)
-    m.vx = ux0 + B * m.qx;
-    m.vy = yact ? uy0 + B * m.qy : uy0;
-    m.vz = uz0 + B * m.qz;
-  } else {
-    // v = u + B q - alpha dt grad p (ydiffusion.jl:133-135)
-    m.vx = (ux0 + B * m.qx) - adt * (pE - p0) * g.rdx;
-    m.vy = yact ? (uy0 + B * m.qy) - adt * (pN - p0) * rdyuJ : uy0;
-    m.vz = (uz0 + B * m.qz) - adt * (pT - p0) * g.rdz;
-  }
-  m.uxS = uxS; m.ux0 = ux0; m.uxN = uxN;
-  m.uyS = uyS; m.uy0 = uy0; m.uyN = uyN;
-  m.uzS = uzS; m.uz0 = uz0; m.uzN = uzN;
   return m;
 }
 
 // momentum_kernel! (src/operators.jl:44-145), one thread per interior cell.
 // MOM_ONLY: q <- A q + dt F(u).
 // MOM_EXPLICIT: also W_c = u_c + B q_c on active DOFs, with ghost images.
-// MOM_IMPLICIT: also V_c = u_c + B q_c - adt * d_c p on active DOFs.
+// MOM_IMPLICIT: also the Crank-Nicolson right-hand side
+//   V_c = (u_c + B q_c - adt d_c p) + theta Dy u_c
+// (coef = [at bt ct an bn cn] rows of ny), so the y-solve reads only V.
+// Implicit mode holds all 34 loads plus the coefficient rows: 2 CTAs of 256
+// per SM keep it free of spills (measured faster than 3-4 CTAs with spills).
 template <int MODE>
-__global__ void __launch_bounds__(256, 4) k_momentum(Geo g, Fields3 q, CFields3 u, Fields3 out,
+__global__ void __launch_bounds__(256, MODE == MOM_IMPLICIT ? 2 : 4) k_momentum(Geo g, Fields3 q, CFields3 u, Fields3 out,
                                                   const double *__restrict__ p, double A, double dt,
-                                                  double B, double adt, int readq) {
+                                                  double B, double adt, int readq,
+                                                  const double *__restrict__ coef, double theta) {
   const int I = blockIdx.x * blockDim.x + threadIdx.x + 1;
   const int J = blockIdx.y * blockDim.y + threadIdx.y + 1;
   const int K = blockIdx.z + 1;
   if (I > g.nx || J > g.ny) return;
   const long long c0 = gidx(g, I, J, K);
-  const MomCell m = momentum_cell<MODE == MOM_ONLY ? MOM_EXPLICIT : MODE>(g, I, J, K, q, u, p, A,
-                                                                          dt, B, adt, readq);
+  const MomCell m = momentum_cell<MODE == MOM_ONLY ? MOM_EXPLICIT : MODE>(
+      g, I, J, K, q, u, p, A, dt, B, adt, readq, coef, theta);
   const bool yact = J <= g.jymax;
   q.x[c0] = m.qx;
   if (yact) q.y[c0] = m.qy;
@@ -240,9 +263,10 @@ __global__ void k_pgrad(Geo g, double *phi, const double *__restrict__ p, int c,
 }
 
 // ranges-wise register update u_c += B q_c then u_c -= s d_c p (the first
-// half of imex_update!, src/ydiffusion.jl:133-135), writing v into V.
+// half of imex_update!, src/ydiffusion.jl:133-135), writing into V the
+// Crank-Nicolson right-hand side v + theta Dy u^n (see cn_rhs).
 __global__ void k_vupdate(Geo g, Fields3 V, CFields3 u, CFields3 q, const double *__restrict__ p,
-                          double B, double adt) {
+                          double B, double adt, const double *__restrict__ coef, double theta) {
   const int I = blockIdx.x * blockDim.x + threadIdx.x + 1;
   const int J = blockIdx.y * blockDim.y + threadIdx.y + 1;
   const int K = blockIdx.z + 1;
@@ -250,10 +274,15 @@ __global__ void k_vupdate(Geo g, Fields3 V, CFields3 u, CFields3 q, const double
   const long long sy = g.NX, sz = (long long)g.NX * g.NY;
   const long long c0 = gidx(g, I, J, K);
   const double p0 = p[c0];
-  V.x[c0] = (u.x[c0] + B * q.x[c0]) - adt * (p[c0 + 1] - p0) * g.rdx;
-  V.y[c0] = J <= g.jymax ? (u.y[c0] + B * q.y[c0]) - adt * (p[c0 + sy] - p0) * __ldg(g.rdyu + J)
-                         : u.y[c0];
-  V.z[c0] = (u.z[c0] + B * q.z[c0]) - adt * (p[c0 + sz] - p0) * g.rdz;
+  const double ux0 = u.x[c0], uy0 = u.y[c0], uz0 = u.z[c0];
+  const double vx = (ux0 + B * q.x[c0]) - adt * (p[c0 + 1] - p0) * g.rdx;
+  const double vy = J <= g.jymax ? (uy0 + B * q.y[c0]) - adt * (p[c0 + sy] - p0) * __ldg(g.rdyu + J)
+                                 : uy0;
+  const double vz = (uz0 + B * q.z[c0]) - adt * (p[c0 + sz] - p0) * g.rdz;
+  const int ny = g.ny, j = J - 1;
+  V.x[c0] = cn_rhs(coef, ny, j, vx, theta, u.x[c0 - sy], ux0, u.x[c0 + sy]);
+  V.y[c0] = cn_rhs(coef + 3 * ny, ny, j, vy, theta, u.y[c0 - sy], uy0, u.y[c0 + sy]);
+  V.z[c0] = cn_rhs(coef, ny, j, vz, theta, u.z[c0 - sy], uz0, u.z[c0 + sy]);
 }
 
 // divergence_kernel! (src/operators.jl:10-26) into the ghost-free r.
