@@ -28,6 +28,7 @@
 #include "fft.cuh"
 #include "spectral.cuh"
 #include "spectral4.cuh"
+#include "ysolve.cuh"
 #include "stencil.cuh"
 
 using namespace dnsb;
@@ -90,6 +91,7 @@ struct dnsb_ctx {
   // scratch
   double2 *S = nullptr;
   double *work = nullptr;
+  double *ycin = nullptr;  // c' entering each y-chunk, per (kx, kz) line
   double *r = nullptr;
   double *W[3] = {nullptr, nullptr, nullptr};
   double *V[3] = {nullptr, nullptr, nullptr};
@@ -517,8 +519,22 @@ int launch_fftz(dnsb_ctx *c, bool inv) {
 int launch_ysolve(dnsb_ctx *c) {
   const Geo &g = c->g;
   if (g.wall) {
-    long long n = (long long)g.nkx * g.nz;
-    LAUNCH(c, DNSB_KIND_YSOLVE, k_thomas<<<(unsigned)((n + 127) / 128), 128, 0, c->stream>>>(g, c->S, c->work, c->ay, c->by, c->cy, c->lam1, c->lam3));
+    const long long n = (long long)g.nkx * g.nz;
+    const dim3 grid((unsigned)((n + TY_LINES - 1) / TY_LINES)), block(TY_LINES, TY_CHUNKS);
+#define YT(MR)                                                                                    \
+  case MR:                                                                                        \
+    LAUNCH(c, DNSB_KIND_YSOLVE,                                                                   \
+           k_ythomas<MR><<<grid, block, 0, c->stream>>>(g, c->S, c->ycin, c->ay, c->by, c->cy,   \
+                                                        c->lam1, c->lam3));                       \
+    break;
+    switch (ythomas_rows(g.ny)) {
+      YT(1) YT(2) YT(3) YT(4) YT(6) YT(8) YT(12) YT(16)
+      default:
+        LAUNCH(c, DNSB_KIND_YSOLVE,
+               k_thomas<<<(unsigned)((n + 127) / 128), 128, 0, c->stream>>>(
+                   g, c->S, c->work, c->ay, c->by, c->cy, c->lam1, c->lam3));
+    }
+#undef YT
   } else {
     dim3 grid(g.nkx * ((g.nz + c->Ly - 1) / c->Ly));
     LAUNCH(c, DNSB_KIND_YSOLVE, k_yfourier<false><<<grid, SPEC_THREADS, c->smem_y, c->stream>>>(g, c->S, c->py, c->Ly, c->twy, c->lam1, c->lam2, c->lam3));
@@ -779,7 +795,7 @@ int dnsb_create(const dnsb_grid *gr, int device, void *stream, dnsb_ctx **out) {
   if ((rc = dalloc(c, &c->ytab, 6 * (size_t)cn_tab_stride(ny)))) return bail(rc);
   c->cn_mr = 1;
   while (c->cn_mr * CN_CHUNKS < ny) c->cn_mr *= 2;
-  c->smem_cn = sizeof(double) * (5 * (size_t)ny + 2 * CN_CHUNKS + 2 * CN_CHUNKS * CN_LINES);
+  c->smem_cn = sizeof(double) * (5 * (size_t)cn_skew_pitch(ny, c->cn_mr) + 2 * CN_CHUNKS + 2 * CN_CHUNKS * CN_LINES);
   if (c->implicit && c->cn_mr > 32) {
     fail(c, DNSB_EUNSUP, "semi-implicit y-diffusion supports ny <= %d", 32 * CN_CHUNKS);
     return bail(DNSB_EUNSUP);
@@ -862,7 +878,17 @@ int dnsb_create(const dnsb_grid *gr, int device, void *stream, dnsb_ctx **out) {
       (rc = dalloc(c, &c->umax, 3 * UMAX_SLOTS + 8)) || (rc = dalloc(c, &c->partial, RED_BLOCKS + 8)) ||
       (rc = dalloc(c, &c->deverr, 4)))
     return bail(rc);
-  if (g.wall && (rc = dalloc(c, &c->work, nspec))) return bail(rc);
+  if (g.wall && ythomas_rows(ny) == 0 && (rc = dalloc(c, &c->work, nspec))) return bail(rc);
+  if (g.wall && ythomas_rows(ny) != 0) {
+    const long long nl = (long long)g.nkx * nz;
+    if ((rc = dalloc(c, &c->ycin, (size_t)nl * TY_CHUNKS))) return bail(rc);
+    k_ythomas_entries<<<(unsigned)((nl + 127) / 128), 128, 0, c->stream>>>(
+        g, ythomas_rows(ny), c->ycin, c->ay, c->by, c->cy, c->lam1, c->lam3);
+    if (cudaGetLastError() != cudaSuccess) {
+      fail(c, DNSB_ECUDA, "launch of the y-solve table kernel failed");
+      return bail(DNSB_ECUDA);
+    }
+  }
   for (int i = 0; i < 3; i++) {
     if (!c->implicit) {
       if ((rc = dalloc(c, &c->W[i], G))) return bail(rc);

@@ -402,6 +402,8 @@ constexpr int CN_LINES = 16;
 
 constexpr int CN_MAXCHUNKS = 32;
 __host__ __device__ constexpr long long cn_tab_stride(int ny) { return 5LL * ny + 2 * CN_MAXCHUNKS; }
+// Shared-memory pitch of one k_cn table with rows skewed by their chunk.
+__host__ __device__ constexpr int cn_skew_pitch(int ny, int mr) { return ny + (ny + mr - 1) / mr; }
 
 __global__ void k_cn_tables(int ny, int m, int nchunks, const double *__restrict__ coef,
                             double *__restrict__ tab, double dt, double visc, double al0,
@@ -479,18 +481,22 @@ __global__ void __launch_bounds__(CN_LINES *CN_CHUNKS, 3) k_cn(Geo g, Fields3 ou
     const int j = s0 + r;
     x[r] = (active && j < ny) ? v[base + j * sy] : 0.0;
   }
-  // 2. stage the tables (line-independent) while the loads are in flight
-  double *ta_ = cs, *ib_ = cs + ny, *cp_ = cs + 2 * ny, *gf_ = cs + 3 * ny, *hb_ = cs + 4 * ny;
-  double *G_ = cs + 5 * ny, *H_ = G_ + CN_CHUNKS;  // copies of G[0..CN_CHUNKS), H[...]
+  // 2. stage the tables (line-independent) while the loads are in flight;
+  // row j sits at j + j/MR so that the two chunks of a warp hit different
+  // banks
+  const int tp = cn_skew_pitch(ny, MR);
+  double *ta_ = cs, *ib_ = cs + tp, *cp_ = cs + 2 * tp, *gf_ = cs + 3 * tp, *hb_ = cs + 4 * tp;
+  double *G_ = cs + 5 * tp, *H_ = G_ + CN_CHUNKS;  // copies of G[0..CN_CHUNKS), H[...]
   double *xa = H_ + CN_CHUNKS, *xb = xa + CN_CHUNKS * CN_LINES;
   {
     const double *ts = tab + set * cn_tab_stride(ny);  // [ta cp ib gf hb] G H
     for (int t = tid; t < ny; t += CN_LINES * CN_CHUNKS) {
-      ta_[t] = ts[t];
-      cp_[t] = ts[ny + t];
-      ib_[t] = ts[2 * ny + t];
-      gf_[t] = ts[3 * ny + t];
-      hb_[t] = ts[4 * ny + t];
+      const int u = t + t / MR;
+      ta_[u] = ts[t];
+      cp_[u] = ts[ny + t];
+      ib_[u] = ts[2 * ny + t];
+      gf_[u] = ts[3 * ny + t];
+      hb_[u] = ts[4 * ny + t];
     }
     if (tid < CN_CHUNKS) {
       G_[tid] = ts[5 * ny + tid];
@@ -504,22 +510,27 @@ __global__ void __launch_bounds__(CN_LINES *CN_CHUNKS, 3) k_cn(Geo g, Fields3 ou
   for (int r = 0; r < MR; r++) {
     const int j = s0 + r;
     if (j < ny) {
-      z = r == 0 ? x[r] * ib_[j] : fma(ta_[j], z, x[r]) * ib_[j];
+      z = r == 0 ? x[r] * ib_[j + ck] : fma(ta_[j + ck], z, x[r]) * ib_[j + ck];
       x[r] = z;
     }
   }
   xa[ck * CN_LINES + i] = z;
   __syncthreads();
-  // 4. carry into this chunk from the earlier chunks, then backward sweep
+  // 4. carry into this chunk from the earlier chunks (unrolled: the
+  // shared-memory loads are independent of the FMA chain), backward sweep
   double cin = 0.0;
-  for (int k = 0; k < ck; k++) cin = xa[k * CN_LINES + i] + G_[k] * cin;
+#pragma unroll
+  for (int k = 0; k < CN_CHUNKS - 1; k++) {
+    const double a = xa[k * CN_LINES + i], gk = G_[k];
+    if (k < ck) cin = fma(gk, cin, a);
+  }
   double bnext = 0.0;
 #pragma unroll
   for (int r = MR - 1; r >= 0; r--) {
     const int j = s0 + r;
     if (j < ny) {
-      const double xp = fma(gf_[j], cin, x[r]);
-      bnext = fma(-cp_[j], bnext, xp);
+      const double xp = fma(gf_[j + ck], cin, x[r]);
+      bnext = fma(-cp_[j + ck], bnext, xp);
       x[r] = bnext;
     }
   }
@@ -527,7 +538,11 @@ __global__ void __launch_bounds__(CN_LINES *CN_CHUNKS, 3) k_cn(Geo g, Fields3 ou
   __syncthreads();
   // 5. carry from the later chunks, final values with ghost images
   double cout = 0.0;
-  for (int k = CN_CHUNKS - 1; k > ck; k--) cout = xb[k * CN_LINES + i] + H_[k] * cout;
+#pragma unroll
+  for (int k = CN_CHUNKS - 1; k > 0; k--) {
+    const double a = xb[k * CN_LINES + i], hk = H_[k];
+    if (k > ck) cout = fma(hk, cout, a);
+  }
   if (active) {
     const bool normal_wall = g.wall && c == STAG_Y;
     const bool line_edge = (I == 1) | (I == g.nx) | (K == 1) | (K == g.nz);
@@ -535,7 +550,7 @@ __global__ void __launch_bounds__(CN_LINES *CN_CHUNKS, 3) k_cn(Geo g, Fields3 ou
     for (int r = 0; r < MR; r++) {
       const int j = s0 + r;
       if (j < ny) {
-        const double xv = fma(hb_[j], cout, x[r]);
+        const double xv = fma(hb_[j + ck], cout, x[r]);
         o[base + j * sy] = xv;
         // ghost images of edge lines and of the first/last rows (the
         // inactive wall face of the normal component has none)
