@@ -30,8 +30,10 @@ struct Geo {
   const double *dy, *dyu, *rdy, *rdyu;  // device, ny+2 entries (ghosted J)
 };
 
-__host__ __device__ __forceinline__ long long gidx(const Geo &g, int I, int J, int K) {
-  return (long long)I + (long long)g.NX * ((long long)J + (long long)g.NY * (long long)K);
+// Linear index of ghosted cell (I, J, K).  32-bit: a context refuses grids
+// whose ghosted field reaches 2^31 values, so offsets stay in one IMAD.
+__host__ __device__ __forceinline__ int gidx(const Geo &g, int I, int J, int K) {
+  return I + g.NX * (J + g.NY * K);
 }
 
 // Spectrum layout: S[kz + nz*(j + ny*kx)] (kz fastest, then y, kx slowest),
@@ -52,26 +54,26 @@ __host__ __device__ __forceinline__ long long sidx(const Geo &g, int kx, int j, 
 // reference compose into exactly this product of per-axis images.
 // Interior threads only test the edge predicate; edge threads run
 // straight-line predicated stores (no local memory).
-__device__ __forceinline__ void store_img(double *__restrict__ f, const Geo &g, int I, int J,
-                                          int K, double v, int stag) {
-  f[gidx(g, I, J, K)] = v;
-  const bool edge = (I == 1) | (I == g.nx) | (K == 1) | (K == g.nz) | (J == 1) | (J >= g.ny - 1);
-  if (!edge) return;
-  const int Ia = (I == 1) ? g.nx + 1 : (I == g.nx) ? 0 : -1;  // nx >= 2: at most one
-  const int Ka = (K == 1) ? g.nz + 1 : (K == g.nz) ? 0 : -1;
-  const int Kb = (K == 1 && K == g.nz) ? 0 : -1;               // nz == 1
+// The images alone (no interior store), from the grid extents passed by
+// value so that no caller has to spill its Geo to local memory.
+__device__ __forceinline__ void store_images_core(double *__restrict__ f, int nx, int ny, int nz,
+                                                  int NX, int NY, int wall, int I, int J, int K,
+                                                  double v, int stag) {
+  const int Ia = (I == 1) ? nx + 1 : (I == nx) ? 0 : -1;  // nx >= 2: at most one
+  const int Ka = (K == 1) ? nz + 1 : (K == nz) ? 0 : -1;
+  const int Kb = (K == 1 && K == nz) ? 0 : -1;             // nz == 1
   int Ja = -1, Jb = -1, Jc = -1;
   double fa = 0.0, fb = 0.0, fc = 0.0;
-  if (!g.wall) {
-    Ja = (J == 1) ? g.ny + 1 : (J == g.ny) ? 0 : -1;
+  if (!wall) {
+    Ja = (J == 1) ? ny + 1 : (J == ny) ? 0 : -1;
     fa = 1.0;
   } else if (stag == STAG_Y) {
     if (J == 1) { Ja = 0; fa = 0.0; }
-    if (J == g.ny - 1) { Jb = g.ny; fb = 0.0; Jc = g.ny + 1; fc = -1.0; }
+    if (J == ny - 1) { Jb = ny; fb = 0.0; Jc = ny + 1; fc = -1.0; }
   } else {
     const double s = stag == STAG_P ? 1.0 : -1.0;
     if (J == 1) { Ja = 0; fa = s; }
-    if (J == g.ny) { Jb = g.ny + 1; fb = s; }
+    if (J == ny) { Jb = ny + 1; fb = s; }
   }
 #pragma unroll
   for (int zc = 0; zc < 3; zc++) {
@@ -87,17 +89,29 @@ __device__ __forceinline__ void store_img(double *__restrict__ f, const Geo &g, 
       for (int xc = 0; xc < 2; xc++) {
         const int Ix = xc == 0 ? I : Ia;
         if (Ix < 0 || (xc == 0 && yc == 0 && zc == 0)) continue;
-        f[gidx(g, Ix, Jy, Kz)] = vv;
+        f[Ix + NX * (Jy + NY * Kz)] = vv;
       }
     }
   }
 }
 
-// Out-of-line variant for callers that write the interior value themselves
+__device__ __forceinline__ bool img_edge(const Geo &g, int I, int J, int K) {
+  return (I == 1) | (I == g.nx) | (K == 1) | (K == g.nz) | (J == 1) | (J >= g.ny - 1);
+}
+
+__device__ __forceinline__ void store_img(double *__restrict__ f, const Geo &g, int I, int J,
+                                          int K, double v, int stag) {
+  f[gidx(g, I, J, K)] = v;
+  if (!img_edge(g, I, J, K)) return;
+  store_images_core(f, g.nx, g.ny, g.nz, g.NX, g.NY, g.wall, I, J, K, v, stag);
+}
+
+// Out-of-line images for callers that write the interior value themselves
 // and only need the ghost images of edge cells (keeps unrolled loops small).
-__device__ __noinline__ void store_images_of(double *__restrict__ f, const Geo &g, int I, int J,
-                                             int K, double v, int stag) {
-  store_img(f, g, I, J, K, v, stag);
+__device__ __noinline__ void store_images_of(double *__restrict__ f, int nx, int ny, int nz,
+                                             int NX, int NY, int wall, int I, int J, int K,
+                                             double v, int stag) {
+  store_images_core(f, nx, ny, nz, NX, NY, wall, I, J, K, v, stag);
 }
 
 // Cooperative copy loop with B loads in flight per thread: element t of

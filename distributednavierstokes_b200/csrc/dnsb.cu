@@ -699,6 +699,8 @@ int dnsb_create(const dnsb_grid *gr, int device, void *stream, dnsb_ctx **out) {
   const int M = nx / 2;
   if (M > 4096 || nz > 4096 || ny > 4096)
     return fail(nullptr, DNSB_EUNSUP, "FFT lengths above 4096 are not supported");
+  if ((long long)(nx + 2) * (ny + 2) * (nz + 2) >= (1LL << 31))
+    return fail(nullptr, DNSB_EUNSUP, "ghosted fields of 2^31 or more values are not supported");
   dnsb_ctx *c = new dnsb_ctx();
   c->device = device;
   c->stream = (cudaStream_t)stream;

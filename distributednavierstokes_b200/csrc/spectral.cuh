@@ -470,9 +470,9 @@ __global__ void __launch_bounds__(CN_LINES *CN_CHUNKS, 3) k_cn(Geo g, Fields3 ou
   const int set = c == STAG_Y ? 1 : 0;
   const double *v = c == 0 ? V.x : c == 1 ? V.y : V.z;
   double *o = c == 0 ? out.x : c == 1 ? out.y : out.z;
-  const long long sy = g.NX;
+  const int sy = g.NX;
   const bool active = I <= g.nx;
-  const long long base = gidx(g, active ? I : I0, 1, K);
+  const int base = gidx(g, active ? I : I0, 1, K);
   const int s0 = ck * MR;
   // 1. this thread's rows of the right-hand side
   double x[MR];
@@ -555,7 +555,7 @@ __global__ void __launch_bounds__(CN_LINES *CN_CHUNKS, 3) k_cn(Geo g, Fields3 ou
         // ghost images of edge lines and of the first/last rows (the
         // inactive wall face of the normal component has none)
         if ((line_edge || j == 0 || j >= ny - 2) && !(normal_wall && j == ny - 1))
-          store_images_of(o, g, I, j + 1, K, xv, c);
+          store_images_of(o, g.nx, g.ny, g.nz, g.NX, g.NY, g.wall, I, j + 1, K, xv, c);
       }
     }
   }
