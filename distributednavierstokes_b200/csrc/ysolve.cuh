@@ -45,7 +45,7 @@ inline int ythomas_rows(int ny) {
 // the value entering chunk k from above (maps TY_CHUNKS-1..k+1 applied to
 // 0).  Call with all TY_LINES warps of the block, between barriers.
 template <bool REV>
-__device__ __forceinline__ void ythomas_scan(double4 (*m)[TY_LINES]) {
+__device__ __forceinline__ void ythomas_scan(double4 (*m)[TY_LINES + 1]) {
   static_assert(TY_CHUNKS == 32, "one lane per chunk");
   const int tid = threadIdx.x + blockDim.x * threadIdx.y;
   const int w = tid >> 5, lane = tid & 31;
@@ -103,8 +103,10 @@ __global__ void __launch_bounds__(TY_LINES *TY_CHUNKS, MR <= 8 ? 2 : 1)
               const double *__restrict__ ay, const double *__restrict__ by,
               const double *__restrict__ cy, const double *__restrict__ lam1,
               const double *__restrict__ lam3) {
-  __shared__ double4 za[TY_CHUNKS][TY_LINES];  // forward chunk maps (Z.re, Z.im, G)
-  __shared__ double4 yb[TY_CHUNKS][TY_LINES];  // backward chunk maps (Y.re, Y.im, H)
+  // chunk maps, one row of lines per chunk padded by one entry so that the
+  // scan's lane-per-chunk reads spread over all banks
+  __shared__ double4 za[TY_CHUNKS][TY_LINES + 1];  // forward (Z.re, Z.im, G)
+  __shared__ double4 yb[TY_CHUNKS][TY_LINES + 1];  // backward (Y.re, Y.im, H)
   const int i = threadIdx.x, ck = threadIdx.y;
   const int ny = g.ny, nz = g.nz;
   const long long nl = (long long)nz * g.nkx;
