@@ -100,7 +100,7 @@ struct dnsb_ctx {
   int *deverr = nullptr;               // device-side error word (bounded waits)
   int use_tma = 1;                     // persistent TMA-pipelined z-FFT
   int x1 = 0, x2 = 0, z1 = 0, z2 = 0;  // four-step splits of nx/2 and nz (0: generic kernels)
-  int L4x = 16, L4r = 8, L4z = 8;      // lines per CTA: irfft-x, rfft-x, z-FFT
+  int L4z = 8;                         // lines per CTA of the z-FFT
   size_t smem_rx4 = 0, smem_ix4 = 0, smem_z4 = 0;
   int nsm = 148;
   size_t smem_zt = 0;
@@ -407,19 +407,21 @@ int ensure_device(dnsb_ctx *c) {
 }
 
 #define FFT4_SPLITS(X) X(16, 24) X(16, 16) X(16, 12) X(16, 8) X(8, 12) X(8, 8) X(8, 6) X(8, 4)
+constexpr int IRX_L = 16;  // lines per CTA of the four-step inverse x-FFT
+constexpr int RFX_L = 8;   // lines per CTA of the four-step forward x-FFT
 
 // four-step kernel launches for the split chosen at create time
 int launch_rfftx4(dnsb_ctx *c, int mode, const double *a, const double *b, const double *cc) {
   const Geo &g = c->g;
-  dim3 grid(g.ny * ((g.nz + c->L4r - 1) / c->L4r));
+  dim3 grid(g.ny * ((g.nz + RFX_L - 1) / RFX_L));
 #define RF4(A, B)                                                                                  \
   if (c->x1 == A && c->x2 == B) {                                                                  \
     if (mode == RIN_DIVERGENCE)                                                                    \
-      LAUNCH(c, DNSB_KIND_RFFTX, k_rfftx4<A, B, RIN_DIVERGENCE><<<grid, F4_THREADS, c->smem_rx4, c->stream>>>(g, c->S, a, b, cc, c->L4r, c->twM, c->twN)); \
+      LAUNCH(c, DNSB_KIND_RFFTX, k_rfftx4<A, B, RFX_L, RIN_DIVERGENCE><<<grid, F4_THREADS, c->smem_rx4, c->stream>>>(g, c->S, a, b, cc, c->twM, c->twN)); \
     else if (mode == RIN_REAL)                                                                     \
-      LAUNCH(c, DNSB_KIND_RFFTX, k_rfftx4<A, B, RIN_REAL><<<grid, F4_THREADS, c->smem_rx4, c->stream>>>(g, c->S, a, b, cc, c->L4r, c->twM, c->twN)); \
+      LAUNCH(c, DNSB_KIND_RFFTX, k_rfftx4<A, B, RFX_L, RIN_REAL><<<grid, F4_THREADS, c->smem_rx4, c->stream>>>(g, c->S, a, b, cc, c->twM, c->twN)); \
     else                                                                                           \
-      LAUNCH(c, DNSB_KIND_RFFTX, k_rfftx4<A, B, RIN_FIELD><<<grid, F4_THREADS, c->smem_rx4, c->stream>>>(g, c->S, a, b, cc, c->L4r, c->twM, c->twN)); \
+      LAUNCH(c, DNSB_KIND_RFFTX, k_rfftx4<A, B, RFX_L, RIN_FIELD><<<grid, F4_THREADS, c->smem_rx4, c->stream>>>(g, c->S, a, b, cc, c->twM, c->twN)); \
     return 0;                                                                                      \
   }
   FFT4_SPLITS(RF4)
@@ -429,15 +431,15 @@ int launch_rfftx4(dnsb_ctx *c, int mode, const double *a, const double *b, const
 
 int launch_irfftx4(dnsb_ctx *c, int mode, double *out) {
   const Geo &g = c->g;
-  dim3 grid(g.ny * ((g.nz + c->L4x - 1) / c->L4x));
+  dim3 grid(g.ny * ((g.nz + IRX_L - 1) / IRX_L));
 #define IF4(A, B)                                                                                  \
   if (c->x1 == A && c->x2 == B) {                                                                  \
     if (mode == ROUT_INTERIOR)                                                                     \
-      LAUNCH(c, DNSB_KIND_IRFFTX, k_irfftx4<A, B, ROUT_INTERIOR><<<grid, F4_THREADS, c->smem_ix4, c->stream>>>(g, c->S, out, c->L4x, c->twM, c->twN)); \
+      LAUNCH(c, DNSB_KIND_IRFFTX, k_irfftx4<A, B, IRX_L, ROUT_INTERIOR><<<grid, F4_THREADS, c->smem_ix4, c->stream>>>(g, c->S, out, c->twM, c->twN)); \
     else if (mode == ROUT_IMAGES)                                                                  \
-      LAUNCH(c, DNSB_KIND_IRFFTX, k_irfftx4<A, B, ROUT_IMAGES><<<grid, F4_THREADS, c->smem_ix4, c->stream>>>(g, c->S, out, c->L4x, c->twM, c->twN)); \
+      LAUNCH(c, DNSB_KIND_IRFFTX, k_irfftx4<A, B, IRX_L, ROUT_IMAGES><<<grid, F4_THREADS, c->smem_ix4, c->stream>>>(g, c->S, out, c->twM, c->twN)); \
     else                                                                                           \
-      LAUNCH(c, DNSB_KIND_IRFFTX, k_irfftx4<A, B, ROUT_REAL><<<grid, F4_THREADS, c->smem_ix4, c->stream>>>(g, c->S, out, c->L4x, c->twM, c->twN)); \
+      LAUNCH(c, DNSB_KIND_IRFFTX, k_irfftx4<A, B, IRX_L, ROUT_REAL><<<grid, F4_THREADS, c->smem_ix4, c->stream>>>(g, c->S, out, c->twM, c->twN)); \
     return 0;                                                                                      \
   }
   FFT4_SPLITS(IF4)
@@ -464,12 +466,12 @@ int launch_fftz4(dnsb_ctx *c, bool inv) {
 template <int A, int B>
 int allow_fft4(dnsb_ctx *c) {
   int rc;
-  if ((rc = allow_smem(c, k_rfftx4<A, B, RIN_DIVERGENCE>, c->smem_rx4)) ||
-      (rc = allow_smem(c, k_rfftx4<A, B, RIN_REAL>, c->smem_rx4)) ||
-      (rc = allow_smem(c, k_rfftx4<A, B, RIN_FIELD>, c->smem_rx4)) ||
-      (rc = allow_smem(c, k_irfftx4<A, B, ROUT_INTERIOR>, c->smem_ix4)) ||
-      (rc = allow_smem(c, k_irfftx4<A, B, ROUT_IMAGES>, c->smem_ix4)) ||
-      (rc = allow_smem(c, k_irfftx4<A, B, ROUT_REAL>, c->smem_ix4)) ||
+  if ((rc = allow_smem(c, k_rfftx4<A, B, RFX_L, RIN_DIVERGENCE>, c->smem_rx4)) ||
+      (rc = allow_smem(c, k_rfftx4<A, B, RFX_L, RIN_REAL>, c->smem_rx4)) ||
+      (rc = allow_smem(c, k_rfftx4<A, B, RFX_L, RIN_FIELD>, c->smem_rx4)) ||
+      (rc = allow_smem(c, k_irfftx4<A, B, IRX_L, ROUT_INTERIOR>, c->smem_ix4)) ||
+      (rc = allow_smem(c, k_irfftx4<A, B, IRX_L, ROUT_IMAGES>, c->smem_ix4)) ||
+      (rc = allow_smem(c, k_irfftx4<A, B, IRX_L, ROUT_REAL>, c->smem_ix4)) ||
       (rc = allow_smem(c, k_fftz4<A, B, false>, c->smem_z4)) ||
       (rc = allow_smem(c, k_fftz4<A, B, true>, c->smem_z4)))
     return rc;
@@ -830,15 +832,13 @@ int dnsb_create(const dnsb_grid *gr, int device, void *stream, dnsb_ctx **out) {
   // four-step kernels for the lengths with a register split (DNSB_FFT4=0: off)
   if (envint("DNSB_FFT4", 1) != 0) {
     int a = 0, b = 0;
-    c->L4x = std::max(1, std::min(envint("DNSB_L4X", 16), nz));
-    c->L4r = std::max(1, std::min(envint("DNSB_L4R", 8), nz));
     c->L4z = std::max(1, envint("DNSB_L4Z", 8));
     if (fft4_split(M, a, b)) {
       c->x1 = a;
       c->x2 = b;
       const size_t pitch = b % 2 == 0 ? b + 1 : b;
-      c->smem_rx4 = sizeof(double2) * ((size_t)c->L4r * a * pitch + (size_t)c->L4r * (M + 1) + M + (M + 1));
-      c->smem_ix4 = sizeof(double2) * ((size_t)c->L4x * (M + 2) + (size_t)c->L4x * a * pitch + M + (M + 1));
+      c->smem_rx4 = sizeof(double2) * ((size_t)RFX_L * a * pitch + (size_t)RFX_L * (M + 1) + M + (M + 1));
+      c->smem_ix4 = sizeof(double2) * ((size_t)IRX_L * (M + 2) + (size_t)IRX_L * a * pitch + M + (M + 1));
     }
     if (fft4_split(nz, a, b)) {
       c->z1 = a;
@@ -847,8 +847,7 @@ int dnsb_create(const dnsb_grid *gr, int device, void *stream, dnsb_ctx **out) {
     }
   }
   // the persistent TMA-pipelined z-FFT is opt-in: at the production size the
-  // non-persistent kernel with more CTAs per SM is faster (the transform is
-  // shared-memory bound)
+  // non-persistent kernel with more CTAs per SM is faster
   c->use_tma = envint("DNSB_TMA", 0) != 0 && c->smem_zt <= 200 * 1024;
   {
     int dev = 0, nsm = 0;

@@ -41,11 +41,11 @@ __global__ void __launch_bounds__(F4_THREADS, 2) k_fftz4(Geo g, double2 *__restr
 // z[m] = r[2m] + i r[2m+1] (r = divergence of in0..in2, a ghost-free real
 // array, or a field's interior) is first staged in shared memory by all
 // threads with batched loads, then transformed.  M = N1*N2 = nx/2.
-template <int N1, int N2, int INMODE>
+template <int N1, int N2, int L, int INMODE>
 __global__ void __launch_bounds__(F4_THREADS, 2) k_rfftx4(Geo g, double2 *__restrict__ S,
                                                           const double *__restrict__ in0,
                                                           const double *__restrict__ in1,
-                                                          const double *__restrict__ in2, int L,
+                                                          const double *__restrict__ in2,
                                                           const double2 *__restrict__ twM,
                                                           const double2 *__restrict__ twN) {
   constexpr int M = N1 * N2;
@@ -75,7 +75,7 @@ __global__ void __launch_bounds__(F4_THREADS, 2) k_rfftx4(Geo g, double2 *__rest
             const double *row = in0 + (long long)g.nx * (j + (long long)g.ny * k);
             z = __ldg(reinterpret_cast<const double2 *>(row + 2 * m));
           } else {
-            const long long c0 = gidx(g, 2 * m + 1, J, k + 1);
+            const int c0 = gidx(g, 2 * m + 1, J, k + 1);
             if (INMODE == RIN_FIELD) {
               z = make_double2(__ldg(in0 + c0), __ldg(in0 + c0 + 1));
             } else {
@@ -102,8 +102,9 @@ __global__ void __launch_bounds__(F4_THREADS, 2) k_rfftx4(Geo g, double2 *__rest
                             [&](int l, int e, double2 v) { res[l * ls + e] = v; }, buf, L, tw);
   // post-process (X = E + w^k O) and store S(kx, j, k0 + l), l fastest
   const int Lv = min(L, g.nz - k0);
-  for (int t = threadIdx.x; t < Lv * (M + 1); t += blockDim.x) {
-    const int kx = t / Lv, l = t - kx * Lv;
+  for (int t = threadIdx.x; t < L * (M + 1); t += blockDim.x) {
+    const int kx = t / L, l = t - kx * L;
+    if (l >= Lv) continue;
     const double2 zk = res[l * ls + (kx == M ? 0 : kx)];
     const double2 zc = cconj(res[l * ls + (kx == 0 ? 0 : M - kx)]);
     const double2 e = make_double2(0.5 * (zk.x + zc.x), 0.5 * (zk.y + zc.y));
@@ -113,39 +114,16 @@ __global__ void __launch_bounds__(F4_THREADS, 2) k_rfftx4(Geo g, double2 *__rest
   }
 }
 
-// Inverse real FFT along x (see k_irfftx): pre-processing of the pairs
-// (k, M-k) in shared memory, then the four-step inverse whose step 2 writes
-// the field (OUTMODE as in k_irfftx).
+// Inverse real FFT along x of one tile (see k_irfftx): the L lines
+// (row j, kz = k0..k0+L-1; Lv valid) of X are in zb (pitch M+2).  The pairs
+// (k, M-k) are pre-processed in place, then the four-step inverse writes
+// the field in its step 2 (OUTMODE as in k_irfftx).  Ends with a barrier.
 template <int N1, int N2, int OUTMODE>
-__global__ void __launch_bounds__(F4_THREADS, 2) k_irfftx4(Geo g, const double2 *__restrict__ S,
-                                                           double *__restrict__ out, int L,
-                                                           const double2 *__restrict__ twM,
-                                                           const double2 *__restrict__ twN) {
+__device__ __forceinline__ void irfftx4_tile(const Geo &g, double2 *zb, int L, int Lv, int j,
+                                             int k0, double *__restrict__ out, double2 *buf,
+                                             const double2 *tw, const double2 *tn) {
   constexpr int M = N1 * N2;
   constexpr int ls = M + 2;
-  extern __shared__ double2 smem[];
-  double2 *zb = smem;
-  double2 *buf = zb + L * ls;
-  double2 *tw = buf + fft4_buf<N1, N2>(L);
-  double2 *tn = tw + M;
-  const int ngrp = (g.nz + L - 1) / L;
-  const int grp = blockIdx.x % ngrp;
-  const int j = blockIdx.x / ngrp;
-  const int k0 = grp * L;
-  const int Lv = min(L, g.nz - k0);
-  for (int t = threadIdx.x; t < M; t += blockDim.x) tw[t] = twM[t];
-  for (int t = threadIdx.x; t <= M; t += blockDim.x) tn[t] = twN[t];
-  batched_copy<8>(
-      L * (M + 1),
-      [&](int t) {
-        const int kx = t / L, l = t - kx * L;
-        return l < Lv ? S[sidx(g, kx, j, k0 + l)] : make_double2(0.0, 0.0);
-      },
-      [&](int t, double2 v) {
-        const int kx = t / L, l = t - kx * L;
-        zb[l * ls + kx] = v;
-      });
-  __syncthreads();
   // Z[k] = E[k] + i O[k], E = (X[k] + conj X[M-k])/2,
   // O = (X[k] - conj X[M-k]) conj(w^k)/2; one thread per pair (k, M-k)
   constexpr int half = M / 2 + 1;
@@ -175,6 +153,11 @@ __global__ void __launch_bounds__(F4_THREADS, 2) k_irfftx4(Geo g, const double2 
   __syncthreads();
   const double sc = 1.0 / M;
   const int J = j + 1;
+  const bool row_edge = (J == 1) | (J >= g.ny - 1);
+  auto line_edge = [&](int l) {
+    const int K = k0 + l + 1;
+    return row_edge | (K == 1) | (K == g.nz);
+  };
   fft4_lines<N1, N2, true>(
       [&](int l, int e) { return zb[l * ls + e]; },
       [&](int l, int m, double2 z) {
@@ -185,15 +168,55 @@ __global__ void __launch_bounds__(F4_THREADS, 2) k_irfftx4(Geo g, const double2 
           double *row = out + (long long)g.nx * (j + (long long)g.ny * (K - 1));
           *reinterpret_cast<double2 *>(row + 2 * m) = make_double2(x0, x1);
         } else if (OUTMODE == ROUT_INTERIOR) {
-          const long long c0 = gidx(g, 2 * m + 1, J, K);
+          const int c0 = gidx(g, 2 * m + 1, J, K);
           out[c0] = x0;
           out[c0 + 1] = x1;
         } else {
-          store_img(out, g, 2 * m + 1, J, K, x0, STAG_P);
-          store_img(out, g, 2 * m + 2, J, K, x1, STAG_P);
+          // ghost images only on edge lines and at the two ends of a line
+          const int c0 = gidx(g, 2 * m + 1, J, K);
+          out[c0] = x0;
+          out[c0 + 1] = x1;
+          if (line_edge(l) | (m == 0) | (m == M - 1)) {
+            store_images_core(out, g.nx, g.ny, g.nz, g.NX, g.NY, g.wall, 2 * m + 1, J, K, x0, STAG_P);
+            store_images_core(out, g.nx, g.ny, g.nz, g.NX, g.NY, g.wall, 2 * m + 2, J, K, x1, STAG_P);
+          }
         }
       },
       buf, L, tw);
+}
+
+// Inverse real FFT along x, one tile of L lines per CTA.
+template <int N1, int N2, int L, int OUTMODE>
+__global__ void __launch_bounds__(F4_THREADS, 2) k_irfftx4(Geo g, const double2 *__restrict__ S,
+                                                           double *__restrict__ out,
+                                                           const double2 *__restrict__ twM,
+                                                           const double2 *__restrict__ twN) {
+  constexpr int M = N1 * N2;
+  constexpr int ls = M + 2;
+  extern __shared__ double2 smem[];
+  double2 *zb = smem;
+  double2 *buf = zb + L * ls;
+  double2 *tw = buf + fft4_buf<N1, N2>(L);
+  double2 *tn = tw + M;
+  const int ngrp = (g.nz + L - 1) / L;
+  const int grp = blockIdx.x % ngrp;
+  const int j = blockIdx.x / ngrp;
+  const int k0 = grp * L;
+  const int Lv = min(L, g.nz - k0);
+  for (int t = threadIdx.x; t < M; t += blockDim.x) tw[t] = twM[t];
+  for (int t = threadIdx.x; t <= M; t += blockDim.x) tn[t] = twN[t];
+  batched_copy<8>(
+      L * (M + 1),
+      [&](int t) {
+        const int kx = t / L, l = t - kx * L;
+        return l < Lv ? S[sidx(g, kx, j, k0 + l)] : make_double2(0.0, 0.0);
+      },
+      [&](int t, double2 v) {
+        const int kx = t / L, l = t - kx * L;
+        zb[l * ls + kx] = v;
+      });
+  __syncthreads();
+  irfftx4_tile<N1, N2, OUTMODE>(g, zb, L, Lv, j, k0, out, buf, tw, tn);
 }
 
 }  // namespace dnsb
