@@ -80,6 +80,7 @@ struct dnsb_ctx {
   double *lam1 = nullptr, *lam2 = nullptr, *lam3 = nullptr;
   double *ay = nullptr, *by = nullptr, *cy = nullptr;
   double *ycoef = nullptr;  // [at bt ct an bn cn] x ny
+  double2 *ymet = nullptr;  // YMET packed per-row metrics of the momentum stencil
   double *ytab = nullptr;   // [3 stages][2 sets][ta cp ib] x ny
   double2 *twM = nullptr, *twN = nullptr, *twz = nullptr, *twy = nullptr;
   FFTPlan pM{}, pz{}, py{};
@@ -596,7 +597,7 @@ int do_step(dnsb_ctx *c, double *ux, double *uy, double *uz, double *p, double *
       LAUNCH(c, DNSB_KIND_MOMENTUM,
              k_momentum<MOM_EXPLICIT><<<c->cgrid, c->cblock, 0, c->stream>>>(
                  g, ff(qx, qy, qz), cf(ux, uy, uz), ff(c->W[0], c->W[1], c->W[2]), nullptr, A, dt,
-                 B, 0.0, readq, nullptr, 0.0));
+                 B, 0.0, readq, c->ymet, 0.0));
       if ((rc = launch_rfftx(c, RIN_DIVERGENCE, c->W[0], c->W[1], c->W[2]))) return rc;
       if ((rc = poisson_from_spectrum(c, ROUT_IMAGES, p))) return rc;
       LAUNCH(c, DNSB_KIND_GRAD,
@@ -608,7 +609,7 @@ int do_step(dnsb_ctx *c, double *ux, double *uy, double *uz, double *p, double *
       LAUNCH(c, DNSB_KIND_MOMENTUM,
              k_momentum<MOM_IMPLICIT><<<c->cgrid, c->cblock, 0, c->stream>>>(
                  g, ff(qx, qy, qz), cf(ux, uy, uz), ff(c->V[0], c->V[1], c->V[2]), p, A, dt, B,
-                 adt, readq, c->ycoef, th));
+                 adt, readq, c->ymet, th));
       LAUNCH(c, DNSB_KIND_CN,
              launch_cn(c, ff(ux, uy, uz), cf(c->V[0], c->V[1], c->V[2]),
                        c->ytab + (long long)s * 2 * cn_tab_stride(g.ny)));
@@ -784,6 +785,17 @@ int dnsb_create(const dnsb_grid *gr, int device, void *stream, dnsb_ctx **out) {
     cn[j - 1] = j == ny - 1 ? 0.0 : cc;
     bn[j - 1] = -(a + cc);
   }
+  std::vector<double2> ym((size_t)YMET * (ny + 2), make_double2(0.0, 0.0));
+  for (int J = 1; J <= ny; J++) {
+    const int j = J - 1;
+    double2 *r = ym.data() + (size_t)YMET * J;
+    r[0] = make_double2(dy[J], dy[J + 1]);
+    r[1] = make_double2(1.0 / dy[J], 1.0 / dy[J + 1]);
+    r[2] = make_double2(1.0 / dyu[J], 1.0 / dyu[J - 1]);
+    r[3] = make_double2(at[j], bt[j]);
+    r[4] = make_double2(ct[j], an[j]);
+    r[5] = make_double2(bn[j], cn[j]);
+  }
   std::vector<double2> twM(M), twN(M + 1), twz(nz), twy(ny);
   for (int t = 0; t < M; t++) twM[t] = unit_root(t, M);
   for (int t = 0; t <= M; t++) twN[t] = unit_root(t, nx);
@@ -792,7 +804,8 @@ int dnsb_create(const dnsb_grid *gr, int device, void *stream, dnsb_ctx **out) {
   if ((rc = upload(c, &c->lam1, lam1)) || (rc = upload(c, &c->lam2, lam2)) ||
       (rc = upload(c, &c->lam3, lam3)) || (rc = upload(c, &c->ay, ay)) ||
       (rc = upload(c, &c->by, by)) || (rc = upload(c, &c->cy, cy)) ||
-      (rc = upload(c, &c->ycoef, yc)) || (rc = upload(c, &c->twM, twM)) ||
+      (rc = upload(c, &c->ycoef, yc)) || (rc = upload(c, &c->ymet, ym)) ||
+      (rc = upload(c, &c->twM, twM)) ||
       (rc = upload(c, &c->twN, twN)) || (rc = upload(c, &c->twz, twz)) ||
       (rc = upload(c, &c->twy, twy)))
     return bail(rc);
@@ -968,7 +981,7 @@ int dnsb_momentum(dnsb_ctx *c, double *qx, double *qy, double *qz, const double 
   if (ensure_device(c)) return DNSB_ECUDA;
   k_momentum<MOM_ONLY><<<cell_grid(c->g), cell_block, 0, c->stream>>>(
       c->g, ff(qx, qy, qz), cf(ux, uy, uz), ff(nullptr, nullptr, nullptr), nullptr, A, dt, 0.0,
-      0.0, 1, nullptr, 0.0);
+      0.0, 1, c->ymet, 0.0);
   CKL(c);
   return 0;
 }
@@ -1008,7 +1021,7 @@ int dnsb_imex_update(dnsb_ctx *c, double *ux, double *uy, double *uz, const doub
   const double adt = alpha * dt;
   const double th = alpha * dt * g.visc / 2;
   k_vupdate<<<cell_grid(g), cell_block, 0, c->stream>>>(
-      g, ff(c->V[0], c->V[1], c->V[2]), cf(ux, uy, uz), cf(qx, qy, qz), p, B, adt, c->ycoef, th);
+      g, ff(c->V[0], c->V[1], c->V[2]), cf(ux, uy, uz), cf(qx, qy, qz), p, B, adt, c->ymet, th);
   CKL(c);
   // tables for this alpha in stage slot 0
   k_cn_tables<<<1, 32, 0, c->stream>>>(g.ny, c->cn_mr, CN_CHUNKS, c->ycoef, c->ytab, dt, g.visc,

@@ -16,18 +16,19 @@ namespace dnsb {
 
 enum MomMode { MOM_ONLY = 0, MOM_EXPLICIT = 1, MOM_IMPLICIT = 2 };
 
+// Per-row metrics of the momentum stencil, packed for 16-byte loads:
+// ymet[6 J + 0..5] = (dy_J, dy_{J+1}), (1/dy_J, 1/dy_{J+1}),
+// (1/dyu_J, 1/dyu_{J-1}), (at, bt), (ct, an), (bn, cn) of row j = J-1 of
+// the Crank-Nicolson operator (ydiffusion_coefficients, src/ydiffusion.jl:31-51).
+constexpr int YMET = 6;
+
 // Right-hand side of the Crank-Nicolson row j = J-1 of one component
 // (imexrhs_kernel!, src/ydiffusion.jl:71-91): v + theta (a u_S + b u_0 +
-// c u_N) with the wall rows folded into the coefficients (a_0 = 0,
-// c_{ny-1} = 0); abc points at the component set's [a | b | c] rows.
-__device__ __forceinline__ double cn_rhs(const double *__restrict__ abc, int ny, int j, double v,
-                                         double theta, double uS, double u0, double uN) {
-  const double a = __ldg(abc + j), b = __ldg(abc + ny + j), c = __ldg(abc + 2 * ny + j);
-  double sum;
-  if (j == 0) sum = b * u0 + (ny > 1 ? c * uN : 0.0);
-  else if (j == ny - 1) sum = a * uS + b * u0;
-  else sum = (a * uS + b * u0) + c * uN;
-  return v + theta * sum;
+// c u_N), the wall rows folded into the coefficients (a_0 = 0 and
+// c_{ny-1} = 0 multiply finite ghost values).
+__device__ __forceinline__ double cn_rhs(double a, double b, double c, double v, double theta,
+                                         double uS, double u0, double uN) {
+  return v + theta * ((a * uS + b * u0) + c * uN);
 }
 
 // momentum_kernel! (src/operators.jl:44-145) at one interior cell: loads
@@ -45,7 +46,7 @@ template <int MODE>
 __device__ __forceinline__ MomCell momentum_cell(const Geo &g, int I, int J, int K, const Fields3 &q,
                                                  const CFields3 &u, const double *__restrict__ p,
                                                  double A, double dt, double B, double adt,
-                                                 int readq, const double *__restrict__ coef,
+                                                 int readq, const double2 *__restrict__ ymet,
                                                  double theta) {
   // 64-bit offsets here: measured faster than 32-bit ones for this kernel
   const long long sy = g.NX, sz = (long long)g.NX * g.NY;
@@ -75,21 +76,23 @@ __device__ __forceinline__ MomCell momentum_cell(const Geo &g, int I, int J, int
     pN = __ldg(p + c0 + sy);
     pT = __ldg(p + c0 + sz);
   }
-  const double dyJ = __ldg(g.dy + J), dyJ1 = __ldg(g.dy + J + 1);
-  const double rdyJ = __ldg(g.rdy + J), rdyJ1 = __ldg(g.rdy + J + 1);
-  const double rdyuJ = __ldg(g.rdyu + J), rdyuJm = __ldg(g.rdyu + J - 1);
+  const double2 *ym = ymet + YMET * J;
+  const double2 m0 = __ldg(ym), m1 = __ldg(ym + 1), m2 = __ldg(ym + 2);
+  const double dyJ = m0.x, dyJ1 = m0.y, rdyJ = m1.x, rdyJ1 = m1.y, rdyuJ = m2.x, rdyuJm = m2.y;
   const double ey = g.epsy, nu = g.visc;
-
+  // The convective products are formed from unhalved midpoint sums and the
+  // flux divergence is scaled by 1/4 once: scaling by powers of two is
+  // exact, so this equals the reference's halved-midpoint form.
   MomCell m;
   // x momentum, at the right x-face of cell (I, J, K)
   {
-    const double uce = 0.5 * (ux0 + uxE), ucw = 0.5 * (uxW + ux0);
-    const double vn = 0.5 * (uy0 + uyE), un = 0.5 * (ux0 + uxN);
-    const double vs = 0.5 * (uyS + uySE), us = 0.5 * (uxS + ux0);
-    const double wt = 0.5 * (uz0 + uzE), ut = 0.5 * (ux0 + uxT);
-    const double wb = 0.5 * (uzB + uzEB), ub = 0.5 * (uxB + ux0);
-    const double conv = (uce * uce - ucw * ucw) * g.rdx + (vn * un - vs * us) * rdyJ +
-                        (wt * ut - wb * ub) * g.rdz;
+    const double uce = ux0 + uxE, ucw = uxW + ux0;
+    const double vn = uy0 + uyE, un = ux0 + uxN;
+    const double vs = uyS + uySE, us = uxS + ux0;
+    const double wt = uz0 + uzE, ut = ux0 + uxT;
+    const double wb = uzB + uzEB, ub = uxB + ux0;
+    const double conv = 0.25 * ((uce * uce - ucw * ucw) * g.rdx + (vn * un - vs * us) * rdyJ +
+                                (wt * ut - wb * ub) * g.rdz);
     const double diff = (uxE - 2 * ux0 + uxW) * g.rdx2 +
                         ey * ((uxN - ux0) * rdyuJ - (ux0 - uxS) * rdyuJm) * rdyJ +
                         (uxT - 2 * ux0 + uxB) * g.rdz2;
@@ -99,20 +102,20 @@ __device__ __forceinline__ MomCell momentum_cell(const Geo &g, int I, int J, int
       m.vx = ux0 + B * m.qx;  // u <- u + B q on ranges[c] (timestep.jl:54-58)
     } else {
       // v = u + B q - alpha dt grad p (ydiffusion.jl:133-135)
-      m.vx = cn_rhs(coef, g.ny, J - 1, (ux0 + B * m.qx) - adt * (pE - p0) * g.rdx, theta, uxS,
-                    ux0, uxN);
+      const double2 m3 = __ldg(ym + 3), m4 = __ldg(ym + 4);
+      m.vx = cn_rhs(m3.x, m3.y, m4.x, (ux0 + B * m.qx) - adt * (pE - p0) * g.rdx, theta, uxS, ux0,
+                    uxN);
     }
   }
   // y momentum, at the top y-face; Delta-y weighted transporters
   {
-    const double h = 0.5 * rdyuJ;
-    const double ue = (ux0 * dyJ + uxN * dyJ1) * h, ve = 0.5 * (uy0 + uyE);
-    const double uw = (uxW * dyJ + uxWN * dyJ1) * h, vw = 0.5 * (uyW + uy0);
-    const double vcn = 0.5 * (uy0 + uyN), vcs = 0.5 * (uyS + uy0);
-    const double wtv = (uz0 * dyJ + uzN * dyJ1) * h, vt = 0.5 * (uy0 + uyT);
-    const double wbv = (uzB * dyJ + uzNB * dyJ1) * h, vb = 0.5 * (uyB + uy0);
-    const double conv = (ue * ve - uw * vw) * g.rdx + (vcn * vcn - vcs * vcs) * rdyuJ +
-                        (wtv * vt - wbv * vb) * g.rdz;
+    const double ue = (ux0 * dyJ + uxN * dyJ1) * rdyuJ, ve = uy0 + uyE;
+    const double uw = (uxW * dyJ + uxWN * dyJ1) * rdyuJ, vw = uyW + uy0;
+    const double vcn = uy0 + uyN, vcs = uyS + uy0;
+    const double wtv = (uz0 * dyJ + uzN * dyJ1) * rdyuJ, vt = uy0 + uyT;
+    const double wbv = (uzB * dyJ + uzNB * dyJ1) * rdyuJ, vb = uyB + uy0;
+    const double conv = 0.25 * ((ue * ve - uw * vw) * g.rdx + (vcn * vcn - vcs * vcs) * rdyuJ +
+                                (wtv * vt - wbv * vb) * g.rdz);
     const double diff = (uyE - 2 * uy0 + uyW) * g.rdx2 +
                         ey * ((uyN - uy0) * rdyJ1 - (uy0 - uyS) * rdyJ) * rdyuJ +
                         (uyT - 2 * uy0 + uyB) * g.rdz2;
@@ -123,18 +126,19 @@ __device__ __forceinline__ MomCell momentum_cell(const Geo &g, int I, int J, int
       m.vy = yact ? uy0 + B * m.qy : uy0;
     } else {
       const double v = yact ? (uy0 + B * m.qy) - adt * (pN - p0) * rdyuJ : uy0;
-      m.vy = cn_rhs(coef + 3 * g.ny, g.ny, J - 1, v, theta, uyS, uy0, uyN);
+      const double2 m4 = __ldg(ym + 4), m5 = __ldg(ym + 5);
+      m.vy = cn_rhs(m4.y, m5.x, m5.y, v, theta, uyS, uy0, uyN);
     }
   }
   // z momentum, at the back z-face
   {
-    const double ue = 0.5 * (ux0 + uxT), we = 0.5 * (uz0 + uzE);
-    const double uw = 0.5 * (uxW + uxWT), ww = 0.5 * (uzW + uz0);
-    const double vnw = 0.5 * (uy0 + uyT), wn = 0.5 * (uz0 + uzN);
-    const double vsw = 0.5 * (uyS + uyST), ws = 0.5 * (uzS + uz0);
-    const double wct = 0.5 * (uz0 + uzT), wcb = 0.5 * (uzB + uz0);
-    const double conv = (ue * we - uw * ww) * g.rdx + (vnw * wn - vsw * ws) * rdyJ +
-                        (wct * wct - wcb * wcb) * g.rdz;
+    const double ue = ux0 + uxT, we = uz0 + uzE;
+    const double uw = uxW + uxWT, ww = uzW + uz0;
+    const double vnw = uy0 + uyT, wn = uz0 + uzN;
+    const double vsw = uyS + uyST, ws = uzS + uz0;
+    const double wct = uz0 + uzT, wcb = uzB + uz0;
+    const double conv = 0.25 * ((ue * we - uw * ww) * g.rdx + (vnw * wn - vsw * ws) * rdyJ +
+                                (wct * wct - wcb * wcb) * g.rdz);
     const double diff = (uzE - 2 * uz0 + uzW) * g.rdx2 +
                         ey * ((uzN - uz0) * rdyuJ - (uz0 - uzS) * rdyuJm) * rdyJ +
                         (uzT - 2 * uz0 + uzB) * g.rdz2;
@@ -143,8 +147,9 @@ __device__ __forceinline__ MomCell momentum_cell(const Geo &g, int I, int J, int
     if (MODE == MOM_EXPLICIT) {
       m.vz = uz0 + B * m.qz;
     } else {
-      m.vz = cn_rhs(coef, g.ny, J - 1, (uz0 + B * m.qz) - adt * (pT - p0) * g.rdz, theta, uzS,
-                    uz0, uzN);
+      const double2 m3 = __ldg(ym + 3), m4 = __ldg(ym + 4);
+      m.vz = cn_rhs(m3.x, m3.y, m4.x, (uz0 + B * m.qz) - adt * (pT - p0) * g.rdz, theta, uzS, uz0,
+                    uzN);
     }
   }
   return m;
@@ -156,20 +161,20 @@ __device__ __forceinline__ MomCell momentum_cell(const Geo &g, int I, int J, int
 // MOM_IMPLICIT: also the Crank-Nicolson right-hand side
 //   V_c = (u_c + B q_c - adt d_c p) + theta Dy u_c
 // (coef = [at bt ct an bn cn] rows of ny), so the y-solve reads only V.
-// Implicit mode holds all 34 loads plus the coefficient rows: 2 CTAs of 256
-// per SM keep it free of spills (measured faster than 3-4 CTAs with spills).
+// All 34 loads are held at once: 2 CTAs of 256 per SM keep the kernel free
+// of spills (measured faster than 3-4 CTAs with spills).
 template <int MODE>
-__global__ void __launch_bounds__(256, MODE == MOM_IMPLICIT ? 2 : 4) k_momentum(Geo g, Fields3 q, CFields3 u, Fields3 out,
+__global__ void __launch_bounds__(256, 2) k_momentum(Geo g, Fields3 q, CFields3 u, Fields3 out,
                                                   const double *__restrict__ p, double A, double dt,
                                                   double B, double adt, int readq,
-                                                  const double *__restrict__ coef, double theta) {
+                                                  const double2 *__restrict__ ymet, double theta) {
   const int I = blockIdx.x * blockDim.x + threadIdx.x + 1;
   const int J = blockIdx.y * blockDim.y + threadIdx.y + 1;
   const int K = blockIdx.z + 1;
   if (I > g.nx || J > g.ny) return;
   const int c0 = gidx(g, I, J, K);
   const MomCell m = momentum_cell<MODE == MOM_ONLY ? MOM_EXPLICIT : MODE>(
-      g, I, J, K, q, u, p, A, dt, B, adt, readq, coef, theta);
+      g, I, J, K, q, u, p, A, dt, B, adt, readq, ymet, theta);
   const bool yact = J <= g.jymax;
   q.x[c0] = m.qx;
   if (yact) q.y[c0] = m.qy;
@@ -267,7 +272,7 @@ __global__ void k_pgrad(Geo g, double *phi, const double *__restrict__ p, int c,
 // half of imex_update!, src/ydiffusion.jl:133-135), writing into V the
 // Crank-Nicolson right-hand side v + theta Dy u^n (see cn_rhs).
 __global__ void k_vupdate(Geo g, Fields3 V, CFields3 u, CFields3 q, const double *__restrict__ p,
-                          double B, double adt, const double *__restrict__ coef, double theta) {
+                          double B, double adt, const double2 *__restrict__ ymet, double theta) {
   const int I = blockIdx.x * blockDim.x + threadIdx.x + 1;
   const int J = blockIdx.y * blockDim.y + threadIdx.y + 1;
   const int K = blockIdx.z + 1;
@@ -280,10 +285,11 @@ __global__ void k_vupdate(Geo g, Fields3 V, CFields3 u, CFields3 q, const double
   const double vy = J <= g.jymax ? (uy0 + B * q.y[c0]) - adt * (p[c0 + sy] - p0) * __ldg(g.rdyu + J)
                                  : uy0;
   const double vz = (uz0 + B * q.z[c0]) - adt * (p[c0 + sz] - p0) * g.rdz;
-  const int ny = g.ny, j = J - 1;
-  V.x[c0] = cn_rhs(coef, ny, j, vx, theta, u.x[c0 - sy], ux0, u.x[c0 + sy]);
-  V.y[c0] = cn_rhs(coef + 3 * ny, ny, j, vy, theta, u.y[c0 - sy], uy0, u.y[c0 + sy]);
-  V.z[c0] = cn_rhs(coef, ny, j, vz, theta, u.z[c0 - sy], uz0, u.z[c0 + sy]);
+  const double2 *ym = ymet + YMET * J;
+  const double2 m3 = ym[3], m4 = ym[4], m5 = ym[5];
+  V.x[c0] = cn_rhs(m3.x, m3.y, m4.x, vx, theta, u.x[c0 - sy], ux0, u.x[c0 + sy]);
+  V.y[c0] = cn_rhs(m4.y, m5.x, m5.y, vy, theta, u.y[c0 - sy], uy0, u.y[c0 + sy]);
+  V.z[c0] = cn_rhs(m3.x, m3.y, m4.x, vz, theta, u.z[c0 - sy], uz0, u.z[c0 + sy]);
 }
 
 // divergence_kernel! (src/operators.jl:10-26) into the ghost-free r.
