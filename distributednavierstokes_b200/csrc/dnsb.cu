@@ -587,7 +587,7 @@ int do_step(dnsb_ctx *c, double *ux, double *uy, double *uz, double *p, double *
   CK(c, cudaMemsetAsync(c->umax, 0, 3 * UMAX_SLOTS * sizeof(unsigned long long), c->stream));
   if (c->implicit)
     LAUNCH(c, DNSB_KIND_OTHER,
-           k_cn_tables<<<1, 32, 0, c->stream>>>(g.ny, c->cn_mr, CN_CHUNKS, c->ycoef, c->ytab, dt,
+           k_cn_tables<<<1, CN_TABLE_THREADS, 0, c->stream>>>(g.ny, c->cn_mr, CN_CHUNKS, c->ycoef, c->ytab, dt,
                                                 g.visc, RK_AL[0], RK_AL[1], RK_AL[2]));
   for (int s = 0; s < 3; s++) {
     const double A = RK_A[s], B = RK_B[s], al = RK_AL[s];
@@ -1024,7 +1024,7 @@ int dnsb_imex_update(dnsb_ctx *c, double *ux, double *uy, double *uz, const doub
       g, ff(c->V[0], c->V[1], c->V[2]), cf(ux, uy, uz), cf(qx, qy, qz), p, B, adt, c->ymet, th);
   CKL(c);
   // tables for this alpha in stage slot 0
-  k_cn_tables<<<1, 32, 0, c->stream>>>(g.ny, c->cn_mr, CN_CHUNKS, c->ycoef, c->ytab, dt, g.visc,
+  k_cn_tables<<<1, CN_TABLE_THREADS, 0, c->stream>>>(g.ny, c->cn_mr, CN_CHUNKS, c->ycoef, c->ytab, dt, g.visc,
                                        alpha, alpha, alpha);
   CKL(c);
   launch_cn(c, ff(ux, uy, uz), cf(c->V[0], c->V[1], c->V[2]), c->ytab);

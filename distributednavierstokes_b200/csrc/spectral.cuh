@@ -391,7 +391,7 @@ __global__ void __launch_bounds__(SPEC_THREADS, 3) k_irfftx(Geo g, const double2
 // computed once per stage and set instead of once per line: beta_j,
 // c'_j = -theta c_j / beta_j, theta a_j.  For the chunked sweeps of k_cn the
 // forward multipliers f_j = theta a_j / beta_j and backward multipliers
-// -c'_j are also accumulated per chunk of CN_CHUNKS rows:
+// -c'_j are also accumulated per chunk of m rows:
 //   g_j = prod_{i=s..j} f_i (s = chunk start), h_j = prod_{i=j..e} (-c'_i)
 // (e = chunk end), G_k = g at the end of chunk k, H_k = h at its start.
 // tab layout per (stage, set): [ta | cp | ib | g | h](ny each), [G | H](CN_CHUNKS
@@ -405,43 +405,55 @@ __host__ __device__ constexpr long long cn_tab_stride(int ny) { return 5LL * ny 
 // Shared-memory pitch of one k_cn table with rows skewed by their chunk.
 __host__ __device__ constexpr int cn_skew_pitch(int ny, int mr) { return ny + (ny + mr - 1) / mr; }
 
+// Launch with CN_TABLE_THREADS threads: threads 0..5 (stage, set) run the
+// sequential factorisation, then thread (stage, set, chunk) forms the
+// products of one chunk.
+constexpr int CN_TABLE_THREADS = 6 * CN_MAXCHUNKS;
 __global__ void k_cn_tables(int ny, int m, int nchunks, const double *__restrict__ coef,
                             double *__restrict__ tab, double dt, double visc, double al0,
                             double al1, double al2) {
   const int t = threadIdx.x;
-  if (t >= 6) return;
-  const int st = t / 2, set = t % 2;
-  const double al = st == 0 ? al0 : st == 1 ? al1 : al2;
-  const double th = al * dt * visc / 2;
-  const double *a = coef + (set ? 3 : 0) * ny;
-  const double *b = a + ny, *c = b + ny;
+  const int seq = t % 6, k = t / 6;
+  const int st = seq / 2, set = seq % 2;
   double *ta = tab + (long long)(st * 2 + set) * cn_tab_stride(ny);
   double *cp = ta + ny, *ib = cp + ny, *gf = ib + ny, *hb = gf + ny;
   double *G = hb + ny, *H = G + CN_MAXCHUNKS;
-  double beta = 1 - th * b[0];
-  double cprev = -th * c[0] / beta;
-  ta[0] = th * a[0];
-  cp[0] = cprev;
-  ib[0] = 1.0 / beta;
-  for (int j = 1; j < ny; j++) {
-    beta = (1 - th * b[j]) + th * a[j] * cprev;
-    cprev = -th * c[j] / beta;
-    ta[j] = th * a[j];
-    cp[j] = cprev;
-    ib[j] = 1.0 / beta;
+  if (k == 0) {
+    const double al = st == 0 ? al0 : st == 1 ? al1 : al2;
+    const double th = al * dt * visc / 2;
+    const double *a = coef + (set ? 3 : 0) * ny;
+    const double *b = a + ny, *c = b + ny;
+    double beta = 1 - th * b[0];
+    double cprev = -th * c[0] / beta;
+    ta[0] = th * a[0];
+    cp[0] = cprev;
+    ib[0] = 1.0 / beta;
+    for (int j = 1; j < ny; j++) {
+      beta = (1 - th * b[j]) + th * a[j] * cprev;
+      cprev = -th * c[j] / beta;
+      ta[j] = th * a[j];
+      cp[j] = cprev;
+      ib[j] = 1.0 / beta;
+    }
   }
-  for (int k = 0; k < nchunks; k++) {
-    const int s0 = k * m, e0 = min(ny, s0 + m) - 1;
-    G[k] = 1.0;
-    H[k] = 1.0;
-    if (s0 > e0) continue;
-    double acc = 1.0;
-    for (int j = s0; j <= e0; j++) { acc *= ta[j] * ib[j]; gf[j] = acc; }
-    G[k] = acc;
-    acc = 1.0;
-    for (int j = e0; j >= s0; j--) { acc *= -cp[j]; hb[j] = acc; }
-    H[k] = acc;
+  __syncthreads();  // also orders the global writes above for the block
+  if (k >= nchunks) return;
+  const int s0 = k * m, e0 = min(ny, s0 + m) - 1;
+  G[k] = 1.0;
+  H[k] = 1.0;
+  if (s0 > e0) return;
+  double acc = 1.0;
+  for (int j = s0; j <= e0; j++) {
+    acc *= ta[j] * ib[j];
+    gf[j] = acc;
   }
+  G[k] = acc;
+  acc = 1.0;
+  for (int j = e0; j >= s0; j--) {
+    acc *= -cp[j];
+    hb[j] = acc;
+  }
+  H[k] = acc;
 }
 
 // imexsolve_kernel! (src/ydiffusion.jl:94-109) on right-hand sides that the
