@@ -17,6 +17,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdarg>
+#include <cstdint>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -87,6 +88,8 @@ struct dnsb_ctx {
   int Lx = 1, Lz = 1, Ly = 1;
   size_t smem_rx = 0, smem_ix = 0, smem_z = 0, smem_y = 0, smem_cn = 0;
   int cn_mr = 1;      // rows per chunk of the CN solve
+  int mom_tile = 1;   // z-marching momentum kernel with staged planes
+  dim3 tgrid, tblock;
 
   dim3 cgrid, cblock;  // launch shape of the per-cell step kernels
   // scratch
@@ -567,6 +570,12 @@ int poisson_from_spectrum(dnsb_ctx *c, int outmode, double *out) {
   return launch_irfftx(c, outmode, out);
 }
 
+// the z-marching momentum kernel copies 16-byte chunks of the velocity rows
+bool use_tile(const dnsb_ctx *c, const double *ux, const double *uy, const double *uz) {
+  auto a16 = [](const double *q) { return (reinterpret_cast<uintptr_t>(q) & 15) == 0; };
+  return c->mom_tile && a16(ux) && a16(uy) && a16(uz);
+}
+
 void launch_cn(dnsb_ctx *c, Fields3 out, CFields3 V, const double *tab) {
   const Geo &g = c->g;
   const dim3 grid = cn_grid(g), block(CN_LINES, CN_CHUNKS);
@@ -594,10 +603,16 @@ int do_step(dnsb_ctx *c, double *ux, double *uy, double *uz, double *p, double *
     const int readq = A != 0.0;
     unsigned long long *um = s == 2 ? c->umax : nullptr;
     if (!c->implicit) {
-      LAUNCH(c, DNSB_KIND_MOMENTUM,
-             k_momentum<MOM_EXPLICIT><<<c->cgrid, c->cblock, 0, c->stream>>>(
-                 g, ff(qx, qy, qz), cf(ux, uy, uz), ff(c->W[0], c->W[1], c->W[2]), nullptr, A, dt,
-                 B, 0.0, readq, c->ymet, 0.0));
+      if (use_tile(c, ux, uy, uz))
+        LAUNCH(c, DNSB_KIND_MOMENTUM,
+               k_momentum_march<MOM_EXPLICIT><<<c->tgrid, c->tblock, 0, c->stream>>>(
+                   g, ff(qx, qy, qz), cf(ux, uy, uz), ff(c->W[0], c->W[1], c->W[2]), nullptr, A,
+                   dt, B, 0.0, readq, c->ymet, 0.0));
+      else
+        LAUNCH(c, DNSB_KIND_MOMENTUM,
+               k_momentum<MOM_EXPLICIT><<<c->cgrid, c->cblock, 0, c->stream>>>(
+                   g, ff(qx, qy, qz), cf(ux, uy, uz), ff(c->W[0], c->W[1], c->W[2]), nullptr, A,
+                   dt, B, 0.0, readq, c->ymet, 0.0));
       if ((rc = launch_rfftx(c, RIN_DIVERGENCE, c->W[0], c->W[1], c->W[2]))) return rc;
       if ((rc = poisson_from_spectrum(c, ROUT_IMAGES, p))) return rc;
       LAUNCH(c, DNSB_KIND_GRAD,
@@ -606,10 +621,16 @@ int do_step(dnsb_ctx *c, double *ux, double *uy, double *uz, double *p, double *
     } else {
       const double adt = al * dt;
       const double th = al * dt * g.visc / 2;
-      LAUNCH(c, DNSB_KIND_MOMENTUM,
-             k_momentum<MOM_IMPLICIT><<<c->cgrid, c->cblock, 0, c->stream>>>(
-                 g, ff(qx, qy, qz), cf(ux, uy, uz), ff(c->V[0], c->V[1], c->V[2]), p, A, dt, B,
-                 adt, readq, c->ymet, th));
+      if (use_tile(c, ux, uy, uz))
+        LAUNCH(c, DNSB_KIND_MOMENTUM,
+               k_momentum_march<MOM_IMPLICIT><<<c->tgrid, c->tblock, 0, c->stream>>>(
+                   g, ff(qx, qy, qz), cf(ux, uy, uz), ff(c->V[0], c->V[1], c->V[2]), p, A, dt, B,
+                   adt, readq, c->ymet, th));
+      else
+        LAUNCH(c, DNSB_KIND_MOMENTUM,
+               k_momentum<MOM_IMPLICIT><<<c->cgrid, c->cblock, 0, c->stream>>>(
+                   g, ff(qx, qy, qz), cf(ux, uy, uz), ff(c->V[0], c->V[1], c->V[2]), p, A, dt, B,
+                   adt, readq, c->ymet, th));
       LAUNCH(c, DNSB_KIND_CN,
              launch_cn(c, ff(ux, uy, uz), cf(c->V[0], c->V[1], c->V[2]),
                        c->ytab + (long long)s * 2 * cn_tab_stride(g.ny)));
@@ -836,6 +857,9 @@ int dnsb_create(const dnsb_grid *gr, int device, void *stream, dnsb_ctx **out) {
     } else { bx = 64; by = 2; }
     c->cblock = dim3(bx, by, 1);
     c->cgrid = dim3((nx + bx - 1) / bx, (ny + by - 1) / by, nz);
+    c->mom_tile = envint("DNSB_MOMTILE", 1) != 0;
+    c->tblock = dim3(MC_X, MC_Y, 1);
+    c->tgrid = dim3((nx + MC_X - 1) / MC_X, (ny + MC_Y - 1) / MC_Y, (nz + MC_Z - 1) / MC_Z);
   }
   c->smem_rx = sizeof(double2) * (2 * (size_t)c->Lx * (M + 1) + M + (M + 1));
   c->smem_ix = sizeof(double2) * (2 * (size_t)c->Lx * (M + 2) + M + (M + 1));
@@ -979,9 +1003,14 @@ int dnsb_momentum(dnsb_ctx *c, double *qx, double *qy, double *qz, const double 
   if (!c || !qx || !qy || !qz || !ux || !uy || !uz)
     return c ? fail(c, DNSB_EINVAL, "null field") : DNSB_EINVAL;
   if (ensure_device(c)) return DNSB_ECUDA;
-  k_momentum<MOM_ONLY><<<cell_grid(c->g), cell_block, 0, c->stream>>>(
-      c->g, ff(qx, qy, qz), cf(ux, uy, uz), ff(nullptr, nullptr, nullptr), nullptr, A, dt, 0.0,
-      0.0, 1, c->ymet, 0.0);
+  if (use_tile(c, ux, uy, uz))
+    k_momentum_march<MOM_ONLY><<<c->tgrid, c->tblock, 0, c->stream>>>(
+        c->g, ff(qx, qy, qz), cf(ux, uy, uz), ff(nullptr, nullptr, nullptr), nullptr, A, dt, 0.0,
+        0.0, 1, c->ymet, 0.0);
+  else
+    k_momentum<MOM_ONLY><<<cell_grid(c->g), cell_block, 0, c->stream>>>(
+        c->g, ff(qx, qy, qz), cf(ux, uy, uz), ff(nullptr, nullptr, nullptr), nullptr, A, dt, 0.0,
+        0.0, 1, c->ymet, 0.0);
   CKL(c);
   return 0;
 }

@@ -11,6 +11,7 @@
 // the reference's divisions); halving uses *0.5 (exact).
 #pragma once
 #include "common.cuh"
+#include "tma.cuh"
 
 namespace dnsb {
 
@@ -42,6 +43,21 @@ struct MomCell {
   double vx, vy, vz;  // stage increments
 };
 
+// The staggered neighbourhood of one cell (E/W: I+-1, N/S: J+-1, T/B:
+// K+-1) with q and p there: the inputs of momentum_kernel!.
+struct MomNb {
+  double ux0, uxE, uxW, uxN, uxS, uxT, uxB, uxWN, uxWT;
+  double uy0, uyE, uyW, uyN, uyS, uyT, uyB, uySE, uyST;
+  double uz0, uzE, uzW, uzN, uzS, uzT, uzB, uzEB, uzNB;
+  double qx0, qy0, qz0, p0, pE, pN, pT;
+};
+
+template <int MODE>
+__device__ __forceinline__ MomCell mom_compute(const Geo &g, int J, const MomNb &nb, double A,
+                                               double dt, double B, double adt, int readq,
+                                               const double2 *__restrict__ ymet, double theta);
+
+// momentum_cell: the neighbourhood straight from HBM (one load per value).
 template <int MODE>
 __device__ __forceinline__ MomCell momentum_cell(const Geo &g, int I, int J, int K, const Fields3 &q,
                                                  const CFields3 &u, const double *__restrict__ p,
@@ -52,30 +68,47 @@ __device__ __forceinline__ MomCell momentum_cell(const Geo &g, int I, int J, int
   const long long sy = g.NX, sz = (long long)g.NX * g.NY;
   const long long c0 = (long long)I + g.NX * ((long long)J + (long long)g.NY * K);
   const double *ux = u.x, *uy = u.y, *uz = u.z;
+  MomNb nb;
 #define LDG(p, o) __ldg((p) + (o))
-  const double ux0 = LDG(ux, c0), uxE = LDG(ux, c0 + 1), uxW = LDG(ux, c0 - 1);
-  const double uxN = LDG(ux, c0 + sy), uxS = LDG(ux, c0 - sy);
-  const double uxT = LDG(ux, c0 + sz), uxB = LDG(ux, c0 - sz);
-  const double uxWN = LDG(ux, c0 - 1 + sy), uxWT = LDG(ux, c0 - 1 + sz);
-  const double uy0 = LDG(uy, c0), uyE = LDG(uy, c0 + 1), uyW = LDG(uy, c0 - 1);
-  const double uyN = LDG(uy, c0 + sy), uyS = LDG(uy, c0 - sy);
-  const double uyT = LDG(uy, c0 + sz), uyB = LDG(uy, c0 - sz);
-  const double uySE = LDG(uy, c0 + 1 - sy), uyST = LDG(uy, c0 - sy + sz);
-  const double uz0 = LDG(uz, c0), uzE = LDG(uz, c0 + 1), uzW = LDG(uz, c0 - 1);
-  const double uzN = LDG(uz, c0 + sy), uzS = LDG(uz, c0 - sy);
-  const double uzT = LDG(uz, c0 + sz), uzB = LDG(uz, c0 - sz);
-  const double uzEB = LDG(uz, c0 + 1 - sz), uzNB = LDG(uz, c0 + sy - sz);
+  nb.ux0 = LDG(ux, c0); nb.uxE = LDG(ux, c0 + 1); nb.uxW = LDG(ux, c0 - 1);
+  nb.uxN = LDG(ux, c0 + sy); nb.uxS = LDG(ux, c0 - sy);
+  nb.uxT = LDG(ux, c0 + sz); nb.uxB = LDG(ux, c0 - sz);
+  nb.uxWN = LDG(ux, c0 - 1 + sy); nb.uxWT = LDG(ux, c0 - 1 + sz);
+  nb.uy0 = LDG(uy, c0); nb.uyE = LDG(uy, c0 + 1); nb.uyW = LDG(uy, c0 - 1);
+  nb.uyN = LDG(uy, c0 + sy); nb.uyS = LDG(uy, c0 - sy);
+  nb.uyT = LDG(uy, c0 + sz); nb.uyB = LDG(uy, c0 - sz);
+  nb.uySE = LDG(uy, c0 + 1 - sy); nb.uyST = LDG(uy, c0 - sy + sz);
+  nb.uz0 = LDG(uz, c0); nb.uzE = LDG(uz, c0 + 1); nb.uzW = LDG(uz, c0 - 1);
+  nb.uzN = LDG(uz, c0 + sy); nb.uzS = LDG(uz, c0 - sy);
+  nb.uzT = LDG(uz, c0 + sz); nb.uzB = LDG(uz, c0 - sz);
+  nb.uzEB = LDG(uz, c0 + 1 - sz); nb.uzNB = LDG(uz, c0 + sy - sz);
 #undef LDG
-
-  const double qx0 = readq ? q.x[c0] : 0.0, qy0 = readq ? q.y[c0] : 0.0;
-  const double qz0 = readq ? q.z[c0] : 0.0;
-  double pE = 0.0, pN = 0.0, pT = 0.0, p0 = 0.0;
+  nb.qx0 = readq ? q.x[c0] : 0.0;
+  nb.qy0 = readq ? q.y[c0] : 0.0;
+  nb.qz0 = readq ? q.z[c0] : 0.0;
+  nb.p0 = nb.pE = nb.pN = nb.pT = 0.0;
   if (MODE == MOM_IMPLICIT) {
-    p0 = __ldg(p + c0);
-    pE = __ldg(p + c0 + 1);
-    pN = __ldg(p + c0 + sy);
-    pT = __ldg(p + c0 + sz);
+    nb.p0 = __ldg(p + c0);
+    nb.pE = __ldg(p + c0 + 1);
+    nb.pN = __ldg(p + c0 + sy);
+    nb.pT = __ldg(p + c0 + sz);
   }
+  return mom_compute<MODE>(g, J, nb, A, dt, B, adt, readq, ymet, theta);
+}
+
+// The arithmetic of momentum_kernel! on a loaded neighbourhood.
+template <int MODE>
+__device__ __forceinline__ MomCell mom_compute(const Geo &g, int J, const MomNb &nb, double A,
+                                               double dt, double B, double adt, int readq,
+                                               const double2 *__restrict__ ymet, double theta) {
+  const double ux0 = nb.ux0, uxE = nb.uxE, uxW = nb.uxW, uxN = nb.uxN, uxS = nb.uxS;
+  const double uxT = nb.uxT, uxB = nb.uxB, uxWN = nb.uxWN, uxWT = nb.uxWT;
+  const double uy0 = nb.uy0, uyE = nb.uyE, uyW = nb.uyW, uyN = nb.uyN, uyS = nb.uyS;
+  const double uyT = nb.uyT, uyB = nb.uyB, uySE = nb.uySE, uyST = nb.uyST;
+  const double uz0 = nb.uz0, uzE = nb.uzE, uzW = nb.uzW, uzN = nb.uzN, uzS = nb.uzS;
+  const double uzT = nb.uzT, uzB = nb.uzB, uzEB = nb.uzEB, uzNB = nb.uzNB;
+  const double qx0 = nb.qx0, qy0 = nb.qy0, qz0 = nb.qz0;
+  const double p0 = nb.p0, pE = nb.pE, pN = nb.pN, pT = nb.pT;
   const double2 *ym = ymet + YMET * J;
   const double2 m0 = __ldg(ym), m1 = __ldg(ym + 1), m2 = __ldg(ym + 2);
   const double dyJ = m0.x, dyJ1 = m0.y, rdyJ = m1.x, rdyJ1 = m1.y, rdyuJ = m2.x, rdyuJm = m2.y;
@@ -155,6 +188,10 @@ __device__ __forceinline__ MomCell momentum_cell(const Geo &g, int I, int J, int
   return m;
 }
 
+template <int MODE>
+__device__ __forceinline__ void mom_store(const Geo &g, int I, int J, int K, const MomCell &m,
+                                          const Fields3 &q, const Fields3 &out);
+
 // momentum_kernel! (src/operators.jl:44-145), one thread per interior cell.
 // MOM_ONLY: q <- A q + dt F(u).
 // MOM_EXPLICIT: also W_c = u_c + B q_c on active DOFs, with ghost images.
@@ -172,9 +209,16 @@ __global__ void __launch_bounds__(256, 2) k_momentum(Geo g, Fields3 q, CFields3 
   const int J = blockIdx.y * blockDim.y + threadIdx.y + 1;
   const int K = blockIdx.z + 1;
   if (I > g.nx || J > g.ny) return;
-  const int c0 = gidx(g, I, J, K);
   const MomCell m = momentum_cell<MODE == MOM_ONLY ? MOM_EXPLICIT : MODE>(
       g, I, J, K, q, u, p, A, dt, B, adt, readq, ymet, theta);
+  mom_store<MODE>(g, I, J, K, m, q, out);
+}
+
+// Stores of one cell of k_momentum / k_momentum_tile.
+template <int MODE>
+__device__ __forceinline__ void mom_store(const Geo &g, int I, int J, int K, const MomCell &m,
+                                          const Fields3 &q, const Fields3 &out) {
+  const int c0 = gidx(g, I, J, K);
   const bool yact = J <= g.jymax;
   q.x[c0] = m.qx;
   if (yact) q.y[c0] = m.qy;
@@ -188,6 +232,89 @@ __global__ void __launch_bounds__(256, 2) k_momentum(Geo g, Fields3 q, CFields3 
     out.y[c0] = m.vy;
     out.z[c0] = m.vz;
   }
+}
+
+// Column of k_momentum_march: MC_X x MC_Y cells per CTA (one thread each)
+// walking MC_Z planes in z.  Planes are staged with a one-cell halo in x
+// and y in a ring of four.
+constexpr int MC_X = 32, MC_Y = 8, MC_Z = 16;  // measured best of 8-64 planes, 4-8 rows
+constexpr int MP_X = MC_X + 2, MP_Y = MC_Y + 2, MP_N = MP_X * MP_Y;
+
+// momentum_kernel! with the velocity planes staged in shared memory: the
+// CTA keeps planes K-1, K, K+1 of u.x, u.y, u.z (each MP_X x MP_Y, rows
+// starting at I0 - 1, a multiple of 32, so every 16-byte cp.async is
+// aligned when the fields are 16-byte aligned and nx is even) and copies
+// plane K+2 into the fourth slot while it computes plane K.  Same
+// arithmetic and stores as k_momentum.
+// 3 CTAs of 256 per SM (80 registers; faster than 2 CTAs without the cap)
+template <int MODE>
+__global__ void __launch_bounds__(MC_X *MC_Y, 3)
+    k_momentum_march(Geo g, Fields3 q, CFields3 u, Fields3 out, const double *__restrict__ p,
+                     double A, double dt, double B, double adt, int readq,
+                     const double2 *__restrict__ ymet, double theta) {
+  __shared__ __align__(16) double ring[4][3][MP_N];
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int tid = tx + MC_X * ty;
+  const int I0 = blockIdx.x * MC_X + 1, J0 = blockIdx.y * MC_Y + 1;
+  const int K0 = blockIdx.z * MC_Z + 1, K1 = min(g.nz, K0 + MC_Z - 1);
+  constexpr int CH = MP_X / 2;  // 16-byte chunks per halo row
+  constexpr int NCH = 3 * MP_Y * CH;
+  // copies plane z (0..NZ-1) into its ring slot; rows and chunks outside the
+  // ghosted array are never read by an interior cell
+  auto issue = [&](int z) {
+    double(*slot)[MP_N] = ring[z & 3];
+    for (int t = tid; t < NCH; t += MC_X * MC_Y) {
+      const int ch = t % CH, r = t / CH;
+      const int c = r / MP_Y, hy = r - c * MP_Y;
+      const int x = I0 - 1 + 2 * ch, y = J0 - 1 + hy;
+      if (x + 1 < g.NX && y < g.NY) {
+        const double *src = (c == 0 ? u.x : c == 1 ? u.y : u.z) + gidx(g, x, y, z);
+        cp_async16(&slot[c][2 * ch + MP_X * hy], src);
+      }
+    }
+    cp_async_commit();
+  };
+  const int I = I0 + tx, J = J0 + ty;
+  const bool inside = I <= g.nx && J <= g.ny;
+  issue(K0 - 1);
+  issue(K0);
+  issue(K0 + 1);
+  constexpr int SY = MP_X;
+  const int h = (tx + 1) + SY * (ty + 1);
+  const int sy = g.NX, sz = g.NX * g.NY;
+  for (int K = K0; K <= K1; K++) {
+    // q and p of this plane from HBM while the plane copies land
+    MomNb nb;
+    const int c0 = gidx(g, inside ? I : 1, inside ? J : 1, K);
+    nb.qx0 = (inside && readq) ? q.x[c0] : 0.0;
+    nb.qy0 = (inside && readq) ? q.y[c0] : 0.0;
+    nb.qz0 = (inside && readq) ? q.z[c0] : 0.0;
+    nb.p0 = nb.pE = nb.pN = nb.pT = 0.0;
+    if (MODE == MOM_IMPLICIT && inside) {
+      nb.p0 = __ldg(p + c0);
+      nb.pE = __ldg(p + c0 + 1);
+      nb.pN = __ldg(p + c0 + sy);
+      nb.pT = __ldg(p + c0 + sz);
+    }
+    cp_async_wait<0>();  // planes up to K+1 have landed (this thread's copies)
+    __syncthreads();     // ... everyone's, and plane K-2's slot is free
+    if (K + 2 <= K1 + 1) issue(K + 2);
+    if (inside) {
+      const double *bx = ring[(K - 1) & 3][0] + h, *cx = ring[K & 3][0] + h, *tx_ = ring[(K + 1) & 3][0] + h;
+      const double *by = ring[(K - 1) & 3][1] + h, *cy = ring[K & 3][1] + h, *ty_ = ring[(K + 1) & 3][1] + h;
+      const double *bz = ring[(K - 1) & 3][2] + h, *cz = ring[K & 3][2] + h, *tz_ = ring[(K + 1) & 3][2] + h;
+      nb.ux0 = cx[0]; nb.uxE = cx[1]; nb.uxW = cx[-1]; nb.uxN = cx[SY]; nb.uxS = cx[-SY];
+      nb.uxT = tx_[0]; nb.uxB = bx[0]; nb.uxWN = cx[SY - 1]; nb.uxWT = tx_[-1];
+      nb.uy0 = cy[0]; nb.uyE = cy[1]; nb.uyW = cy[-1]; nb.uyN = cy[SY]; nb.uyS = cy[-SY];
+      nb.uyT = ty_[0]; nb.uyB = by[0]; nb.uySE = cy[1 - SY]; nb.uyST = ty_[-SY];
+      nb.uz0 = cz[0]; nb.uzE = cz[1]; nb.uzW = cz[-1]; nb.uzN = cz[SY]; nb.uzS = cz[-SY];
+      nb.uzT = tz_[0]; nb.uzB = bz[0]; nb.uzEB = bz[1]; nb.uzNB = bz[SY];
+      const MomCell m = mom_compute<MODE == MOM_ONLY ? MOM_EXPLICIT : MODE>(
+          g, J, nb, A, dt, B, adt, readq, ymet, theta);
+      mom_store<MODE>(g, I, J, K, m, q, out);
+    }
+  }
+  cp_async_wait<0>();
 }
 
 enum GradMode { GRAD_EXPLICIT = 0, GRAD_IMPLICIT = 1 };
