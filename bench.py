@@ -50,12 +50,16 @@ COMMON = dict(lims=((0.0, 4 * math.pi), (-1.0, 1.0), (0.0, 4 * math.pi / 3)),
 # Algorithmic HBM passes (one FP64 field = nx*ny*nz*8 bytes) per launch of
 # each kernel kind on the default path; the half-spectrum counts
 # (nx/2+1)/(nx/2) of a real field.  Momentum reads q only from stage 2 on.
-def passes(kind, implicit, spec):
+# With the fused projection + momentum (grad_momentum: r u*3 delta1 p1 q3,
+# w p1 q3 V3) the stand-alone momentum runs at stage 1 only (q not read).
+def passes(kind, implicit, spec, fused=False):
     if kind == "momentum":
+        if fused:
+            return 12.0
         return (12 + 13 + 13) / 3 if implicit else (9 + 12 + 12) / 3
     return {"cn_solve": 6.0, "div_rfft_x": 3 + spec, "fft_z": 2 * spec, "y_solve": 2 * spec,
             "ifft_z": 2 * spec, "irfft_x": spec + 1, "grad_update": 9.0 if implicit else 7.0,
-            "other": 0.0}[kind]
+            "grad_momentum": 15.0, "other": 0.0}[kind]
 
 
 def tanhstretch(beta):
@@ -292,9 +296,10 @@ def b200_arm(args, wl, world, rank, local):
     # roofline of the dominant kernel kind (by device time in the timed region)
     peak, peak_kind = measured_peaks()
     spec = (nx // 2 + 1) / (nx // 2)
+    fused = kinds.get("grad_momentum", (0.0, 0))[1] > 0
     dom = max((k for k in kinds if k != "other"), key=lambda k: kinds[k][0])
     t_dom, n_dom = kinds[dom]
-    bytes_launch = passes(dom, s.imexy, spec) * cells * 8
+    bytes_launch = passes(dom, s.imexy, spec, fused) * cells * 8
     achieved = bytes_launch / (t_dom / n_dom / 1e3) / 1e9
     traffic = None
     tpath = os.path.join(ROOT, "profiles", f"traffic_{args.workload}.json")
@@ -305,7 +310,7 @@ def b200_arm(args, wl, world, rank, local):
     for k, (t, n) in kinds.items():
         if n == 0:
             continue
-        b = passes(k, s.imexy, spec) * cells * 8
+        b = passes(k, s.imexy, spec, fused) * cells * 8
         per_kernel[k] = {"launches": n, "ms_avg": t / n, "share": t / sum(v[0] for v in kinds.values()),
                          "gbs": (b / (t / n / 1e3) / 1e9) if b else None}
     step_bytes = wl["bytes_per_cell_step"] * cells

@@ -65,7 +65,7 @@ SIGNATURES = {
 }
 
 KINDS = ["momentum", "cn_solve", "div_rfft_x", "fft_z", "y_solve", "ifft_z", "irfft_x",
-         "grad_update", "other"]
+         "grad_update", "other", "grad_momentum"]
 
 _LIB = None
 

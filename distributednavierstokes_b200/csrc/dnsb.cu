@@ -31,6 +31,7 @@
 #include "spectral4.cuh"
 #include "ysolve.cuh"
 #include "stencil.cuh"
+#include "gradmom.cuh"
 
 using namespace dnsb;
 
@@ -89,6 +90,8 @@ struct dnsb_ctx {
   size_t smem_rx = 0, smem_ix = 0, smem_z = 0, smem_y = 0, smem_cn = 0;
   int cn_mr = 1;      // rows per chunk of the CN solve
   int mom_tile = 1;   // z-marching momentum kernel with staged planes
+  int fuse = 1;       // fused projection + momentum between implicit stages
+  double *pn = nullptr;  // pressure after stage 1 when fused
   dim3 tgrid, tblock;
 
   dim3 cgrid, cblock;  // launch shape of the per-cell step kernels
@@ -155,7 +158,8 @@ int fail(dnsb_ctx *c, int code, const char *fmt, ...) {
 #define CKL(ctx) CK(ctx, cudaGetLastError())
 
 const char *KIND_NAMES[DNSB_NKINDS] = {"momentum", "cn_solve", "div_rfft_x", "fft_z", "y_solve",
-                                       "ifft_z", "irfft_x", "grad_update", "other"};
+                                       "ifft_z", "irfft_x", "grad_update", "other",
+                                       "grad_momentum"};
 
 int prof_harvest(dnsb_ctx *c) {
   if (c->recs.empty()) { c->evused = 0; return 0; }
@@ -570,10 +574,11 @@ int poisson_from_spectrum(dnsb_ctx *c, int outmode, double *out) {
   return launch_irfftx(c, outmode, out);
 }
 
+bool aligned16(const double *q) { return (reinterpret_cast<uintptr_t>(q) & 15) == 0; }
+
 // the z-marching momentum kernel copies 16-byte chunks of the velocity rows
 bool use_tile(const dnsb_ctx *c, const double *ux, const double *uy, const double *uz) {
-  auto a16 = [](const double *q) { return (reinterpret_cast<uintptr_t>(q) & 15) == 0; };
-  return c->mom_tile && a16(ux) && a16(uy) && a16(uz);
+  return c->mom_tile && aligned16(ux) && aligned16(uy) && aligned16(uz);
 }
 
 void launch_cn(dnsb_ctx *c, Fields3 out, CFields3 V, const double *tab) {
@@ -593,6 +598,9 @@ int do_step(dnsb_ctx *c, double *ux, double *uy, double *uz, double *p, double *
             double *qz, double *delta, double dt) {
   const Geo &g = c->g;
   int rc;
+  // projection + next momentum fused (needs 16-byte aligned planes to stage)
+  const bool fused = c->implicit && c->fuse && c->pn && use_tile(c, ux, uy, uz) &&
+                     aligned16(delta) && aligned16(p);
   CK(c, cudaMemsetAsync(c->umax, 0, 3 * UMAX_SLOTS * sizeof(unsigned long long), c->stream));
   if (c->implicit)
     LAUNCH(c, DNSB_KIND_OTHER,
@@ -621,7 +629,9 @@ int do_step(dnsb_ctx *c, double *ux, double *uy, double *uz, double *p, double *
     } else {
       const double adt = al * dt;
       const double th = al * dt * g.visc / 2;
-      if (use_tile(c, ux, uy, uz))
+      if (s > 0 && fused) {
+        // the momentum of this stage ran inside the previous stage's projection
+      } else if (use_tile(c, ux, uy, uz))
         LAUNCH(c, DNSB_KIND_MOMENTUM,
                k_momentum_march<MOM_IMPLICIT><<<c->tgrid, c->tblock, 0, c->stream>>>(
                    g, ff(qx, qy, qz), cf(ux, uy, uz), ff(c->V[0], c->V[1], c->V[2]), p, A, dt, B,
@@ -636,9 +646,22 @@ int do_step(dnsb_ctx *c, double *ux, double *uy, double *uz, double *p, double *
                        c->ytab + (long long)s * 2 * cn_tab_stride(g.ny)));
       if ((rc = launch_rfftx(c, RIN_DIVERGENCE, ux, uy, uz))) return rc;
       if ((rc = poisson_from_spectrum(c, ROUT_IMAGES, delta))) return rc;
-      LAUNCH(c, DNSB_KIND_GRAD,
-             k_grad<GRAD_IMPLICIT><<<c->cgrid, c->cblock, 0, c->stream>>>(
-                 g, ff(ux, uy, uz), cf(ux, uy, uz), delta, p, 1.0 / adt, um));
+      if (s < 2 && fused) {
+        // projection of this stage + momentum of the next; the pressure
+        // goes p -> pn (stage 1) -> p (stage 2), never in place
+        const double A1 = RK_A[s + 1], B1 = RK_B[s + 1], al1 = RK_AL[s + 1];
+        const double *pin = s == 0 ? p : c->pn;
+        double *pout = s == 0 ? c->pn : p;
+        LAUNCH(c, DNSB_KIND_GRADMOM,
+               k_gradmom_march<<<c->tgrid, c->tblock, GRADMOM_SMEM, c->stream>>>(
+                   g, cf(ux, uy, uz), delta, pin, pout, 1.0 / adt, ff(qx, qy, qz),
+                   ff(c->V[0], c->V[1], c->V[2]), A1, dt, B1, al1 * dt, c->ymet,
+                   al1 * dt * g.visc / 2));
+      } else {
+        LAUNCH(c, DNSB_KIND_GRAD,
+               k_grad<GRAD_IMPLICIT><<<c->cgrid, c->cblock, 0, c->stream>>>(
+                   g, ff(ux, uy, uz), cf(ux, uy, uz), delta, p, 1.0 / adt, um));
+      }
     }
   }
   c->umax_for[0] = ux;
@@ -858,6 +881,7 @@ int dnsb_create(const dnsb_grid *gr, int device, void *stream, dnsb_ctx **out) {
     c->cblock = dim3(bx, by, 1);
     c->cgrid = dim3((nx + bx - 1) / bx, (ny + by - 1) / by, nz);
     c->mom_tile = envint("DNSB_MOMTILE", 1) != 0;
+    c->fuse = envint("DNSB_FUSE", 1) != 0;
     c->tblock = dim3(MC_X, MC_Y, 1);
     c->tgrid = dim3((nx + MC_X - 1) / MC_X, (ny + MC_Y - 1) / MC_Y, (nz + MC_Z - 1) / MC_Z);
   }
@@ -938,6 +962,10 @@ int dnsb_create(const dnsb_grid *gr, int device, void *stream, dnsb_ctx **out) {
     if (c->implicit) {
       if ((rc = dalloc(c, &c->V[i], G))) return bail(rc);
     }
+  }
+  if (c->implicit && c->fuse) {
+    if ((rc = dalloc(c, &c->pn, G))) return bail(rc);
+    if ((rc = allow_smem(c, k_gradmom_march, GRADMOM_SMEM))) return bail(rc);
   }
   if (cudaMemset(c->deverr, 0, 4 * sizeof(int)) != cudaSuccess) {
     fail(c, DNSB_ECUDA, "cudaMemset failed");

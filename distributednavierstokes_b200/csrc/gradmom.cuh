@@ -1,0 +1,193 @@
+// gradmom.cuh -- the projection of one semi-implicit RK3 stage fused with
+// the momentum of the next.
+//
+// Between stages s and s+1 of step! (src/timestep.jl:41-63) with implicit
+// y-diffusion, the reference runs
+//   pressuregrad!/project: u = u* - grad delta, p += delta / (alpha_s dt)
+//                          (timestep.jl:49-52, operators.jl:180-220)
+//   momentum! + imex_update! of stage s+1 (operators.jl:44-145,
+//                          ydiffusion.jl:71-154)
+// and u after the projection is read by nothing but that momentum (the
+// Crank-Nicolson solve of stage s+1 overwrites it).  k_gradmom_march
+// therefore never stores it: it stages u*, delta and p in shared memory
+// plane by plane (the z-marching scheme of k_momentum_march), rebuilds
+// u = u* - grad delta on the CTA's tile and its one-cell halo, and feeds the
+// momentum arithmetic from there; p + delta / (alpha_s dt) is formed where
+// it is read.  Halo cells outside the interior are the ghost images of
+// exchange_halo! (halo.jl:26-45,81-126): periodic images follow from the
+// images already held by u* and delta (one more period is read for the
+// gradient at the last ghost layer), wall images mirror interior rows.
+#pragma once
+#include "common.cuh"
+#include "stencil.cuh"
+#include "tma.cuh"
+
+namespace dnsb {
+
+// Raw planes are staged as GP_X x GP_Y boxes starting at (I0-1, J0-1): one
+// halo cell on the low sides, two on the high sides (the gradient of the
+// last halo cell reads one further cell); rows of 18 aligned 16-byte chunks.
+constexpr int GP_X = MC_X + 4, GP_Y = MC_Y + 3, GP_N = GP_X * GP_Y;
+
+// Projection fused with the next stage's momentum (implicit y-diffusion).
+// Reads u* (ux, uy, uz after the Crank-Nicolson solve of stage s), delta,
+// p_in (lagged pressure before stage s's update), q; writes p_out =
+// p_in + delta * radt on the interior with ghost images, q, and V (the
+// Crank-Nicolson right-hand side of stage s+1, as k_momentum<IMPLICIT>).
+// p_out must not alias p_in (other CTAs stage p_in while this one writes).
+// 3 CTAs of 256 per SM (80 registers, no spills; faster than 2)
+__global__ void __launch_bounds__(MC_X *MC_Y, 3)
+    k_gradmom_march(Geo g, CFields3 us, const double *__restrict__ delta,
+                    const double *__restrict__ p_in, double *__restrict__ p_out, double radt,
+                    Fields3 q, Fields3 out, double A, double dt, double B, double adt,
+                    const double2 *__restrict__ ymet, double theta) {
+  extern __shared__ __align__(16) double gsm[];
+  double *ustar = gsm;                    // [2 slots][3][GP_N]   u* (one plane ahead)
+  double *pold = ustar + 2 * 3 * GP_N;    // [3 slots][GP_N]      p_in
+  double *dl = pold + 3 * GP_N;           // [4 slots][GP_N]      delta
+  double *unew = dl + 4 * GP_N;           // [3 slots][3][GP_N]   projected u
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int tid = tx + MC_X * ty;
+  constexpr int NT = MC_X * MC_Y;
+  const int I0 = blockIdx.x * MC_X + 1, J0 = blockIdx.y * MC_Y + 1;
+  const int K0 = blockIdx.z * MC_Z + 1, K1 = min(g.nz, K0 + MC_Z - 1);
+  const bool wall = g.wall;
+  constexpr int CH = GP_X / 2;
+  // one GP_X x GP_Y box of field f at plane z into dst; x, y, z beyond the
+  // ghosted array wrap by one period (periodic directions; wall rows there
+  // are never read)
+  auto box = [&](const double *f, int z, double *dst) {
+    if (z >= g.NZ) z -= g.nz;
+    for (int t = tid; t < GP_Y * CH; t += NT) {
+      const int ch = t % CH, hy = t / CH;
+      int x = I0 - 1 + 2 * ch, y = J0 - 1 + hy;
+      if (x >= g.NX) x -= g.nx;
+      if (y >= g.NY) {
+        if (wall) continue;
+        y -= g.ny;
+      }
+      cp_async16(dst + 2 * ch + GP_X * hy, f + gidx(g, x, y, z));
+    }
+  };
+  auto us_slot = [&](int z) { return ustar + (z & 1) * 3 * GP_N; };
+  auto p_slot = [&](int z) { return pold + (z % 3) * GP_N; };
+  auto d_slot = [&](int z) { return dl + (z & 3) * GP_N; };
+  auto un_slot = [&](int z) { return unew + (z % 3) * 3 * GP_N; };
+  auto issue_us = [&](int z) {
+    double *s = us_slot(z);
+    box(us.x, z, s);
+    box(us.y, z, s + GP_N);
+    box(us.z, z, s + 2 * GP_N);
+  };
+  // Per-CTA row map of the projected tile (the same for every plane): row hy
+  // of component c holds sgn * (value of staged row src); sgn = 0 for the
+  // zero wall faces and for rows beyond the ghosted array; rg = the
+  // y-metric of the gradient of the y component at that row.
+  constexpr int HX = MC_X + 2, HY = MC_Y + 2;
+  __shared__ int rsrc[3][HY];
+  __shared__ double rsgn[3][HY], rg[HY];
+  if (tid < 3 * HY) {
+    const int c = tid / HY, hy = tid - c * HY;
+    const int y = J0 - 1 + hy;
+    int hs = hy;
+    double sgn = y <= g.NY - 1 ? 1.0 : 0.0;
+    if (wall && sgn != 0.0) {
+      if (c == STAG_Y) {
+        if (y == 0 || y == g.ny) sgn = 0.0;                   // wall faces
+        else if (y == g.ny + 1) { hs = hy - 2; sgn = -1.0; }  // -(ny-1)
+      } else {
+        if (y == 0) { hs = 1; sgn = -1.0; }                   // -(1)
+        else if (y == g.ny + 1) { hs = hy - 1; sgn = -1.0; }  // -(ny)
+      }
+    }
+    rsrc[c][hy] = hs;
+    rsgn[c][hy] = sgn;
+    if (c == STAG_Y) rg[hy] = sgn != 0.0 ? __ldg(g.rdyu + (J0 - 1 + hs)) : 0.0;
+  }
+  // projected u of plane z on the HX x HY tile + halo, from u* of plane z
+  // and delta of planes z, z+1 (all staged)
+  auto project_plane = [&](int z) {
+    const double *su = us_slot(z), *d0 = d_slot(z), *d1 = d_slot(z + 1);
+    double *dst = un_slot(z);
+    for (int t = tid; t < 3 * HX * HY; t += NT) {
+      const int c = t / (HX * HY), r = t - c * HX * HY;
+      const int hy = r / HX, hx = r - hy * HX;
+      const int a = hx + GP_X * rsrc[c][hy];
+      const double sgn = rsgn[c][hy];
+      double v;
+      if (c == STAG_X) v = su[a] - (d0[a + 1] - d0[a]) * g.rdx;
+      else if (c == STAG_Y) v = su[GP_N + a] - (d0[a + GP_X] - d0[a]) * rg[hy];
+      else v = su[2 * GP_N + a] - (d1[a] - d0[a]) * g.rdz;
+      dst[c * GP_N + hx + GP_X * hy] = sgn * v;
+    }
+  };
+  // prologue: u* of K0-1, K0; p of K0; delta of K0-1, K0, K0+1
+  issue_us(K0 - 1);
+  box(delta, K0 - 1, d_slot(K0 - 1));
+  box(delta, K0, d_slot(K0));
+  cp_async_commit();
+  cp_async_wait<0>();
+  __syncthreads();
+  project_plane(K0 - 1);
+  __syncthreads();  // u* slot of K0-1 is reused by K0+1 below
+  issue_us(K0);
+  box(delta, K0 + 1, d_slot(K0 + 1));
+  box(p_in, K0, p_slot(K0));
+  cp_async_commit();
+  cp_async_wait<0>();
+  __syncthreads();
+  project_plane(K0);
+  // plane K+1's raw data for the first iteration
+  issue_us(K0 + 1);
+  box(p_in, K0 + 1, p_slot(K0 + 1));
+  box(delta, K0 + 2, d_slot(K0 + 2));
+  cp_async_commit();
+  const int I = I0 + tx, J = J0 + ty;
+  const bool inside = I <= g.nx && J <= g.ny;
+  constexpr int SY = GP_X;
+  const int h = (tx + 1) + SY * (ty + 1);
+  for (int K = K0; K <= K1; K++) {
+    MomNb nb;
+    const int c0 = gidx(g, inside ? I : 1, inside ? J : 1, K);
+    nb.qx0 = inside ? q.x[c0] : 0.0;
+    nb.qy0 = inside ? q.y[c0] : 0.0;
+    nb.qz0 = inside ? q.z[c0] : 0.0;
+    cp_async_wait<0>();  // u*, p of K+1 and delta of K+2 have landed
+    __syncthreads();     // ... for every thread; plane K-1's raw slots are free
+    project_plane(K + 1);
+    if (K + 1 <= K1) {   // raw data of plane K+2 for the next iteration
+      issue_us(K + 2);
+      box(p_in, K + 2, p_slot(K + 2));
+      box(delta, K + 3, d_slot(K + 3));
+    }
+    cp_async_commit();
+    __syncthreads();     // projected plane K+1 complete
+    if (inside) {
+      const double *pk = p_slot(K) + h, *pk1 = p_slot(K + 1) + h;
+      const double *dk = d_slot(K) + h, *dk1 = d_slot(K + 1) + h;
+      nb.p0 = pk[0] + dk[0] * radt;
+      nb.pE = pk[1] + dk[1] * radt;
+      nb.pN = pk[SY] + dk[SY] * radt;
+      nb.pT = pk1[0] + dk1[0] * radt;
+      const double *ub = un_slot(K - 1) + h, *uc = un_slot(K) + h, *ut = un_slot(K + 1) + h;
+      const double *bx = ub, *cx = uc, *tx_ = ut;
+      const double *by = ub + GP_N, *cy = uc + GP_N, *ty_ = ut + GP_N;
+      const double *bz = ub + 2 * GP_N, *cz = uc + 2 * GP_N, *tz_ = ut + 2 * GP_N;
+      nb.ux0 = cx[0]; nb.uxE = cx[1]; nb.uxW = cx[-1]; nb.uxN = cx[SY]; nb.uxS = cx[-SY];
+      nb.uxT = tx_[0]; nb.uxB = bx[0]; nb.uxWN = cx[SY - 1]; nb.uxWT = tx_[-1];
+      nb.uy0 = cy[0]; nb.uyE = cy[1]; nb.uyW = cy[-1]; nb.uyN = cy[SY]; nb.uyS = cy[-SY];
+      nb.uyT = ty_[0]; nb.uyB = by[0]; nb.uySE = cy[1 - SY]; nb.uyST = ty_[-SY];
+      nb.uz0 = cz[0]; nb.uzE = cz[1]; nb.uzW = cz[-1]; nb.uzN = cz[SY]; nb.uzS = cz[-SY];
+      nb.uzT = tz_[0]; nb.uzB = bz[0]; nb.uzEB = bz[1]; nb.uzNB = bz[SY];
+      const MomCell m = mom_compute<MOM_IMPLICIT>(g, J, nb, A, dt, B, adt, 1, ymet, theta);
+      mom_store<MOM_IMPLICIT>(g, I, J, K, m, q, out);
+      store_img(p_out, g, I, J, K, nb.p0, STAG_P);
+    }
+  }
+  cp_async_wait<0>();
+}
+
+// Dynamic shared memory of k_gradmom_march.
+constexpr size_t GRADMOM_SMEM = sizeof(double) * (2 * 3 + 3 + 4 + 3 * 3) * GP_N;
+
+}  // namespace dnsb
