@@ -53,21 +53,29 @@ __global__ void __launch_bounds__(MC_X *MC_Y, 3)
   const int K0 = blockIdx.z * MC_Z + 1, K1 = min(g.nz, K0 + MC_Z - 1);
   const bool wall = g.wall;
   constexpr int CH = GP_X / 2;
-  // one GP_X x GP_Y box of field f at plane z into dst; x, y, z beyond the
-  // ghosted array wrap by one period (periodic directions; wall rows there
-  // are never read)
+  static_assert(GP_Y * CH <= NT, "one staging chunk per thread and field plane");
+  // This thread's 16-byte chunk of every staged GP_X x GP_Y box: the same
+  // in-plane offsets for every plane and field.  x and y beyond the ghosted
+  // array wrap by one period (periodic directions; wall rows there are never
+  // read).
+  const long long plane = (long long)g.NX * g.NY;
+  bool stage = tid < GP_Y * CH;
+  int goff = 0, soff = 0;
+  if (stage) {
+    const int ch = tid % CH, hy = tid / CH;
+    int x = I0 - 1 + 2 * ch, y = J0 - 1 + hy;
+    if (x >= g.NX) x -= g.nx;
+    if (y >= g.NY) {
+      if (wall) stage = false;
+      y -= g.ny;
+    }
+    goff = x + g.NX * y;
+    soff = 2 * ch + GP_X * hy;
+  }
+  // the box of field f at plane z (z beyond the array wraps, z is periodic)
   auto box = [&](const double *f, int z, double *dst) {
     if (z >= g.NZ) z -= g.nz;
-    for (int t = tid; t < GP_Y * CH; t += NT) {
-      const int ch = t % CH, hy = t / CH;
-      int x = I0 - 1 + 2 * ch, y = J0 - 1 + hy;
-      if (x >= g.NX) x -= g.nx;
-      if (y >= g.NY) {
-        if (wall) continue;
-        y -= g.ny;
-      }
-      cp_async16(dst + 2 * ch + GP_X * hy, f + gidx(g, x, y, z));
-    }
+    if (stage) cp_async16(dst + soff, f + (plane * z + goff));
   };
   auto us_slot = [&](int z) { return ustar + (z & 1) * 3 * GP_N; };
   auto p_slot = [&](int z) { return pold + (z % 3) * GP_N; };
@@ -105,20 +113,31 @@ __global__ void __launch_bounds__(MC_X *MC_Y, 3)
     if (c == STAG_Y) rg[hy] = sgn != 0.0 ? __ldg(g.rdyu + (J0 - 1 + hs)) : 0.0;
   }
   // projected u of plane z on the HX x HY tile + halo, from u* of plane z
-  // and delta of planes z, z+1 (all staged)
+  // and delta of planes z, z+1 (all staged); thread (tx, ty) covers columns
+  // tx, tx + MC_X and rows ty, ty + MC_Y of each component
   auto project_plane = [&](int z) {
     const double *su = us_slot(z), *d0 = d_slot(z), *d1 = d_slot(z + 1);
     double *dst = un_slot(z);
-    for (int t = tid; t < 3 * HX * HY; t += NT) {
-      const int c = t / (HX * HY), r = t - c * HX * HY;
-      const int hy = r / HX, hx = r - hy * HX;
-      const int a = hx + GP_X * rsrc[c][hy];
-      const double sgn = rsgn[c][hy];
-      double v;
-      if (c == STAG_X) v = su[a] - (d0[a + 1] - d0[a]) * g.rdx;
-      else if (c == STAG_Y) v = su[GP_N + a] - (d0[a + GP_X] - d0[a]) * rg[hy];
-      else v = su[2 * GP_N + a] - (d1[a] - d0[a]) * g.rdz;
-      dst[c * GP_N + hx + GP_X * hy] = sgn * v;
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+#pragma unroll
+      for (int ry = 0; ry < 2; ry++) {
+        const int hy = ty + ry * MC_Y;
+        if (hy >= HY) continue;
+        const int srow = GP_X * rsrc[c][hy];
+        const double sgn = rsgn[c][hy];
+#pragma unroll
+        for (int rx = 0; rx < 2; rx++) {
+          const int hx = tx + rx * MC_X;
+          if (hx >= HX) continue;
+          const int a = hx + srow;
+          double v;
+          if (c == STAG_X) v = su[a] - (d0[a + 1] - d0[a]) * g.rdx;
+          else if (c == STAG_Y) v = su[GP_N + a] - (d0[a + GP_X] - d0[a]) * rg[hy];
+          else v = su[2 * GP_N + a] - (d1[a] - d0[a]) * g.rdz;
+          dst[c * GP_N + hx + GP_X * hy] = sgn * v;
+        }
+      }
     }
   };
   // prologue: u* of K0-1, K0; p of K0; delta of K0-1, K0, K0+1

@@ -258,19 +258,28 @@ __global__ void __launch_bounds__(MC_X *MC_Y, 3)
   const int I0 = blockIdx.x * MC_X + 1, J0 = blockIdx.y * MC_Y + 1;
   const int K0 = blockIdx.z * MC_Z + 1, K1 = min(g.nz, K0 + MC_Z - 1);
   constexpr int CH = MP_X / 2;  // 16-byte chunks per halo row
-  constexpr int NCH = 3 * MP_Y * CH;
-  // copies plane z (0..NZ-1) into its ring slot; rows and chunks outside the
-  // ghosted array are never read by an interior cell
+  static_assert(MP_Y * CH <= MC_X * MC_Y, "one staging chunk per thread and field plane");
+  // this thread's chunk of every staged plane (the same in-plane offset for
+  // all planes and components); chunks outside the ghosted array are never
+  // read by an interior cell
+  const long long plane = (long long)g.NX * g.NY;
+  int goff = 0, soff = 0;
+  bool stage = tid < MP_Y * CH;
+  if (stage) {
+    const int ch = tid % CH, hy = tid / CH;
+    const int x = I0 - 1 + 2 * ch, y = J0 - 1 + hy;
+    stage = x + 1 < g.NX && y < g.NY;
+    goff = x + g.NX * y;
+    soff = 2 * ch + MP_X * hy;
+  }
+  // copies plane z (0..NZ-1) of the three components into its ring slot
   auto issue = [&](int z) {
     double(*slot)[MP_N] = ring[z & 3];
-    for (int t = tid; t < NCH; t += MC_X * MC_Y) {
-      const int ch = t % CH, r = t / CH;
-      const int c = r / MP_Y, hy = r - c * MP_Y;
-      const int x = I0 - 1 + 2 * ch, y = J0 - 1 + hy;
-      if (x + 1 < g.NX && y < g.NY) {
-        const double *src = (c == 0 ? u.x : c == 1 ? u.y : u.z) + gidx(g, x, y, z);
-        cp_async16(&slot[c][2 * ch + MP_X * hy], src);
-      }
+    if (stage) {
+      const long long o = plane * z + goff;
+      cp_async16(&slot[0][soff], u.x + o);
+      cp_async16(&slot[1][soff], u.y + o);
+      cp_async16(&slot[2][soff], u.z + o);
     }
     cp_async_commit();
   };
