@@ -4,7 +4,7 @@ DistributedNavierStokes as hand-written sm_100a CUDA kernels behind a C ABI
 setup/solve API (api.py).
 """
 from .api import (  # noqa: F401
-    RK3, State, VectorField, channelprofiles, channelstats, cfl_timestep, divergence,
+    RK3, Ensemble, State, VectorField, channelprofiles, channelstats, cfl_timestep, divergence,
     energyspectrum, exchange_halo, imex_update, interior, kinetic_energy, logger, maxdiv,
     momentum, noise, poisson, pressuregrad_component, pressuregrad_update, project,
     scalarfield, setup, solve, spectrumstats, step, vectorfield, velocityfield,

@@ -62,6 +62,12 @@ SIGNATURES = {
     "dnsb_launch_count": (c_long, [P]),
     "dnsb_kind_name": (ctypes.c_char_p, [c_int]),
     "dnsb_poisson_noalloc": (c_int, [ctypes.POINTER(dnsb_grid), P, P, P]),
+    "dnsb_ensemble_create": (c_int, [c_int, ctypes.POINTER(dnsb_grid), c_int, P,
+                                     ctypes.POINTER(c_void_p)]),
+    "dnsb_ensemble_destroy": (None, [P]),
+    "dnsb_ensemble_last_error": (ctypes.c_char_p, [P]),
+    "dnsb_ensemble_member": (P, [P, c_int]),
+    "dnsb_ensemble_run": (c_int, [P, ctypes.POINTER(c_void_p), ctypes.POINTER(c_double), c_long]),
 }
 
 KINDS = ["momentum", "cn_solve", "div_rfft_x", "fft_z", "y_solve", "ifft_z", "irfft_x",

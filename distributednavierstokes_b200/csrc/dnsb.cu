@@ -15,6 +15,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <map>
+#include <mutex>
 #include <cmath>
 #include <cstdarg>
 #include <cstdint>
@@ -233,10 +235,27 @@ CFields3 cf(const double *x, const double *y, const double *z) { return CFields3
 Fields3 ff(double *x, double *y, double *z) { return Fields3{x, y, z}; }
 
 // opt in to the dynamic shared memory a kernel launches with (needed whenever
-// static + dynamic shared memory exceeds 48 KB; set unconditionally)
+// static + dynamic shared memory exceeds 48 KB; requested unconditionally).
+// The attribute belongs to the kernel function (per device), not to the
+// context, so contexts of different sizes in one process may only ever raise
+// it: the largest request per (device, kernel) is kept.
+template <class K>
+cudaError_t raise_smem(int device, K kernel, size_t bytes) {
+  static std::mutex mu;
+  static std::map<std::pair<int, const void *>, size_t> granted;
+  std::lock_guard<std::mutex> lock(mu);
+  size_t &cur = granted[{device, reinterpret_cast<const void *>(kernel)}];
+  if (bytes <= cur && cur != 0) return cudaSuccess;
+  const size_t want = std::max(bytes, cur);
+  const cudaError_t e =
+      cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)want);
+  if (e == cudaSuccess) cur = want;
+  return e;
+}
+
 template <class K>
 int allow_smem(dnsb_ctx *c, K kernel, size_t bytes) {
-  CK(c, cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  CK(c, raise_smem(c->device, kernel, bytes));
   return 0;
 }
 
@@ -1291,6 +1310,169 @@ int dnsb_solve_host(dnsb_ctx *c, double *ux, double *uy, double *uz, double *p, 
   return rc;
 }
 
+// ---------------------------------------------------------------- ensembles
+// Members are ordinary contexts with their own streams.  One RK3 step of all
+// members is captured from an internal origin stream (capture cannot start
+// on the legacy default stream a caller may pass): fork event -> member
+// streams -> join events; the executable graph is replayed on the origin
+// stream, which is ordered after and before the caller's stream by events.
+
+struct dnsb_ensemble {
+  int n = 0, device = 0;
+  cudaStream_t stream = nullptr;  // the caller's
+  cudaStream_t origin = nullptr;
+  std::vector<dnsb_ctx *> m;
+  std::vector<cudaStream_t> ms;
+  std::vector<cudaEvent_t> done;
+  cudaEvent_t fork = nullptr, in = nullptr, out = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  std::vector<double *> key_fields;
+  std::vector<double> key_dts;
+  std::string err;
+};
+
+static int efail(dnsb_ensemble *e, int code, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  if (e) e->err = buf;
+  else snprintf(g_create_err, sizeof g_create_err, "%s", buf);
+  return code;
+}
+
+static void ens_drop_graph(dnsb_ensemble *e) {
+  if (e->exec) cudaGraphExecDestroy(e->exec);
+  if (e->graph) cudaGraphDestroy(e->graph);
+  e->exec = nullptr;
+  e->graph = nullptr;
+  e->key_fields.clear();
+  e->key_dts.clear();
+}
+
+void dnsb_ensemble_destroy(dnsb_ensemble *e) {
+  if (!e) return;
+  cudaSetDevice(e->device);
+  if (e->origin) cudaStreamSynchronize(e->origin);
+  ens_drop_graph(e);
+  for (dnsb_ctx *c : e->m) dnsb_destroy(c);
+  for (cudaStream_t st : e->ms) cudaStreamDestroy(st);
+  for (cudaEvent_t ev : e->done) cudaEventDestroy(ev);
+  if (e->fork) cudaEventDestroy(e->fork);
+  if (e->in) cudaEventDestroy(e->in);
+  if (e->out) cudaEventDestroy(e->out);
+  if (e->origin) cudaStreamDestroy(e->origin);
+  delete e;
+}
+
+int dnsb_ensemble_create(int n, const dnsb_grid *grids, int device, void *stream,
+                         dnsb_ensemble **out) {
+  if (!out || !grids || n <= 0) return efail(nullptr, DNSB_EINVAL, "need n >= 1 grids and an output");
+  *out = nullptr;
+  if (cudaSetDevice(device) != cudaSuccess)
+    return efail(nullptr, DNSB_ECUDA, "cudaSetDevice(%d) failed", device);
+  dnsb_ensemble *e = new dnsb_ensemble();
+  e->n = n;
+  e->device = device;
+  e->stream = (cudaStream_t)stream;
+  auto bail = [&](int rc, const char *msg) {
+    snprintf(g_create_err, sizeof g_create_err, "%.500s", msg);
+    dnsb_ensemble_destroy(e);
+    return rc;
+  };
+  if (cudaStreamCreateWithFlags(&e->origin, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&e->in, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&e->out, cudaEventDisableTiming) != cudaSuccess)
+    return bail(DNSB_ECUDA, "stream or event creation failed");
+  for (int i = 0; i < n; i++) {
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev = nullptr;
+    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess)
+      return bail(DNSB_ECUDA, "member stream creation failed");
+    e->ms.push_back(st);
+    if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess)
+      return bail(DNSB_ECUDA, "member event creation failed");
+    e->done.push_back(ev);
+    dnsb_ctx *c = nullptr;
+    const int rc = dnsb_create(&grids[i], device, st, &c);
+    if (rc) {
+      char msg[600];
+      snprintf(msg, sizeof msg, "member %d: %.480s", i, g_create_err);
+      return bail(rc, msg);
+    }
+    e->m.push_back(c);
+  }
+  *out = e;
+  return 0;
+}
+
+const char *dnsb_ensemble_last_error(const dnsb_ensemble *e) { return e ? e->err.c_str() : g_create_err; }
+
+dnsb_ctx *dnsb_ensemble_member(dnsb_ensemble *e, int i) {
+  return (e && i >= 0 && i < e->n) ? e->m[i] : nullptr;
+}
+
+int dnsb_ensemble_run(dnsb_ensemble *e, double *const *fields, const double *dts, long nsteps) {
+  if (!e) return DNSB_EINVAL;
+  if (!fields || !dts || nsteps < 0) return efail(e, DNSB_EINVAL, "null fields/dts or nsteps < 0");
+  if (cudaSetDevice(e->device) != cudaSuccess) return efail(e, DNSB_ECUDA, "cudaSetDevice failed");
+  const int n = e->n;
+  std::vector<double *> f(fields, fields + 8 * (size_t)n);
+  std::vector<double> d(dts, dts + n);
+  for (int i = 0; i < n; i++) {
+    if (!(d[i] > 0.0)) return efail(e, DNSB_EINVAL, "member %d: dt must be positive", i);
+    for (int k = 0; k < 7; k++)
+      if (!f[8 * i + k]) return efail(e, DNSB_EINVAL, "member %d: null field %d", i, k);
+  }
+  if (nsteps == 0) return 0;
+  if (!e->exec || f != e->key_fields || d != e->key_dts) {
+    ens_drop_graph(e);
+    if (cudaStreamBeginCapture(e->origin, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+      return efail(e, DNSB_ECUDA, "stream capture could not start");
+    int rc = 0;
+    cudaEventRecord(e->fork, e->origin);
+    for (int i = 0; i < n && !rc; i++) {
+      cudaStreamWaitEvent(e->ms[i], e->fork, 0);
+      double *const *fi = f.data() + 8 * (size_t)i;
+      rc = dnsb_step(e->m[i], fi[0], fi[1], fi[2], fi[3], fi[4], fi[5], fi[6], fi[7], d[i]);
+      if (rc) {
+        efail(e, rc, "member %d: %s", i, dnsb_last_error(e->m[i]));
+        break;
+      }
+      cudaEventRecord(e->done[i], e->ms[i]);
+      cudaStreamWaitEvent(e->origin, e->done[i], 0);
+    }
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(e->origin, &graph);
+    if (rc) {
+      if (graph) cudaGraphDestroy(graph);
+      return rc;
+    }
+    if (ce != cudaSuccess || !graph)
+      return efail(e, DNSB_ECUDA, "stream capture failed: %s", cudaGetErrorString(ce));
+    e->graph = graph;
+    if (cudaGraphInstantiate(&e->exec, e->graph, 0) != cudaSuccess) {
+      ens_drop_graph(e);
+      return efail(e, DNSB_ECUDA, "graph instantiation failed");
+    }
+    e->key_fields = f;
+    e->key_dts = d;
+  }
+  cudaEventRecord(e->in, e->stream);
+  cudaStreamWaitEvent(e->origin, e->in, 0);
+  for (long s = 0; s < nsteps; s++)
+    if (cudaGraphLaunch(e->exec, e->origin) != cudaSuccess)
+      return efail(e, DNSB_ECUDA, "graph launch failed");
+  cudaEventRecord(e->out, e->origin);
+  cudaStreamWaitEvent(e->stream, e->out, 0);
+  const cudaError_t le = cudaGetLastError();
+  if (le != cudaSuccess) return efail(e, DNSB_ECUDA, "%s", cudaGetErrorString(le));
+  return 0;
+}
+
 }  // extern "C"
 
 // ====================================================== allocation-free ==
@@ -1339,11 +1521,11 @@ int noalloc_setup(int dev, double **out) {
       return fail(nullptr, DNSB_ECUDA, "cudaGetSymbolAddress(scratch): %s", cudaGetErrorString(e));
     const int big = 200 * 1024;
     cudaError_t a = cudaSuccess;
-    a = a != cudaSuccess ? a : cudaFuncSetAttribute(k_rfftx<RIN_REAL>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
-    a = a != cudaSuccess ? a : cudaFuncSetAttribute(k_fftz<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
-    a = a != cudaSuccess ? a : cudaFuncSetAttribute(k_fftz<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
-    a = a != cudaSuccess ? a : cudaFuncSetAttribute(k_yfourier<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
-    a = a != cudaSuccess ? a : cudaFuncSetAttribute(k_irfftx<ROUT_INTERIOR>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+    a = a != cudaSuccess ? a : raise_smem(dev, k_rfftx<RIN_REAL>, big);
+    a = a != cudaSuccess ? a : raise_smem(dev, k_fftz<false>, big);
+    a = a != cudaSuccess ? a : raise_smem(dev, k_fftz<true>, big);
+    a = a != cudaSuccess ? a : raise_smem(dev, k_yfourier<false>, big);
+    a = a != cudaSuccess ? a : raise_smem(dev, k_irfftx<ROUT_INTERIOR>, big);
     if (a != cudaSuccess)
       return fail(nullptr, DNSB_ECUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(a));
     g_noalloc_ptr[dev] = (double *)ptr;

@@ -173,6 +173,25 @@ int dnsb_noise(dnsb_ctx *ctx, double *phi, int c, unsigned long long seed, doubl
  * reported by dnsb_last_error(NULL). */
 int dnsb_poisson_noalloc(const dnsb_grid *grid, const double *r, double *p, void *stream);
 
+/* Ensembles (no counterpart in the reference; the batched periodic-box
+ * ensemble of the north star): n independent members, each a context of its
+ * own grid and viscosity with its own stream.  dnsb_ensemble_run advances
+ * every member nsteps RK3 steps with a fixed step dts[i] (dnsb_step on each
+ * member): one step of all members is captured once into a CUDA graph whose
+ * member branches run concurrently (fork/join from the caller's stream) and
+ * the graph is replayed nsteps times on that stream.  fields holds 8 device
+ * pointers per member: ux, uy, uz, p, qx, qy, qz, delta (delta NULL for an
+ * explicit member).  The graph is re-captured when the pointers or steps
+ * change.  Results equal those of stepping each member alone. */
+typedef struct dnsb_ensemble dnsb_ensemble;
+int dnsb_ensemble_create(int n, const dnsb_grid *grids, int device, void *stream,
+                         dnsb_ensemble **out);
+void dnsb_ensemble_destroy(dnsb_ensemble *ens);
+const char *dnsb_ensemble_last_error(const dnsb_ensemble *ens);
+/* Context of member i (for the per-member calls: cfl, noise, project, ...). */
+dnsb_ctx *dnsb_ensemble_member(dnsb_ensemble *ens, int i);
+int dnsb_ensemble_run(dnsb_ensemble *ens, double *const *fields, const double *dts, long nsteps);
+
 /* Instrumentation (no counterpart in the reference, which has no profiling
  * for the FV path): launches are counted always; with dnsb_profile(ctx, 1)
  * every launch of the step path is bracketed by CUDA events on the context's

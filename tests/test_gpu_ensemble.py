@@ -1,0 +1,96 @@
+"""The batched ensemble (dnsb_ensemble_*, api.Ensemble): members of uneven
+sizes and viscosities advanced through one CUDA graph must equal, bit for
+bit, each member stepped alone with dnsb_step (the north star's batched
+periodic-box ensemble; the reference has no ensemble path)."""
+import math
+
+import pytest
+
+import refcases as R
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+MEMBERS = [
+    dict(n=(16, 16, 16), visc=1e-2),
+    dict(n=(24, 20, 16), visc=3e-3),
+    dict(n=(32, 32, 32), visc=1e-3),
+    R.channel_kwargs(visc=0.05, bodyforce=(1.0, 0.0, 0.0), ydiffusion="implicit"),
+]
+
+
+@pytest.fixture(scope="module")
+def D():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    import distributednavierstokes_b200 as dns
+
+    return dns
+
+
+def _state(D, s, seed):
+    u = D.vectorfield(s)
+    for i, c in enumerate("xyz"):
+        D.noise(u[c], c, s, seed + i, 0.5)
+    D.exchange_halo(u, s)
+    p = D.scalarfield(s)
+    D.project(u, p, s)
+    q = D.vectorfield(s)
+    delta = D.scalarfield(s) if s.imexy else None
+    return u, p, q, delta
+
+
+def _clone(st):
+    u, p, q, delta = st
+    return ({c: u[c].clone() for c in "xyz"}, p.clone(), {c: q[c].clone() for c in "xyz"},
+            None if delta is None else delta.clone())
+
+
+def _as_fields(D, st):
+    u, p, q, delta = st
+    return (D.VectorField(x=u["x"], y=u["y"], z=u["z"]), p,
+            D.VectorField(x=q["x"], y=q["y"], z=q["z"]), delta)
+
+
+def test_ensemble_equals_members_stepped_alone(D):
+    setups = [D.setup(**kw) for kw in MEMBERS]
+    ref = [_state(D, s, 10 * i) for i, s in enumerate(setups)]
+    ens_states = [_as_fields(D, _clone(st)) for st in ref]
+    ref = [_as_fields(D, st) for st in ref]
+    dts = [0.5 * D.cfl_timestep(st[0], s, 0.5) for st, s in zip(ref, setups)]
+    E = D.Ensemble(setups)
+    for nsteps in (3, 2):  # the second call replays the captured graph
+        E.run(ens_states, dts, nsteps)
+        for st, s, dt in zip(ref, setups, dts):
+            for _ in range(nsteps):
+                D.step(st[0], st[1], st[2], st[3] if st[3] is not None else st[1], s, dt)
+        torch.cuda.synchronize()
+        for i, (a, b) in enumerate(zip(ens_states, ref)):
+            for c in "xyz":
+                assert torch.equal(a[0][c], b[0][c]), (i, c)
+                assert torch.equal(a[2][c], b[2][c]), (i, c)
+            assert torch.equal(a[1], b[1]), i
+    # new steps: the graph is captured again
+    dts2 = [0.8 * dt for dt in dts]
+    E.run(ens_states, dts2, 2)
+    for st, s, dt in zip(ref, setups, dts2):
+        for _ in range(2):
+            D.step(st[0], st[1], st[2], st[3] if st[3] is not None else st[1], s, dt)
+    torch.cuda.synchronize()
+    for i, (a, b) in enumerate(zip(ens_states, ref)):
+        for c in "xyz":
+            assert torch.equal(a[0][c], b[0][c]), (i, c)
+    for (u, _, _, _), s in zip(ens_states, setups):
+        assert D.maxdiv(u, s) < 1e-12
+    E.close()
+
+
+def test_ensemble_rejects_bad_arguments(D):
+    s = D.setup(**MEMBERS[0])
+    E = D.Ensemble([s])
+    st = _as_fields(D, _state(D, s, 1))
+    with pytest.raises(Exception):
+        E.run([st], [0.0], 1)  # non-positive step
+    with pytest.raises(ValueError):
+        E.run([st, st], [0.1], 1)
+    E.close()
