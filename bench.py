@@ -1,7 +1,8 @@
 """Benchmark: FP64 finite-volume channel DNS cell-steps/s on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                    [--workload channel384_implicit|channel64_explicit]
+                    [--workload channel384_implicit|channel256_implicit|
+                                channel64_explicit|ensemble64_periodic]
 
 One "step" is one full RK3 time step (3 stages: momentum, semi-implicit
 wall-normal Crank-Nicolson, FFT/Thomas projection, lagged-pressure update)
@@ -43,6 +44,12 @@ WORKLOADS = {
     "channel64_explicit": dict(
         n=(64, 64, 64), ydiffusion="explicit", visc=1 / 180, cfl=0.5, amp=0.1, retau=None,
         bytes_per_cell_step=792.0),
+    # batched ensemble of triply periodic boxes (2 pi)^3, explicit: 64 members,
+    # sizes from SIZES and viscosities log-uniform in [1e-3, 1e-2] drawn with a
+    # fixed seed, a fixed step per member (CFL 0.5 of its initial field)
+    "ensemble64_periodic": dict(
+        members=64, sizes=(32, 48, 64, 96, 128), visc=(1e-3, 1e-2), cfl=0.5, amp=1.0,
+        ydiffusion="explicit", bytes_per_cell_step=792.0),
 }
 COMMON = dict(lims=((0.0, 4 * math.pi), (-1.0, 1.0), (0.0, 4 * math.pi / 3)),
               bc=("periodic", "wall", "periodic"), bodyforce=(1.0, 0.0, 0.0))
@@ -219,6 +226,82 @@ def reference_arm(args, wl, world, rank):
 
 
 # ----------------------------------------------------------------- GPU arm
+
+def ensemble_arm(args, wl, world, rank, local):
+    """The batched ensemble: one CUDA graph replay advances every member one
+    RK3 step; timed against the same members stepped one after another."""
+    import torch
+
+    import distributednavierstokes_b200 as dns
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    rng = np.random.default_rng(12345)
+    ns = rng.choice(wl["sizes"], size=wl["members"])
+    lo, hi = np.log(wl["visc"][0]), np.log(wl["visc"][1])
+    viscs = np.exp(rng.uniform(lo, hi, size=wl["members"]))
+    setups, states, dts = [], [], []
+    for i, (n, nu) in enumerate(zip(ns, viscs)):
+        s = dns.setup(n=(int(n),) * 3, visc=float(nu), device=dev)
+        u = dns.vectorfield(s)
+        for k, c in enumerate("xyz"):
+            dns.noise(u[c], c, s, 3 * i + k, wl["amp"])
+        dns.exchange_halo(u, s)
+        p = dns.scalarfield(s)
+        dns.project(u, p, s)
+        q = dns.vectorfield(s)
+        dts.append(dns.cfl_timestep(u, s, wl["cfl"]))
+        setups.append(s)
+        states.append((u, p, q, None))
+    cells = int(sum(int(n) ** 3 for n in ns))
+    E = dns.Ensemble(setups)
+    E.run(states, dts, max(args.warmup, 1))  # captures the graph
+    torch.cuda.synchronize(dev)
+    stream = torch.cuda.current_stream(dev)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clocks = ClockSampler(local)
+    clocks.start()
+    ev0.record(stream)
+    E.run(states, dts, args.steps)
+    ev1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms = ev0.elapsed_time(ev1)
+    clk = clocks.stop()
+    # the same members stepped one after another on one stream
+    ev0.record(stream)
+    for _ in range(args.steps):
+        for s, (u, p, q, _), dt in zip(setups, states, dts):
+            dns.step(u, p, q, None, s, dt)
+    ev1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms_seq = ev0.elapsed_time(ev1)
+    for (u, _, _, _), s in zip(states, setups):
+        assert dns.maxdiv(u, s) < 1e-10, "ensemble member lost incompressibility"
+    E.close()
+    peak, peak_kind = measured_peaks()
+    value = cells * args.steps / (ms / 1e3)
+    step_gbs = wl["bytes_per_cell_step"] * cells / (ms / args.steps / 1e3) / 1e9
+    if rank == 0:
+        line = {
+            "metric": "DNS cell-steps/s (FP64)", "value": value, "unit": "cell-steps/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (splitmix64 noise initial fields, projected; the random-phase "
+                    "E(k) initial condition and shell forcing of the configuration are not built)",
+            "config": {"workload": args.workload, "members": wl["members"],
+                       "sizes": sorted(set(int(n) for n in ns)), "total_cells": cells,
+                       "visc_range": list(wl["visc"]), "parallelism": "1 GPU, one CUDA graph"},
+            "sequential": {"value": cells * args.steps / (ms_seq / 1e3), "unit": "cell-steps/s",
+                           "ms_per_step": ms_seq / args.steps,
+                           "note": "the same members stepped one after another on one stream"},
+            "step_roofline": {"bytes_per_cell_step": wl["bytes_per_cell_step"],
+                              "achieved": step_gbs, "peak": peak, "unit": "GB/s",
+                              "frac": step_gbs / peak, "peak_source": peak_kind},
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+
 
 def b200_arm(args, wl, world, rank, local):
     import ctypes
@@ -415,7 +498,14 @@ def main():
     args.warmup = max(args.warmup, 3) if args.impl == "b200" else args.warmup
     wl = WORKLOADS[args.workload]
     world, rank, local = dist_init()
-    if args.impl == "reference":
+    if "members" in wl:
+        if args.impl == "reference":
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "unavailable":
+                                  "the reference has no ensemble path"}), flush=True)
+        else:
+            ensemble_arm(args, wl, world, rank, local)
+    elif args.impl == "reference":
         reference_arm(args, wl, world, rank)
     else:
         b200_arm(args, wl, world, rank, local)
