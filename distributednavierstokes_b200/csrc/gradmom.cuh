@@ -115,17 +115,19 @@ __global__ void __launch_bounds__(MC_X *MC_Y, 3)
   // projected u of plane z on the HX x HY tile + halo, from u* of plane z
   // and delta of planes z, z+1 (all staged); thread (tx, ty) covers columns
   // tx, tx + MC_X and rows ty, ty + MC_Y of each component
-  auto project_plane = [&](int z) {
+  // CTAs away from the walls take every row as it is (no row map)
+  const bool plain = wall ? (J0 >= 2 && J0 + MC_Y <= g.ny - 1) : (J0 + MC_Y <= g.ny + 1);
+  auto project_plane = [&](int z, double *dst) {
     const double *su = us_slot(z), *d0 = d_slot(z), *d1 = d_slot(z + 1);
-    double *dst = un_slot(z);
 #pragma unroll
     for (int c = 0; c < 3; c++) {
 #pragma unroll
       for (int ry = 0; ry < 2; ry++) {
         const int hy = ty + ry * MC_Y;
         if (hy >= HY) continue;
-        const int srow = GP_X * rsrc[c][hy];
-        const double sgn = rsgn[c][hy];
+        const int srow = GP_X * (plain ? hy : rsrc[c][hy]);
+        const double sgn = plain ? 1.0 : rsgn[c][hy];
+        const double gy = c == STAG_Y ? rg[hy] : 0.0;
 #pragma unroll
         for (int rx = 0; rx < 2; rx++) {
           const int hx = tx + rx * MC_X;
@@ -133,9 +135,9 @@ __global__ void __launch_bounds__(MC_X *MC_Y, 3)
           const int a = hx + srow;
           double v;
           if (c == STAG_X) v = su[a] - (d0[a + 1] - d0[a]) * g.rdx;
-          else if (c == STAG_Y) v = su[GP_N + a] - (d0[a + GP_X] - d0[a]) * rg[hy];
+          else if (c == STAG_Y) v = su[GP_N + a] - (d0[a + GP_X] - d0[a]) * gy;
           else v = su[2 * GP_N + a] - (d1[a] - d0[a]) * g.rdz;
-          dst[c * GP_N + hx + GP_X * hy] = sgn * v;
+          dst[c * GP_N + hx + GP_X * hy] = plain ? v : sgn * v;
         }
       }
     }
@@ -147,18 +149,21 @@ __global__ void __launch_bounds__(MC_X *MC_Y, 3)
   cp_async_commit();
   cp_async_wait<0>();
   __syncthreads();
-  project_plane(K0 - 1);
+  // ring slots, rotated once per plane
+  double *un_prev = un_slot(K0 - 1), *un_cur = un_slot(K0), *un_next = un_slot(K0 + 1);
+  double *p_cur = p_slot(K0), *p_next = p_slot(K0 + 1), *p_nn = p_slot(K0 + 2);
+  project_plane(K0 - 1, un_prev);
   __syncthreads();  // u* slot of K0-1 is reused by K0+1 below
   issue_us(K0);
   box(delta, K0 + 1, d_slot(K0 + 1));
-  box(p_in, K0, p_slot(K0));
+  box(p_in, K0, p_cur);
   cp_async_commit();
   cp_async_wait<0>();
   __syncthreads();
-  project_plane(K0);
+  project_plane(K0, un_cur);
   // plane K+1's raw data for the first iteration
   issue_us(K0 + 1);
-  box(p_in, K0 + 1, p_slot(K0 + 1));
+  box(p_in, K0 + 1, p_next);
   box(delta, K0 + 2, d_slot(K0 + 2));
   cp_async_commit();
   const int I = I0 + tx, J = J0 + ty;
@@ -173,22 +178,22 @@ __global__ void __launch_bounds__(MC_X *MC_Y, 3)
     nb.qz0 = inside ? q.z[c0] : 0.0;
     cp_async_wait<0>();  // u*, p of K+1 and delta of K+2 have landed
     __syncthreads();     // ... for every thread; plane K-1's raw slots are free
-    project_plane(K + 1);
+    project_plane(K + 1, un_next);
     if (K + 1 <= K1) {   // raw data of plane K+2 for the next iteration
       issue_us(K + 2);
-      box(p_in, K + 2, p_slot(K + 2));
+      box(p_in, K + 2, p_nn);
       box(delta, K + 3, d_slot(K + 3));
     }
     cp_async_commit();
     __syncthreads();     // projected plane K+1 complete
     if (inside) {
-      const double *pk = p_slot(K) + h, *pk1 = p_slot(K + 1) + h;
+      const double *pk = p_cur + h, *pk1 = p_next + h;
       const double *dk = d_slot(K) + h, *dk1 = d_slot(K + 1) + h;
       nb.p0 = pk[0] + dk[0] * radt;
       nb.pE = pk[1] + dk[1] * radt;
       nb.pN = pk[SY] + dk[SY] * radt;
       nb.pT = pk1[0] + dk1[0] * radt;
-      const double *ub = un_slot(K - 1) + h, *uc = un_slot(K) + h, *ut = un_slot(K + 1) + h;
+      const double *ub = un_prev + h, *uc = un_cur + h, *ut = un_next + h;
       const double *bx = ub, *cx = uc, *tx_ = ut;
       const double *by = ub + GP_N, *cy = uc + GP_N, *ty_ = ut + GP_N;
       const double *bz = ub + 2 * GP_N, *cz = uc + 2 * GP_N, *tz_ = ut + 2 * GP_N;
@@ -202,6 +207,14 @@ __global__ void __launch_bounds__(MC_X *MC_Y, 3)
       mom_store<MOM_IMPLICIT>(g, I, J, K, m, q, out);
       store_img(p_out, g, I, J, K, nb.p0, STAG_P);
     }
+    double *t = un_prev;
+    un_prev = un_cur;
+    un_cur = un_next;
+    un_next = t;
+    t = p_cur;
+    p_cur = p_next;
+    p_next = p_nn;
+    p_nn = t;
   }
   cp_async_wait<0>();
 }
