@@ -195,6 +195,40 @@ def test_one_step(oracle_mod, D, cfg):
     assert D.maxdiv(ud, sd) < 1e-12
 
 
+# Production lengths in one direction at a time (the other two small, so the
+# oracle stays fast): ny = 256 takes the 16-row Crank-Nicolson chunks and the
+# 8-row chunked Poisson y-solve; nx = nz = 384 take the four-step 16 x 12
+# x-transforms and 16 x 24 z-transforms of the 384 x 256 x 384 benchmark.
+PRODUCTION = {
+    "ny256": dict(n=(16, 256, 8), lims=((0, 4 * math.pi), (-1, 1), (0, 4 * math.pi / 3)),
+                  bc=("periodic", "wall", "periodic"), stretch=R.tanhstretch(1.5),
+                  visc=1 / 395, bodyforce=(1.0, 0.0, 0.0), ydiffusion="implicit"),
+    "nx384_nz384": dict(n=(384, 8, 384), lims=((0, 4 * math.pi), (-1, 1), (0, 4 * math.pi / 3)),
+                        bc=("periodic", "wall", "periodic"), stretch=R.tanhstretch(1.5),
+                        visc=1 / 395, bodyforce=(1.0, 0.0, 0.0), ydiffusion="implicit"),
+}
+
+
+@pytest.mark.parametrize("cfg", list(PRODUCTION))
+def test_one_step_production_lengths(oracle_mod, D, cfg):
+    """One semi-implicit RK3 step at the benchmark's line lengths: <= 1e-12."""
+    so, sd = both(oracle_mod, D, **PRODUCTION[cfg])
+    u = rand_fields(so)
+    p = so.scalarfield()
+    so.project(u, p)
+    ud, pd = to_dev(D, u), T(p)
+    q, qd = so.vectorfield(), D.vectorfield(sd)
+    delta, deltad = so.scalarfield(), D.scalarfield(sd)
+    dt = 0.5 * so.cfl_timestep(u, 0.5)
+    so.step(u, p, q, delta, dt)
+    D.step(ud, pd, qd, deltad, sd, dt)
+    for c in "xyz":
+        assert rel(N(ud[c]), u[c]) <= TOL_STEP, c
+        assert rel(N(qd[c]), q[c]) <= 1e-11, c
+    assert rel(N(pd), p) <= 1e-10
+    assert D.maxdiv(ud, sd) < 1e-12
+
+
 def T_offset(a):
     """Device copy of a whose data starts 8 bytes past a 16-byte boundary."""
     a = np.ascontiguousarray(a)
