@@ -205,7 +205,7 @@ __global__ void __launch_bounds__(F4_THREADS, 2) k_irfftx4(Geo g, const double2 
   const int Lv = min(L, g.nz - k0);
   for (int t = threadIdx.x; t < M; t += blockDim.x) tw[t] = twM[t];
   for (int t = threadIdx.x; t <= M; t += blockDim.x) tn[t] = twN[t];
-  batched_copy<8>(
+  batched_copy<16>(  // one round of loads for L = 16 lines of 193
       L * (M + 1),
       [&](int t) {
         const int kx = t / L, l = t - kx * L;
