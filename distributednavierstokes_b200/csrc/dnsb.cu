@@ -553,8 +553,8 @@ int launch_ysolve(dnsb_ctx *c) {
 #define YT(MR)                                                                                    \
   case MR:                                                                                        \
     LAUNCH(c, DNSB_KIND_YSOLVE,                                                                   \
-           k_ythomas<MR><<<grid, block, 0, c->stream>>>(g, c->S, c->ycin, c->ay, c->by, c->cy,   \
-                                                        c->lam1, c->lam3));                       \
+           k_ythomas<MR><<<grid, block, ythomas_smem(MR), c->stream>>>(g, c->S, c->ycin, c->ay,   \
+                                                        c->by, c->cy, c->lam1, c->lam3));         \
     break;
     switch (ythomas_rows(g.ny)) {
       YT(1) YT(2) YT(3) YT(4) YT(6) YT(8) YT(12) YT(16)
@@ -961,6 +961,10 @@ int dnsb_create(const dnsb_grid *gr, int device, void *stream, dnsb_ctx **out) {
     return bail(rc);
   if (g.wall && ythomas_rows(ny) == 0 && (rc = dalloc(c, &c->work, nspec))) return bail(rc);
   if (g.wall && ythomas_rows(ny) != 0) {
+#define YTS(MR)                                                                                    \
+  if (ythomas_rows(ny) == MR && (rc = allow_smem(c, k_ythomas<MR>, ythomas_smem(MR)))) return bail(rc);
+    YTS(1) YTS(2) YTS(3) YTS(4) YTS(6) YTS(8) YTS(12) YTS(16)
+#undef YTS
     const long long nl = (long long)g.nkx * nz;
     if ((rc = dalloc(c, &c->ycin, (size_t)nl * TY_CHUNKS))) return bail(rc);
     k_ythomas_entries<<<(unsigned)((nl + 127) / 128), 128, 0, c->stream>>>(

@@ -97,8 +97,11 @@ __global__ void k_ythomas_entries(Geo g, int mr, double *__restrict__ cin,
   }
 }
 
+// dynamic shared memory of k_ythomas<MR>
+constexpr size_t ythomas_smem(int mr) { return sizeof(double) * (size_t)mr * TY_LINES * TY_CHUNKS; }
+
 template <int MR>
-__global__ void __launch_bounds__(TY_LINES *TY_CHUNKS, MR <= 8 ? 2 : 1)
+__global__ void __launch_bounds__(TY_LINES *TY_CHUNKS, MR <= 8 ? 3 : 1)
     k_ythomas(Geo g, double2 *__restrict__ S, const double *__restrict__ cin,
               const double *__restrict__ ay, const double *__restrict__ by,
               const double *__restrict__ cy, const double *__restrict__ lam1,
@@ -138,8 +141,17 @@ __global__ void __launch_bounds__(TY_LINES *TY_CHUNKS, MR <= 8 ? 2 : 1)
   }
   if (pin && s0 == 0) d[0] = make_double2(0.0, 0.0);
   double cprev = act ? __ldg(cin + t * TY_CHUNKS + ck) : 0.0;
-  // forward: c'_j and 1/beta_j of the chunk, its affine map d'_e = Z + G d'_{s-1}
-  double cp[MR], ib[MR];
+  // forward: 1/beta_j of the chunk (kept in shared memory, one column per
+  // thread; c'_j = c_j / beta_j is re-formed where needed), its affine map
+  // d'_e = Z + G d'_{s-1}
+  extern __shared__ double ibs[];  // [MR][TY_LINES * TY_CHUNKS] (dynamic: ythomas_smem)
+  const int tid = i + TY_LINES * ck;
+  constexpr int NT = TY_LINES * TY_CHUNKS;
+  auto cpj = [&](int r) {  // c'_j of row j = s0 + r from the stored 1/beta_j
+    const int j = s0 + r;
+    const double c = (pin && j == 0) ? 0.0 : __ldg(cy + j);
+    return c * ibs[r * NT + tid];
+  };
   {
     double2 z = make_double2(0.0, 0.0);
     double G = 1.0;
@@ -152,13 +164,11 @@ __global__ void __launch_bounds__(TY_LINES *TY_CHUNKS, MR <= 8 ? 2 : 1)
         const double beta = b - a * cprev;
         const double rb = 1.0 / beta;
         cprev = c * rb;
-        cp[r] = cprev;
-        ib[r] = rb;
+        ibs[r * NT + tid] = rb;
         z = make_double2((d[r].x - a * z.x) * rb, (d[r].y - a * z.y) * rb);
         G *= -a * rb;
       } else {
-        cp[r] = 0.0;
-        ib[r] = 0.0;
+        ibs[r * NT + tid] = 0.0;
       }
     }
     za[ck][i] = make_double4(z.x, z.y, G, 0.0);
@@ -174,7 +184,8 @@ __global__ void __launch_bounds__(TY_LINES *TY_CHUNKS, MR <= 8 ? 2 : 1)
       const int j = s0 + r;
       if (j < ny) {
         const double a = (pin && j == 0) ? 0.0 : __ldg(ay + j);
-        dp = make_double2((d[r].x - a * dp.x) * ib[r], (d[r].y - a * dp.y) * ib[r]);
+        const double rb = ibs[r * NT + tid];
+        dp = make_double2((d[r].x - a * dp.x) * rb, (d[r].y - a * dp.y) * rb);
         d[r] = dp;
       }
     }
@@ -187,8 +198,9 @@ __global__ void __launch_bounds__(TY_LINES *TY_CHUNKS, MR <= 8 ? 2 : 1)
     for (int r = MR - 1; r >= 0; r--) {
       const int j = s0 + r;
       if (j < ny) {
-        y = make_double2(d[r].x - cp[r] * y.x, d[r].y - cp[r] * y.y);
-        H *= -cp[r];
+        const double cpr = cpj(r);
+        y = make_double2(d[r].x - cpr * y.x, d[r].y - cpr * y.y);
+        H *= -cpr;
       }
     }
     yb[ck][i] = make_double4(y.x, y.y, H, 0.0);
@@ -202,7 +214,8 @@ __global__ void __launch_bounds__(TY_LINES *TY_CHUNKS, MR <= 8 ? 2 : 1)
   for (int r = MR - 1; r >= 0; r--) {
     const int j = s0 + r;
     if (j < ny) {
-      xn = make_double2(d[r].x - cp[r] * xn.x, d[r].y - cp[r] * xn.y);
+      const double cpr = cpj(r);
+      xn = make_double2(d[r].x - cpr * xn.x, d[r].y - cpr * xn.y);
       if (act) x[j * st] = xn;
     }
   }
