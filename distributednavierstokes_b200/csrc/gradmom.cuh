@@ -69,6 +69,9 @@ __global__ void __launch_bounds__(MC_X *MC_Y, 3)
       if (wall) stage = false;
       y -= g.ny;
     }
+    // on grids narrower than the box, columns/rows still beyond the array
+    // after one wrap are never read by an interior cell: not copied
+    if (x + 1 >= g.NX || y >= g.NY) stage = false;
     goff = x + g.NX * y;
     soff = 2 * ch + GP_X * hy;
   }
