@@ -7,7 +7,8 @@ from .api import (  # noqa: F401
     RK3, Ensemble, State, VectorField, channelprofiles, channelstats, cfl_timestep, divergence,
     energyspectrum, exchange_halo, imex_update, interior, kinetic_energy, logger, maxdiv,
     momentum, noise, poisson, pressuregrad_component, pressuregrad_update, project,
-    scalarfield, setup, solve, spectrumstats, step, vectorfield, velocityfield,
+    random_field, rescale_shell, scalarfield, setup, shell_count, shell_energies, shellforcing,
+    solve, spectrumstats, step, vectorfield, velocityfield,
 )
 
 __version__ = "0.1.0"

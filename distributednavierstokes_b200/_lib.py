@@ -57,6 +57,12 @@ SIGNATURES = {
     "dnsb_channel_sample": (c_int, [P, P, P, P, P]),
     "dnsb_spectrum_sample": (c_int, [P, P, P, P, P, c_int]),
     "dnsb_noise": (c_int, [P, P, c_int, ctypes.c_ulonglong, c_double]),
+    "dnsb_shell_count": (c_int, [P]),
+    "dnsb_shell_energies": (c_int, [P, P, P, P, ctypes.POINTER(c_double), c_int]),
+    "dnsb_shell_rescale": (c_int, [P, P, P, P, ctypes.POINTER(c_double), c_int]),
+    "dnsb_random_field": (c_int, [P, P, P, P, c_double, c_double, ctypes.c_ulonglong,
+                                  ctypes.POINTER(c_double), c_int]),
+    "dnsb_shell_clamp": (c_int, [P, P, P, P, ctypes.POINTER(c_double), c_int]),
     "dnsb_profile": (c_int, [P, c_int]),
     "dnsb_profile_read": (c_int, [P, c_int, ctypes.POINTER(c_double), ctypes.POINTER(c_long)]),
     "dnsb_launch_count": (c_long, [P]),

@@ -268,6 +268,78 @@ def noise(phi, c, s, seed=0, amp=1.0):
     return phi
 
 
+# ----------------------------------------------- wavenumber shells (periodic)
+# Finite-volume counterparts of the reference's pseudo-spectral random
+# initial condition and shell-clamp forcing (src/spectral/ic.jl:53-84,
+# src/spectral/forcing.jl:1-56).  Shell s = modes with s <= |k| < s+1.
+
+def _dbuf(values):
+    a = np.ascontiguousarray(values, dtype=np.float64)
+    return a, a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _u3(u):
+    return _ptr(u["x"]), _ptr(u["y"]), _ptr(u["z"])
+
+
+def shell_count(s):
+    """Number of integer shells of a periodic box (floor(|k|max) + 1)."""
+    return int(_lib.load().dnsb_shell_count(s.ctx))
+
+
+def shell_energies(u, s, shells):
+    """shell_energies(uh, s, shells) (src/spectral/forcing.jl:12-24)."""
+    shells = [int(v) for v in shells]
+    nb = max(shells) + 1 if shells else 1
+    E, ptr = _dbuf(np.zeros(nb))
+    check(_lib.load().dnsb_shell_energies(s.ctx, *_u3(u), ptr, nb), s._ctx)
+    return np.array([E[v] for v in shells])
+
+
+def rescale_shell(u, s, sh, factor):
+    """rescale_shell!(uh, s, sh, factor) (src/spectral/forcing.jl:26-35)."""
+    f = np.ones(int(sh) + 1)
+    f[int(sh)] = factor
+    f, ptr = _dbuf(f)
+    check(_lib.load().dnsb_shell_rescale(s.ctx, *_u3(u), ptr, len(f)), s._ctx)
+    return u
+
+
+def random_field(u, s, totalenergy=1.0, kpeak=4.0, seed=0, profile=None):
+    """spectral_randomfield!(uh, s; totalenergy, kpeak, seed, profile)
+    (src/spectral/ic.jl:53-84) on the staggered velocity of a periodic box:
+    Gaussian counter-based noise, FV projection, shells rescaled to the
+    profile (default k^4 exp(-2 (k/kpeak)^2))."""
+    lib = _lib.load()
+    if profile is None:
+        ptr, nprof = None, 0
+    else:
+        prof, ptr = _dbuf([profile(k) for k in range(shell_count(s))])
+        nprof = len(prof)
+    check(lib.dnsb_random_field(s.ctx, *_u3(u), float(totalenergy), float(kpeak), int(seed),
+                                ptr, nprof), s._ctx)
+    return u
+
+
+def shellforcing(u, s, shells=(1, 2), eref=None):
+    """shellforcing(uh, s; shells, eref) (src/spectral/forcing.jl:37-56):
+    records the energies of `shells` (or takes `eref`) and returns the
+    closure forcing(u, s) that clamps them back, entirely on the device."""
+    shells = [int(v) for v in shells]
+    eref = shell_energies(u, s, shells) if eref is None else np.asarray(eref, dtype=np.float64)
+    table = -np.ones(max(shells) + 1)
+    for sh, e in zip(shells, eref):
+        table[sh] = e
+    table, ptr = _dbuf(table)
+
+    def forcing(u2, s2):
+        check(_lib.load().dnsb_shell_clamp(s2.ctx, *_u3(u2), ptr, len(table)), s2._ctx)
+
+    forcing.eref = np.array(eref)
+    forcing._table = table
+    return forcing
+
+
 # -------------------------------------------------------------- operators
 
 def exchange_halo(phi, stag, s=None):
@@ -424,12 +496,14 @@ def kinetic_energy(u, s):
     return out.value
 
 
-def solve(*, u, setup, tlims, dt=None, cfl=0.5, processors=None, max_steps=None):
+def solve(*, u, setup, tlims, dt=None, cfl=0.5, processors=None, max_steps=None, forcing=None):
     """solve!(; u, setup, tlims, Δt, cfl, processors) (src/timestep.jl:92-111).
 
     Each processor is called as proc(state, setup) after every step (and
     once initially) with state = State(u, p, t, n).  Returns the final state.
     `max_steps` (not in the reference) stops the loop after that many steps.
+    `forcing(u, setup)` is applied after every step, before the processors,
+    as the spectral solver's hook (src/spectral/step.jl:109,162).
     """
     s = setup
     processors = dict(processors or {})
@@ -448,11 +522,13 @@ def solve(*, u, setup, tlims, dt=None, cfl=0.5, processors=None, max_steps=None)
         if max_steps is not None and n >= max_steps:
             break
         if dt is None:
-            dtn = cfl_timestep(u, s, cfl, use_step_max=stepped and not processors)
+            dtn = cfl_timestep(u, s, cfl, use_step_max=stepped and not processors and forcing is None)
         else:
             dtn = dt
         dtn = min(dtn, tend - t)
         step(u, p, q, delta, s, dtn)
+        if forcing is not None:
+            forcing(u, s)
         stepped = True
         t += dtn
         n += 1

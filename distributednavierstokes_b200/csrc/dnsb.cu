@@ -106,6 +106,9 @@ struct dnsb_ctx {
   double *V[3] = {nullptr, nullptr, nullptr};
   unsigned long long *umax = nullptr;  // [3] max |u_c| of the last step; [3] scratch
   double *partial = nullptr;           // reduction partials
+  double *shellbuf = nullptr;          // periodic boxes: [E | factors | eref] x nshell_max
+  int nshell_max = 0;                  // floor(|k|max) + 1
+  std::vector<double> eref_host;       // shell-clamp reference energies on the device
   int *deverr = nullptr;               // device-side error word (bounded waits)
   int use_tma = 1;                     // persistent TMA-pipelined z-FFT
   int x1 = 0, x2 = 0, z1 = 0, z2 = 0;  // four-step splits of nx/2 and nz (0: generic kernels)
@@ -382,24 +385,54 @@ __global__ void k_channel(Geo g, CFields3 u, double *acc, int nf) {
   }
 }
 
+// Integer shell of the spectrum entry t (S layout): round(|k|) for the
+// statistics of stats.jl:152, floor(|k|) for the shell operations of
+// src/spectral/forcing.jl:12-35; w = rfft double-counting weight.
+template <bool FLOORED>
+__device__ __forceinline__ int shell_of(const Geo &g, long long t, double &w) {
+  const int kz0 = (int)(t % g.nz);
+  const long long r = t / g.nz;
+  const int j = (int)(r % g.ny), kx = (int)(r / g.ny);
+  const int ky = j > g.ny / 2 ? j - g.ny : j;
+  const int kz = kz0 > g.nz / 2 ? kz0 - g.nz : kz0;
+  const long long k2 = (long long)kx * kx + (long long)ky * ky + (long long)kz * kz;
+  w = (0 < kx && 2 * kx < g.nx) ? 2.0 : 1.0;
+  if (FLOORED) {
+    long long s = (long long)sqrt((double)k2);  // integer square root, corrected
+    while (s * s > k2) s--;
+    while ((s + 1) * (s + 1) <= k2) s++;
+    return (int)s;
+  }
+  return (int)llrint(sqrt((double)k2));
+}
+
 // binshells! (src/stats.jl:143-157): 1/2 |u_hat|^2 / N^2 into integer
-// shells round(|k|), conjugate modes 0 < kx < nx/2 counted twice
+// shells round(|k|) (FLOORED: floor(|k|), shell_energies of
+// src/spectral/forcing.jl:12-24), conjugate modes 0 < kx < nx/2 counted twice
+template <bool FLOORED>
 __global__ void k_binshells(Geo g, const double2 *S, double *E, int nbins) {
   const long long n = (long long)g.nkx * g.ny * g.nz;
   const double N = (double)g.nx * g.ny * g.nz;
   const double N2 = N * N;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
        t += (long long)gridDim.x * blockDim.x) {
-    const int kz0 = (int)(t % g.nz);
-    const long long r = t / g.nz;
-    const int j = (int)(r % g.ny), kx = (int)(r / g.ny);
-    const int ky = j > g.ny / 2 ? j - g.ny : j;
-    const int kz = kz0 > g.nz / 2 ? kz0 - g.nz : kz0;
-    const int kap = (int)llrint(sqrt((double)(kx * kx + ky * ky + kz * kz)));
-    const double wgt = (0 < kx && 2 * kx < g.nx) ? 2.0 : 1.0;
+    double wgt;
+    const int kap = shell_of<FLOORED>(g, t, wgt);
     const double2 a = S[t];
     const double a2 = a.x * a.x + a.y * a.y;
     if (kap < nbins) atomicAdd(E + kap, wgt * a2 / 2 / N2);
+  }
+}
+
+// rescale_shell! (src/spectral/forcing.jl:26-35) for every shell at once:
+// entry t of S times f[floor(|k|)] (shells >= nbins unchanged)
+__global__ void k_scaleshells(Geo g, double2 *S, const double *__restrict__ f, int nbins) {
+  const long long n = (long long)g.nkx * g.ny * g.nz;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+       t += (long long)gridDim.x * blockDim.x) {
+    double w;
+    const int sh = shell_of<true>(g, t, w);
+    if (sh < nbins) S[t] = cscale(S[t], f[sh]);
   }
 }
 
@@ -424,6 +457,22 @@ __global__ void k_noise(Geo g, double *phi, int c, unsigned long long seed, doub
   // explicit roundings (no FMA contraction) so that the field is bit-identical
   // to a host evaluation of phi + amp*(2U - 1)
   phi[c0] = __dadd_rn(phi[c0], __dmul_rn(amp, __dsub_rn(2 * U, 1.0)));
+}
+
+// noise_kernel! (src/spectral/ic.jl:37-51) on the interior of component c:
+// standard normal values from two counter-based uniforms (Box-Muller),
+// key = ((c*nz + K-1)*ny + J-1)*nx + I-1 (the reference's key on its cube)
+__global__ void k_gauss_noise(Geo g, double *phi, int c, unsigned long long seed) {
+  const int I = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int J = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  const int K = blockIdx.z + 1;
+  if (I > g.nx || J > g.ny) return;
+  const unsigned long long key =
+      (((unsigned long long)c * g.nz + (K - 1)) * g.ny + (J - 1)) * g.nx + (I - 1);
+  const unsigned long long r1 = splitmix64(seed + 2 * key), r2 = splitmix64(seed + 2 * key + 1);
+  const double u1 = ((double)(r1 >> 11) + 0.5) * 0x1p-53;
+  const double u2 = ((double)(r2 >> 11) + 0.5) * 0x1p-53;
+  phi[gidx(g, I, J, K)] = sqrt(-2.0 * log(u1)) * cospi(2.0 * u2);
 }
 
 // ------------------------------------------------------------- pipeline --
@@ -566,7 +615,7 @@ int launch_ysolve(dnsb_ctx *c) {
 #undef YT
   } else {
     dim3 grid(g.nkx * ((g.nz + c->Ly - 1) / c->Ly));
-    LAUNCH(c, DNSB_KIND_YSOLVE, k_yfourier<false><<<grid, SPEC_THREADS, c->smem_y, c->stream>>>(g, c->S, c->py, c->Ly, c->twy, c->lam1, c->lam2, c->lam3));
+    LAUNCH(c, DNSB_KIND_YSOLVE, k_yfourier<YF_SOLVE><<<grid, SPEC_THREADS, c->smem_y, c->stream>>>(g, c->S, c->py, c->Ly, c->twy, c->lam1, c->lam2, c->lam3));
   }
   return 0;
 }
@@ -736,6 +785,82 @@ int cfl_from_max(dnsb_ctx *c, double cfl, const unsigned long long *bits, double
   const double invdy2 = c->implicit ? 0.0 : 1 / (c->dymin * c->dymin);
   const double diff = 1 / (2 * g.visc * (1 / (g.dx * g.dx) + invdy2 + 1 / (g.dz * g.dz)) + eps);
   *dt_out = std::fmin(cfl * conv, cfl * diff);
+  return 0;
+}
+
+// --------------------------------------------- integer-wavenumber shells --
+// Periodic boxes only.  Every velocity component is transformed on its own
+// staggered grid; a real factor per shell |k| multiplies the same modes of
+// all three components, so the discrete divergence stays zero.
+
+int alloc_shells(dnsb_ctx *c) {
+  const Geo &g = c->g;
+  if (g.wall) return 0;
+  const long long k2 = (long long)(g.nx / 2) * (g.nx / 2) + (long long)(g.ny / 2) * (g.ny / 2) +
+                       (long long)(g.nz / 2) * (g.nz / 2);
+  long long s = (long long)sqrt((double)k2);
+  while (s * s > k2) s--;
+  while ((s + 1) * (s + 1) <= k2) s++;
+  c->nshell_max = (int)s + 1;
+  return dalloc(c, &c->shellbuf, 3 * (size_t)c->nshell_max);
+}
+
+// S = the 3-D transform of the interior of component u
+int spectrum_of(dnsb_ctx *c, const double *u) {
+  const Geo &g = c->g;
+  int rc;
+  if ((rc = launch_rfftx(c, RIN_FIELD, u, nullptr, nullptr))) return rc;
+  if ((rc = launch_fftz(c, false))) return rc;
+  dim3 grid(g.nkx * ((g.nz + c->Ly - 1) / c->Ly));
+  k_yfourier<YF_FORWARD><<<grid, SPEC_THREADS, c->smem_y, c->stream>>>(g, c->S, c->py, c->Ly, c->twy,
+                                                                       c->lam1, c->lam2, c->lam3);
+  CKL(c);
+  return 0;
+}
+
+// E[0..nb) (device) = energies of the floor shells
+int shell_energies_dev(dnsb_ctx *c, const double *const u[3], double *E, int nb) {
+  CK(c, cudaMemsetAsync(E, 0, nb * sizeof(double), c->stream));
+  int rc;
+  for (int comp = 0; comp < 3; comp++) {
+    if ((rc = spectrum_of(c, u[comp]))) return rc;
+    k_binshells<true><<<RED_BLOCKS, 256, 0, c->stream>>>(c->g, c->S, E, nb);
+    CKL(c);
+  }
+  return 0;
+}
+
+// u <- u with shell s scaled by f[s] (device), s < nb; images rewritten
+int shell_scale_dev(dnsb_ctx *c, double *const u[3], const double *f, int nb) {
+  const Geo &g = c->g;
+  int rc;
+  for (int comp = 0; comp < 3; comp++) {
+    if ((rc = spectrum_of(c, u[comp]))) return rc;
+    k_scaleshells<<<RED_BLOCKS, 256, 0, c->stream>>>(g, c->S, f, nb);
+    CKL(c);
+    dim3 grid(g.nkx * ((g.nz + c->Ly - 1) / c->Ly));
+    k_yfourier<YF_INVERSE><<<grid, SPEC_THREADS, c->smem_y, c->stream>>>(g, c->S, c->py, c->Ly, c->twy,
+                                                                         c->lam1, c->lam2, c->lam3);
+    CKL(c);
+    if ((rc = launch_fftz(c, true))) return rc;
+    if ((rc = launch_irfftx(c, ROUT_IMAGES, u[comp]))) return rc;
+  }
+  c->umax_for[0] = c->umax_for[1] = c->umax_for[2] = nullptr;
+  return 0;
+}
+
+// shellforcing's closure (src/spectral/forcing.jl:50-55) on the device:
+// f[s] = sqrt(eref[s] / E[s]) for forced shells (eref[s] >= 0) with E > 0, else 1
+__global__ void k_clamp_factors(const double *E, const double *eref, double *f, int nb) {
+  for (int s = threadIdx.x; s < nb; s += blockDim.x)
+    f[s] = (eref[s] >= 0 && E[s] > 0) ? sqrt(eref[s] / E[s]) : 1.0;
+}
+
+int check_shells(dnsb_ctx *c, const void *ux, const void *uy, const void *uz) {
+  if (!c) return DNSB_EINVAL;
+  if (!ux || !uy || !uz) return fail(c, DNSB_EINVAL, "null field");
+  if (c->g.wall) return fail(c, DNSB_EINVAL, "wavenumber shells require a fully periodic box");
+  if (ensure_device(c)) return DNSB_ECUDA;
   return 0;
 }
 
@@ -948,8 +1073,9 @@ int dnsb_create(const dnsb_grid *gr, int device, void *stream, dnsb_ctx **out) {
       (rc = allow_smem(c, k_fftz<true>, c->smem_z)) ||
       (rc = allow_smem(c, k_fftz_tma<false>, c->smem_zt)) ||
       (rc = allow_smem(c, k_fftz_tma<true>, c->smem_zt)) ||
-      (rc = allow_smem(c, k_yfourier<false>, c->smem_y)) ||
-      (rc = allow_smem(c, k_yfourier<true>, c->smem_y)))
+      (rc = allow_smem(c, k_yfourier<YF_SOLVE>, c->smem_y)) ||
+      (rc = allow_smem(c, k_yfourier<YF_FORWARD>, c->smem_y)) ||
+      (rc = allow_smem(c, k_yfourier<YF_INVERSE>, c->smem_y)))
     return bail(rc);
 
   // scratch
@@ -957,6 +1083,7 @@ int dnsb_create(const dnsb_grid *gr, int device, void *stream, dnsb_ctx **out) {
   const size_t nspec = (size_t)g.nkx * ny * nz;
   if ((rc = dalloc(c, &c->S, nspec)) || (rc = dalloc(c, &c->r, (size_t)nx * ny * nz)) ||
       (rc = dalloc(c, &c->umax, 3 * UMAX_SLOTS + 8)) || (rc = dalloc(c, &c->partial, RED_BLOCKS + 8)) ||
+      (rc = alloc_shells(c)) ||
       (rc = dalloc(c, &c->deverr, 4)))
     return bail(rc);
   if (g.wall && ythomas_rows(ny) == 0 && (rc = dalloc(c, &c->work, nspec))) return bail(rc);
@@ -1197,13 +1324,94 @@ int dnsb_spectrum_sample(dnsb_ctx *c, const double *ux, const double *uy, const 
     if ((rc = launch_rfftx(c, RIN_FIELD, u[comp], nullptr, nullptr))) return rc;
     if ((rc = launch_fftz(c, false))) return rc;
     dim3 grid(g.nkx * ((g.nz + c->Ly - 1) / c->Ly));
-    k_yfourier<true><<<grid, SPEC_THREADS, c->smem_y, c->stream>>>(g, c->S, c->py, c->Ly, c->twy,
+    k_yfourier<YF_FORWARD><<<grid, SPEC_THREADS, c->smem_y, c->stream>>>(g, c->S, c->py, c->Ly, c->twy,
                                                                   c->lam1, c->lam2, c->lam3);
     CKL(c);
-    k_binshells<<<RED_BLOCKS, 256, 0, c->stream>>>(g, c->S, E, nbins);
+    k_binshells<false><<<RED_BLOCKS, 256, 0, c->stream>>>(g, c->S, E, nbins);
     CKL(c);
   }
   return 0;
+}
+
+int dnsb_shell_count(const dnsb_ctx *c) { return c ? c->nshell_max : -1; }
+
+int dnsb_shell_energies(dnsb_ctx *c, const double *ux, const double *uy, const double *uz, double *E,
+                        int nshells) {
+  int rc = check_shells(c, ux, uy, uz);
+  if (rc) return rc;
+  if (!E || nshells < 1) return fail(c, DNSB_EINVAL, "bad shell count");
+  const int nb = std::min(nshells, c->nshell_max);
+  const double *u[3] = {ux, uy, uz};
+  if ((rc = shell_energies_dev(c, u, c->shellbuf, nb))) return rc;
+  CK(c, cudaMemcpyAsync(E, c->shellbuf, nb * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(c, cudaStreamSynchronize(c->stream));
+  for (int s = nb; s < nshells; s++) E[s] = 0;
+  return 0;
+}
+
+int dnsb_shell_rescale(dnsb_ctx *c, double *ux, double *uy, double *uz, const double *factors,
+                       int nshells) {
+  int rc = check_shells(c, ux, uy, uz);
+  if (rc) return rc;
+  if (!factors || nshells < 1) return fail(c, DNSB_EINVAL, "bad shell count");
+  const int nb = std::min(nshells, c->nshell_max);
+  double *f = c->shellbuf + c->nshell_max;
+  CK(c, cudaMemcpyAsync(f, factors, nb * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  double *u[3] = {ux, uy, uz};
+  rc = shell_scale_dev(c, u, f, nb);
+  if (rc) return rc;
+  CK(c, cudaStreamSynchronize(c->stream));  // factors may be pageable host memory
+  return 0;
+}
+
+int dnsb_random_field(dnsb_ctx *c, double *ux, double *uy, double *uz, double totalenergy,
+                      double kpeak, unsigned long long seed, const double *profile, int nprofile) {
+  int rc = check_shells(c, ux, uy, uz);
+  if (rc) return rc;
+  if (profile ? nprofile < 1 : !(kpeak > 0)) return fail(c, DNSB_EINVAL, "bad spectrum profile");
+  const Geo &g = c->g;
+  double *u[3] = {ux, uy, uz};
+  for (int comp = 0; comp < 3; comp++) {
+    k_gauss_noise<<<cell_grid(g), cell_block, 0, c->stream>>>(g, u[comp], comp, seed);
+    CKL(c);
+  }
+  if ((rc = fill3(c, ux, uy, uz))) return rc;
+  if ((rc = do_project(c, ux, uy, uz, c->implicit ? c->V[0] : c->W[0]))) return rc;
+  const int nb = c->nshell_max;
+  std::vector<double> E(nb), prof(nb), f(nb);
+  if ((rc = dnsb_shell_energies(c, ux, uy, uz, E.data(), nb))) return rc;
+  double tot = 0;
+  for (int s = 0; s < nb; s++) {
+    const double k = s;
+    prof[s] = profile ? (s < nprofile ? profile[s] : 0.0) : k * k * k * k * exp(-2 * (k / kpeak) * (k / kpeak));
+    tot += prof[s];
+  }
+  if (!(tot > 0)) return fail(c, DNSB_EINVAL, "spectrum profile sums to zero");
+  for (int s = 0; s < nb; s++) {
+    const double e0 = totalenergy * prof[s] / tot;
+    f[s] = E[s] > 0 ? sqrt(e0 / E[s]) : 0.0;
+  }
+  return dnsb_shell_rescale(c, ux, uy, uz, f.data(), nb);
+}
+
+int dnsb_shell_clamp(dnsb_ctx *c, double *ux, double *uy, double *uz, const double *eref,
+                     int nshells) {
+  int rc = check_shells(c, ux, uy, uz);
+  if (rc) return rc;
+  if (!eref || nshells < 1) return fail(c, DNSB_EINVAL, "bad shell count");
+  const int nb = std::min(nshells, c->nshell_max);
+  double *E = c->shellbuf, *f = E + c->nshell_max, *er = f + c->nshell_max;
+  if (c->eref_host.size() != (size_t)nb || !std::equal(eref, eref + nb, c->eref_host.begin())) {
+    CK(c, cudaMemcpyAsync(er, eref, nb * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    c->eref_host.assign(eref, eref + nb);
+  }
+  const double *cu[3] = {ux, uy, uz};
+  if ((rc = shell_energies_dev(c, cu, E, nb))) return rc;
+  k_clamp_factors<<<1, 256, 0, c->stream>>>(E, er, f, nb);
+  CKL(c);
+  double *u[3] = {ux, uy, uz};
+  return shell_scale_dev(c, u, f, nb);
 }
 
 int dnsb_noise(dnsb_ctx *c, double *phi, int comp, unsigned long long seed, double amp) {
@@ -1528,7 +1736,7 @@ int noalloc_setup(int dev, double **out) {
     a = a != cudaSuccess ? a : raise_smem(dev, k_rfftx<RIN_REAL>, big);
     a = a != cudaSuccess ? a : raise_smem(dev, k_fftz<false>, big);
     a = a != cudaSuccess ? a : raise_smem(dev, k_fftz<true>, big);
-    a = a != cudaSuccess ? a : raise_smem(dev, k_yfourier<false>, big);
+    a = a != cudaSuccess ? a : raise_smem(dev, k_yfourier<YF_SOLVE>, big);
     a = a != cudaSuccess ? a : raise_smem(dev, k_irfftx<ROUT_INTERIOR>, big);
     if (a != cudaSuccess)
       return fail(nullptr, DNSB_ECUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(a));
@@ -1646,7 +1854,7 @@ extern "C" int dnsb_poisson_noalloc(const dnsb_grid *gr, const double *r, double
     const long long nl = (long long)g.nkx * nz;
     k_thomas<<<(unsigned)((nl + 127) / 128), 128, 0, st>>>(g, S, work, d_ay, d_by, d_cy, d_lam1, d_lam3);
   } else {
-    k_yfourier<false><<<dim3(g.nkx * ((nz + Ly - 1) / Ly)), SPEC_THREADS, smem_y, st>>>(
+    k_yfourier<YF_SOLVE><<<dim3(g.nkx * ((nz + Ly - 1) / Ly)), SPEC_THREADS, smem_y, st>>>(
         g, S, py, Ly, d_twy, d_lam1, d_lam2, d_lam3);
   }
   k_fftz<true><<<gz, SPEC_THREADS, smem_z, st>>>(g, S, pz, Lz, d_twz);

@@ -257,8 +257,10 @@ __global__ void __launch_bounds__(128) k_thomas(Geo g, double2 *__restrict__ S,
 // Periodic y (src/poisson.jl:106-118,135-138, modedivide_kernel! :43-49):
 // per CTA a tile of L consecutive kz for one kx with all ny rows: FFT along
 // y, divide by lambda1+lambda2+lambda3 (0 for the mean), inverse, 1/ny.
-// SPECTRUM_ONLY leaves the forward transform in S (for energy spectra).
-template <bool SPECTRUM_ONLY>
+// YF_FORWARD leaves the forward transform in S (spectra, shell operations);
+// YF_INVERSE only applies the inverse (with 1/ny).
+enum YFourierMode { YF_SOLVE = 0, YF_FORWARD = 1, YF_INVERSE = 2 };
+template <int YMODE>
 __global__ void __launch_bounds__(SPEC_THREADS, 3) k_yfourier(Geo g, double2 *__restrict__ S,
                                                           FFTPlan plan, int L,
                                                           const double2 *__restrict__ twy,
@@ -280,12 +282,16 @@ __global__ void __launch_bounds__(SPEC_THREADS, 3) k_yfourier(Geo g, double2 *__
   auto ld = [&](int l, int e) {
     return l < Lv ? S[sidx(g, kx, e, k0 + l)] : make_double2(0.0, 0.0);
   };
-  const double sc = SPECTRUM_ONLY ? 1.0 : 1.0 / n;
+  const double sc = YMODE == YF_FORWARD ? 1.0 : 1.0 / n;
   auto st = [&](int l, int e, double2 v) {
-    if (l < Lv) S[sidx(g, kx, e, k0 + l)] = SPECTRUM_ONLY ? v : cscale(v, sc);
+    if (l < Lv) S[sidx(g, kx, e, k0 + l)] = YMODE == YF_FORWARD ? v : cscale(v, sc);
   };
-  if (SPECTRUM_ONLY) {
+  if (YMODE == YF_FORWARD) {
     fft_lines_io<false>(ld, st, buf, buf2, plan, L, L, 1, false, tw, true, true);
+    return;
+  }
+  if (YMODE == YF_INVERSE) {
+    fft_lines_io<true>(ld, st, buf, buf2, plan, L, L, 1, false, tw, true, true);
     return;
   }
   double2 *res = fft_lines_io<false>(ld, st, buf, buf2, plan, L, L, 1, false, tw, true, false);

@@ -152,6 +152,48 @@ int dnsb_spectrum_sample(dnsb_ctx *ctx, const double *ux, const double *uy, cons
  * key = ((c*nz + K-1)*ny + J-1)*nx + I-1. */
 int dnsb_noise(dnsb_ctx *ctx, double *phi, int c, unsigned long long seed, double amp);
 
+/* Integer-wavenumber shells of a fully periodic box (EINVAL with walls).
+ * The reference defines them on its pseudo-spectral state
+ * (src/spectral/forcing.jl:1-56, src/spectral/ic.jl:53-84); these are the
+ * finite-volume counterparts, with no FV entry point in the reference to
+ * replace.  Every velocity component is transformed on its own staggered
+ * grid; shell s holds the modes with s <= |k| < s+1 (k the integer
+ * wavenumber vector), energies are (1/2)|u_hat|^2 / N^2 with the rfft
+ * double-counting weights, so their sum is the mean kinetic energy. */
+
+/* Number of shells a box has: floor(|k|max) + 1, |k|max the Nyquist corner. */
+int dnsb_shell_count(const dnsb_ctx *ctx);
+
+/* shell_energies (src/spectral/forcing.jl:12-24) for shells 0..nshells-1
+ * into the HOST array E; synchronises the stream. */
+int dnsb_shell_energies(dnsb_ctx *ctx, const double *ux, const double *uy, const double *uz,
+                        double *E, int nshells);
+
+/* rescale_shell! (src/spectral/forcing.jl:26-35) for shells 0..nshells-1
+ * at once: shell s times the HOST factor factors[s]; ghost images rewritten.
+ * Real factors keep the discrete divergence. */
+int dnsb_shell_rescale(dnsb_ctx *ctx, double *ux, double *uy, double *uz, const double *factors,
+                       int nshells);
+
+/* spectral_randomfield! (src/spectral/ic.jl:53-84): Gaussian counter-based
+ * noise on the interior of every component (Box-Muller of two splitmix64
+ * uniforms, key = ((c*nz + K-1)*ny + J-1)*nx + I-1 as in noise_kernel!,
+ * src/spectral/ic.jl:37-51), ghosts filled, projected onto discretely
+ * divergence-free fields, then every shell s < dnsb_shell_count rescaled
+ * to energy totalenergy * profile[s] / sum(profile) (factor 0 where the
+ * projected field has none).  profile = NULL uses k^4 exp(-2 (k/kpeak)^2);
+ * otherwise profile[0..nprofile) (shells beyond are 0).  Synchronises. */
+int dnsb_random_field(dnsb_ctx *ctx, double *ux, double *uy, double *uz, double totalenergy,
+                      double kpeak, unsigned long long seed, const double *profile, int nprofile);
+
+/* The closure of shellforcing (src/spectral/forcing.jl:37-56): shells s
+ * with eref[s] >= 0 are rescaled to energy eref[s] (unchanged where they
+ * hold none), shells with eref[s] < 0 are not forced.  Energies, factors
+ * and the rescale stay on the device (no host synchronisation once eref
+ * is uploaded; a changed eref is uploaded synchronously). */
+int dnsb_shell_clamp(dnsb_ctx *ctx, double *ux, double *uy, double *uz, const double *eref,
+                     int nshells);
+
 /* Allocation-free Poisson solve (no counterpart in the reference): the same
  * computation as dnsb_poisson(ctx, r, p) for callers that cannot allocate
  * device memory -- e.g. callers whose device memory is held by a pooling

@@ -250,8 +250,9 @@ class Setup:
     def noise(self, phi, c, seed, amp):
         lib().dnso_noise(self._h, _p(phi), STAG[c], int(seed), float(amp))
 
-    def solve(self, u, tlims, dt=None, cfl=0.5, processors=(), max_steps=None):
-        """solve! (src/timestep.jl:92-111); returns (p, t, n)."""
+    def solve(self, u, tlims, dt=None, cfl=0.5, processors=(), max_steps=None, forcing=None):
+        """solve! (src/timestep.jl:92-111); returns (p, t, n).  forcing(u) is
+        applied after every step, as spectral_solve! does (src/spectral/step.jl:162)."""
         p = self.scalarfield()
         q = self.vectorfield()
         delta = self.scalarfield() if self.imexy else p
@@ -266,11 +267,104 @@ class Setup:
                 break
             dtn = min(dt if dt is not None else self.cfl_timestep(u, cfl), tend - t)
             self.step(u, p, q, delta, dtn)
+            if forcing is not None:
+                forcing(u)
             t += dtn
             n += 1
             for proc in processors:
                 proc(u, p, t, n)
         return p, t, n
+
+    # ------------------------------------------- wavenumber shells (numpy)
+    # FV restatement of the pseudo-spectral random initial condition and
+    # shell-clamp forcing (src/spectral/ic.jl:37-84,
+    # src/spectral/forcing.jl:1-56) on a fully periodic box.  Every velocity
+    # component is transformed on its own staggered grid with a full 3-D
+    # FFT, so no rfft double-counting weights are needed.
+
+    def gauss_noise(self, phi, c, seed):
+        """noise_kernel! (src/spectral/ic.jl:37-51): Box-Muller of two
+        splitmix64 uniforms per point, key = ((c*nz + K-1)*ny + J-1)*nx + I-1."""
+        nx, ny, nz = self.n
+        K, J, I = np.meshgrid(np.arange(nz, dtype=np.uint64), np.arange(ny, dtype=np.uint64),
+                              np.arange(nx, dtype=np.uint64), indexing="ij")
+        cc = np.uint64(STAG[c])
+        key = ((cc * np.uint64(nz) + K) * np.uint64(ny) + J) * np.uint64(nx) + I
+        seed = np.uint64(seed)
+        two = np.uint64(2)
+        r1 = _splitmix64(seed + two * key)
+        r2 = _splitmix64(seed + two * key + np.uint64(1))
+        u1 = ((r1 >> np.uint64(11)).astype(np.float64) + 0.5) * 2.0 ** -53
+        u2 = ((r2 >> np.uint64(11)).astype(np.float64) + 0.5) * 2.0 ** -53
+        phi[1:-1, 1:-1, 1:-1] = np.sqrt(-2 * np.log(u1)) * np.cos(2 * np.pi * u2)
+
+    def _shells(self):
+        nx, ny, nz = self.n
+        kz = np.fft.fftfreq(nz, 1.0 / nz).round().astype(np.int64)
+        ky = np.fft.fftfreq(ny, 1.0 / ny).round().astype(np.int64)
+        kx = np.fft.fftfreq(nx, 1.0 / nx).round().astype(np.int64)
+        k2 = kz[:, None, None] ** 2 + ky[None, :, None] ** 2 + kx[None, None, :] ** 2
+        sh = np.floor(np.sqrt(k2.astype(np.float64))).astype(np.int64)
+        sh -= sh * sh > k2
+        sh += (sh + 1) ** 2 <= k2
+        return sh
+
+    def shell_count(self):
+        return int(self._shells().max()) + 1
+
+    def shell_energies(self, u, nshells):
+        """shell_energies (src/spectral/forcing.jl:12-24) for shells 0..nshells-1."""
+        sh = self._shells()
+        N = float(np.prod(self.n))
+        e = sum(np.abs(np.fft.fftn(self.interior(u[c]))) ** 2 for c in "xyz") / 2 / N ** 2
+        E = np.zeros(nshells)
+        m = sh < nshells
+        np.add.at(E, sh[m], e[m])
+        return E
+
+    def rescale_shells(self, u, factors):
+        """rescale_shell! (src/spectral/forcing.jl:26-35), every shell s <
+        len(factors) times factors[s]; halos refilled."""
+        sh = self._shells()
+        f = np.ones(sh.shape)
+        m = sh < len(factors)
+        f[m] = np.asarray(factors)[sh[m]]
+        for c in "xyz":
+            u[c][1:-1, 1:-1, 1:-1] = np.fft.ifftn(np.fft.fftn(self.interior(u[c])) * f).real
+        self.exchange_halo(u)
+
+    def random_field(self, u, totalenergy=1.0, kpeak=4.0, seed=0, profile=None):
+        """spectral_randomfield! (src/spectral/ic.jl:59-84) on the staggered
+        velocity: noise, halos, FV projection, shells rescaled to the profile."""
+        for c in "xyz":
+            self.gauss_noise(u[c], c, seed)
+        self.exchange_halo(u)
+        self.project(u, self.scalarfield())
+        nb = self.shell_count()
+        E = self.shell_energies(u, nb)
+        k = np.arange(nb, dtype=np.float64)
+        prof = (np.array([profile(v) for v in range(nb)]) if profile is not None
+                else k ** 4 * np.exp(-2 * (k / kpeak) ** 2))
+        e0 = totalenergy * prof / prof.sum()
+        f = np.where(E > 0, np.sqrt(e0 / np.where(E > 0, E, 1.0)), 0.0)
+        self.rescale_shells(u, f)
+        return u
+
+    def shellforcing(self, u, shells=(1, 2), eref=None):
+        """shellforcing (src/spectral/forcing.jl:37-56): returns forcing(u)."""
+        shells = list(shells)
+        nb = max(shells) + 1
+        eref = self.shell_energies(u, nb)[shells] if eref is None else np.asarray(eref)
+
+        def forcing(u2):
+            e = self.shell_energies(u2, nb)
+            f = np.ones(nb)
+            for sh, e0 in zip(shells, eref):
+                f[sh] = np.sqrt(e0 / e[sh]) if e[sh] > 0 else 1.0
+            self.rescale_shells(u2, f)
+
+        forcing.eref = eref
+        return forcing
 
     # ------------------------------------------------------------- stats
     def channel_sample(self, u, acc):
@@ -324,6 +418,15 @@ class Setup:
     def energyspectrum(self, sp):
         E = sp["E"] / max(sp["nsamples"], 1)
         return np.arange(len(E)), E
+
+
+def _splitmix64(x):
+    """splitmix64 (src/spectral/ic.jl:31-36) on uint64 arrays (wrapping)."""
+    with np.errstate(over="ignore"):
+        z = x + np.uint64(0x9E3779B97F4A7C15)
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        return z ^ (z >> np.uint64(31))
 
 
 def cfft(x, inverse=False):
