@@ -59,7 +59,9 @@ COMMON = dict(lims=((0.0, 4 * math.pi), (-1.0, 1.0), (0.0, 4 * math.pi / 3)),
 # (nx/2+1)/(nx/2) of a real field.  Momentum reads q only from stage 2 on.
 # Momentum: r u3 q3 (p1), w q3 V3; q is not read at stage 1 (A = 0).  With
 # the fused projection + momentum (grad_momentum: r u*3 delta1 p1 q3,
-# w p1 q3 V3) the stand-alone momentum runs at stage 1 only.
+# w p1 q3 V3) the stand-alone momentum runs at stage 1 only.  The fused
+# z-FFT / y-solve / inverse z-FFT (fft_z_y_solve) reads and writes the
+# half spectrum once.
 def passes(kind, implicit, spec, fused=False):
     if kind == "momentum":
         if fused:
@@ -67,7 +69,7 @@ def passes(kind, implicit, spec, fused=False):
         return (10 + 13 + 13) / 3 if implicit else (9 + 12 + 12) / 3
     return {"cn_solve": 6.0, "div_rfft_x": 3 + spec, "fft_z": 2 * spec, "y_solve": 2 * spec,
             "ifft_z": 2 * spec, "irfft_x": spec + 1, "grad_update": 9.0 if implicit else 7.0,
-            "grad_momentum": 15.0, "other": 0.0}[kind]
+            "grad_momentum": 15.0, "fft_z_y_solve": 2 * spec, "other": 0.0}[kind]
 
 
 def tanhstretch(beta):

@@ -77,7 +77,7 @@ SIGNATURES = {
 }
 
 KINDS = ["momentum", "cn_solve", "div_rfft_x", "fft_z", "y_solve", "ifft_z", "irfft_x",
-         "grad_update", "other", "grad_momentum"]
+         "grad_update", "other", "grad_momentum", "fft_z_y_solve"]
 
 _LIB = None
 

@@ -34,6 +34,7 @@
 #include "ysolve.cuh"
 #include "stencil.cuh"
 #include "gradmom.cuh"
+#include "zyz.cuh"
 
 using namespace dnsb;
 
@@ -111,6 +112,7 @@ struct dnsb_ctx {
   std::vector<double> eref_host;       // shell-clamp reference energies on the device
   int *deverr = nullptr;               // device-side error word (bounded waits)
   int use_tma = 1;                     // persistent TMA-pipelined z-FFT
+  int zyz_c = 0;                       // CTAs per cluster of k_zyz (0: three kernels)
   int x1 = 0, x2 = 0, z1 = 0, z2 = 0;  // four-step splits of nx/2 and nz (0: generic kernels)
   int L4z = 8;                         // lines per CTA of the z-FFT
   size_t smem_rx4 = 0, smem_ix4 = 0, smem_z4 = 0;
@@ -164,7 +166,7 @@ int fail(dnsb_ctx *c, int code, const char *fmt, ...) {
 
 const char *KIND_NAMES[DNSB_NKINDS] = {"momentum", "cn_solve", "div_rfft_x", "fft_z", "y_solve",
                                        "ifft_z", "irfft_x", "grad_update", "other",
-                                       "grad_momentum"};
+                                       "grad_momentum", "fft_z_y_solve"};
 
 int prof_harvest(dnsb_ctx *c) {
   if (c->recs.empty()) { c->evused = 0; return 0; }
@@ -633,12 +635,66 @@ int launch_irfftx(dnsb_ctx *c, int mode, double *out) {
   return 0;
 }
 
+// k_zyz for this context's z split: one cluster of zyz_c CTAs per kx plane
+template <int N1, int N2>
+cudaError_t launch_zyz_as(dnsb_ctx *c, bool query, int *nclusters) {
+  const Geo &g = c->g;
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = (unsigned)c->zyz_c;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.gridDim = dim3((unsigned)(g.nkx * c->zyz_c));
+  cfg.blockDim = dim3(ZYZ_THREADS);
+  cfg.dynamicSmemBytes = zyz_smem<N1, N2>();
+  cfg.stream = c->stream;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  if (query) return cudaOccupancyMaxActiveClusters(nclusters, k_zyz<N1, N2>, &cfg);
+  return cudaLaunchKernelEx(&cfg, k_zyz<N1, N2>, g, c->S, (const double *)c->ycin,
+                            (const double *)c->ay, (const double *)c->by, (const double *)c->cy,
+                            (const double *)c->lam1, (const double *)c->lam3,
+                            (const double2 *)c->twz);
+}
+
+cudaError_t launch_zyz_split(dnsb_ctx *c, bool query, int *nclusters) {
+  if (c->z1 == 16 && c->z2 == 24) return launch_zyz_as<16, 24>(c, query, nclusters);
+  if (c->z1 == 16 && c->z2 == 16) return launch_zyz_as<16, 16>(c, query, nclusters);
+  return cudaErrorInvalidValue;
+}
+
+// Chooses the fused z-FFT / y-solve / inverse z-FFT kernel where it applies:
+// walls, nz in {256, 384} (four-step 16 x 16 / 16 x 24), ny a multiple of
+// 32 with at most 8 chunks, and a cluster of that size can be resident.
+int setup_zyz(dnsb_ctx *c) {
+  const Geo &g = c->g;
+  c->zyz_c = 0;
+  if (!(c->z1 == 16 && (c->z2 == 24 || c->z2 == 16))) return 0;
+  if (g.ny % ZYZ_ROWS != 0 || g.ny / ZYZ_ROWS > ZYZ_MAXC) return 0;
+  int rc;
+  if (c->z2 == 24) rc = allow_smem(c, k_zyz<16, 24>, zyz_smem<16, 24>());
+  else rc = allow_smem(c, k_zyz<16, 16>, zyz_smem<16, 16>());
+  if (rc) return rc;
+  c->zyz_c = g.ny / ZYZ_ROWS;
+  int n = 0;
+  if (launch_zyz_split(c, true, &n) != cudaSuccess || n < 1) {
+    cudaGetLastError();  // the query's error is not the context's
+    c->zyz_c = 0;
+  }
+  return 0;
+}
+
 // S already holds rfft_x(rhs): finish the Poisson solve into out
 int poisson_from_spectrum(dnsb_ctx *c, int outmode, double *out) {
   int rc;
-  if ((rc = launch_fftz(c, false))) return rc;
-  if ((rc = launch_ysolve(c))) return rc;
-  if ((rc = launch_fftz(c, true))) return rc;
+  if (c->zyz_c) {
+    LAUNCH(c, DNSB_KIND_ZYZ, CK(c, launch_zyz_split(c, false, nullptr)));
+  } else {
+    if ((rc = launch_fftz(c, false))) return rc;
+    if ((rc = launch_ysolve(c))) return rc;
+    if ((rc = launch_fftz(c, true))) return rc;
+  }
   return launch_irfftx(c, outmode, out);
 }
 
@@ -1087,7 +1143,10 @@ int dnsb_create(const dnsb_grid *gr, int device, void *stream, dnsb_ctx **out) {
       (rc = dalloc(c, &c->deverr, 4)))
     return bail(rc);
   if (g.wall && ythomas_rows(ny) == 0 && (rc = dalloc(c, &c->work, nspec))) return bail(rc);
-  if (g.wall && ythomas_rows(ny) != 0) {
+  // the fused z-FFT / y-solve / inverse z-FFT is opt-in: at 384 x 256 x 384
+  // it measured 0.44-0.46 ms against 0.43 ms for the three kernels
+  if (g.wall && !c->use_tma && envint("DNSB_ZYZ", 0) != 0 && (rc = setup_zyz(c))) return bail(rc);
+  if (g.wall && (c->zyz_c || ythomas_rows(ny) != 0)) {
 #define YTS(MR)                                                                                    \
   if (ythomas_rows(ny) == MR && (rc = allow_smem(c, k_ythomas<MR>, ythomas_smem(MR)))) return bail(rc);
     YTS(1) YTS(2) YTS(3) YTS(4) YTS(6) YTS(8) YTS(12) YTS(16)
@@ -1095,7 +1154,7 @@ int dnsb_create(const dnsb_grid *gr, int device, void *stream, dnsb_ctx **out) {
     const long long nl = (long long)g.nkx * nz;
     if ((rc = dalloc(c, &c->ycin, (size_t)nl * TY_CHUNKS))) return bail(rc);
     k_ythomas_entries<<<(unsigned)((nl + 127) / 128), 128, 0, c->stream>>>(
-        g, ythomas_rows(ny), c->ycin, c->ay, c->by, c->cy, c->lam1, c->lam3);
+        g, c->zyz_c ? ZYZ_ROWS : ythomas_rows(ny), c->ycin, c->ay, c->by, c->cy, c->lam1, c->lam3);
     if (cudaGetLastError() != cudaSuccess) {
       fail(c, DNSB_ECUDA, "launch of the y-solve table kernel failed");
       return bail(DNSB_ECUDA);

@@ -239,11 +239,13 @@ int dnsb_ensemble_run(dnsb_ensemble *ens, double *const *fields, const double *d
  * every launch of the step path is bracketed by CUDA events on the context's
  * stream and its device time is accumulated per kernel kind.  Enabling
  * resets the accumulators; dnsb_profile_read synchronises.  GRADMOM is the
- * projection of a semi-implicit stage fused with the next stage's momentum. */
+ * projection of a semi-implicit stage fused with the next stage's momentum;
+ * ZYZ the z-FFT, y-solve and inverse z-FFT of wall-bounded grids in one
+ * kernel (one thread-block cluster per kx plane). */
 enum {
   DNSB_KIND_MOMENTUM = 0, DNSB_KIND_CN = 1, DNSB_KIND_RFFTX = 2, DNSB_KIND_FFTZ = 3,
   DNSB_KIND_YSOLVE = 4, DNSB_KIND_IFFTZ = 5, DNSB_KIND_IRFFTX = 6, DNSB_KIND_GRAD = 7,
-  DNSB_KIND_OTHER = 8, DNSB_KIND_GRADMOM = 9, DNSB_NKINDS = 10
+  DNSB_KIND_OTHER = 8, DNSB_KIND_GRADMOM = 9, DNSB_KIND_ZYZ = 10, DNSB_NKINDS = 11
 };
 int dnsb_profile(dnsb_ctx *ctx, int enable);
 int dnsb_profile_read(dnsb_ctx *ctx, int kind, double *ms, long *launches);
