@@ -11,4 +11,8 @@ from .api import (  # noqa: F401
     solve, spectrumstats, step, vectorfield, velocityfield,
 )
 
+from .les import (  # noqa: F401
+    les_cube, lescells, lessampler, load_snapshot, save_snapshot, sfs_from_cube, sfs_sample,
+)
+
 __version__ = "0.1.0"

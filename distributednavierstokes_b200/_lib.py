@@ -63,6 +63,7 @@ SIGNATURES = {
     "dnsb_random_field": (c_int, [P, P, P, P, c_double, c_double, ctypes.c_ulonglong,
                                   ctypes.POINTER(c_double), c_int]),
     "dnsb_shell_clamp": (c_int, [P, P, P, P, ctypes.POINTER(c_double), c_int]),
+    "dnsb_les_cube": (c_int, [P, P, P, P, c_int, ctypes.POINTER(c_double)]),
     "dnsb_profile": (c_int, [P, c_int]),
     "dnsb_profile_read": (c_int, [P, c_int, ctypes.POINTER(c_double), ctypes.POINTER(c_long)]),
     "dnsb_launch_count": (c_long, [P]),

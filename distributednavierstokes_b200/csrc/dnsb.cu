@@ -110,6 +110,8 @@ struct dnsb_ctx {
   double *shellbuf = nullptr;          // periodic boxes: [E | factors | eref] x nshell_max
   int nshell_max = 0;                  // floor(|k|max) + 1
   std::vector<double> eref_host;       // shell-clamp reference energies on the device
+  double2 *cube = nullptr;             // LES cubes of the filtered-field sampler
+  size_t cube_cap = 0;
   int *deverr = nullptr;               // device-side error word (bounded waits)
   int use_tma = 1;                     // persistent TMA-pipelined z-FFT
   int zyz_c = 0;                       // CTAs per cluster of k_zyz (0: three kernels)
@@ -475,6 +477,43 @@ __global__ void k_gauss_noise(Geo g, double *phi, int c, unsigned long long seed
   const double u1 = ((double)(r1 >> 11) + 0.5) * 0x1p-53;
   const double u2 = ((double)(r2 >> 11) + 0.5) * 0x1p-53;
   phi[gidx(g, I, J, K)] = sqrt(-2.0 * log(u1)) * cospi(2.0 * u2);
+}
+
+// Cell-centred velocity products for the filtered-field sampler: out = v_a
+// (b < 0) or v_a v_b on the interior, v_c the average of the two faces of
+// the cell along c (the cell-centre interpolation of operators.jl:71-72).
+__global__ void k_cellprod(Geo g, CFields3 u, int a, int b, double *out) {
+  const int I = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int J = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  const int K = blockIdx.z + 1;
+  if (I > g.nx || J > g.ny) return;
+  const int c0 = gidx(g, I, J, K);
+  auto vc = [&](int c) {
+    const double *f = c == 0 ? u.x : c == 1 ? u.y : u.z;
+    const int o = c == 0 ? 1 : c == 1 ? g.NX : g.NX * g.NY;
+    return (f[c0 - o] + f[c0]) / 2;
+  };
+  const double va = vc(a);
+  out[c0] = b < 0 ? va : va * vc(b);
+}
+
+// The LES cube |k_i| <= M/2 of a transformed field (S, unnormalised) into
+// the coarse rfft layout cube[(kc*M + jc)*(M/2+1) + kx] (kx = 0..M/2; jc, kc
+// wrapped: 0..M/2-1 then -M/2..-1), times sc (1/N: u_hat = F[u]/N), after
+// lesboxes / lescoarse (src/spectral/les.jl:146-168).
+__global__ void k_lescube(Geo g, const double2 *__restrict__ S, int M, double sc,
+                          double2 *__restrict__ cube) {
+  const int h = M / 2 + 1;
+  const long long n = (long long)h * M * M;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int kx = (int)(t % h);
+    const long long r = t / h;
+    const int jc = (int)(r % M), kc = (int)(r / M);
+    const int ky = jc < M / 2 ? jc : jc - M, kz = kc < M / 2 ? kc : kc - M;
+    const int j = ky >= 0 ? ky : ky + g.ny, k = kz >= 0 ? kz : kz + g.nz;
+    cube[t] = cscale(S[sidx(g, kx, j, k)], sc);
+  }
 }
 
 // ------------------------------------------------------------- pipeline --
@@ -915,7 +954,7 @@ __global__ void k_clamp_factors(const double *E, const double *eref, double *f, 
 int check_shells(dnsb_ctx *c, const void *ux, const void *uy, const void *uz) {
   if (!c) return DNSB_EINVAL;
   if (!ux || !uy || !uz) return fail(c, DNSB_EINVAL, "null field");
-  if (c->g.wall) return fail(c, DNSB_EINVAL, "wavenumber shells require a fully periodic box");
+  if (c->g.wall) return fail(c, DNSB_EINVAL, "spectral operations require a fully periodic box");
   if (ensure_device(c)) return DNSB_ECUDA;
   return 0;
 }
@@ -1471,6 +1510,36 @@ int dnsb_shell_clamp(dnsb_ctx *c, double *ux, double *uy, double *uz, const doub
   CKL(c);
   double *u[3] = {ux, uy, uz};
   return shell_scale_dev(c, u, f, nb);
+}
+
+int dnsb_les_cube(dnsb_ctx *c, const double *ux, const double *uy, const double *uz, int M,
+                  double *out) {
+  int rc = check_shells(c, ux, uy, uz);
+  if (rc) return rc;
+  const Geo &g = c->g;
+  if (!out || M < 2 || M % 2 || M / 2 > g.nx / 2 || M / 2 > g.ny / 2 || M / 2 > g.nz / 2)
+    return fail(c, DNSB_EINVAL, "LES cube needs an even M with M/2 <= n/2 in every direction");
+  const size_t per = (size_t)(M / 2 + 1) * M * M;
+  if (c->cube_cap < 9 * per) {
+    double2 *nb = nullptr;
+    if ((rc = dalloc(c, &nb, 9 * per))) return rc;
+    c->cube = nb;  // the previous, smaller buffer stays in the context's list until destroy
+    c->cube_cap = 9 * per;
+  }
+  double *scr = c->implicit ? c->V[0] : c->W[0];
+  const CFields3 u = cf(ux, uy, uz);
+  static const int pa[9] = {0, 1, 2, 0, 1, 2, 0, 1, 2}, pb[9] = {-1, -1, -1, 0, 1, 2, 1, 2, 0};
+  const double sc = 1.0 / ((double)g.nx * g.ny * g.nz);
+  for (int f = 0; f < 9; f++) {
+    k_cellprod<<<cell_grid(g), cell_block, 0, c->stream>>>(g, u, pa[f], pb[f], scr);
+    CKL(c);
+    if ((rc = spectrum_of(c, scr))) return rc;
+    k_lescube<<<RED_BLOCKS, 256, 0, c->stream>>>(g, c->S, M, sc, c->cube + f * per);
+    CKL(c);
+  }
+  CK(c, cudaMemcpyAsync(out, c->cube, 9 * per * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
+  CK(c, cudaStreamSynchronize(c->stream));
+  return 0;
 }
 
 int dnsb_noise(dnsb_ctx *c, double *phi, int comp, unsigned long long seed, double amp) {

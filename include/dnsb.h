@@ -186,6 +186,21 @@ int dnsb_shell_rescale(dnsb_ctx *ctx, double *ux, double *uy, double *uz, const 
 int dnsb_random_field(dnsb_ctx *ctx, double *ux, double *uy, double *uz, double totalenergy,
                       double kpeak, unsigned long long seed, const double *profile, int nprofile);
 
+/* The distributed half of sfs_sample! (src/spectral/les.jl:313-334) on the
+ * FV state of a periodic box: the cell-centred velocity v_c (average of the
+ * two faces of each cell, as operators.jl:71-72; u needs valid halos), its
+ * six products v_i v_j, their transforms scaled by 1/N (u_hat = F[u]/N),
+ * and the LES cube |k_i| <= M/2 of each (lesboxes / lescoarse,
+ * src/spectral/les.jl:146-168) written to the HOST array out as 9 coarse
+ * rfft arrays of (M/2+1) x M x M complex values (interleaved re, im; kx
+ * fastest, ky and kz wrapped 0..M/2-1 then -M/2..-1), in the order
+ * u_hat x, y, z, sigma_hat xx, yy, zz, xy, yz, zx.  M even, M/2 <= n/2.
+ * The reference gathers these to rank 0 and post-processes them on the
+ * host (filter, truncation, coarse nonlinearity, tau); so does the mirror
+ * (api.sfs_sample).  Synchronises. */
+int dnsb_les_cube(dnsb_ctx *ctx, const double *ux, const double *uy, const double *uz, int M,
+                  double *out);
+
 /* The closure of shellforcing (src/spectral/forcing.jl:37-56): shells s
  * with eref[s] >= 0 are rescaled to energy eref[s] (unchanged where they
  * hold none), shells with eref[s] < 0 are not forced.  Energies, factors
