@@ -75,6 +75,7 @@ SIGNATURES = {
     "dnsb_ensemble_last_error": (ctypes.c_char_p, [P]),
     "dnsb_ensemble_member": (P, [P, c_int]),
     "dnsb_ensemble_run": (c_int, [P, ctypes.POINTER(c_void_p), ctypes.POINTER(c_double), c_long]),
+    "dnsb_ensemble_forcing": (c_int, [P, c_int, ctypes.POINTER(c_double), c_int]),
 }
 
 KINDS = ["momentum", "cn_solve", "div_rfft_x", "fft_z", "y_solve", "ifft_z", "irfft_x",

@@ -460,6 +460,21 @@ class Ensemble:
             raise _lib.DNSBError(lib.dnsb_ensemble_last_error(self._ens).decode())
         return states
 
+    def set_forcing(self, i, forcing):
+        """Applies the shell-clamp forcing `forcing` (from shellforcing(u, s)
+        on member i's setup) to member i after each of its steps, inside the
+        graph; None removes it."""
+        lib = _lib.load()
+        if forcing is None:
+            rc = lib.dnsb_ensemble_forcing(self._ens, int(i), None, 0)
+        else:
+            table = forcing._table
+            rc = lib.dnsb_ensemble_forcing(self._ens, int(i),
+                                           table.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                           len(table))
+        if rc != 0:
+            raise _lib.DNSBError(lib.dnsb_ensemble_last_error(self._ens).decode())
+
     def close(self):
         if getattr(self, "_ens", None) is not None:
             _lib.load().dnsb_ensemble_destroy(self._ens)

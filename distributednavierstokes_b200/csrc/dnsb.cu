@@ -951,6 +951,17 @@ __global__ void k_clamp_factors(const double *E, const double *eref, double *f, 
     f[s] = (eref[s] >= 0 && E[s] > 0) ? sqrt(eref[s] / E[s]) : 1.0;
 }
 
+// the shell-clamp reference table on the device (synchronous; skipped when
+// it is already there, so that a captured clamp never synchronises)
+int upload_eref(dnsb_ctx *c, const double *eref, int nb) {
+  if (c->eref_host.size() == (size_t)nb && std::equal(eref, eref + nb, c->eref_host.begin())) return 0;
+  double *er = c->shellbuf + 2 * c->nshell_max;
+  CK(c, cudaMemcpyAsync(er, eref, nb * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(c, cudaStreamSynchronize(c->stream));
+  c->eref_host.assign(eref, eref + nb);
+  return 0;
+}
+
 int check_shells(dnsb_ctx *c, const void *ux, const void *uy, const void *uz) {
   if (!c) return DNSB_EINVAL;
   if (!ux || !uy || !uz) return fail(c, DNSB_EINVAL, "null field");
@@ -1499,11 +1510,7 @@ int dnsb_shell_clamp(dnsb_ctx *c, double *ux, double *uy, double *uz, const doub
   if (!eref || nshells < 1) return fail(c, DNSB_EINVAL, "bad shell count");
   const int nb = std::min(nshells, c->nshell_max);
   double *E = c->shellbuf, *f = E + c->nshell_max, *er = f + c->nshell_max;
-  if (c->eref_host.size() != (size_t)nb || !std::equal(eref, eref + nb, c->eref_host.begin())) {
-    CK(c, cudaMemcpyAsync(er, eref, nb * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-    CK(c, cudaStreamSynchronize(c->stream));
-    c->eref_host.assign(eref, eref + nb);
-  }
+  if ((rc = upload_eref(c, eref, nb))) return rc;
   const double *cu[3] = {ux, uy, uz};
   if ((rc = shell_energies_dev(c, cu, E, nb))) return rc;
   k_clamp_factors<<<1, 256, 0, c->stream>>>(E, er, f, nb);
@@ -1669,6 +1676,7 @@ struct dnsb_ensemble {
   cudaGraphExec_t exec = nullptr;
   std::vector<double *> key_fields;
   std::vector<double> key_dts;
+  std::vector<std::vector<double>> eref;  // per member: shell-clamp table (empty: no forcing)
   std::string err;
 };
 
@@ -1715,6 +1723,7 @@ int dnsb_ensemble_create(int n, const dnsb_grid *grids, int device, void *stream
     return efail(nullptr, DNSB_ECUDA, "cudaSetDevice(%d) failed", device);
   dnsb_ensemble *e = new dnsb_ensemble();
   e->n = n;
+  e->eref.resize(n);
   e->device = device;
   e->stream = (cudaStream_t)stream;
   auto bail = [&](int rc, const char *msg) {
@@ -1755,6 +1764,25 @@ dnsb_ctx *dnsb_ensemble_member(dnsb_ensemble *e, int i) {
   return (e && i >= 0 && i < e->n) ? e->m[i] : nullptr;
 }
 
+int dnsb_ensemble_forcing(dnsb_ensemble *e, int i, const double *eref, int nshells) {
+  if (!e) return DNSB_EINVAL;
+  if (i < 0 || i >= e->n) return efail(e, DNSB_EINVAL, "member %d out of range", i);
+  if (cudaSetDevice(e->device) != cudaSuccess) return efail(e, DNSB_ECUDA, "cudaSetDevice failed");
+  dnsb_ctx *c = e->m[i];
+  std::vector<double> t;
+  if (eref && nshells > 0) {
+    if (c->g.wall) return efail(e, DNSB_EINVAL, "member %d: shell forcing needs a periodic box", i);
+    t.assign(eref, eref + std::min(nshells, c->nshell_max));
+    const int rc = upload_eref(c, t.data(), (int)t.size());
+    if (rc) return efail(e, rc, "member %d: %s", i, dnsb_last_error(c));
+  }
+  if (t != e->eref[i]) {
+    e->eref[i] = t;
+    ens_drop_graph(e);
+  }
+  return 0;
+}
+
 int dnsb_ensemble_run(dnsb_ensemble *e, double *const *fields, const double *dts, long nsteps) {
   if (!e) return DNSB_EINVAL;
   if (!fields || !dts || nsteps < 0) return efail(e, DNSB_EINVAL, "null fields/dts or nsteps < 0");
@@ -1781,6 +1809,13 @@ int dnsb_ensemble_run(dnsb_ensemble *e, double *const *fields, const double *dts
       if (rc) {
         efail(e, rc, "member %d: %s", i, dnsb_last_error(e->m[i]));
         break;
+      }
+      if (!e->eref[i].empty()) {
+        rc = dnsb_shell_clamp(e->m[i], fi[0], fi[1], fi[2], e->eref[i].data(), (int)e->eref[i].size());
+        if (rc) {
+          efail(e, rc, "member %d forcing: %s", i, dnsb_last_error(e->m[i]));
+          break;
+        }
       }
       cudaEventRecord(e->done[i], e->ms[i]);
       cudaStreamWaitEvent(e->origin, e->done[i], 0);

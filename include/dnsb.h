@@ -248,6 +248,11 @@ const char *dnsb_ensemble_last_error(const dnsb_ensemble *ens);
 /* Context of member i (for the per-member calls: cfl, noise, project, ...). */
 dnsb_ctx *dnsb_ensemble_member(dnsb_ensemble *ens, int i);
 int dnsb_ensemble_run(dnsb_ensemble *ens, double *const *fields, const double *dts, long nsteps);
+/* Shell-clamp forcing of member i after each of its steps (as
+ * dnsb_shell_clamp with the table eref[0..nshells), uploaded here; periodic
+ * members only); eref = NULL removes it.  The graph is re-captured on the
+ * next run when the forcing changes. */
+int dnsb_ensemble_forcing(dnsb_ensemble *ens, int i, const double *eref, int nshells);
 
 /* Instrumentation (no counterpart in the reference, which has no profiling
  * for the FV path): launches are counted always; with dnsb_profile(ctx, 1)

@@ -94,3 +94,42 @@ def test_ensemble_rejects_bad_arguments(D):
     with pytest.raises(ValueError):
         E.run([st, st], [0.1], 1)
     E.close()
+
+
+def test_forced_ensemble_equals_members_alone(D):
+    """Random-phase initial fields and shell-clamp forcing inside the graph
+    (the ensemble configuration's IC and forcing) equal stepping and forcing
+    each member alone."""
+    kws = [dict(n=(16, 16, 16), visc=1e-2), dict(n=(24, 24, 24), visc=3e-3),
+           dict(n=(32, 32, 32), visc=1e-3)]
+    setups = [D.setup(**kw) for kw in kws]
+    ref, ens_states, forcings, dts = [], [], [], []
+    for i, s in enumerate(setups):
+        u = D.random_field(D.vectorfield(s), s, totalenergy=0.5, kpeak=4, seed=i)
+        st = (u, D.scalarfield(s), D.vectorfield(s), None)
+        forcings.append(D.shellforcing(u, s, shells=(1, 2)))
+        dts.append(0.5 * D.cfl_timestep(u, s, 0.5))
+        ens_states.append(_as_fields(D, _clone(st)))
+        ref.append(_as_fields(D, st))
+    E = D.Ensemble(setups)
+    for i, f in enumerate(forcings):
+        E.set_forcing(i, f)
+    E.run(ens_states, dts, 3)
+    for st, s, dt, f in zip(ref, setups, dts, forcings):
+        for _ in range(3):
+            D.step(st[0], st[1], st[2], st[1], s, dt)
+            f(st[0], s)
+    torch.cuda.synchronize()
+    for i, (a, b) in enumerate(zip(ens_states, ref)):
+        for c in "xyz":
+            assert torch.equal(a[0][c], b[0][c]), (i, c)
+        e = D.shell_energies(a[0], setups[i], (1, 2))
+        assert all(math.isclose(x, y, rel_tol=1e-13) for x, y in zip(e, forcings[i].eref))
+    # forcing removed: plain steps again (graph re-captured)
+    E.set_forcing(0, None)
+    E.run(ens_states, dts, 1)
+    D.step(ref[0][0], ref[0][1], ref[0][2], ref[0][1], setups[0], dts[0])
+    torch.cuda.synchronize()
+    for c in "xyz":
+        assert torch.equal(ens_states[0][0][c], ref[0][0][c])
+    E.close()
