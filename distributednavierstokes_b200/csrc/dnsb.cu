@@ -109,6 +109,7 @@ struct dnsb_ctx {
   double *partial = nullptr;           // reduction partials
   double *shellbuf = nullptr;          // periodic boxes: [E | factors | eref] x nshell_max
   int nshell_max = 0;                  // floor(|k|max) + 1
+  double *shellpart = nullptr;         // per-block partial shell sums (fixed-order path)
   std::vector<double> eref_host;       // shell-clamp reference energies on the device
   double2 *cube = nullptr;             // LES cubes of the filtered-field sampler
   size_t cube_cap = 0;
@@ -426,6 +427,77 @@ __global__ void k_binshells(Geo g, const double2 *S, double *E, int nbins) {
     const double a2 = a.x * a.x + a.y * a.y;
     if (kap < nbins) atomicAdd(E + kap, wgt * a2 / 2 / N2);
   }
+}
+
+// Shell energies of the lowest SHELL_DET shells in a fixed summation order
+// (bit-reproducible from run to run, which the atomics of k_binshells are
+// not): every thread sums its grid-stride entries in order, the block
+// reduces them in a fixed tree, k_sum_shells adds the blocks in order.
+constexpr int SHELL_DET = 8;
+__global__ void __launch_bounds__(256) k_binshells_det(Geo g, const double2 *S, double *partial) {
+  const long long n = (long long)g.nkx * g.ny * g.nz;
+  const double N = (double)g.nx * g.ny * g.nz;
+  const double N2 = N * N;
+  double acc[SHELL_DET];
+#pragma unroll
+  for (int s = 0; s < SHELL_DET; s++) acc[s] = 0.0;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+       t += (long long)gridDim.x * blockDim.x) {
+    double wgt;
+    const int kap = shell_of<true>(g, t, wgt);
+    if (kap >= SHELL_DET) continue;
+    const double2 a = S[t];
+    const double v = wgt * (a.x * a.x + a.y * a.y) / 2 / N2;
+#pragma unroll
+    for (int s = 0; s < SHELL_DET; s++) acc[s] += kap == s ? v : 0.0;
+  }
+  __shared__ double red[SHELL_DET][256];
+  const int tid = threadIdx.x;
+#pragma unroll
+  for (int s = 0; s < SHELL_DET; s++) red[s][tid] = acc[s];
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (tid < o) {
+#pragma unroll
+      for (int s = 0; s < SHELL_DET; s++) red[s][tid] += red[s][tid + o];
+    }
+    __syncthreads();
+  }
+  if (tid < SHELL_DET) partial[blockIdx.x * SHELL_DET + tid] = red[tid][0];
+}
+
+// The same for any number of shells (set-up time: the random initial
+// field): block s sums shell s over the whole spectrum in a fixed order.
+__global__ void __launch_bounds__(256) k_binshells_byshell(Geo g, const double2 *S, double *E) {
+  const long long n = (long long)g.nkx * g.ny * g.nz;
+  const double N = (double)g.nx * g.ny * g.nz;
+  const double N2 = N * N;
+  const int sh = blockIdx.x;
+  double acc = 0.0;
+  for (long long t = threadIdx.x; t < n; t += blockDim.x) {
+    double wgt;
+    if (shell_of<true>(g, t, wgt) != sh) continue;
+    const double2 a = S[t];
+    acc += wgt * (a.x * a.x + a.y * a.y) / 2 / N2;
+  }
+  __shared__ double red[256];
+  const int tid = threadIdx.x;
+  red[tid] = acc;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (tid < o) red[tid] += red[tid + o];
+    __syncthreads();
+  }
+  if (tid == 0) E[sh] += red[0];
+}
+
+// E[s] += the block partials of shell s, in block order
+__global__ void k_sum_shells(const double *partial, int nblocks, int nb, double *E) {
+  const int s = threadIdx.x;
+  if (s >= nb) return;
+  double a = 0.0;
+  for (int b = 0; b < nblocks; b++) a += partial[b * SHELL_DET + s];
+  E[s] += a;
 }
 
 // rescale_shell! (src/spectral/forcing.jl:26-35) for every shell at once:
@@ -897,6 +969,8 @@ int alloc_shells(dnsb_ctx *c) {
   while (s * s > k2) s--;
   while ((s + 1) * (s + 1) <= k2) s++;
   c->nshell_max = (int)s + 1;
+  int rc = dalloc(c, &c->shellpart, (size_t)RED_BLOCKS * SHELL_DET);
+  if (rc) return rc;
   return dalloc(c, &c->shellbuf, 3 * (size_t)c->nshell_max);
 }
 
@@ -913,13 +987,21 @@ int spectrum_of(dnsb_ctx *c, const double *u) {
   return 0;
 }
 
-// E[0..nb) (device) = energies of the floor shells
+// E[0..nb) (device) = energies of the floor shells, summed in a fixed order
+// (bit-reproducible): per block and shell for nb <= SHELL_DET (the clamp
+// forcing, every step), one block per shell otherwise
 int shell_energies_dev(dnsb_ctx *c, const double *const u[3], double *E, int nb) {
   CK(c, cudaMemsetAsync(E, 0, nb * sizeof(double), c->stream));
   int rc;
   for (int comp = 0; comp < 3; comp++) {
     if ((rc = spectrum_of(c, u[comp]))) return rc;
-    k_binshells<true><<<RED_BLOCKS, 256, 0, c->stream>>>(c->g, c->S, E, nb);
+    if (nb <= SHELL_DET) {
+      k_binshells_det<<<RED_BLOCKS, 256, 0, c->stream>>>(c->g, c->S, c->shellpart);
+      CKL(c);
+      k_sum_shells<<<1, 32, 0, c->stream>>>(c->shellpart, RED_BLOCKS, nb, E);
+    } else {
+      k_binshells_byshell<<<nb, 256, 0, c->stream>>>(c->g, c->S, E);
+    }
     CKL(c);
   }
   return 0;
