@@ -76,6 +76,19 @@ SIGNATURES = {
     "dnsb_ensemble_member": (P, [P, c_int]),
     "dnsb_ensemble_run": (c_int, [P, ctypes.POINTER(c_void_p), ctypes.POINTER(c_double), c_long]),
     "dnsb_ensemble_forcing": (c_int, [P, c_int, ctypes.POINTER(c_double), c_int]),
+    "dnsb_spectral_create": (c_int, [c_int, c_int, c_double, c_double, c_int, P,
+                                     ctypes.POINTER(c_void_p)]),
+    "dnsb_spectral_destroy": (None, [P]),
+    "dnsb_spectral_last_error": (ctypes.c_char_p, [P]),
+    "dnsb_spectral_set_stream": (c_int, [P, P]),
+    "dnsb_spectral_size": (c_long, [P]),
+    "dnsb_spectral_to_phys": (c_int, [P, P, P]),
+    "dnsb_spectral_from_phys": (c_int, [P, P, P]),
+    "dnsb_spectral_rhs": (c_int, [P, P, P]),
+    "dnsb_spectral_project": (c_int, [P, P]),
+    "dnsb_spectral_step": (c_int, [P, P, c_double, ctypes.POINTER(c_double)]),
+    "dnsb_spectral_vsummax": (c_int, [P, P, ctypes.POINTER(c_double)]),
+    "dnsb_spectral_diagnostic": (c_int, [P, P, c_int, ctypes.POINTER(c_double)]),
 }
 
 KINDS = ["momentum", "cn_solve", "div_rfft_x", "fft_z", "y_solve", "ifft_z", "irfft_x",

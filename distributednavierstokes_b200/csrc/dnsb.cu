@@ -35,6 +35,7 @@
 #include "stencil.cuh"
 #include "gradmom.cuh"
 #include "zyz.cuh"
+#include "spsolver.cuh"
 
 using namespace dnsb;
 
@@ -1928,6 +1929,302 @@ int dnsb_ensemble_run(dnsb_ensemble *e, double *const *fields, const double *dts
   const cudaError_t le = cudaGetLastError();
   if (le != cudaSuccess) return efail(e, DNSB_ECUDA, "%s", cudaGetErrorString(le));
   return 0;
+}
+
+}  // extern "C"
+
+// ================================================ pseudo-spectral solver ==
+//
+// The reference's second solver (src/spectral/*.jl) on a periodic cube:
+// state = the compact truncated spectrum (spsolver.cuh), transforms on a
+// finite-volume context of the n^3 transform grid (its FFT plans and
+// spectrum buffer), the nonlinear term in divergence form from the six
+// velocity products (spectral_rhs!, operators.jl:66-96), Wray RK3 with the
+// integrating-factor viscosity (spectral_step!, step.jl:60-92).
+struct dnsb_spectral {
+  dnsb_ctx *c = nullptr;
+  SpGeo s{};
+  double visc = 0, l = 0;
+  double *v[3] = {nullptr, nullptr, nullptr};  // physical velocity, n^3 each (x fastest)
+  double *r = nullptr;                         // one product, n^3
+  double2 *ustart = nullptr, *du = nullptr;    // 3 x nc each
+  double *partial = nullptr;                   // RED_BLOCKS + 1
+  unsigned long long *umax = nullptr;          // 2 slots
+  double *host = nullptr;                      // pinned, 4 doubles
+  std::vector<void *> allocs;
+  std::string err;
+};
+
+namespace {
+
+int spfail(dnsb_spectral *p, int code, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  if (p) p->err = buf;
+  else snprintf(g_create_err, sizeof g_create_err, "%s", buf);
+  return code;
+}
+
+#define SPK(p, call)                                                                         \
+  do {                                                                                       \
+    cudaError_t e_ = (call);                                                                 \
+    if (e_ != cudaSuccess) return spfail(p, DNSB_ECUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+  } while (0)
+#define SPKL(p) SPK(p, cudaGetLastError())
+#define SPRC(p, expr)                                                     \
+  do {                                                                    \
+    int rc_ = (expr);                                                     \
+    if (rc_) return spfail(p, rc_, "%s", dnsb_last_error((p)->c));        \
+  } while (0)
+
+template <class T>
+int spalloc(dnsb_spectral *p, T **out, size_t n) {
+  void *v = nullptr;
+  if (cudaMalloc(&v, n * sizeof(T)) != cudaSuccess)
+    return spfail(p, DNSB_ENOMEM, "cudaMalloc(%zu bytes) failed", n * sizeof(T));
+  p->allocs.push_back(v);
+  *out = (T *)v;
+  return 0;
+}
+
+long long sp_n3(const dnsb_spectral *p) { return (long long)p->s.n * p->s.n * p->s.n; }
+
+// spec_to_phys! of one component: v = sum over retained modes of u_hat e^{ikx}
+int sp_to_phys(dnsb_spectral *p, const double2 *uhc, double *v) {
+  dnsb_ctx *c = p->c;
+  const Geo &g = c->g;
+  const double n3 = (double)sp_n3(p);
+  SPK(p, cudaMemsetAsync(c->S, 0, sizeof(double2) * (size_t)g.nkx * g.ny * g.nz, c->stream));
+  k_sp_scatter<<<RED_BLOCKS, 256, 0, c->stream>>>(p->s, uhc, c->S, n3);
+  SPKL(p);
+  dim3 grid(g.nkx * ((g.nz + c->Ly - 1) / c->Ly));
+  k_yfourier<YF_INVERSE><<<grid, SPEC_THREADS, c->smem_y, c->stream>>>(g, c->S, c->py, c->Ly, c->twy,
+                                                                       c->lam1, c->lam2, c->lam3);
+  SPKL(p);
+  SPRC(p, launch_fftz(c, true));
+  SPRC(p, launch_irfftx(c, ROUT_REAL, v));
+  return 0;
+}
+
+// the full forward transform of a real n^3 array into S (unnormalised)
+int sp_from_phys(dnsb_spectral *p, const double *r) {
+  dnsb_ctx *c = p->c;
+  const Geo &g = c->g;
+  SPRC(p, launch_rfftx(c, RIN_REAL, r, nullptr, nullptr));
+  SPRC(p, launch_fftz(c, false));
+  dim3 grid(g.nkx * ((g.nz + c->Ly - 1) / c->Ly));
+  k_yfourier<YF_FORWARD><<<grid, SPEC_THREADS, c->smem_y, c->stream>>>(g, c->S, c->py, c->Ly, c->twy,
+                                                                       c->lam1, c->lam2, c->lam3);
+  SPKL(p);
+  return 0;
+}
+
+// spectral_rhs!: du = -i k_j F[v_i v_j] / n^3; leaves v = the physical velocity
+int sp_rhs(dnsb_spectral *p, const double2 *uh, double2 *du) {
+  dnsb_ctx *c = p->c;
+  const long long n3 = sp_n3(p);
+  int rc;
+  for (int comp = 0; comp < 3; comp++)
+    if ((rc = sp_to_phys(p, uh + comp * p->s.nc, p->v[comp]))) return rc;
+  static const int pa[6] = {0, 1, 2, 0, 1, 2}, pb[6] = {0, 1, 2, 1, 2, 0};
+  for (int f = 0; f < 6; f++) {
+    k_sp_product<<<RED_BLOCKS, 256, 0, c->stream>>>(n3, p->v[pa[f]], p->v[pb[f]], p->r);
+    SPKL(p);
+    if ((rc = sp_from_phys(p, p->r))) return rc;
+    k_sp_div<<<RED_BLOCKS, 256, 0, c->stream>>>(p->s, c->S, du, pa[f], pb[f], 1.0 / (double)n3);
+    SPKL(p);
+  }
+  return 0;
+}
+
+int sp_check(dnsb_spectral *p, const void *a) {
+  if (!p) return DNSB_EINVAL;
+  if (!a) return spfail(p, DNSB_EINVAL, "null array");
+  if (cudaSetDevice(p->c->device) != cudaSuccess) return spfail(p, DNSB_ECUDA, "cudaSetDevice failed");
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int dnsb_spectral_create(int n, int kcut, double l, double visc, int device, void *stream,
+                         dnsb_spectral **out) {
+  if (!out) return spfail(nullptr, DNSB_EINVAL, "null output");
+  *out = nullptr;
+  if (n < 4 || n % 2) return spfail(nullptr, DNSB_EINVAL, "n must be even");
+  if (kcut <= 0) kcut = n / 3;
+  if (3 * kcut > n) return spfail(nullptr, DNSB_EINVAL, "aliasing: 3kcut <= n is required (2/3 rule)");
+  if (!(l > 0) || !(visc >= 0)) return spfail(nullptr, DNSB_EINVAL, "bad l or visc");
+  std::vector<double> dy(n + 2, l / n);
+  dnsb_grid gr{};
+  gr.nx = gr.ny = gr.nz = n;
+  gr.bc_y = DNSB_BC_PERIODIC;
+  gr.ydiffusion = DNSB_YDIFF_EXPLICIT;
+  gr.dx = gr.dz = l / n;
+  gr.dy = dy.data();
+  gr.dyu = dy.data();
+  gr.visc = visc;
+  dnsb_ctx *c = nullptr;
+  int rc = dnsb_create(&gr, device, stream, &c);
+  if (rc) return rc;  // message in dnsb_last_error(NULL)
+  dnsb_spectral *p = new dnsb_spectral();
+  p->c = c;
+  p->visc = visc;
+  p->l = l;
+  p->s.n = n;
+  p->s.kcut = kcut;
+  p->s.m = 2 * kcut + 1;
+  p->s.nc = (long long)(kcut + 1) * p->s.m * p->s.m;
+  p->s.kfac = 2 * M_PI / l;
+  const size_t n3 = (size_t)n * n * n;
+  if ((rc = spalloc(p, &p->v[0], n3)) || (rc = spalloc(p, &p->v[1], n3)) ||
+      (rc = spalloc(p, &p->v[2], n3)) || (rc = spalloc(p, &p->r, n3)) ||
+      (rc = spalloc(p, &p->ustart, 3 * (size_t)p->s.nc)) ||
+      (rc = spalloc(p, &p->du, 3 * (size_t)p->s.nc)) ||
+      (rc = spalloc(p, &p->partial, (size_t)RED_BLOCKS + 1)) || (rc = spalloc(p, &p->umax, 2))) {
+    snprintf(g_create_err, sizeof g_create_err, "%s", p->err.c_str());
+    dnsb_spectral_destroy(p);
+    return rc;
+  }
+  if (cudaMallocHost(&p->host, 4 * sizeof(double)) != cudaSuccess) {
+    snprintf(g_create_err, sizeof g_create_err, "cudaMallocHost failed");
+    dnsb_spectral_destroy(p);
+    return DNSB_ENOMEM;
+  }
+  *out = p;
+  return 0;
+}
+
+void dnsb_spectral_destroy(dnsb_spectral *p) {
+  if (!p) return;
+  if (p->c) cudaSetDevice(p->c->device);
+  for (void *a : p->allocs) cudaFree(a);
+  if (p->host) cudaFreeHost(p->host);
+  dnsb_destroy(p->c);
+  delete p;
+}
+
+const char *dnsb_spectral_last_error(const dnsb_spectral *p) { return p ? p->err.c_str() : g_create_err; }
+
+long dnsb_spectral_size(const dnsb_spectral *p) { return p ? (long)p->s.nc : -1; }
+
+int dnsb_spectral_to_phys(dnsb_spectral *p, const double *uh, double *v) {
+  int rc = sp_check(p, uh);
+  if (rc || (rc = sp_check(p, v))) return rc;
+  const long long n3 = sp_n3(p);
+  for (int comp = 0; comp < 3; comp++)
+    if ((rc = sp_to_phys(p, reinterpret_cast<const double2 *>(uh) + comp * p->s.nc, v + comp * n3)))
+      return rc;
+  return 0;
+}
+
+int dnsb_spectral_from_phys(dnsb_spectral *p, const double *v, double *uh) {
+  int rc = sp_check(p, uh);
+  if (rc || (rc = sp_check(p, v))) return rc;
+  const long long n3 = sp_n3(p);
+  dnsb_ctx *c = p->c;
+  double2 *u2 = reinterpret_cast<double2 *>(uh);
+  for (int comp = 0; comp < 3; comp++) {
+    if ((rc = sp_from_phys(p, v + comp * n3))) return rc;
+    k_sp_gather<<<RED_BLOCKS, 256, 0, c->stream>>>(p->s, c->S, u2 + comp * p->s.nc, 1.0 / (double)n3);
+    SPKL(p);
+  }
+  return 0;
+}
+
+int dnsb_spectral_rhs(dnsb_spectral *p, const double *uh, double *du) {
+  int rc = sp_check(p, uh);
+  if (rc || (rc = sp_check(p, du))) return rc;
+  return sp_rhs(p, reinterpret_cast<const double2 *>(uh), reinterpret_cast<double2 *>(du));
+}
+
+int dnsb_spectral_project(dnsb_spectral *p, double *uh) {
+  int rc = sp_check(p, uh);
+  if (rc) return rc;
+  k_sp_project<<<RED_BLOCKS, 256, 0, p->c->stream>>>(p->s, reinterpret_cast<double2 *>(uh));
+  SPKL(p);
+  return 0;
+}
+
+int dnsb_spectral_step(dnsb_spectral *p, double *uh, double dt, double *vmax_out) {
+  int rc = sp_check(p, uh);
+  if (rc) return rc;
+  if (!(dt > 0)) return spfail(p, DNSB_EINVAL, "dt must be positive");
+  dnsb_ctx *c = p->c;
+  double2 *u2 = reinterpret_cast<double2 *>(uh);
+  static const double A[3] = {8.0 / 15, 5.0 / 12, 3.0 / 4}, B[3] = {1.0 / 4, 0.0, 0.0},
+                      DC[3] = {8.0 / 15, 2.0 / 15, 1.0 / 3};
+  SPK(p, cudaMemcpyAsync(p->ustart, u2, sizeof(double2) * 3 * (size_t)p->s.nc,
+                         cudaMemcpyDeviceToDevice, c->stream));
+  SPK(p, cudaMemsetAsync(p->umax, 0, sizeof(unsigned long long), c->stream));
+  for (int i = 0; i < 3; i++) {
+    if ((rc = sp_rhs(p, u2, p->du))) return rc;
+    if (i == 0) {
+      k_sp_vsummax<<<RED_BLOCKS, 256, 0, c->stream>>>(sp_n3(p), p->v[0], p->v[1], p->v[2], p->umax);
+      SPKL(p);
+    }
+    k_sp_ifstage<<<RED_BLOCKS, 256, 0, c->stream>>>(p->s, u2, p->ustart, p->du, A[i], B[i],
+                                                     p->visc * DC[i] * dt, dt);
+    SPKL(p);
+    k_sp_project<<<RED_BLOCKS, 256, 0, c->stream>>>(p->s, u2);
+    SPKL(p);
+  }
+  if (vmax_out) {
+    SPK(p, cudaMemcpyAsync(p->host, p->umax, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    SPK(p, cudaStreamSynchronize(c->stream));
+    *vmax_out = p->host[0];
+  }
+  return 0;
+}
+
+int dnsb_spectral_vsummax(dnsb_spectral *p, const double *uh, double *out) {
+  int rc = sp_check(p, uh);
+  if (rc || (rc = sp_check(p, out))) return rc;
+  dnsb_ctx *c = p->c;
+  for (int comp = 0; comp < 3; comp++)
+    if ((rc = sp_to_phys(p, reinterpret_cast<const double2 *>(uh) + comp * p->s.nc, p->v[comp])))
+      return rc;
+  SPK(p, cudaMemsetAsync(p->umax, 0, sizeof(unsigned long long), c->stream));
+  k_sp_vsummax<<<RED_BLOCKS, 256, 0, c->stream>>>(sp_n3(p), p->v[0], p->v[1], p->v[2], p->umax);
+  SPKL(p);
+  SPK(p, cudaMemcpyAsync(p->host, p->umax, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  SPK(p, cudaStreamSynchronize(c->stream));
+  *out = p->host[0];
+  return 0;
+}
+
+// which: 0 = spectral_energy, 1 = spectral_dissipation, 2 = spectral_maxdiv
+int dnsb_spectral_diagnostic(dnsb_spectral *p, const double *uh, int which, double *out) {
+  int rc = sp_check(p, uh);
+  if (rc || (rc = sp_check(p, out))) return rc;
+  if (which < 0 || which > 2) return spfail(p, DNSB_EINVAL, "bad diagnostic");
+  dnsb_ctx *c = p->c;
+  const double2 *u2 = reinterpret_cast<const double2 *>(uh);
+  if (which == 2) {
+    SPK(p, cudaMemsetAsync(p->umax + 1, 0, sizeof(unsigned long long), c->stream));
+    k_sp_maxdiv<<<RED_BLOCKS, 256, 0, c->stream>>>(p->s, u2, p->umax + 1);
+    SPKL(p);
+    SPK(p, cudaMemcpyAsync(p->host, p->umax + 1, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  } else {
+    k_sp_sum<<<RED_BLOCKS, 256, 0, c->stream>>>(p->s, u2, which, p->partial);
+    SPKL(p);
+    k_sum_final<<<1, 1024, 0, c->stream>>>(p->partial, RED_BLOCKS, p->partial + RED_BLOCKS);
+    SPKL(p);
+    SPK(p, cudaMemcpyAsync(p->host, p->partial + RED_BLOCKS, sizeof(double), cudaMemcpyDeviceToHost,
+                           c->stream));
+  }
+  SPK(p, cudaStreamSynchronize(c->stream));
+  *out = which == 1 ? p->visc * p->host[0] : p->host[0];
+  return 0;
+}
+
+int dnsb_spectral_set_stream(dnsb_spectral *p, void *stream) {
+  if (!p) return DNSB_EINVAL;
+  return dnsb_set_stream(p->c, stream);
 }
 
 }  // extern "C"

@@ -1,0 +1,187 @@
+// spsolver.cuh -- pointwise kernels of the pseudo-spectral solver for a
+// periodic cube (src/spectral/operators.jl, src/spectral/step.jl).
+//
+// The state is the reference's compact truncated spectrum: per component
+// (kcut+1) x m x m complex values, m = 2 kcut + 1, kx fastest
+// (q = i + (kcut+1) (j + m k); kx = i, ky / kz = compactfreq(j / k)),
+// u_hat = F[u] / n^3.  The transforms run on the finite-volume context's
+// FFT kernels over the full half spectrum S[kz + n (ky + n kx)] of the
+// n^3 transform grid: scatter (zero padding) before the inverse, gather
+// (truncation) after the forward transform.
+#pragma once
+#include "common.cuh"
+#include "fft.cuh"
+
+namespace dnsb {
+
+struct SpGeo {
+  int n, kcut, m;
+  long long nc;  // compact values per component
+  double kfac;   // 2 pi / l
+};
+
+// compact index -> (integer kx, ky, kz) and the full-spectrum index
+__device__ __forceinline__ void sp_modes(const SpGeo &s, long long q, int &kx, int &ky, int &kz) {
+  const int h = s.kcut + 1;
+  kx = (int)(q % h);
+  const long long r = q / h;
+  const int j = (int)(r % s.m), k = (int)(r / s.m);
+  ky = j <= s.kcut ? j : j - s.m;  // compactfreq (src/spectral/operators.jl:7)
+  kz = k <= s.kcut ? k : k - s.m;
+}
+__device__ __forceinline__ long long sp_full(const SpGeo &s, int kx, int ky, int kz) {
+  const int j = ky >= 0 ? ky : ky + s.n, k = kz >= 0 ? kz : kz + s.n;
+  return (long long)k + (long long)s.n * ((long long)j + (long long)s.n * kx);
+}
+
+#define SP_LOOP(q, n)                                                                   \
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < (n); \
+       q += (long long)gridDim.x * blockDim.x)
+
+// S (already zeroed) <- the retained modes of one state component x scale
+__global__ void k_sp_scatter(SpGeo s, const double2 *__restrict__ uh, double2 *__restrict__ S,
+                             double scale) {
+  SP_LOOP(q, s.nc) {
+    int kx, ky, kz;
+    sp_modes(s, q, kx, ky, kz);
+    S[sp_full(s, kx, ky, kz)] = cscale(uh[q], scale);
+  }
+}
+
+// the retained modes of S x sc into one state component (truncation)
+__global__ void k_sp_gather(SpGeo s, const double2 *__restrict__ S, double2 *__restrict__ uh,
+                            double sc) {
+  SP_LOOP(q, s.nc) {
+    int kx, ky, kz;
+    sp_modes(s, q, kx, ky, kz);
+    uh[q] = cscale(S[sp_full(s, kx, ky, kz)], sc);
+  }
+}
+
+// The convective right-hand side -i k_j sigma_hat_ij from the transformed
+// product a*b in S (times sc = 1/n^3), divdiag_kernel! / divoffdiag_kernel!
+// (src/spectral/operators.jl:31-52): a == b sets du_a = -i k_a sigma;
+// a != b subtracts i k_b sigma from du_a and i k_a sigma from du_b.
+__global__ void k_sp_div(SpGeo s, const double2 *__restrict__ S, double2 *__restrict__ du, int a,
+                         int b, double sc) {
+  SP_LOOP(q, s.nc) {
+    int kk[3];
+    sp_modes(s, q, kk[0], kk[1], kk[2]);
+    const double2 sg = cscale(S[sp_full(s, kk[0], kk[1], kk[2])], sc);
+    const double ka = s.kfac * kk[a], kb = s.kfac * kk[b];
+    double2 *da = du + a * s.nc, *db = du + b * s.nc;
+    if (a == b) {
+      da[q] = make_double2(ka * sg.y, -ka * sg.x);  // -i k sigma
+    } else {
+      const double2 x = da[q], y = db[q];
+      da[q] = make_double2(x.x + kb * sg.y, x.y - kb * sg.x);  // - i k_b sigma
+      db[q] = make_double2(y.x + ka * sg.y, y.y - ka * sg.x);  // - i k_a sigma
+    }
+  }
+}
+
+// r = va * vb on the n^3 transform grid
+__global__ void k_sp_product(long long n3, const double *__restrict__ va,
+                             const double *__restrict__ vb, double *__restrict__ r) {
+  SP_LOOP(t, n3) r[t] = va[t] * vb[t];
+}
+
+// ifstage_kernel! (src/spectral/step.jl:22-43): one Wray stage with the
+// integrating factor phi = exp(-nu dc dt k^2)
+__global__ void k_sp_ifstage(SpGeo s, double2 *__restrict__ uh, double2 *__restrict__ ustart,
+                             const double2 *__restrict__ du, double a, double b, double nudcdt,
+                             double dt) {
+  SP_LOOP(q, s.nc) {
+    int kx, ky, kz;
+    sp_modes(s, q, kx, ky, kz);
+    const double k1 = s.kfac * kx, k2 = s.kfac * ky, k3 = s.kfac * kz;
+    const double kk = k1 * k1 + k2 * k2 + k3 * k3;
+    const double phi = exp(-nudcdt * kk);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const long long i = c * s.nc + q;
+      const double2 st = ustart[i], d = du[i];
+      uh[i] = make_double2(phi * (st.x + a * dt * d.x), phi * (st.y + a * dt * d.y));
+      ustart[i] = make_double2(phi * (st.x + b * dt * d.x), phi * (st.y + b * dt * d.y));
+    }
+  }
+}
+
+// project_kernel! (src/spectral/operators.jl:10-23)
+__global__ void k_sp_project(SpGeo s, double2 *__restrict__ uh) {
+  SP_LOOP(q, s.nc) {
+    int kx, ky, kz;
+    sp_modes(s, q, kx, ky, kz);
+    const double k1 = s.kfac * kx, k2 = s.kfac * ky, k3 = s.kfac * kz;
+    const double kk = k1 * k1 + k2 * k2 + k3 * k3;
+    const double2 ux = uh[q], uy = uh[s.nc + q], uz = uh[2 * s.nc + q];
+    double2 p = make_double2((k1 * ux.x + k2 * uy.x + k3 * uz.x) / kk,
+                             (k1 * ux.y + k2 * uy.y + k3 * uz.y) / kk);
+    if (kk == 0) p = make_double2(0.0, 0.0);
+    uh[q] = make_double2(ux.x - k1 * p.x, ux.y - k1 * p.y);
+    uh[s.nc + q] = make_double2(uy.x - k2 * p.x, uy.y - k2 * p.y);
+    uh[2 * s.nc + q] = make_double2(uz.x - k3 * p.x, uz.y - k3 * p.y);
+  }
+}
+
+// Per-block partial sums over the compact state with the rfft
+// double-counting weight (kx > 0 twice; kx <= kcut < n/2 has no Nyquist):
+// mode 0 = |u_hat|^2 / 2 (spectral_energy), mode 1 = k^2 |u_hat|^2
+// (spectral_dissipation without nu), src/spectral/operators.jl:60-102
+__global__ void k_sp_sum(SpGeo s, const double2 *__restrict__ uh, int mode, double *partial) {
+  double acc = 0.0;
+  SP_LOOP(q, s.nc) {
+    int kx, ky, kz;
+    sp_modes(s, q, kx, ky, kz);
+    double a2 = 0.0;
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const double2 v = uh[c * s.nc + q];
+      a2 += v.x * v.x + v.y * v.y;
+    }
+    const double k1 = s.kfac * kx, k2 = s.kfac * ky, k3 = s.kfac * kz;
+    const double w = kx > 0 ? 2.0 : 1.0;
+    acc += w * (mode == 0 ? a2 / 2 : a2 * (k1 * k1 + k2 * k2 + k3 * k3));
+  }
+  __shared__ double sh[256];
+  sh[threadIdx.x] = acc;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partial[blockIdx.x] = sh[0];
+}
+
+__device__ __forceinline__ unsigned long long sp_bits(double v) {
+  return (unsigned long long)__double_as_longlong(v);
+}
+
+// max |k . u_hat| (spectral_maxdiv, src/spectral/operators.jl:104-110)
+__global__ void k_sp_maxdiv(SpGeo s, const double2 *__restrict__ uh, unsigned long long *out) {
+  double m = 0.0;
+  SP_LOOP(q, s.nc) {
+    int kx, ky, kz;
+    sp_modes(s, q, kx, ky, kz);
+    const double k1 = s.kfac * kx, k2 = s.kfac * ky, k3 = s.kfac * kz;
+    const double2 ux = uh[q], uy = uh[s.nc + q], uz = uh[2 * s.nc + q];
+    const double re = k1 * ux.x + k2 * uy.x + k3 * uz.x, im = k1 * ux.y + k2 * uy.y + k3 * uz.y;
+    m = fmax(m, sqrt(re * re + im * im));
+  }
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, sp_bits(m));
+}
+
+// vsummax (src/spectral/step.jl:45-58): max over the grid of |v1|+|v2|+|v3|
+__global__ void k_sp_vsummax(long long n3, const double *__restrict__ v0,
+                             const double *__restrict__ v1, const double *__restrict__ v2,
+                             unsigned long long *out) {
+  double m = 0.0;
+  SP_LOOP(t, n3) m = fmax(m, fabs(v0[t]) + fabs(v1[t]) + fabs(v2[t]));
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, sp_bits(m));
+}
+
+#undef SP_LOOP
+
+}  // namespace dnsb

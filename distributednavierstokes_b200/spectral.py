@@ -1,0 +1,221 @@
+"""Host mirror of the reference's pseudo-spectral solver for a periodic cube
+(src/spectral/setup.jl, step.jl, operators.jl, ic.jl), single rank, on
+libdnsb's dnsb_spectral_* entry points.
+
+The state `uh` is a complex128 CUDA tensor of shape (3, m, m, kcut+1) —
+component, kz, ky, kx in C order, i.e. the reference's column-major
+(kcut+1, m, m, 3) compact spectrum with kx fastest — and u_hat = F[u]/n^3.
+Physical fields are float64 tensors of shape (3, n, n, n) (component, z, y,
+x) at the cell centres (i - 1/2) l / n.
+"""
+import ctypes
+import math
+
+import numpy as np
+import torch
+
+from . import _lib
+
+
+class SpectralError(RuntimeError):
+    pass
+
+
+def _ptr(t):
+    if not (t.is_cuda and t.is_contiguous() and t.dtype in (torch.float64, torch.complex128)):
+        raise ValueError("arrays must be contiguous float64/complex128 CUDA tensors")
+    return ctypes.c_void_p(t.data_ptr())
+
+
+class SpectralSetup:
+    """spectral_setup(; n, l, visc, kcut) (src/spectral/setup.jl:28-110),
+    one rank."""
+
+    def __init__(self, n, l=2 * math.pi, visc=1e-3, kcut=None, device=None):
+        if n % 2:
+            raise ValueError("n must be even")
+        kcut = n // 3 if kcut is None else int(kcut)
+        if kcut < 1:
+            raise ValueError("kcut must be at least 1")
+        if 3 * kcut > n:
+            raise ValueError("aliasing: 3kcut <= n is required (2/3 rule)")
+        self.n, self.l, self.visc, self.kcut = int(n), float(l), float(visc), kcut
+        self.m = 2 * kcut + 1
+        self.device = torch.device(device if device is not None else "cuda")
+        self.T = torch.float64
+        self._sp = None
+        lib = _lib.load()
+        sp = ctypes.c_void_p()
+        with torch.cuda.device(self.device):
+            stream = torch.cuda.current_stream(self.device).cuda_stream
+            rc = lib.dnsb_spectral_create(self.n, kcut, self.l, self.visc, self.device.index or 0,
+                                          ctypes.c_void_p(stream), ctypes.byref(sp))
+        if rc != 0:
+            raise _lib.DNSBError(f"spectral setup failed: {lib.dnsb_spectral_last_error(None).decode()}")
+        self._sp = sp
+        kf = 2 * math.pi / self.l
+        cf = np.array([j if j <= kcut else j - self.m for j in range(self.m)], dtype=np.float64)
+        self.kx, self.ky, self.kz = kf * np.arange(kcut + 1), kf * cf, kf * cf
+
+    @property
+    def sp(self):
+        if self._sp is None:
+            raise RuntimeError("spectral setup has been closed")
+        lib = _lib.load()
+        stream = torch.cuda.current_stream(self.device).cuda_stream
+        self._call(lib.dnsb_spectral_set_stream(self._sp, ctypes.c_void_p(stream)))
+        return self._sp
+
+    def _call(self, rc):
+        if rc != 0:
+            raise _lib.DNSBError(_lib.load().dnsb_spectral_last_error(self._sp).decode())
+
+    def close(self):
+        if self._sp is not None:
+            _lib.load().dnsb_spectral_destroy(self._sp)
+            self._sp = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def spectral_setup(*, n, l=2 * math.pi, visc=1e-3, kcut=None, device=None):
+    return SpectralSetup(n, l, visc, kcut, device)
+
+
+def specvelocity(s):
+    """specvelocity(s): a zero spectral state."""
+    return torch.zeros((3, s.m, s.m, s.kcut + 1), dtype=torch.complex128, device=s.device)
+
+
+def physvelocity(s):
+    return torch.zeros((3, s.n, s.n, s.n), dtype=torch.float64, device=s.device)
+
+
+def spec_to_phys(v, uh, s):
+    """spec_to_phys!(v, uh, s): the physical velocity of uh."""
+    s._call(_lib.load().dnsb_spectral_to_phys(s.sp, _ptr(uh), _ptr(v)))
+    return v
+
+
+def phys_to_spec(uh, v, s):
+    """phys_to_spec!(uh, v, s) with the truncation to the retained modes."""
+    s._call(_lib.load().dnsb_spectral_from_phys(s.sp, _ptr(v), _ptr(uh)))
+    return uh
+
+
+def spectral_rhs(du, uh, s):
+    """spectral_rhs!(du, uh, s) (src/spectral/operators.jl:66-96)."""
+    s._call(_lib.load().dnsb_spectral_rhs(s.sp, _ptr(uh), _ptr(du)))
+    return du
+
+
+def spectral_project(uh, s):
+    """spectral_project!(uh, s) (src/spectral/operators.jl:25-29)."""
+    s._call(_lib.load().dnsb_spectral_project(s.sp, _ptr(uh)))
+    return uh
+
+
+def spectral_step(uh, s, dt):
+    """spectral_step!(uh, s, dt, cache) (src/spectral/step.jl:60-92);
+    returns the first stage's vsummax."""
+    out = ctypes.c_double()
+    s._call(_lib.load().dnsb_spectral_step(s.sp, _ptr(uh), float(dt), ctypes.byref(out)))
+    return out.value
+
+
+def vsummax(uh, s):
+    out = ctypes.c_double()
+    s._call(_lib.load().dnsb_spectral_vsummax(s.sp, _ptr(uh), ctypes.byref(out)))
+    return out.value
+
+
+def _diag(uh, s, which):
+    out = ctypes.c_double()
+    s._call(_lib.load().dnsb_spectral_diagnostic(s.sp, _ptr(uh), which, ctypes.byref(out)))
+    return out.value
+
+
+def spectral_energy(uh, s):
+    """spectral_energy(uh, s): <|u|^2>/2 (src/spectral/operators.jl:98-99)."""
+    return _diag(uh, s, 0)
+
+
+def spectral_dissipation(uh, s):
+    """spectral_dissipation(uh, s): nu sum k^2 |u_hat|^2 (:101-107)."""
+    return _diag(uh, s, 1)
+
+
+def spectral_maxdiv(uh, s):
+    """spectral_maxdiv(uh, s): max |k . u_hat| (:109-110)."""
+    return _diag(uh, s, 2)
+
+
+def spectral_velocityfield(uh, s, x, y, z, project=True):
+    """spectral_velocityfield!(uh, s; x, y, z, project) (src/spectral/ic.jl:6-25):
+    the three functions at the cell centres, forward transformed."""
+    c = s.l / s.n * (np.arange(s.n) + 0.5)
+    Z, Y, X = np.meshgrid(c, c, c, indexing="ij")
+    h = np.stack([np.vectorize(f)(X, Y, Z) if f is not None else np.zeros_like(X)
+                  for f in (x, y, z)]).astype(np.float64)
+    v = torch.from_numpy(h).to(s.device)
+    phys_to_spec(uh, v, s)
+    if project:
+        spectral_project(uh, s)
+    return uh
+
+
+def taylorgreen(uh, s, V0=1.0):
+    """taylorgreen!(uh, s; V0) (src/spectral/ic.jl:86-97)."""
+    l = s.l
+    return spectral_velocityfield(
+        uh, s,
+        x=lambda x, y, z: V0 * math.sin(2 * math.pi * x / l) * math.cos(2 * math.pi * y / l)
+        * math.cos(2 * math.pi * z / l),
+        y=lambda x, y, z: -V0 * math.cos(2 * math.pi * x / l) * math.sin(2 * math.pi * y / l)
+        * math.cos(2 * math.pi * z / l),
+        z=lambda x, y, z: 0.0)
+
+
+SpectralState = __import__("collections").namedtuple("SpectralState", "uh t n")
+
+
+def spectral_solve(*, uh, setup, tlims, dt=None, cfl=0.85, forcing=None, tstops=(), nstart=0,
+                   processors=None):
+    """spectral_solve!(; uh, setup, tlims, Δt, cfl, forcing, tstops, nstart,
+    processors) (src/spectral/step.jl:94-170).  forcing(uh, s) after every
+    step; a processor returning "stop" ends the solve after that step."""
+    s = setup
+    processors = dict(processors or {})
+    spectral_project(uh, s)
+    kmax = 2 * math.pi * s.kcut / s.l
+    eps = np.finfo(np.float64).eps
+    vmax = vsummax(uh, s) if dt is None else 0.0
+    t, tend = float(tlims[0]), float(tlims[1])
+    tol = 1e-10 * (abs(tend) + 1)
+    stops = sorted(x for x in tstops if t + tol < x < tend - tol)
+    istop = 0
+    n = nstart
+    stop = False
+    state = SpectralState(uh, t, n)
+    for proc in processors.values():
+        stop |= proc(state, s) == "stop"
+    while not stop and t < tend - tol:
+        while istop < len(stops) and stops[istop] <= t + tol:
+            istop += 1
+        tnext = stops[istop] if istop < len(stops) else tend
+        dtn = min(dt if dt is not None else cfl * math.sqrt(3) / (kmax * (vmax + eps)), tnext - t)
+        vloc = spectral_step(uh, s, dtn)
+        if forcing is not None:
+            forcing(uh, s)
+        if dt is None:
+            vmax = vloc
+        t += dtn
+        n += 1
+        state = SpectralState(uh, t, n)
+        for proc in processors.values():
+            stop |= proc(state, s) == "stop"
+    return state

@@ -254,6 +254,43 @@ int dnsb_ensemble_run(dnsb_ensemble *ens, double *const *fields, const double *d
  * next run when the forcing changes. */
 int dnsb_ensemble_forcing(dnsb_ensemble *ens, int i, const double *eref, int nshells);
 
+/* The pseudo-spectral solver of a periodic cube (the reference's second
+ * solver, src/spectral/*.jl): transform grid n^3 (even; FFT lengths with
+ * factors 2, 3, 5), side l, viscosity visc, truncation kcut (<= 0: n/3;
+ * 3 kcut <= n).  The state uh is the reference's compact spectrum
+ * (spectral_setup, src/spectral/setup.jl:62-73): 3 components, each
+ * (kcut+1) x m x m complex values (interleaved re, im), m = 2 kcut + 1,
+ * column-major with kx = 0..kcut fastest, ky and kz in compact fftfreq order
+ * (0..kcut, then -kcut..-1); u_hat = F[u] / n^3.  Physical fields are 3
+ * real n^3 arrays (x fastest) at the cell centres (i - 1/2) l / n.
+ * Device pointers; work on the solver's stream; errors as elsewhere, with
+ * dnsb_spectral_last_error. */
+typedef struct dnsb_spectral dnsb_spectral;
+int dnsb_spectral_create(int n, int kcut, double l, double visc, int device, void *stream,
+                         dnsb_spectral **out);
+void dnsb_spectral_destroy(dnsb_spectral *sp);
+const char *dnsb_spectral_last_error(const dnsb_spectral *sp);
+int dnsb_spectral_set_stream(dnsb_spectral *sp, void *stream);
+/* Compact values per component, (kcut+1) m^2. */
+long dnsb_spectral_size(const dnsb_spectral *sp);
+/* spec_to_phys! (src/spectral/fft.jl): v = the physical velocity of uh. */
+int dnsb_spectral_to_phys(dnsb_spectral *sp, const double *uh, double *v);
+/* phys_to_spec! + truncation: uh = the retained modes of F[v] / n^3. */
+int dnsb_spectral_from_phys(dnsb_spectral *sp, const double *v, double *uh);
+/* spectral_rhs! (src/spectral/operators.jl:66-96): du = -i k_j F[v_i v_j] / n^3. */
+int dnsb_spectral_rhs(dnsb_spectral *sp, const double *uh, double *du);
+/* spectral_project! (src/spectral/operators.jl:10-29). */
+int dnsb_spectral_project(dnsb_spectral *sp, double *uh);
+/* spectral_step! (src/spectral/step.jl:60-92): one Wray RK3 step with the
+ * integrating-factor viscosity, projected after every stage; vmax_out
+ * (optional, synchronises) = vsummax of the first stage's velocity. */
+int dnsb_spectral_step(dnsb_spectral *sp, double *uh, double dt, double *vmax_out);
+/* vsummax of the physical velocity of uh (src/spectral/step.jl:45-58). */
+int dnsb_spectral_vsummax(dnsb_spectral *sp, const double *uh, double *out);
+/* which = 0: spectral_energy, 1: spectral_dissipation, 2: spectral_maxdiv
+ * (src/spectral/operators.jl:98-110), single rank.  Synchronises. */
+int dnsb_spectral_diagnostic(dnsb_spectral *sp, const double *uh, int which, double *out);
+
 /* Instrumentation (no counterpart in the reference, which has no profiling
  * for the FV path): launches are counted always; with dnsb_profile(ctx, 1)
  * every launch of the step path is bracketed by CUDA events on the context's

@@ -1,0 +1,112 @@
+"""Oracle for the pseudo-spectral solver -- TEST INFRASTRUCTURE ONLY
+(imported by tests/ alone; the product never does).
+
+A numpy restatement of the reference's single-rank spectral solver on a
+periodic cube: the compact truncated state of spectral_setup
+(src/spectral/setup.jl:62-73, compactfreq operators.jl:7), spec_to_phys! /
+phys_to_spec! as zero-padded / truncated numpy real FFTs with
+u_hat = F[u]/n^3, spectral_rhs! (operators.jl:66-96, divergence form with
+the reference's grouping of the off-diagonal terms), project_kernel!
+(:10-23), Wray's RK3 with the integrating-factor viscosity
+(step.jl:1-43,60-92) and the diagnostics (:98-110).  The state is numpy
+complex (3, m, m, kcut+1) = [component, kz, ky, kx].
+"""
+import math
+
+import numpy as np
+
+WRAY_A = (8 / 15, 5 / 12, 3 / 4)
+WRAY_B = (1 / 4, 0.0, 0.0)
+WRAY_DC = (8 / 15, 2 / 15, 1 / 3)
+
+
+class Spectral:
+    def __init__(self, n, l=2 * math.pi, visc=1e-3, kcut=None):
+        self.n, self.l, self.visc = n, l, visc
+        self.kcut = n // 3 if kcut is None else kcut
+        self.m = 2 * self.kcut + 1
+        cf = np.array([j if j <= self.kcut else j - self.m for j in range(self.m)])
+        self.idx = cf % n                       # compact -> full index along y and z
+        kf = 2 * math.pi / l
+        self.kx = kf * np.arange(self.kcut + 1)[None, None, :]
+        self.ky = kf * cf[None, :, None]
+        self.kz = kf * cf[:, None, None]
+        self.kk = self.kx ** 2 + self.ky ** 2 + self.kz ** 2
+
+    def zeros(self):
+        return np.zeros((3, self.m, self.m, self.kcut + 1), dtype=np.complex128)
+
+    def to_phys(self, uh):
+        n = self.n
+        v = np.zeros((3, n, n, n))
+        for c in range(3):
+            full = np.zeros((n, n, n // 2 + 1), dtype=np.complex128)
+            full[np.ix_(self.idx, self.idx, np.arange(self.kcut + 1))] = uh[c]
+            v[c] = np.fft.irfftn(full, s=(n, n, n), axes=(0, 1, 2)) * n ** 3
+        return v
+
+    def from_phys(self, v):
+        n = self.n
+        out = self.zeros()
+        for c in range(3):
+            F = np.fft.rfftn(v[c], axes=(0, 1, 2)) / n ** 3
+            out[c] = F[np.ix_(self.idx, self.idx, np.arange(self.kcut + 1))]
+        return out
+
+    def _spec(self, r):
+        F = np.fft.rfftn(r, axes=(0, 1, 2)) / self.n ** 3
+        return F[np.ix_(self.idx, self.idx, np.arange(self.kcut + 1))]
+
+    def rhs(self, uh):
+        v = self.to_phys(uh)
+        sxx, syy, szz = (self._spec(v[c] * v[c]) for c in range(3))
+        du = np.stack([-1j * self.kx * sxx, -1j * self.ky * syy, -1j * self.kz * szz])
+        sxy, syz, szx = self._spec(v[0] * v[1]), self._spec(v[1] * v[2]), self._spec(v[2] * v[0])
+        du[0] -= 1j * (self.ky * sxy + self.kz * szx)
+        du[1] -= 1j * (self.kx * sxy + self.kz * syz)
+        du[2] -= 1j * (self.kx * szx + self.ky * syz)
+        return du, v
+
+    def project(self, uh):
+        kk = np.where(self.kk == 0, 1.0, self.kk)
+        p = (self.kx * uh[0] + self.ky * uh[1] + self.kz * uh[2]) / kk
+        p = np.where(self.kk == 0, 0.0, p)
+        return np.stack([uh[0] - self.kx * p, uh[1] - self.ky * p, uh[2] - self.kz * p])
+
+    def step(self, uh, dt):
+        ustart = uh.copy()
+        vmax = 0.0
+        for i in range(3):
+            du, v = self.rhs(uh)
+            if i == 0:
+                vmax = float(np.max(np.abs(v[0]) + np.abs(v[1]) + np.abs(v[2])))
+            phi = np.exp(-self.visc * WRAY_DC[i] * dt * self.kk)
+            uh = phi * (ustart + WRAY_A[i] * dt * du)
+            ustart = phi * (ustart + WRAY_B[i] * dt * du)
+            uh = self.project(uh)
+        return uh, vmax
+
+    def _w(self):
+        return np.where(np.arange(self.kcut + 1) > 0, 2.0, 1.0)[None, None, :]
+
+    def energy(self, uh):
+        return float(np.sum(self._w() * np.sum(np.abs(uh) ** 2, axis=0)) / 2)
+
+    def dissipation(self, uh):
+        return float(self.visc * np.sum(self._w() * self.kk * np.sum(np.abs(uh) ** 2, axis=0)))
+
+    def maxdiv(self, uh):
+        return float(np.max(np.abs(self.kx * uh[0] + self.ky * uh[1] + self.kz * uh[2])))
+
+    def velocityfield(self, x, y, z):
+        c = self.l / self.n * (np.arange(self.n) + 0.5)
+        Z, Y, X = np.meshgrid(c, c, c, indexing="ij")
+        v = np.stack([np.vectorize(f)(X, Y, Z) if f is not None else np.zeros_like(X)
+                      for f in (x, y, z)]).astype(np.float64)
+        return self.project(self.from_phys(v))
+
+    def random(self, seed, amp=1.0):
+        """A random solenoidal state (test input): projected Gaussian noise."""
+        rng = np.random.default_rng(seed)
+        v = rng.standard_normal((3, self.n, self.n, self.n)) * amp
+        return self.project(self.from_phys(v))

@@ -1,0 +1,101 @@
+"""GPU parity of the pseudo-spectral solver (dnsb_spectral_*,
+distributednavierstokes_b200/spectral.py) against the numpy oracle
+(oracle/spectral_oracle.py): transforms, right-hand side, projection, one
+and five IF-RK3 steps, diagnostics, and the exact viscous decay of a shear
+wave.  Tolerances (FP64): 1e-12 relative for transforms, right-hand side
+and steps; diagnostics 1e-12.
+"""
+import math
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def SP():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from distributednavierstokes_b200 import _lib, spectral
+
+    _lib.load()
+    return spectral
+
+
+def rel(a, b):
+    return float(np.max(np.abs(a - b))) / max(float(np.max(np.abs(b))), 1e-300)
+
+
+def dev(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+@pytest.mark.parametrize("n,kcut", [(12, None), (16, None), (24, 7), (32, None)])
+def test_transforms_rhs_project(SP, n, kcut):
+    import spectral_oracle as SO
+
+    O = SO.Spectral(n, visc=2e-3, kcut=kcut)
+    s = SP.spectral_setup(n=n, visc=2e-3, kcut=kcut)
+    uh = O.random(n, amp=0.7)
+    v = O.to_phys(uh)
+    vd = SP.spec_to_phys(SP.physvelocity(s), dev(uh), s)
+    assert rel(vd.cpu().numpy(), v) < 1e-12
+    back = SP.phys_to_spec(SP.specvelocity(s), dev(v), s)
+    assert rel(back.cpu().numpy(), O.from_phys(v)) < 1e-12
+    du, _ = O.rhs(uh)
+    dud = SP.spectral_rhs(SP.specvelocity(s), dev(uh), s)
+    assert rel(dud.cpu().numpy(), du) < 1e-12
+    raw = O.from_phys(np.random.default_rng(1).standard_normal((3, n, n, n)))
+    pd = SP.spectral_project(dev(raw), s)
+    assert rel(pd.cpu().numpy(), O.project(raw)) < 1e-13
+    for f, g in ((SP.spectral_energy, O.energy), (SP.spectral_dissipation, O.dissipation)):
+        assert math.isclose(f(dev(uh), s), g(uh), rel_tol=1e-12)
+    assert SP.spectral_maxdiv(dev(uh), s) < 1e-12 * float(np.max(np.abs(uh))) * n
+    s.close()
+
+
+@pytest.mark.parametrize("n", [16, 24])
+def test_steps_match_oracle(SP, n):
+    import spectral_oracle as SO
+
+    O = SO.Spectral(n, visc=5e-3)
+    s = SP.spectral_setup(n=n, visc=5e-3)
+    uh = O.random(7, amp=1.0)
+    ud = dev(uh)
+    for k in range(5):
+        uh, vmax = O.step(uh, 0.01)
+        vd = SP.spectral_step(ud, s, 0.01)
+        assert math.isclose(vd, vmax, rel_tol=1e-12)
+        assert rel(ud.cpu().numpy(), uh) < 1e-12 * (k + 1)
+    assert SP.spectral_maxdiv(ud, s) < 1e-12
+    s.close()
+
+
+def test_shear_wave_exact_decay_and_solve(SP):
+    s = SP.spectral_setup(n=16, visc=0.05)
+    uh = SP.specvelocity(s)
+    SP.spectral_velocityfield(uh, s, x=lambda x, y, z: 0.7 * math.sin(2 * y), y=None, z=None)
+    e0 = SP.spectral_energy(uh, s)
+    st = SP.spectral_solve(uh=uh, setup=s, tlims=(0.0, 0.3), dt=0.03)
+    assert st.n == 10
+    assert abs(SP.spectral_energy(uh, s) / e0 - math.exp(-8 * 0.05 * 0.3)) < 1e-13
+    # CFL-adaptive solve of a Taylor-Green vortex: stays solenoidal, energy decays
+    tg = SP.taylorgreen(SP.specvelocity(s), s)
+    e1 = SP.spectral_energy(tg, s)
+    st = SP.spectral_solve(uh=tg, setup=s, tlims=(0.0, 0.2), cfl=0.5)
+    assert st.n > 1 and SP.spectral_energy(tg, s) < e1
+    assert SP.spectral_maxdiv(tg, s) < 1e-12
+    s.close()
+
+
+def test_bad_setups(SP):
+    from distributednavierstokes_b200._lib import DNSBError
+
+    with pytest.raises(ValueError):
+        SP.spectral_setup(n=15)
+    with pytest.raises(ValueError):
+        SP.spectral_setup(n=16, kcut=6)
+    with pytest.raises(DNSBError):
+        SP.spectral_setup(n=14)  # FFT length with a factor 7
