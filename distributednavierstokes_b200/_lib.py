@@ -89,6 +89,12 @@ SIGNATURES = {
     "dnsb_spectral_step": (c_int, [P, P, c_double, ctypes.POINTER(c_double)]),
     "dnsb_spectral_vsummax": (c_int, [P, P, ctypes.POINTER(c_double)]),
     "dnsb_spectral_diagnostic": (c_int, [P, P, c_int, ctypes.POINTER(c_double)]),
+    "dnsb_spectral_shell_count": (c_int, [P]),
+    "dnsb_spectral_shell_energies": (c_int, [P, P, ctypes.POINTER(c_double), c_int]),
+    "dnsb_spectral_shell_rescale": (c_int, [P, P, ctypes.POINTER(c_double), c_int]),
+    "dnsb_spectral_random_field": (c_int, [P, P, c_double, c_double, ctypes.c_ulonglong,
+                                           ctypes.POINTER(c_double), c_int]),
+    "dnsb_spectral_shell_clamp": (c_int, [P, P, ctypes.POINTER(c_double), c_int]),
 }
 
 KINDS = ["momentum", "cn_solve", "div_rfft_x", "fft_z", "y_solve", "ifft_z", "irfft_x",

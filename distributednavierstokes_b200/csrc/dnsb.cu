@@ -513,12 +513,6 @@ __global__ void k_scaleshells(Geo g, double2 *S, const double *__restrict__ f, i
   }
 }
 
-__device__ __forceinline__ unsigned long long splitmix64(unsigned long long x) {
-  unsigned long long z = x + 0x9e3779b97f4a7c15ULL;
-  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
-  z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
-  return z ^ (z >> 31);
-}
 
 __global__ void k_noise(Geo g, double *phi, int c, unsigned long long seed, double amp) {
   const int I = blockIdx.x * blockDim.x + threadIdx.x + 1;
@@ -1951,6 +1945,10 @@ struct dnsb_spectral {
   double *partial = nullptr;                   // RED_BLOCKS + 1
   unsigned long long *umax = nullptr;          // 2 slots
   double *host = nullptr;                      // pinned, 4 doubles
+  int nshell = 0;                              // floor(sqrt(3) kcut) + 1 shells
+  double *shellbuf = nullptr;                  // [E | factors | eref] x nshell
+  double *shellpart = nullptr;                 // RED_BLOCKS x SP_SHELLS partial sums
+  std::vector<double> eref_host;
   std::vector<void *> allocs;
   std::string err;
 };
@@ -2040,6 +2038,29 @@ int sp_rhs(dnsb_spectral *p, const double2 *uh, double2 *du) {
   return 0;
 }
 
+// E[0..nb) (device) = shell energies in a fixed summation order
+int sp_shell_energies_dev(dnsb_spectral *p, const double2 *uh, double *E, int nb) {
+  cudaStream_t st = p->c->stream;
+  if (nb <= SP_SHELLS) {
+    k_sp_shells_det<<<RED_BLOCKS, 256, 0, st>>>(p->s, uh, p->shellpart);
+    SPKL(p);
+    k_sp_shells_fold<<<1, 32, 0, st>>>(p->shellpart, RED_BLOCKS, nb, E);
+  } else {
+    k_sp_shells_byshell<<<nb, 256, 0, st>>>(p->s, uh, E);
+  }
+  SPKL(p);
+  return 0;
+}
+
+int sp_upload_eref(dnsb_spectral *p, const double *eref, int nb) {
+  if (p->eref_host.size() == (size_t)nb && std::equal(eref, eref + nb, p->eref_host.begin())) return 0;
+  SPK(p, cudaMemcpyAsync(p->shellbuf + 2 * p->nshell, eref, nb * sizeof(double),
+                         cudaMemcpyHostToDevice, p->c->stream));
+  SPK(p, cudaStreamSynchronize(p->c->stream));
+  p->eref_host.assign(eref, eref + nb);
+  return 0;
+}
+
 int sp_check(dnsb_spectral *p, const void *a) {
   if (!p) return DNSB_EINVAL;
   if (!a) return spfail(p, DNSB_EINVAL, "null array");
@@ -2085,7 +2106,9 @@ int dnsb_spectral_create(int n, int kcut, double l, double visc, int device, voi
       (rc = spalloc(p, &p->v[2], n3)) || (rc = spalloc(p, &p->r, n3)) ||
       (rc = spalloc(p, &p->ustart, 3 * (size_t)p->s.nc)) ||
       (rc = spalloc(p, &p->du, 3 * (size_t)p->s.nc)) ||
-      (rc = spalloc(p, &p->partial, (size_t)RED_BLOCKS + 1)) || (rc = spalloc(p, &p->umax, 2))) {
+      (rc = spalloc(p, &p->partial, (size_t)RED_BLOCKS + 1)) || (rc = spalloc(p, &p->umax, 2)) ||
+      (rc = spalloc(p, &p->shellbuf, 3 * (size_t)(p->nshell = (int)std::floor(std::sqrt(3.0) * kcut) + 1))) ||
+      (rc = spalloc(p, &p->shellpart, (size_t)RED_BLOCKS * SP_SHELLS))) {
     snprintf(g_create_err, sizeof g_create_err, "%s", p->err.c_str());
     dnsb_spectral_destroy(p);
     return rc;
@@ -2219,6 +2242,83 @@ int dnsb_spectral_diagnostic(dnsb_spectral *p, const double *uh, int which, doub
   }
   SPK(p, cudaStreamSynchronize(c->stream));
   *out = which == 1 ? p->visc * p->host[0] : p->host[0];
+  return 0;
+}
+
+int dnsb_spectral_shell_count(const dnsb_spectral *p) { return p ? p->nshell : -1; }
+
+int dnsb_spectral_shell_energies(dnsb_spectral *p, const double *uh, double *E, int nshells) {
+  int rc = sp_check(p, uh);
+  if (rc || (rc = sp_check(p, E))) return rc;
+  if (nshells < 1) return spfail(p, DNSB_EINVAL, "bad shell count");
+  const int nb = std::min(nshells, p->nshell);
+  if ((rc = sp_shell_energies_dev(p, reinterpret_cast<const double2 *>(uh), p->shellbuf, nb))) return rc;
+  SPK(p, cudaMemcpyAsync(E, p->shellbuf, nb * sizeof(double), cudaMemcpyDeviceToHost, p->c->stream));
+  SPK(p, cudaStreamSynchronize(p->c->stream));
+  for (int i = nb; i < nshells; i++) E[i] = 0;
+  return 0;
+}
+
+int dnsb_spectral_shell_rescale(dnsb_spectral *p, double *uh, const double *factors, int nshells) {
+  int rc = sp_check(p, uh);
+  if (rc || (rc = sp_check(p, factors))) return rc;
+  if (nshells < 1) return spfail(p, DNSB_EINVAL, "bad shell count");
+  const int nb = std::min(nshells, p->nshell);
+  double *f = p->shellbuf + p->nshell;
+  SPK(p, cudaMemcpyAsync(f, factors, nb * sizeof(double), cudaMemcpyHostToDevice, p->c->stream));
+  k_sp_scale_shells<<<RED_BLOCKS, 256, 0, p->c->stream>>>(p->s, reinterpret_cast<double2 *>(uh), f, nb);
+  SPKL(p);
+  SPK(p, cudaStreamSynchronize(p->c->stream));
+  return 0;
+}
+
+int dnsb_spectral_random_field(dnsb_spectral *p, double *uh, double totalenergy, double kpeak,
+                               unsigned long long seed, const double *profile, int nprofile) {
+  int rc = sp_check(p, uh);
+  if (rc) return rc;
+  if (profile ? nprofile < 1 : !(kpeak > 0)) return spfail(p, DNSB_EINVAL, "bad spectrum profile");
+  dnsb_ctx *c = p->c;
+  double2 *u2 = reinterpret_cast<double2 *>(uh);
+  const double n3 = (double)sp_n3(p);
+  for (int comp = 0; comp < 3; comp++) {
+    k_sp_noise<<<RED_BLOCKS, 256, 0, c->stream>>>(p->s.n, p->v[comp], comp, seed);
+    SPKL(p);
+    if ((rc = sp_from_phys(p, p->v[comp]))) return rc;
+    k_sp_gather<<<RED_BLOCKS, 256, 0, c->stream>>>(p->s, c->S, u2 + comp * p->s.nc, 1.0 / n3);
+    SPKL(p);
+  }
+  k_sp_project<<<RED_BLOCKS, 256, 0, c->stream>>>(p->s, u2);
+  SPKL(p);
+  const int nb = p->nshell;
+  std::vector<double> E(nb), f(nb), prof(nb);
+  if ((rc = dnsb_spectral_shell_energies(p, uh, E.data(), nb))) return rc;
+  double tot = 0;
+  for (int i = 0; i < nb; i++) {
+    const double k = i;
+    prof[i] = profile ? (i < nprofile ? profile[i] : 0.0) : k * k * k * k * exp(-2 * (k / kpeak) * (k / kpeak));
+    tot += prof[i];
+  }
+  if (!(tot > 0)) return spfail(p, DNSB_EINVAL, "spectrum profile sums to zero");
+  for (int i = 0; i < nb; i++) {
+    const double e0 = totalenergy * prof[i] / tot;
+    f[i] = E[i] > 0 ? sqrt(e0 / E[i]) : 0.0;
+  }
+  return dnsb_spectral_shell_rescale(p, uh, f.data(), nb);
+}
+
+int dnsb_spectral_shell_clamp(dnsb_spectral *p, double *uh, const double *eref, int nshells) {
+  int rc = sp_check(p, uh);
+  if (rc || (rc = sp_check(p, eref))) return rc;
+  if (nshells < 1) return spfail(p, DNSB_EINVAL, "bad shell count");
+  const int nb = std::min(nshells, p->nshell);
+  if ((rc = sp_upload_eref(p, eref, nb))) return rc;
+  double *E = p->shellbuf, *f = E + p->nshell, *er = f + p->nshell;
+  double2 *u2 = reinterpret_cast<double2 *>(uh);
+  if ((rc = sp_shell_energies_dev(p, u2, E, nb))) return rc;
+  k_sp_clamp_factors<<<1, 256, 0, p->c->stream>>>(E, er, f, nb);
+  SPKL(p);
+  k_sp_scale_shells<<<RED_BLOCKS, 256, 0, p->c->stream>>>(p->s, u2, f, nb);
+  SPKL(p);
   return 0;
 }
 

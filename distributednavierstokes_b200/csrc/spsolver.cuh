@@ -14,6 +14,15 @@
 
 namespace dnsb {
 
+// splitmix64 (src/spectral/ic.jl:31-36): one step of the published
+// SplitMix64 generator from state x
+__device__ __forceinline__ unsigned long long splitmix64(unsigned long long x) {
+  unsigned long long z = x + 0x9e3779b97f4a7c15ULL;
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+  return z ^ (z >> 31);
+}
+
 struct SpGeo {
   int n, kcut, m;
   long long nc;  // compact values per component
@@ -180,6 +189,121 @@ __global__ void k_sp_vsummax(long long n3, const double *__restrict__ v0,
   SP_LOOP(t, n3) m = fmax(m, fabs(v0[t]) + fabs(v1[t]) + fabs(v2[t]));
   for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
   if ((threadIdx.x & 31) == 0) atomicMax(out, sp_bits(m));
+}
+
+// noise_kernel! (src/spectral/ic.jl:37-51) on the n^3 grid of component c
+// (one rank: offsets 0): Box-Muller of two splitmix64 uniforms,
+// key = ((c n + k) n + j) n + i
+__global__ void k_sp_noise(int n, double *__restrict__ v, int c, unsigned long long seed) {
+  const long long n3 = (long long)n * n * n;
+  SP_LOOP(t, n3) {
+    const unsigned long long key = (unsigned long long)c * (unsigned long long)n3 + (unsigned long long)t;
+    const unsigned long long r1 = splitmix64(seed + 2 * key), r2 = splitmix64(seed + 2 * key + 1);
+    const double u1 = ((double)(r1 >> 11) + 0.5) * 0x1p-53;
+    const double u2 = ((double)(r2 >> 11) + 0.5) * 0x1p-53;
+    v[t] = sqrt(-2.0 * log(u1)) * cospi(2.0 * u2);
+  }
+}
+
+// integer shell floor(sqrt(kx^2 + ky^2 + kz^2)) of a compact mode
+// (src/spectral/forcing.jl:17) and its rfft weight
+__device__ __forceinline__ int sp_shell(const SpGeo &s, long long q, double &w) {
+  int kx, ky, kz;
+  sp_modes(s, q, kx, ky, kz);
+  const long long k2 = (long long)kx * kx + (long long)ky * ky + (long long)kz * kz;
+  long long r = (long long)sqrt((double)k2);
+  while (r * r > k2) r--;
+  while ((r + 1) * (r + 1) <= k2) r++;
+  w = kx > 0 ? 2.0 : 1.0;
+  return (int)r;
+}
+
+// shell_energies (src/spectral/forcing.jl:12-24), fixed summation order:
+// per-block partial sums of the lowest SP_SHELLS shells ...
+constexpr int SP_SHELLS = 8;
+__global__ void __launch_bounds__(256) k_sp_shells_det(SpGeo s, const double2 *__restrict__ uh,
+                                                       double *partial) {
+  double acc[SP_SHELLS];
+#pragma unroll
+  for (int i = 0; i < SP_SHELLS; i++) acc[i] = 0.0;
+  SP_LOOP(q, s.nc) {
+    double w;
+    const int sh = sp_shell(s, q, w);
+    if (sh >= SP_SHELLS) continue;
+    double a2 = 0.0;
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const double2 v = uh[c * s.nc + q];
+      a2 += v.x * v.x + v.y * v.y;
+    }
+    const double e = w * a2 / 2;
+#pragma unroll
+    for (int i = 0; i < SP_SHELLS; i++) acc[i] += sh == i ? e : 0.0;
+  }
+  __shared__ double red[SP_SHELLS][256];
+  const int tid = threadIdx.x;
+#pragma unroll
+  for (int i = 0; i < SP_SHELLS; i++) red[i][tid] = acc[i];
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (tid < o) {
+#pragma unroll
+      for (int i = 0; i < SP_SHELLS; i++) red[i][tid] += red[i][tid + o];
+    }
+    __syncthreads();
+  }
+  if (tid < SP_SHELLS) partial[blockIdx.x * SP_SHELLS + tid] = red[tid][0];
+}
+__global__ void k_sp_shells_fold(const double *partial, int nblocks, int nb, double *E) {
+  const int sh = threadIdx.x;
+  if (sh >= nb) return;
+  double a = 0.0;
+  for (int b = 0; b < nblocks; b++) a += partial[b * SP_SHELLS + sh];
+  E[sh] = a;
+}
+// ... or one block per shell for any number of shells (set-up time)
+__global__ void __launch_bounds__(256) k_sp_shells_byshell(SpGeo s, const double2 *__restrict__ uh,
+                                                           double *E) {
+  const int target = blockIdx.x;
+  double acc = 0.0;
+  for (long long q = threadIdx.x; q < s.nc; q += blockDim.x) {
+    double w;
+    if (sp_shell(s, q, w) != target) continue;
+    double a2 = 0.0;
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const double2 v = uh[c * s.nc + q];
+      a2 += v.x * v.x + v.y * v.y;
+    }
+    acc += w * a2 / 2;
+  }
+  __shared__ double red[256];
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) E[target] = red[0];
+}
+
+// rescale_shell! (src/spectral/forcing.jl:26-35) for all shells < nb at once
+__global__ void k_sp_scale_shells(SpGeo s, double2 *__restrict__ uh, const double *__restrict__ f,
+                                  int nb) {
+  SP_LOOP(q, s.nc) {
+    double w;
+    const int sh = sp_shell(s, q, w);
+    if (sh >= nb) continue;
+    const double fs = f[sh];
+#pragma unroll
+    for (int c = 0; c < 3; c++) uh[c * s.nc + q] = cscale(uh[c * s.nc + q], fs);
+  }
+}
+
+// shellforcing's closure: f = sqrt(eref / E) for forced shells with E > 0
+__global__ void k_sp_clamp_factors(const double *E, const double *eref, double *f, int nb) {
+  for (int i = threadIdx.x; i < nb; i += blockDim.x)
+    f[i] = (eref[i] >= 0 && E[i] > 0) ? sqrt(eref[i] / E[i]) : 1.0;
 }
 
 #undef SP_LOOP

@@ -219,3 +219,63 @@ def spectral_solve(*, uh, setup, tlims, dt=None, cfl=0.85, forcing=None, tstops=
         for proc in processors.values():
             stop |= proc(state, s) == "stop"
     return state
+
+
+# ----------------------------------------------- shells, random field, forcing
+# src/spectral/ic.jl:53-84 and src/spectral/forcing.jl:1-56 on the compact
+# state: shell s = the modes with s <= |k_int| < s+1.
+
+def _dptr(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def shell_count(s):
+    """floor(sqrt(3) kcut) + 1: the shells 0..kdiag of spectral_randomfield!."""
+    return int(_lib.load().dnsb_spectral_shell_count(s.sp))
+
+
+def shell_energies(uh, s, shells):
+    """shell_energies(uh, s, shells) (src/spectral/forcing.jl:12-24)."""
+    shells = [int(v) for v in shells]
+    nb = max(shells) + 1
+    E = np.zeros(nb)
+    s._call(_lib.load().dnsb_spectral_shell_energies(s.sp, _ptr(uh), _dptr(E), nb))
+    return np.array([E[v] for v in shells])
+
+
+def rescale_shell(uh, s, sh, factor):
+    """rescale_shell!(uh, s, sh, factor) (src/spectral/forcing.jl:26-35)."""
+    f = np.ones(int(sh) + 1)
+    f[int(sh)] = factor
+    s._call(_lib.load().dnsb_spectral_shell_rescale(s.sp, _ptr(uh), _dptr(f), len(f)))
+    return uh
+
+
+def spectral_randomfield(uh, s, totalenergy=1.0, kpeak=4.0, seed=0, profile=None):
+    """spectral_randomfield!(uh, s; totalenergy, kpeak, seed, profile)
+    (src/spectral/ic.jl:53-84)."""
+    if profile is None:
+        prof, ptr, nprof = None, None, 0
+    else:
+        prof = np.array([profile(k) for k in range(shell_count(s))], dtype=np.float64)
+        ptr, nprof = _dptr(prof), len(prof)
+    s._call(_lib.load().dnsb_spectral_random_field(s.sp, _ptr(uh), float(totalenergy), float(kpeak),
+                                                   int(seed), ptr, nprof))
+    return uh
+
+
+def shellforcing(uh, s, shells=(1, 2), eref=None):
+    """shellforcing(uh, s; shells, eref) (src/spectral/forcing.jl:37-56):
+    the closure forcing(uh, s) clamps the shells back to eref on the device."""
+    shells = [int(v) for v in shells]
+    eref = shell_energies(uh, s, shells) if eref is None else np.asarray(eref, dtype=np.float64)
+    table = -np.ones(max(shells) + 1)
+    for sh, e in zip(shells, eref):
+        table[sh] = e
+
+    def forcing(uh2, s2):
+        s2._call(_lib.load().dnsb_spectral_shell_clamp(s2.sp, _ptr(uh2), _dptr(table), len(table)))
+
+    forcing.eref = np.array(eref)
+    forcing._table = table
+    return forcing

@@ -287,6 +287,20 @@ int dnsb_spectral_project(dnsb_spectral *sp, double *uh);
 int dnsb_spectral_step(dnsb_spectral *sp, double *uh, double dt, double *vmax_out);
 /* vsummax of the physical velocity of uh (src/spectral/step.jl:45-58). */
 int dnsb_spectral_vsummax(dnsb_spectral *sp, const double *uh, double *out);
+/* Integer shells floor(|k|) of the spectral state (src/spectral/forcing.jl):
+ * count = floor(sqrt(3) kcut) + 1; energies into the HOST array E (fixed
+ * summation order); rescale by HOST factors; spectral_randomfield!
+ * (src/spectral/ic.jl:53-84: Gaussian counter-based noise on the n^3 grid
+ * with noise_kernel!'s key, phys_to_spec!, projection, every shell rescaled
+ * to totalenergy * profile[s] / sum(profile), profile = NULL: k^4
+ * exp(-2 (k/kpeak)^2)); and the closure of shellforcing (:37-56) with the
+ * table eref (eref[s] < 0: shell s not forced), on the device. */
+int dnsb_spectral_shell_count(const dnsb_spectral *sp);
+int dnsb_spectral_shell_energies(dnsb_spectral *sp, const double *uh, double *E, int nshells);
+int dnsb_spectral_shell_rescale(dnsb_spectral *sp, double *uh, const double *factors, int nshells);
+int dnsb_spectral_random_field(dnsb_spectral *sp, double *uh, double totalenergy, double kpeak,
+                               unsigned long long seed, const double *profile, int nprofile);
+int dnsb_spectral_shell_clamp(dnsb_spectral *sp, double *uh, const double *eref, int nshells);
 /* which = 0: spectral_energy, 1: spectral_dissipation, 2: spectral_maxdiv
  * (src/spectral/operators.jl:98-110), single rank.  Synchronises. */
 int dnsb_spectral_diagnostic(dnsb_spectral *sp, const double *uh, int which, double *out);

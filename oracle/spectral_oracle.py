@@ -15,6 +15,8 @@ import math
 
 import numpy as np
 
+from oracle import _splitmix64
+
 WRAY_A = (8 / 15, 5 / 12, 3 / 4)
 WRAY_B = (1 / 4, 0.0, 0.0)
 WRAY_DC = (8 / 15, 2 / 15, 1 / 3)
@@ -110,3 +112,71 @@ class Spectral:
         rng = np.random.default_rng(seed)
         v = rng.standard_normal((3, self.n, self.n, self.n)) * amp
         return self.project(self.from_phys(v))
+
+    # -------------------------------------------- shells, random field, forcing
+    def shells(self):
+        kx = np.arange(self.kcut + 1)[None, None, :]
+        cf = np.array([j if j <= self.kcut else j - self.m for j in range(self.m)])
+        k2 = kx ** 2 + cf[None, :, None] ** 2 + cf[:, None, None] ** 2
+        sh = np.floor(np.sqrt(k2.astype(np.float64))).astype(np.int64)
+        sh -= sh * sh > k2
+        sh += (sh + 1) ** 2 <= k2
+        return sh
+
+    def shell_energies(self, uh, nb):
+        """shell_energies (src/spectral/forcing.jl:12-24) for shells 0..nb-1."""
+        sh = np.broadcast_to(self.shells(), uh.shape[1:])
+        e = np.broadcast_to(self._w() * np.sum(np.abs(uh) ** 2, axis=0) / 2, uh.shape[1:])
+        E = np.zeros(nb)
+        m = sh < nb
+        np.add.at(E, sh[m], e[m])
+        return E
+
+    def rescale(self, uh, f):
+        sh = self.shells()
+        fac = np.ones(sh.shape)
+        m = sh < len(f)
+        fac[m] = np.asarray(f)[sh[m]]
+        return uh * fac[None]
+
+    def noise(self, seed):
+        """noise_kernel! (src/spectral/ic.jl:37-51), one rank."""
+        n = self.n
+        v = np.zeros((3, n, n, n))
+        K, J, I = np.meshgrid(*(np.arange(n, dtype=np.uint64),) * 3, indexing="ij")
+        for c in range(3):
+            key = ((np.uint64(c) * np.uint64(n) + K) * np.uint64(n) + J) * np.uint64(n) + I
+            sd = np.uint64(seed)
+            r1 = _splitmix64(sd + np.uint64(2) * key)
+            r2 = _splitmix64(sd + np.uint64(2) * key + np.uint64(1))
+            u1 = ((r1 >> np.uint64(11)).astype(np.float64) + 0.5) * 2.0 ** -53
+            u2 = ((r2 >> np.uint64(11)).astype(np.float64) + 0.5) * 2.0 ** -53
+            v[c] = np.sqrt(-2 * np.log(u1)) * np.cos(2 * np.pi * u2)
+        return v
+
+    def randomfield(self, totalenergy=1.0, kpeak=4.0, seed=0, profile=None):
+        """spectral_randomfield! (src/spectral/ic.jl:59-84)."""
+        uh = self.project(self.from_phys(self.noise(seed)))
+        kdiag = int(math.floor(math.sqrt(3) * self.kcut))
+        E = self.shell_energies(uh, kdiag + 1)
+        k = np.arange(kdiag + 1, dtype=np.float64)
+        prof = (np.array([profile(v) for v in range(kdiag + 1)]) if profile is not None
+                else k ** 4 * np.exp(-2 * (k / kpeak) ** 2))
+        e0 = totalenergy * prof / prof.sum()
+        f = np.where(E > 0, np.sqrt(e0 / np.where(E > 0, E, 1.0)), 0.0)
+        return self.rescale(uh, f)
+
+    def shellforcing(self, uh, shells=(1, 2), eref=None):
+        shells = list(shells)
+        nb = max(shells) + 1
+        eref = self.shell_energies(uh, nb)[shells] if eref is None else np.asarray(eref)
+
+        def forcing(u2):
+            e = self.shell_energies(u2, nb)
+            f = np.ones(nb)
+            for sh, e0 in zip(shells, eref):
+                f[sh] = math.sqrt(e0 / e[sh]) if e[sh] > 0 else 1.0
+            return self.rescale(u2, f)
+
+        forcing.eref = eref
+        return forcing

@@ -99,3 +99,37 @@ def test_bad_setups(SP):
         SP.spectral_setup(n=16, kcut=6)
     with pytest.raises(DNSBError):
         SP.spectral_setup(n=14)  # FFT length with a factor 7
+
+
+def test_random_field_and_forcing_match_oracle(SP):
+    """spectral_randomfield! and shellforcing on the GPU against the oracle,
+    with the reference's own checks (test/spectralmpitests.jl:128-161:
+    n = 18, totalenergy 0.4, kpeak 2, seed 7)."""
+    import spectral_oracle as SO
+
+    O = SO.Spectral(18, visc=5e-3)
+    s = SP.spectral_setup(n=18, visc=5e-3)
+    assert SP.shell_count(s) == int(math.floor(math.sqrt(3) * s.kcut)) + 1
+    uo = O.randomfield(totalenergy=0.4, kpeak=2, seed=7)
+    uh = SP.spectral_randomfield(SP.specvelocity(s), s, totalenergy=0.4, kpeak=2, seed=7)
+    assert rel(uh.cpu().numpy(), uo) < 1e-12
+    again = SP.spectral_randomfield(SP.specvelocity(s), s, totalenergy=0.4, kpeak=2, seed=7)
+    assert torch.equal(again, uh)
+    assert abs(SP.spectral_energy(uh, s) - 0.4) < 1e-13
+    assert SP.spectral_maxdiv(uh, s) < 1e-13
+    nb = SP.shell_count(s)
+    k = np.arange(nb)
+    prof = k ** 4 * np.exp(-2 * (k / 2) ** 2)
+    E = SP.shell_energies(uh, s, range(nb))
+    assert np.max(np.abs(E[:s.kcut + 1] - (0.4 * prof / prof.sum())[:s.kcut + 1])) < 1e-13
+    fo = O.shellforcing(uo, shells=(1, 2))
+    f = SP.shellforcing(uh, s, shells=(1, 2))
+    assert np.allclose(f.eref, fo.eref, rtol=1e-12, atol=0)
+    for _ in range(4):
+        uo, _ = O.step(uo, 0.02)
+        uo = fo(uo)
+    st = SP.spectral_solve(uh=uh, setup=s, tlims=(0.0, 0.08), dt=0.02, forcing=f)
+    assert st.n == 4
+    assert rel(uh.cpu().numpy(), uo) < 1e-11
+    assert np.allclose(SP.shell_energies(uh, s, (1, 2)), f.eref, rtol=1e-13, atol=0)
+    s.close()

@@ -56,3 +56,25 @@ def test_dissipation_matches_energy_decay_rate():
     # conserves E)
     rate = (S.energy(uh1) - e0) / dt
     assert abs(rate + d0) < 1e-3 * d0
+
+
+def test_random_field_reference_checks():
+    """The reference's own checks of spectral_randomfield! and shellforcing
+    (test/spectralmpitests.jl:128-161: n = 18, totalenergy 0.4, kpeak 2,
+    seed 7): energy 0.4, divergence-free, spectrum = profile over the
+    shells 0..kcut to 1e-13, forced shells held through a run."""
+    S = SO.Spectral(18, visc=5e-3)
+    uh = S.randomfield(totalenergy=0.4, kpeak=2, seed=7)
+    assert abs(S.energy(uh) - 0.4) < 1e-14
+    assert S.maxdiv(uh) < 1e-14
+    kdiag = int(math.floor(math.sqrt(3) * S.kcut))
+    k = np.arange(kdiag + 1)
+    prof = k ** 4 * np.exp(-2 * (k / 2) ** 2)
+    target = 0.4 * prof / prof.sum()
+    E = S.shell_energies(uh, kdiag + 1)
+    assert np.max(np.abs(E[:S.kcut + 1] - target[:S.kcut + 1])) < 1e-13
+    f = S.shellforcing(uh, shells=(1, 2))
+    for _ in range(4):
+        uh, _ = S.step(uh, 0.02)
+        uh = f(uh)
+    assert np.allclose(S.shell_energies(uh, 3)[1:], f.eref, rtol=1e-13, atol=0)
