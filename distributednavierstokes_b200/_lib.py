@@ -95,6 +95,7 @@ SIGNATURES = {
     "dnsb_spectral_random_field": (c_int, [P, P, c_double, c_double, ctypes.c_ulonglong,
                                            ctypes.POINTER(c_double), c_int]),
     "dnsb_spectral_shell_clamp": (c_int, [P, P, ctypes.POINTER(c_double), c_int]),
+    "dnsb_spectral_les_cube": (c_int, [P, P, c_int, ctypes.POINTER(c_double)]),
 }
 
 KINDS = ["momentum", "cn_solve", "div_rfft_x", "fft_z", "y_solve", "ifft_z", "irfft_x",

@@ -2322,6 +2322,39 @@ int dnsb_spectral_shell_clamp(dnsb_spectral *p, double *uh, const double *eref, 
   return 0;
 }
 
+int dnsb_spectral_les_cube(dnsb_spectral *p, const double *uh, int M, double *out) {
+  int rc = sp_check(p, uh);
+  if (rc || (rc = sp_check(p, out))) return rc;
+  if (M < 2 || M % 2 || M / 2 > p->s.kcut)
+    return spfail(p, DNSB_EINVAL, "LES cube needs an even M with M/2 <= kcut");
+  dnsb_ctx *c = p->c;
+  const size_t per = (size_t)(M / 2 + 1) * M * M;
+  if (c->cube_cap < 9 * per) {
+    double2 *nb = nullptr;
+    if ((rc = dalloc(c, &nb, 9 * per))) return spfail(p, rc, "%s", dnsb_last_error(c));
+    c->cube = nb;
+    c->cube_cap = 9 * per;
+  }
+  const double2 *u2 = reinterpret_cast<const double2 *>(uh);
+  const long long n3 = sp_n3(p);
+  for (int comp = 0; comp < 3; comp++) {
+    k_sp_cube<<<RED_BLOCKS, 256, 0, c->stream>>>(p->s, u2 + comp * p->s.nc, M, c->cube + comp * per);
+    SPKL(p);
+    if ((rc = sp_to_phys(p, u2 + comp * p->s.nc, p->v[comp]))) return rc;
+  }
+  static const int pa[6] = {0, 1, 2, 0, 1, 2}, pb[6] = {0, 1, 2, 1, 2, 0};
+  for (int f = 0; f < 6; f++) {
+    k_sp_product<<<RED_BLOCKS, 256, 0, c->stream>>>(n3, p->v[pa[f]], p->v[pb[f]], p->r);
+    SPKL(p);
+    if ((rc = sp_from_phys(p, p->r))) return rc;
+    k_lescube<<<RED_BLOCKS, 256, 0, c->stream>>>(c->g, c->S, M, 1.0 / (double)n3, c->cube + (3 + f) * per);
+    SPKL(p);
+  }
+  SPK(p, cudaMemcpyAsync(out, c->cube, 9 * per * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
+  SPK(p, cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
 int dnsb_spectral_set_stream(dnsb_spectral *p, void *stream) {
   if (!p) return DNSB_EINVAL;
   return dnsb_set_stream(p->c, stream);

@@ -191,6 +191,23 @@ __global__ void k_sp_vsummax(long long n3, const double *__restrict__ v0,
   if ((threadIdx.x & 31) == 0) atomicMax(out, sp_bits(m));
 }
 
+// The LES cube |k_i| <= M/2 (M/2 <= kcut) of one state component in the
+// coarse rfft layout cube[(kc M + jc)(M/2+1) + kx] (jc, kc wrapped: 0..M/2-1
+// then -M/2..-1), straight from the compact state (lesboxes,
+// src/spectral/les.jl:146-168: the cube of u_hat is a plain truncation)
+__global__ void k_sp_cube(SpGeo s, const double2 *__restrict__ uh, int M, double2 *__restrict__ cube) {
+  const int h = M / 2 + 1;
+  const long long n = (long long)h * M * M;
+  SP_LOOP(t, n) {
+    const int kx = (int)(t % h);
+    const long long r = t / h;
+    const int jc = (int)(r % M), kc = (int)(r / M);
+    const int ky = jc < M / 2 ? jc : jc - M, kz = kc < M / 2 ? kc : kc - M;
+    const int j = ky >= 0 ? ky : ky + s.m, k = kz >= 0 ? kz : kz + s.m;  // compact index
+    cube[t] = uh[kx + (long long)(s.kcut + 1) * (j + (long long)s.m * k)];
+  }
+}
+
 // noise_kernel! (src/spectral/ic.jl:37-51) on the n^3 grid of component c
 // (one rank: offsets 0): Box-Muller of two splitmix64 uniforms,
 // key = ((c n + k) n + j) n + i

@@ -279,3 +279,43 @@ def shellforcing(uh, s, shells=(1, 2), eref=None):
     forcing.eref = np.array(eref)
     forcing._table = table
     return forcing
+
+
+# ------------------------------------------- filtered-field / SFS sampling
+# sfs_sample! (src/spectral/les.jl:302-370) on the spectral state: the cube
+# on the GPU (dnsb_spectral_les_cube), the coarse-grid half on the host
+# (les.sfs_from_cube, the reference's rank-0 code).
+
+def les_cube(uh, s, M):
+    """The 9 coarse cubes (u_hat x, y, z, sigma_hat xx, yy, zz, xy, yz, zx),
+    numpy (9, M, M, M//2+1)."""
+    out = np.zeros((9, M, M, M // 2 + 1), dtype=np.complex128)
+    s._call(_lib.load().dnsb_spectral_les_cube(s.sp, _ptr(uh), int(M), _dptr(out.view(np.float64))))
+    return out
+
+
+def lessampler(s, nles=None, filters=None, cells=None, protectshells=2,
+               outtype=lambda M: np.float64):
+    """lessampler(s; nles, filters, cells, protectshells, outtype)
+    (src/spectral/les.jl:239-300), one rank."""
+    from .les import LES_KERNELS, lescells
+
+    cells = lescells(nles, filters, cells)
+    for c in cells:
+        if c["M"] % 2:
+            raise ValueError(f"coarse grid M must be even (got {c['M']})")
+        if c["kernel"] not in LES_KERNELS:
+            raise ValueError(f"kernel must be one of {LES_KERNELS}")
+        if not c["dfac"] > 0:
+            raise ValueError("dfac must be positive")
+    Mmax = max(c["M"] for c in cells)
+    if Mmax // 2 > s.kcut:
+        raise ValueError(f"LES cube needs M/2 <= kcut (M = {Mmax}, kcut = {s.kcut})")
+    return dict(cells=cells, nles=Mmax, protectshells=int(protectshells), outtype=outtype, l=s.l)
+
+
+def sfs_sample(sam, uh, s):
+    """sfs_sample!(sam, uh, s): per bank cell dict(ubar, tau, redelta, spectrum)."""
+    from .les import sfs_from_cube
+
+    return sfs_from_cube(sam, les_cube(uh, s, sam["nles"]), s.visc)

@@ -301,6 +301,11 @@ int dnsb_spectral_shell_rescale(dnsb_spectral *sp, double *uh, const double *fac
 int dnsb_spectral_random_field(dnsb_spectral *sp, double *uh, double totalenergy, double kpeak,
                                unsigned long long seed, const double *profile, int nprofile);
 int dnsb_spectral_shell_clamp(dnsb_spectral *sp, double *uh, const double *eref, int nshells);
+/* The distributed half of sfs_sample! (src/spectral/les.jl:313-334): the
+ * LES cube |k_i| <= M/2 (M even, M/2 <= kcut) of u_hat (a truncation of
+ * the state) and of sigma_hat = F[v_i v_j] / n^3 (products on the n^3
+ * grid), into the HOST array out as in dnsb_les_cube.  Synchronises. */
+int dnsb_spectral_les_cube(dnsb_spectral *sp, const double *uh, int M, double *out);
 /* which = 0: spectral_energy, 1: spectral_dissipation, 2: spectral_maxdiv
  * (src/spectral/operators.jl:98-110), single rank.  Synchronises. */
 int dnsb_spectral_diagnostic(dnsb_spectral *sp, const double *uh, int which, double *out);

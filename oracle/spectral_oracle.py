@@ -180,3 +180,19 @@ class Spectral:
 
         forcing.eref = eref
         return forcing
+
+    def les_cube(self, uh, M):
+        """The LES cube of u_hat (truncation) and sigma_hat = F[v_i v_j]/n^3
+        (src/spectral/les.jl:313-334), coarse rfft layout (M, M, M//2+1)."""
+        h = M // 2 + 1
+        wrap = np.array([j if j < M // 2 else j - M for j in range(M)])
+        ci = wrap % self.m                       # compact index of ky / kz
+        out = np.zeros((9, M, M, h), dtype=np.complex128)
+        for c in range(3):
+            out[c] = uh[c][np.ix_(ci, ci, np.arange(h))]
+        v = self.to_phys(uh)
+        for f, (a, b) in enumerate(((0, 0), (1, 1), (2, 2), (0, 1), (1, 2), (2, 0))):
+            F = np.fft.rfftn(v[a] * v[b], axes=(0, 1, 2)) / self.n ** 3
+            fi = wrap % self.n
+            out[3 + f] = F[np.ix_(fi, fi, np.arange(h))]
+        return out

@@ -133,3 +133,32 @@ def test_random_field_and_forcing_match_oracle(SP):
     assert rel(uh.cpu().numpy(), uo) < 1e-11
     assert np.allclose(SP.shell_energies(uh, s, (1, 2)), f.eref, rtol=1e-13, atol=0)
     s.close()
+
+
+def test_spectral_sfs_sample_matches_oracle(SP):
+    """sfs_sample! on the spectral state: the GPU cube against the oracle's,
+    then the bank through the host half against the loop restatement."""
+    import les_oracle as LO
+    import spectral_oracle as SO
+
+    O = SO.Spectral(24, visc=5e-3)
+    s = SP.spectral_setup(n=24, visc=5e-3)
+    uo = O.randomfield(totalenergy=0.4, kpeak=3, seed=5)
+    uh = SP.spectral_randomfield(SP.specvelocity(s), s, totalenergy=0.4, kpeak=3, seed=5)
+    cube = SP.les_cube(uh, s, 12)
+    ref = O.les_cube(uo, 12)
+    for f in range(9):
+        assert rel(cube[f], ref[f]) < 1e-12, f
+    cells = [dict(M=12, kernel="gaussian", dfac=2.0), dict(M=8, kernel="helmholtz", dfac=1.5)]
+    sam = SP.lessampler(s, cells=cells)
+    got = SP.sfs_sample(sam, uh, s)
+    want = LO.sfs(sam["cells"], 12, 2, s.l, 5e-3, ref)
+    for g, r in zip(got, want):
+        for i, k in enumerate("xyz"):
+            assert rel(g["ubar"][k], r["ubar"][i]) < 1e-11
+        for i, name in enumerate(("xx", "yy", "zz", "xy", "yz", "zx")):
+            assert rel(g["tau"][name], r["tau"][i]) < 1e-11
+        assert math.isclose(g["redelta"], r["redelta"], rel_tol=1e-11)
+    with pytest.raises(ValueError):
+        SP.lessampler(s, nles=20, filters=[2.0])  # M/2 > kcut
+    s.close()
