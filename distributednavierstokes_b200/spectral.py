@@ -319,3 +319,48 @@ def sfs_sample(sam, uh, s):
     from .les import sfs_from_cube
 
     return sfs_from_cube(sam, les_cube(uh, s, sam["nles"]), s.visc)
+
+
+# ------------------------------------------------------------ statistics
+
+def spectral_stats(uh, s):
+    """spectral_stats(uh, s) (src/spectral/stats.jl:5-25): the K41
+    statistics of the state (single rank)."""
+    visc, n, l = s.visc, s.n, s.l
+    e = spectral_energy(uh, s)
+    diss = spectral_dissipation(uh, s)
+    uavg = math.sqrt(2 * e / 3)
+    l_kol = (visc ** 3 / diss) ** 0.25
+    l_tay = math.sqrt(15 * visc / diss) * uavg
+    l_int = uavg ** 3 / diss
+    return dict(e=e, uavg=uavg, diss=diss, l_int=l_int, l_tay=l_tay, l_kol=l_kol,
+                t_int=l_int / uavg, t_tay=l_tay / uavg, t_kol=math.sqrt(visc / diss),
+                Re_int=l_int * uavg / visc, Re_tay=l_tay * uavg / visc,
+                kmax_eta=(math.pi * n / l) * l_kol)
+
+
+def spectral_spectrum(uh, s):
+    """spectral_spectrum(uh, s) (src/spectral/stats.jl:27-36): shells 0..kcut."""
+    return dict(k=np.arange(s.kcut + 1), E=shell_energies(uh, s, range(s.kcut + 1)))
+
+
+def statswriter(file, nupdate=10):
+    """statswriter(; file, nupdate) (src/spectral/io.jl:231-262): appends a
+    CSV row t, step, the statistics, walltime every nupdate steps."""
+    import os
+    import time as _time
+
+    def proc(state, s):
+        if state.n % nupdate:
+            return None
+        st = spectral_stats(state.uh, s)
+        d = os.path.dirname(os.path.abspath(file))
+        os.makedirs(d, exist_ok=True)
+        fresh = not os.path.isfile(file) or os.path.getsize(file) == 0
+        with open(file, "a") as fh:
+            if fresh:
+                fh.write(",".join(["t", "step", *st.keys(), "walltime"]) + "\n")
+            fh.write(",".join(str(v) for v in (state.t, state.n, *st.values(), _time.time())) + "\n")
+        return None
+
+    return proc

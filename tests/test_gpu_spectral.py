@@ -162,3 +162,25 @@ def test_spectral_sfs_sample_matches_oracle(SP):
     with pytest.raises(ValueError):
         SP.lessampler(s, nles=20, filters=[2.0])  # M/2 > kcut
     s.close()
+
+
+def test_spectral_stats_and_spectrum(SP, tmp_path):
+    import spectral_oracle as SO
+
+    O = SO.Spectral(18, visc=5e-3)
+    s = SP.spectral_setup(n=18, visc=5e-3)
+    uh = SP.spectral_randomfield(SP.specvelocity(s), s, totalenergy=0.4, kpeak=2, seed=7)
+    uo = O.randomfield(totalenergy=0.4, kpeak=2, seed=7)
+    st = SP.spectral_stats(uh, s)
+    e, d = O.energy(uo), O.dissipation(uo)
+    assert math.isclose(st["e"], e, rel_tol=1e-12) and math.isclose(st["diss"], d, rel_tol=1e-12)
+    assert math.isclose(st["l_kol"], (5e-3 ** 3 / d) ** 0.25, rel_tol=1e-12)
+    assert math.isclose(st["kmax_eta"], math.pi * 18 / s.l * st["l_kol"], rel_tol=1e-14)
+    sp = SP.spectral_spectrum(uh, s)
+    assert np.allclose(sp["E"], O.shell_energies(uo, s.kcut + 1), rtol=1e-12, atol=1e-18)
+    f = str(tmp_path / "stats.csv")
+    SP.spectral_solve(uh=uh, setup=s, tlims=(0.0, 0.04), dt=0.01,
+                      processors={"stats": SP.statswriter(f, nupdate=2)})
+    rows = open(f).read().strip().splitlines()
+    assert rows[0].startswith("t,step,e,uavg,diss") and len(rows) == 4  # n = 0, 2, 4
+    s.close()
