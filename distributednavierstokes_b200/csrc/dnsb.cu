@@ -604,6 +604,8 @@ int launch_rfftx4(dnsb_ctx *c, int mode, const double *a, const double *b, const
       LAUNCH(c, DNSB_KIND_RFFTX, k_rfftx4<A, B, RFX_L, RIN_DIVERGENCE><<<grid, F4_THREADS, c->smem_rx4, c->stream>>>(g, c->S, a, b, cc, c->twM, c->twN)); \
     else if (mode == RIN_REAL)                                                                     \
       LAUNCH(c, DNSB_KIND_RFFTX, k_rfftx4<A, B, RFX_L, RIN_REAL><<<grid, F4_THREADS, c->smem_rx4, c->stream>>>(g, c->S, a, b, cc, c->twM, c->twN)); \
+    else if (mode == RIN_PRODUCT)                                                                  \
+      LAUNCH(c, DNSB_KIND_RFFTX, k_rfftx4<A, B, RFX_L, RIN_PRODUCT><<<grid, F4_THREADS, c->smem_rx4, c->stream>>>(g, c->S, a, b, cc, c->twM, c->twN)); \
     else                                                                                           \
       LAUNCH(c, DNSB_KIND_RFFTX, k_rfftx4<A, B, RFX_L, RIN_FIELD><<<grid, F4_THREADS, c->smem_rx4, c->stream>>>(g, c->S, a, b, cc, c->twM, c->twN)); \
     return 0;                                                                                      \
@@ -653,6 +655,7 @@ int allow_fft4(dnsb_ctx *c) {
   if ((rc = allow_smem(c, k_rfftx4<A, B, RFX_L, RIN_DIVERGENCE>, c->smem_rx4)) ||
       (rc = allow_smem(c, k_rfftx4<A, B, RFX_L, RIN_REAL>, c->smem_rx4)) ||
       (rc = allow_smem(c, k_rfftx4<A, B, RFX_L, RIN_FIELD>, c->smem_rx4)) ||
+      (rc = allow_smem(c, k_rfftx4<A, B, RFX_L, RIN_PRODUCT>, c->smem_rx4)) ||
       (rc = allow_smem(c, k_irfftx4<A, B, IRX_L, ROUT_INTERIOR>, c->smem_ix4)) ||
       (rc = allow_smem(c, k_irfftx4<A, B, IRX_L, ROUT_IMAGES>, c->smem_ix4)) ||
       (rc = allow_smem(c, k_irfftx4<A, B, IRX_L, ROUT_REAL>, c->smem_ix4)) ||
@@ -2020,6 +2023,25 @@ int sp_from_phys(dnsb_spectral *p, const double *r) {
   return 0;
 }
 
+// the full forward transform of the product va * vb into S: fused into the
+// x-transform's loads where the four-step kernel applies
+int sp_from_product(dnsb_spectral *p, const double *va, const double *vb) {
+  dnsb_ctx *c = p->c;
+  const Geo &g = c->g;
+  if (!c->x1) {
+    k_sp_product<<<RED_BLOCKS, 256, 0, c->stream>>>(sp_n3(p), va, vb, p->r);
+    SPKL(p);
+    return sp_from_phys(p, p->r);
+  }
+  SPRC(p, launch_rfftx(c, RIN_PRODUCT, va, vb, nullptr));
+  SPRC(p, launch_fftz(c, false));
+  dim3 grid(g.nkx * ((g.nz + c->Ly - 1) / c->Ly));
+  k_yfourier<YF_FORWARD><<<grid, SPEC_THREADS, c->smem_y, c->stream>>>(g, c->S, c->py, c->Ly, c->twy,
+                                                                       c->lam1, c->lam2, c->lam3);
+  SPKL(p);
+  return 0;
+}
+
 // spectral_rhs!: du = -i k_j F[v_i v_j] / n^3; leaves v = the physical velocity
 int sp_rhs(dnsb_spectral *p, const double2 *uh, double2 *du) {
   dnsb_ctx *c = p->c;
@@ -2029,9 +2051,7 @@ int sp_rhs(dnsb_spectral *p, const double2 *uh, double2 *du) {
     if ((rc = sp_to_phys(p, uh + comp * p->s.nc, p->v[comp]))) return rc;
   static const int pa[6] = {0, 1, 2, 0, 1, 2}, pb[6] = {0, 1, 2, 1, 2, 0};
   for (int f = 0; f < 6; f++) {
-    k_sp_product<<<RED_BLOCKS, 256, 0, c->stream>>>(n3, p->v[pa[f]], p->v[pb[f]], p->r);
-    SPKL(p);
-    if ((rc = sp_from_phys(p, p->r))) return rc;
+    if ((rc = sp_from_product(p, p->v[pa[f]], p->v[pb[f]]))) return rc;
     k_sp_div<<<RED_BLOCKS, 256, 0, c->stream>>>(p->s, c->S, du, pa[f], pb[f], 1.0 / (double)n3);
     SPKL(p);
   }
@@ -2344,9 +2364,7 @@ int dnsb_spectral_les_cube(dnsb_spectral *p, const double *uh, int M, double *ou
   }
   static const int pa[6] = {0, 1, 2, 0, 1, 2}, pb[6] = {0, 1, 2, 1, 2, 0};
   for (int f = 0; f < 6; f++) {
-    k_sp_product<<<RED_BLOCKS, 256, 0, c->stream>>>(n3, p->v[pa[f]], p->v[pb[f]], p->r);
-    SPKL(p);
-    if ((rc = sp_from_phys(p, p->r))) return rc;
+    if ((rc = sp_from_product(p, p->v[pa[f]], p->v[pb[f]]))) return rc;
     k_lescube<<<RED_BLOCKS, 256, 0, c->stream>>>(c->g, c->S, M, 1.0 / (double)n3, c->cube + (3 + f) * per);
     SPKL(p);
   }

@@ -19,7 +19,7 @@ namespace dnsb {
 
 constexpr int SPEC_THREADS = 256;
 
-enum RInMode { RIN_DIVERGENCE = 0, RIN_REAL = 1, RIN_FIELD = 2 };
+enum RInMode { RIN_DIVERGENCE = 0, RIN_REAL = 1, RIN_FIELD = 2, RIN_PRODUCT = 3 };
 enum ROutMode { ROUT_INTERIOR = 0, ROUT_IMAGES = 1, ROUT_REAL = 2 };
 
 // Real forward FFT along x of L lines (j fixed, kz = k0..k0+L-1) through
@@ -28,7 +28,8 @@ enum ROutMode { ROUT_INTERIOR = 0, ROUT_IMAGES = 1, ROUT_REAL = 2 };
 // O = (Z[k] - conj Z[M-k])/(2i), w = exp(-2 pi i/nx), k = 0..M.
 // RIN_DIVERGENCE: r is the divergence of (in0, in1, in2) (operators.jl:10-26).
 // RIN_REAL: r is the ghost-free array in0.  RIN_FIELD: the interior of the
-// ghosted field in0.
+// ghosted field in0.  RIN_PRODUCT (four-step kernel only): r = in0 * in1,
+// both ghost-free (the velocity products of the spectral solver).
 // Shared memory: 2*L*(M+1) complex (ping-pong lines) + M + (M+1) twiddles.
 template <int INMODE>
 __global__ void __launch_bounds__(SPEC_THREADS, 3) k_rfftx(Geo g, double2 *__restrict__ S,

@@ -73,9 +73,13 @@ __global__ void __launch_bounds__(F4_THREADS, 3) k_rfftx4(Geo g, double2 *__rest
         const int k = k0 + l;
         double2 z = make_double2(0.0, 0.0);
         if (k < g.nz) {
-          if (INMODE == RIN_REAL) {
-            const double *row = in0 + (long long)g.nx * (j + (long long)g.ny * k);
-            z = __ldg(reinterpret_cast<const double2 *>(row + 2 * m));
+          if (INMODE == RIN_REAL || INMODE == RIN_PRODUCT) {
+            const long long ro = (long long)g.nx * (j + (long long)g.ny * k);
+            z = __ldg(reinterpret_cast<const double2 *>(in0 + ro + 2 * m));
+            if (INMODE == RIN_PRODUCT) {
+              const double2 w = __ldg(reinterpret_cast<const double2 *>(in1 + ro + 2 * m));
+              z = make_double2(z.x * w.x, z.y * w.y);
+            }
           } else {
             const int c0 = gidx(g, 2 * m + 1, J, k + 1);
             if (INMODE == RIN_FIELD) {
