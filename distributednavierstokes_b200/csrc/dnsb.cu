@@ -117,6 +117,7 @@ struct dnsb_ctx {
   int *deverr = nullptr;               // device-side error word (bounded waits)
   int use_tma = 1;                     // persistent TMA-pipelined z-FFT
   int zyz_c = 0;                       // CTAs per cluster of k_zyz (0: three kernels)
+  int nkx_active = 0;                  // z-FFTs on kx < nkx_active only (0: all; spectral solver)
   int x1 = 0, x2 = 0, z1 = 0, z2 = 0;  // four-step splits of nx/2 and nz (0: generic kernels)
   int L4z = 8;                         // lines per CTA of the z-FFT
   size_t smem_rx4 = 0, smem_ix4 = 0, smem_z4 = 0;
@@ -635,7 +636,7 @@ int launch_irfftx4(dnsb_ctx *c, int mode, double *out) {
 
 int launch_fftz4(dnsb_ctx *c, bool inv) {
   const Geo &g = c->g;
-  const long long nlines = (long long)g.ny * g.nkx;
+  const long long nlines = (long long)g.ny * (c->nkx_active ? c->nkx_active : g.nkx);
   dim3 grid((unsigned)((nlines + c->L4z - 1) / c->L4z));
 #define ZF4(A, B)                                                                                  \
   if (c->z1 == A && c->z2 == B) {                                                                  \
@@ -691,7 +692,7 @@ int launch_rfftx(dnsb_ctx *c, int mode, const double *a, const double *b, const 
 int launch_fftz(dnsb_ctx *c, bool inv) {
   const Geo &g = c->g;
   if (c->z1 && !c->use_tma) return launch_fftz4(c, inv);
-  long long nlines = (long long)g.ny * g.nkx;
+  long long nlines = (long long)g.ny * (c->nkx_active && !c->use_tma ? c->nkx_active : g.nkx);
   if (c->use_tma) {
     const long long ngroups = (nlines + c->Lz - 1) / c->Lz;
     dim3 grid((unsigned)std::min<long long>(ngroups, 2LL * c->nsm));
@@ -2001,7 +2002,7 @@ int sp_to_phys(dnsb_spectral *p, const double2 *uhc, double *v) {
   SPK(p, cudaMemsetAsync(c->S, 0, sizeof(double2) * (size_t)g.nkx * g.ny * g.nz, c->stream));
   k_sp_scatter<<<RED_BLOCKS, 256, 0, c->stream>>>(p->s, uhc, c->S, n3);
   SPKL(p);
-  dim3 grid(g.nkx * ((g.nz + c->Ly - 1) / c->Ly));
+  dim3 grid(c->nkx_active * ((g.nz + c->Ly - 1) / c->Ly));
   k_yfourier<YF_INVERSE><<<grid, SPEC_THREADS, c->smem_y, c->stream>>>(g, c->S, c->py, c->Ly, c->twy,
                                                                        c->lam1, c->lam2, c->lam3);
   SPKL(p);
@@ -2016,7 +2017,7 @@ int sp_from_phys(dnsb_spectral *p, const double *r) {
   const Geo &g = c->g;
   SPRC(p, launch_rfftx(c, RIN_REAL, r, nullptr, nullptr));
   SPRC(p, launch_fftz(c, false));
-  dim3 grid(g.nkx * ((g.nz + c->Ly - 1) / c->Ly));
+  dim3 grid(c->nkx_active * ((g.nz + c->Ly - 1) / c->Ly));
   k_yfourier<YF_FORWARD><<<grid, SPEC_THREADS, c->smem_y, c->stream>>>(g, c->S, c->py, c->Ly, c->twy,
                                                                        c->lam1, c->lam2, c->lam3);
   SPKL(p);
@@ -2035,7 +2036,7 @@ int sp_from_product(dnsb_spectral *p, const double *va, const double *vb) {
   }
   SPRC(p, launch_rfftx(c, RIN_PRODUCT, va, vb, nullptr));
   SPRC(p, launch_fftz(c, false));
-  dim3 grid(g.nkx * ((g.nz + c->Ly - 1) / c->Ly));
+  dim3 grid(c->nkx_active * ((g.nz + c->Ly - 1) / c->Ly));
   k_yfourier<YF_FORWARD><<<grid, SPEC_THREADS, c->smem_y, c->stream>>>(g, c->S, c->py, c->Ly, c->twy,
                                                                        c->lam1, c->lam2, c->lam3);
   SPKL(p);
@@ -2114,6 +2115,10 @@ int dnsb_spectral_create(int n, int kcut, double l, double visc, int device, voi
   if (rc) return rc;  // message in dnsb_last_error(NULL)
   dnsb_spectral *p = new dnsb_spectral();
   p->c = c;
+  // only the planes kx <= kcut carry retained modes: the z- and y-transforms
+  // between the x-transform and the state skip the others (zero after the
+  // scatter, never gathered)
+  c->nkx_active = kcut + 1;
   p->visc = visc;
   p->l = l;
   p->s.n = n;
