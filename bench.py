@@ -487,12 +487,15 @@ def e2e_leg(lib, s, host_ic, wl, args, world, dev, cells, G):
     torch.cuda.synchronize(dev)
     if world > 1:
         torch.distributed.barrier()
+    clocks = ClockSampler(dev.index or 0)
+    clocks.start()
     t0 = time.perf_counter()
     rc = lib.dnsb_solve_host(s.ctx, *(ctypes.c_void_p(h.data_ptr()) for h in
                                       (hu["x"], hu["y"], hu["z"], hp)),
                              0.0, 1e9, 0.0, wl["cfl"], args.steps, ctypes.byref(t_out),
                              ctypes.byref(n_out))
     e2e_s = time.perf_counter() - t0
+    clk = clocks.stop()
     _lib.check(rc, s._ctx)
     if world > 1:
         t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
@@ -502,7 +505,7 @@ def e2e_leg(lib, s, host_ic, wl, args, world, dev, cells, G):
     h2d = 3 * G * 8 / n_out.value
     d2h = (4 * G * 8 + 24 * n_out.value) / n_out.value
     return {"value": e2e, "unit": "cell-steps/s", "h2d_bytes_per_step": h2d,
-            "d2h_bytes_per_step": d2h,
+            "d2h_bytes_per_step": d2h, "clocks": clk,
             "note": "dnsb_solve_host: pinned host u in, initial projection, "
                     f"{n_out.value} CFL steps, u and p out"}
 

@@ -112,6 +112,7 @@ struct dnsb_ctx {
   int nshell_max = 0;                  // floor(|k|max) + 1
   double *shellpart = nullptr;         // per-block partial shell sums (fixed-order path)
   std::vector<double> eref_host;       // shell-clamp reference energies on the device
+  double *hostsolve = nullptr;         // device fields of dnsb_solve_host (first call on)
   double2 *cube = nullptr;             // LES cubes of the filtered-field sampler
   size_t cube_cap = 0;
   int *deverr = nullptr;               // device-side error word (bounded waits)
@@ -1710,9 +1711,14 @@ int dnsb_solve_host(dnsb_ctx *c, double *ux, double *uy, double *uz, double *p, 
   if (ensure_device(c)) return DNSB_ECUDA;
   const Geo &g = c->g;
   const size_t G = (size_t)g.NX * g.NY * g.NZ;
-  double *buf = nullptr;
   const int nf = c->implicit ? 8 : 7;
-  CK(c, cudaMallocAsync((void **)&buf, nf * G * sizeof(double), c->stream));
+  // the device fields persist in the context after the first call, so that
+  // repeated calls neither map memory nor synchronise on an allocation
+  if (!c->hostsolve) {
+    int arc = dalloc(c, &c->hostsolve, nf * G);
+    if (arc) return arc;
+  }
+  double *buf = c->hostsolve;
   double *f[8];
   for (int i = 0; i < nf; i++) f[i] = buf + i * G;
   int rc = 0;
@@ -1732,7 +1738,6 @@ int dnsb_solve_host(dnsb_ctx *c, double *ux, double *uy, double *uz, double *p, 
     if (!rc && p && cudaMemcpyAsync(p, f[3], G * sizeof(double), cudaMemcpyDeviceToHost, c->stream) != cudaSuccess)
       rc = fail(c, DNSB_ECUDA, "device to host copy failed");
   } while (0);
-  cudaFreeAsync(buf, c->stream);
   cudaError_t e = cudaStreamSynchronize(c->stream);
   if (!rc && e != cudaSuccess) rc = fail(c, DNSB_ECUDA, "%s", cudaGetErrorString(e));
   return rc;

@@ -121,7 +121,9 @@ int dnsb_solve(dnsb_ctx *ctx, double *ux, double *uy, double *uz, double *p, dou
 
 /* The same with HOST arrays for u (in/out) and p (out): the velocity is
  * copied to the device, solved, and u, p copied back (for callers without
- * device arrays; pinned host memory makes the copies faster). */
+ * device arrays; pinned host memory makes the copies faster).  The device
+ * fields (7-8 ghosted fields) are allocated on the first call and kept by
+ * the context until dnsb_destroy. */
 int dnsb_solve_host(dnsb_ctx *ctx, double *ux, double *uy, double *uz, double *p, double t0,
                     double t1, double dt, double cfl, long max_steps, double *t_out,
                     long *n_out);
