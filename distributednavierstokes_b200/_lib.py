@@ -96,6 +96,7 @@ SIGNATURES = {
                                            ctypes.POINTER(c_double), c_int]),
     "dnsb_spectral_shell_clamp": (c_int, [P, P, ctypes.POINTER(c_double), c_int]),
     "dnsb_spectral_les_cube": (c_int, [P, P, c_int, ctypes.POINTER(c_double)]),
+    "dnsb_spectral_phaserandomize": (c_int, [P, P, ctypes.c_ulonglong]),
 }
 
 KINDS = ["momentum", "cn_solve", "div_rfft_x", "fft_z", "y_solve", "ifft_z", "irfft_x",

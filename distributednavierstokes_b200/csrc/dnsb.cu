@@ -2383,6 +2383,14 @@ int dnsb_spectral_les_cube(dnsb_spectral *p, const double *uh, int M, double *ou
   return 0;
 }
 
+int dnsb_spectral_phaserandomize(dnsb_spectral *p, double *uh, unsigned long long seed) {
+  int rc = sp_check(p, uh);
+  if (rc) return rc;
+  k_sp_phaserand<<<RED_BLOCKS, 256, 0, p->c->stream>>>(p->s, reinterpret_cast<double2 *>(uh), seed);
+  SPKL(p);
+  return 0;
+}
+
 int dnsb_spectral_set_stream(dnsb_spectral *p, void *stream) {
   if (!p) return DNSB_EINVAL;
   return dnsb_set_stream(p->c, stream);

@@ -323,6 +323,30 @@ __global__ void k_sp_clamp_factors(const double *E, const double *eref, double *
     f[i] = (eref[i] >= 0 && E[i] > 0) ? sqrt(eref[i] / E[i]) : 1.0;
 }
 
+// phaserand_kernel! (src/spectral/ic.jl:108-128): every retained mode but
+// the mean times a unit-modulus phase from splitmix64 of the mode's key;
+// in the kx = 0 plane (0, k2, k3) and (0, -k2, -k3) share the canonical
+// member's phase and the other member takes its conjugate
+__global__ void k_sp_phaserand(SpGeo s, double2 *__restrict__ uh, unsigned long long seed) {
+  SP_LOOP(q, s.nc) {
+    int k1, k2, k3;
+    sp_modes(s, q, k1, k2, k3);
+    if (k1 == 0 && k2 == 0 && k3 == 0) continue;
+    const bool canon = k1 > 0 || k2 > 0 || (k2 == 0 && k3 > 0);
+    const long long c2 = canon ? k2 : -k2, c3 = canon ? k3 : -k3;
+    const unsigned long long w = 2ULL * s.kcut + 2ULL;
+    const unsigned long long key =
+        ((unsigned long long)k1 * w + (unsigned long long)(c2 + s.kcut)) * w +
+        (unsigned long long)(c3 + s.kcut);
+    const double u = ((double)(splitmix64(seed + key) >> 11) + 0.5) * 0x1p-53;
+    double sn, cs;
+    sincospi(2.0 * u, &sn, &cs);
+    const double2 ph = make_double2(cs, canon ? sn : -sn);
+#pragma unroll
+    for (int c = 0; c < 3; c++) uh[c * s.nc + q] = cmul(uh[c * s.nc + q], ph);
+  }
+}
+
 #undef SP_LOOP
 
 }  // namespace dnsb

@@ -364,3 +364,9 @@ def statswriter(file, nupdate=10):
         return None
 
     return proc
+
+
+def spectral_phaserandomize(uh, s, seed=0):
+    """spectral_phaserandomize!(uh, s; seed) (src/spectral/ic.jl:130-143)."""
+    s._call(_lib.load().dnsb_spectral_phaserandomize(s.sp, _ptr(uh), int(seed)))
+    return uh

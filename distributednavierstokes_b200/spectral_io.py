@@ -145,10 +145,11 @@ def checkpointer(prefix, interval=900.0, stopfile=None, keep=2, meta=None):
     return proc
 
 
-def snapshotsaver(prefix, times, meta=None, tstart=-math.inf):
-    """snapshotsaver(prefix; times, meta, tstart) (src/spectral/io.jl:186-229)
-    without the K41 statistics: saves <prefix>_0001, ... the first time t
-    reaches each entry of `times` (pass them as tstops); entries before
+def snapshotsaver(prefix, times, meta=None, stats=True, tstart=-math.inf):
+    """snapshotsaver(prefix; times, meta, stats, tstart) (src/spectral/
+    io.jl:186-229): saves <prefix>_0001, ... the first time t reaches each
+    entry of `times` (pass them as tstops); with stats the sidecar's meta
+    also carries eta, t_int, e, diss of spectral_stats; entries before
     tstart are skipped on restart."""
     times = sorted(float(t) for t in times)
     i0 = next((i for i, t in enumerate(times) if t >= tstart - 1e-10 * (abs(t) + 1)), len(times))
@@ -156,8 +157,14 @@ def snapshotsaver(prefix, times, meta=None, tstart=-math.inf):
 
     def proc(state, s):
         while inext[0] < len(times) and state.t >= times[inext[0]] - 1e-10 * (abs(times[inext[0]]) + 1):
+            m = dict(meta or {})
+            if stats:
+                from .spectral import spectral_stats
+
+                st = spectral_stats(state.uh, s)
+                m.update(eta=st["l_kol"], t_int=st["t_int"], e=st["e"], diss=st["diss"])
             spectral_save("%s_%04d" % (prefix, inext[0] + 1), state.uh, s, time=state.t,
-                          step=state.n, meta=meta)
+                          step=state.n, meta=m)
             inext[0] += 1
         return None
 
@@ -184,3 +191,137 @@ def spectral_from_rfft(uh, F, s):
     else:
         uh[...] = A
     return uh
+
+
+# ---------------------------------------------------- the SFS bank writers
+# sfscollector / sfswriter / sfs_offline (src/spectral/les.jl:384-540) with
+# the reference's directory layout and array names; the archives are numpy
+# .npz files (there is no JLD2/HDF5 writer in this environment), written
+# atomically like jldsave_atomic.
+
+def etacells(deta, eta, l, Ms, kernels=("gaussian",), window=(2.0, 5.0)):
+    """etacells(; deta, eta, l, Ms, kernels, window) (src/spectral/les.jl:207-224):
+    for each width (in units of the Kolmogorov length eta) and kernel, every
+    coarse grid M whose Delta/h = deta eta M / l lies inside the window."""
+    out = []
+    for de in deta:
+        for kernel in kernels:
+            for M in sorted(Ms):
+                r = de * eta * M / l
+                if window[0] - 1e-9 <= r <= window[1] + 1e-9:
+                    out.append(dict(M=int(M), kernel=str(kernel), dfac=float(f"{r:.4g}"),
+                                    deta=float(de)))
+    return out
+
+
+def celldir(d, cell, legacy):
+    """celldir (src/spectral/les.jl:397-407)."""
+    if legacy:
+        return os.path.join(d, f"delta={cell['dfac']}")
+    return os.path.join(d, f"filter={cell['kernel']}", f"M={cell['M']}", f"delta={cell['dfac']}")
+
+
+def _save_npz_atomic(path, **arrays):
+    tmp = path + ".tmp.npz"
+    try:
+        np.savez(tmp, **arrays)
+        os.replace(tmp, path)
+    except BaseException:
+        if os.path.exists(tmp):
+            os.remove(tmp)
+        raise
+
+
+def sfscollector(sam, s, d):
+    """sfscollector (src/spectral/les.jl:409-475): record(t, uh) samples the
+    bank; finish() writes dns_meta.npz and, per cell, fields.npz and
+    les_meta.npz."""
+    from . import spectral as S
+
+    cells = sam["cells"]
+    tstart = _time.time()
+    st = dict(times=[], spectra_dns=[], statistics=[], inputs=[[] for _ in cells],
+              outputs=[[] for _ in cells], redelta=[[] for _ in cells],
+              spectra_les=[[] for _ in cells])
+
+    def record(t, uh):
+        stats = S.spectral_stats(uh, s)
+        sp = S.spectral_spectrum(uh, s)
+        samples = S.sfs_sample(sam, uh, s)
+        st["times"].append(float(t))
+        st["spectra_dns"].append(np.asarray(sp["E"][1:], dtype=np.float64))
+        st["statistics"].append(stats)
+        for k, smp in enumerate(samples):
+            st["inputs"][k].append(np.stack([smp["ubar"][c] for c in "xyz"]))
+            st["outputs"][k].append(np.stack([smp["tau"][c]
+                                              for c in ("xx", "yy", "zz", "xy", "yz", "zx")]))
+            st["redelta"][k].append(smp["redelta"])
+            st["spectra_les"][k].append(smp["spectrum"])
+
+    def finish():
+        if not st["times"]:
+            return
+        os.makedirs(d, exist_ok=True)
+        keys = list(st["statistics"][0].keys())
+        _save_npz_atomic(os.path.join(d, "dns_meta.npz"), times=np.array(st["times"]),
+                         spectra_dns=np.array(st["spectra_dns"]),
+                         statistics_dns=np.array([[x[k] for k in keys] for x in st["statistics"]]),
+                         statistics_names=np.array(keys),
+                         t_int=st["statistics"][0]["t_int"], walltime=_time.time() - tstart)
+        legacy = all(c["kernel"] == "gaussian" and c["M"] == sam["nles"] and c.get("deta") is None
+                     for c in cells)
+        for k, cell in enumerate(cells):
+            dd = celldir(d, cell, legacy)
+            os.makedirs(dd, exist_ok=True)
+            _save_npz_atomic(os.path.join(dd, "fields.npz"),
+                             inputs=np.array(st["inputs"][k]), outputs=np.array(st["outputs"][k]),
+                             redelta=np.array(st["redelta"][k]),
+                             **{"Δ": cell["dfac"] * s.l / cell["M"], "Δ_factor": cell["dfac"]},
+                             visc=s.visc, kernel=cell["kernel"], M=cell["M"],
+                             delta_eta=np.nan if cell.get("deta") is None else cell["deta"])
+            _save_npz_atomic(os.path.join(dd, "les_meta.npz"),
+                             spectra_les=np.array(st["spectra_les"][k]),
+                             redelta_mean=float(np.mean(st["redelta"][k])))
+
+    return record, finish
+
+
+def sfswriter(s, d, times, nles=None, filters=None, cells=None, protectshells=2,
+              outtype=lambda M: np.float64):
+    """sfswriter(s; dir, times, ...) (src/spectral/les.jl:477-519): a
+    spectral_solve processor sampling the bank at `times` (pass them as
+    tstops) and writing it after the last one."""
+    from . import spectral as S
+
+    sam = S.lessampler(s, nles, filters, cells, protectshells, outtype)
+    record, finish = sfscollector(sam, s, d)
+    times = sorted(float(t) for t in times)
+    inext = [0]
+
+    def proc(state, _s):
+        while inext[0] < len(times) and state.t >= times[inext[0]] - 1e-10 * (abs(times[inext[0]]) + 1):
+            record(state.t, state.uh)
+            inext[0] += 1
+            if inext[0] == len(times):
+                finish()
+        return None
+
+    return proc
+
+
+def sfs_offline(prefixes, s, d, nles=None, filters=None, cells=None, protectshells=2,
+                outtype=lambda M: np.float64, phaseseed=None):
+    """sfs_offline(prefixes, s; dir, ..., phaseseed) (src/spectral/les.jl:521-540):
+    the bank over stored snapshots, in order; phaseseed applies the phase
+    randomisation (the kinematic null) to each snapshot first."""
+    from . import spectral as S
+
+    sam = S.lessampler(s, nles, filters, cells, protectshells, outtype)
+    record, finish = sfscollector(sam, s, d)
+    uh = S.specvelocity(s)
+    for prefix in prefixes:
+        md = spectral_load(uh, prefix, s)
+        if phaseseed is not None:
+            S.spectral_phaserandomize(uh, s, seed=phaseseed)
+        record(md["time"], uh)
+    finish()

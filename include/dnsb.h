@@ -308,6 +308,10 @@ int dnsb_spectral_shell_clamp(dnsb_spectral *sp, double *uh, const double *eref,
  * the state) and of sigma_hat = F[v_i v_j] / n^3 (products on the n^3
  * grid), into the HOST array out as in dnsb_les_cube.  Synchronises. */
 int dnsb_spectral_les_cube(dnsb_spectral *sp, const double *uh, int M, double *out);
+/* spectral_phaserandomize! (src/spectral/ic.jl:98-143): every retained
+ * mode but the mean times a counter-based unit-modulus phase (Hermitian-safe
+ * in the kx = 0 plane); |u_hat| and k . u_hat = 0 are preserved. */
+int dnsb_spectral_phaserandomize(dnsb_spectral *sp, double *uh, unsigned long long seed);
 /* which = 0: spectral_energy, 1: spectral_dissipation, 2: spectral_maxdiv
  * (src/spectral/operators.jl:98-110), single rank.  Synchronises. */
 int dnsb_spectral_diagnostic(dnsb_spectral *sp, const double *uh, int which, double *out);

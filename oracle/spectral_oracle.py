@@ -196,3 +196,24 @@ class Spectral:
             fi = wrap % self.n
             out[3 + f] = F[np.ix_(fi, fi, np.arange(h))]
         return out
+
+    def phaserandomize(self, uh, seed=0):
+        """phaserand_kernel! (src/spectral/ic.jl:108-128)."""
+        out = uh.copy()
+        w = 2 * self.kcut + 2
+        cf = [j if j <= self.kcut else j - self.m for j in range(self.m)]
+        for k in range(self.m):
+            for j in range(self.m):
+                for i in range(self.kcut + 1):
+                    k1, k2, k3 = i, cf[j], cf[k]
+                    if (k1, k2, k3) == (0, 0, 0):
+                        continue
+                    canon = k1 > 0 or k2 > 0 or (k2 == 0 and k3 > 0)
+                    c2, c3 = (k2, k3) if canon else (-k2, -k3)
+                    key = (k1 * w + (c2 + self.kcut)) * w + (c3 + self.kcut)
+                    r = int(_splitmix64(np.array([seed + key], dtype=np.uint64))[0])
+                    u = ((r >> 11) + 0.5) * 2.0 ** -53
+                    ph = complex(math.cos(2 * math.pi * u),
+                                 (1 if canon else -1) * math.sin(2 * math.pi * u))
+                    out[:, k, j, i] *= ph
+        return out

@@ -184,3 +184,43 @@ def test_spectral_stats_and_spectrum(SP, tmp_path):
     rows = open(f).read().strip().splitlines()
     assert rows[0].startswith("t,step,e,uavg,diss") and len(rows) == 4  # n = 0, 2, 4
     s.close()
+
+
+def test_phaserandomize_and_offline_bank(SP, tmp_path):
+    """spectral_phaserandomize! against the oracle (|u_hat| and the
+    divergence kept, the result still a real field), and sfs_offline over
+    saved snapshots = sfs_sample of the phase-randomised states."""
+    import os
+
+    import spectral_oracle as SO
+    from distributednavierstokes_b200 import spectral_io as SIO
+
+    O = SO.Spectral(12, visc=5e-3)
+    s = SP.spectral_setup(n=12, visc=5e-3)
+    uo = O.randomfield(totalenergy=0.4, kpeak=2, seed=3)
+    uh = dev(uo)
+    SP.spectral_phaserandomize(uh, s, seed=9)
+    ref = O.phaserandomize(uo, seed=9)
+    got = uh.cpu().numpy()
+    assert rel(got, ref) < 1e-14
+    assert np.max(np.abs(np.abs(got) - np.abs(uo))) < 1e-15
+    assert SP.spectral_maxdiv(uh, s) < 1e-13
+    assert rel(O.from_phys(O.to_phys(got)), got) < 1e-13  # Hermitian-consistent
+    pre = [os.path.join(tmp_path, f"raw_{i}") for i in (1, 2)]
+    u1 = dev(uo)
+    SIO.spectral_save(pre[0], u1, s, time=0.5, step=5)
+    SP.spectral_step(u1, s, 0.01)
+    SIO.spectral_save(pre[1], u1, s, time=0.51, step=6)
+    cells = [dict(M=8, kernel="gaussian", dfac=2.0)]
+    SIO.sfs_offline(pre, s, str(tmp_path / "bank"), cells=cells, phaseseed=4)
+    f = np.load(tmp_path / "bank" / "delta=2.0" / "fields.npz")
+    assert f["inputs"].shape == (2, 3, 8, 8, 5) and f["outputs"].shape == (2, 6, 8, 8, 5)
+    m = np.load(tmp_path / "bank" / "dns_meta.npz")
+    assert list(m["times"]) == [0.5, 0.51] and m["spectra_dns"].shape == (2, s.kcut)
+    u2 = SP.specvelocity(s)
+    SIO.spectral_load(u2, pre[1], s)
+    SP.spectral_phaserandomize(u2, s, seed=4)
+    direct = SP.sfs_sample(SP.lessampler(s, cells=cells), u2, s)[0]
+    assert np.array_equal(f["inputs"][1][0], direct["ubar"]["x"])
+    assert np.array_equal(f["outputs"][1][5], direct["tau"]["zx"])
+    s.close()

@@ -65,7 +65,8 @@ def test_checkpoints_and_snapshots(tmp_path):
     assert sio.spectral_latest(prefix) == lst[-1]
     open(stop, "w").close()
     assert proc(State(uh, 3.0, 30), s) == "stop"
-    snap = sio.snapshotsaver(os.path.join(tmp_path, "snap"), times=[0.5, 0.2, 1.0], tstart=0.3)
+    snap = sio.snapshotsaver(os.path.join(tmp_path, "snap"), times=[0.5, 0.2, 1.0], stats=False,
+                             tstart=0.3)
     for n, t in ((1, 0.25), (2, 0.5), (3, 0.75), (4, 1.0)):
         snap(State(uh, t, n), s)
     names = sorted(f for f in os.listdir(tmp_path) if f.startswith("snap"))
@@ -83,3 +84,13 @@ def test_from_rfft_matches_truncation():
     assert np.array_equal(uh[2], F[2][np.ix_(cf % 16, cf % 16, np.arange(s.kcut + 1))])
     with pytest.raises(ValueError):
         sio.spectral_from_rfft(O.zeros(), [f[:8, :8, :5] for f in F], Setup(12))
+
+
+def test_etacells_and_celldir():
+    cells = sio.etacells(deta=[2.0, 4.0], eta=0.05, l=2 * math.pi, Ms=[64, 256, 128])
+    # delta/h = deta * eta * M / l inside [2, 5]
+    assert [(c["M"], c["deta"]) for c in cells] == [(128, 2.0), (256, 2.0), (64, 4.0), (128, 4.0)]
+    assert cells[0]["dfac"] == float(f"{2.0 * 0.05 * 128 / (2 * math.pi):.4g}")
+    c = dict(M=64, kernel="gaussian", dfac=2.0)
+    assert sio.celldir("out", c, True) == os.path.join("out", "delta=2.0")
+    assert sio.celldir("out", c, False) == os.path.join("out", "filter=gaussian", "M=64", "delta=2.0")
