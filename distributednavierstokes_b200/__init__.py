@@ -15,4 +15,6 @@ from .les import (  # noqa: F401
     les_cube, lescells, lessampler, load_snapshot, save_snapshot, sfs_from_cube, sfs_sample,
 )
 
+from . import spectral, spectral_io  # noqa: F401,E402  (the pseudo-spectral solver)
+
 __version__ = "0.1.0"
