@@ -50,6 +50,11 @@ WORKLOADS = {
     "ensemble64_periodic": dict(
         members=64, sizes=(32, 48, 64, 96, 128), visc=(1e-3, 1e-2), cfl=0.5, energy=0.5,
         kpeak=4.0, forced_shells=(1, 2), ydiffusion="explicit", bytes_per_cell_step=792.0),
+    # the pseudo-spectral solver on a 256^3 periodic cube (nu = 5e-4, kcut 85):
+    # random-phase E(k) ~ k^4 exp(-2 (k/4)^2) initial field, shell-clamp
+    # forcing of shells 1-2 after every step, CFL-adaptive Wray steps
+    "spectral256_hit": dict(
+        spectral=True, n=256, visc=5e-4, cfl=0.85, energy=0.5, kpeak=4.0, forced_shells=(1, 2)),
 }
 COMMON = dict(lims=((0.0, 4 * math.pi), (-1.0, 1.0), (0.0, 4 * math.pi / 3)),
               bc=("periodic", "wall", "periodic"), bodyforce=(1.0, 0.0, 0.0))
@@ -311,6 +316,70 @@ def ensemble_arm(args, wl, world, rank, local):
         print(json.dumps(line), flush=True)
 
 
+def spectral_arm(args, wl, world, rank, local):
+    """The pseudo-spectral solver: K CFL-adaptive forced Wray steps of the
+    n^3 cube, device-timed; the numpy oracle times one step on the host."""
+    import torch
+
+    from distributednavierstokes_b200 import spectral as S
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    s = S.spectral_setup(n=wl["n"], visc=wl["visc"], device=dev)
+    uh = S.spectral_randomfield(S.specvelocity(s), s, totalenergy=wl["energy"], kpeak=wl["kpeak"],
+                                seed=0)
+    f = S.shellforcing(uh, s, shells=wl["forced_shells"])
+    kmax = 2 * math.pi * s.kcut / s.l
+    vmax = [S.vsummax(uh, s)]
+
+    def one_step():
+        dt = wl["cfl"] * math.sqrt(3) / (kmax * (vmax[0] + 1e-300))
+        vmax[0] = S.spectral_step(uh, s, dt)
+        f(uh, s)
+
+    for _ in range(args.warmup):
+        one_step()
+    torch.cuda.synchronize(dev)
+    stream = torch.cuda.current_stream(dev)
+    clocks = ClockSampler(local)
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        one_step()
+    ev1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms = ev0.elapsed_time(ev1)
+    clk = clocks.stop()
+    assert S.spectral_maxdiv(uh, s) < 1e-9, "spectral state lost incompressibility"
+    n3 = wl["n"] ** 3
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import spectral_oracle as SO
+
+        O = SO.Spectral(wl["n"], visc=wl["visc"])
+        u0 = uh.cpu().numpy()
+        t0 = time.perf_counter()
+        O.step(u0, 1e-3)
+        secs = time.perf_counter() - t0
+        cpu = {"value": n3 / secs, "unit": "grid-point steps/s", "cores": 1, "kind": "port",
+               "sample": "1 Wray step of the full grid by the numpy oracle (numpy's FFTs, "
+                         "one thread; the Julia reference is not available)"}
+    if rank == 0:
+        print(json.dumps({
+            "metric": "spectral grid-point steps/s (FP64)", "value": world * n3 * args.steps / (ms / 1e3),
+            "unit": "grid-point steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: random-phase E(k) ~ k^4 exp(-2 (k/4)^2) initial field (seed 0), "
+                    "shell-clamp forcing of shells 1-2",
+            "config": {"workload": args.workload, "n": wl["n"], "kcut": s.kcut, "visc": wl["visc"],
+                       "cfl": wl["cfl"], "parallelism": "1 GPU" if world == 1 else f"replicas x{world}"},
+            "clocks": clk, "cpu_baseline": cpu}), flush=True)
+    s.close()
+
+
 def b200_arm(args, wl, world, rank, local):
     import ctypes
 
@@ -524,7 +593,16 @@ def main():
     args.warmup = max(args.warmup, 3) if args.impl == "b200" else args.warmup
     wl = WORKLOADS[args.workload]
     world, rank, local = dist_init()
-    if "members" in wl:
+    if wl.get("spectral"):
+        if args.impl == "reference":
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "unavailable":
+                                  "the spectral workload has no CPU reference arm (Julia is absent; "
+                                  "the b200 line carries the numpy oracle's one-step time)"}),
+                      flush=True)
+        else:
+            spectral_arm(args, wl, world, rank, local)
+    elif "members" in wl:
         if args.impl == "reference":
             if rank == 0:
                 print(json.dumps({"impl": "reference", "unavailable":
