@@ -135,3 +135,21 @@ def test_replica_timing_max_over_ranks_gloo():
         assert p.exitcode == 0
     assert [r[1] for r in res] == [11.0, 11.0]
     assert res[0][2] == res[1][2] == 2 * 1000 * 5 / 0.011
+
+
+def test_ensemble_partition_balanced_and_deterministic():
+    """Ensemble members are partitioned across ranks with no collective:
+    every rank derives the same owner list, each member has one owner, and
+    the largest-first assignment keeps the loads within one member."""
+    import numpy as np
+
+    import bench
+
+    rng = np.random.default_rng(12345)
+    cells = [int(n) ** 3 for n in rng.choice((32, 48, 64, 96, 128), size=64)]
+    for world in (1, 2, 4, 8):
+        owner = bench.partition_members(cells, world)
+        assert owner == bench.partition_members(cells, world)
+        assert sorted(set(owner)) == list(range(world))
+        loads = [sum(c for c, o in zip(cells, owner) if o == r) for r in range(world)]
+        assert max(loads) - min(loads) <= max(cells)
