@@ -101,6 +101,7 @@ struct dnsb_ctx {
   dim3 cgrid, cblock;  // launch shape of the per-cell step kernels
   // scratch
   double2 *S = nullptr;
+  double2 *Sx[2] = {nullptr, nullptr};  // spectra of u.y, u.z during a shell clamp
   double *work = nullptr;
   double *ycin = nullptr;  // c' entering each y-chunk, per (kx, kz) line
   double *r = nullptr;
@@ -1026,6 +1027,55 @@ int shell_scale_dev(dnsb_ctx *c, double *const u[3], const double *f, int nb) {
   return 0;
 }
 
+// The clamp with the three spectra kept: each component is transformed
+// once, its shell energies summed (fixed order), the factors formed, and
+// the same spectra scaled and transformed back -- 6 transforms instead of
+// the 9 of energies followed by rescale.  c->S is pointed at each
+// component's buffer in turn and restored on every return.
+struct SpecSwap {
+  dnsb_ctx *c;
+  double2 *s0;
+  ~SpecSwap() { c->S = s0; }
+};
+
+__global__ void k_clamp_factors(const double *E, const double *eref, double *f, int nb);
+
+int shell_clamp_dev(dnsb_ctx *c, double *const u[3], double *E, const double *er, double *f,
+                    int nb) {
+  const Geo &g = c->g;
+  SpecSwap guard{c, c->S};
+  double2 *Ss[3] = {c->S, c->Sx[0], c->Sx[1]};
+  CK(c, cudaMemsetAsync(E, 0, nb * sizeof(double), c->stream));
+  int rc;
+  for (int comp = 0; comp < 3; comp++) {
+    c->S = Ss[comp];
+    if ((rc = spectrum_of(c, u[comp]))) return rc;
+    if (nb <= SHELL_DET) {
+      k_binshells_det<<<RED_BLOCKS, 256, 0, c->stream>>>(g, c->S, c->shellpart);
+      CKL(c);
+      k_sum_shells<<<1, 32, 0, c->stream>>>(c->shellpart, RED_BLOCKS, nb, E);
+    } else {
+      k_binshells_byshell<<<nb, 256, 0, c->stream>>>(g, c->S, E);
+    }
+    CKL(c);
+  }
+  k_clamp_factors<<<1, 256, 0, c->stream>>>(E, er, f, nb);
+  CKL(c);
+  for (int comp = 0; comp < 3; comp++) {
+    c->S = Ss[comp];
+    k_scaleshells<<<RED_BLOCKS, 256, 0, c->stream>>>(g, c->S, f, nb);
+    CKL(c);
+    dim3 grid(g.nkx * ((g.nz + c->Ly - 1) / c->Ly));
+    k_yfourier<YF_INVERSE><<<grid, SPEC_THREADS, c->smem_y, c->stream>>>(g, c->S, c->py, c->Ly, c->twy,
+                                                                         c->lam1, c->lam2, c->lam3);
+    CKL(c);
+    if ((rc = launch_fftz(c, true))) return rc;
+    if ((rc = launch_irfftx(c, ROUT_IMAGES, u[comp]))) return rc;
+  }
+  c->umax_for[0] = c->umax_for[1] = c->umax_for[2] = nullptr;
+  return 0;
+}
+
 // shellforcing's closure (src/spectral/forcing.jl:50-55) on the device:
 // f[s] = sqrt(eref[s] / E[s]) for forced shells (eref[s] >= 0) with E > 0, else 1
 __global__ void k_clamp_factors(const double *E, const double *eref, double *f, int nb) {
@@ -1036,6 +1086,11 @@ __global__ void k_clamp_factors(const double *E, const double *eref, double *f, 
 // the shell-clamp reference table on the device (synchronous; skipped when
 // it is already there, so that a captured clamp never synchronises)
 int upload_eref(dnsb_ctx *c, const double *eref, int nb) {
+  if (!c->Sx[0]) {  // the clamp keeps all three spectra (first clamp only)
+    const size_t nspec = (size_t)c->g.nkx * c->g.ny * c->g.nz;
+    int rc;
+    if ((rc = dalloc(c, &c->Sx[0], nspec)) || (rc = dalloc(c, &c->Sx[1], nspec))) return rc;
+  }
   if (c->eref_host.size() == (size_t)nb && std::equal(eref, eref + nb, c->eref_host.begin())) return 0;
   double *er = c->shellbuf + 2 * c->nshell_max;
   CK(c, cudaMemcpyAsync(er, eref, nb * sizeof(double), cudaMemcpyHostToDevice, c->stream));
@@ -1593,12 +1648,8 @@ int dnsb_shell_clamp(dnsb_ctx *c, double *ux, double *uy, double *uz, const doub
   const int nb = std::min(nshells, c->nshell_max);
   double *E = c->shellbuf, *f = E + c->nshell_max, *er = f + c->nshell_max;
   if ((rc = upload_eref(c, eref, nb))) return rc;
-  const double *cu[3] = {ux, uy, uz};
-  if ((rc = shell_energies_dev(c, cu, E, nb))) return rc;
-  k_clamp_factors<<<1, 256, 0, c->stream>>>(E, er, f, nb);
-  CKL(c);
   double *u[3] = {ux, uy, uz};
-  return shell_scale_dev(c, u, f, nb);
+  return shell_clamp_dev(c, u, E, er, f, nb);
 }
 
 int dnsb_les_cube(dnsb_ctx *c, const double *ux, const double *uy, const double *uz, int M,

@@ -207,7 +207,9 @@ int dnsb_les_cube(dnsb_ctx *ctx, const double *ux, const double *uy, const doubl
  * with eref[s] >= 0 are rescaled to energy eref[s] (unchanged where they
  * hold none), shells with eref[s] < 0 are not forced.  Energies, factors
  * and the rescale stay on the device (no host synchronisation once eref
- * is uploaded; a changed eref is uploaded synchronously). */
+ * is uploaded; a changed eref is uploaded synchronously, and the first call
+ * allocates two spectrum buffers that the context keeps: make it outside a
+ * stream capture).  Each component is transformed once and back. */
 int dnsb_shell_clamp(dnsb_ctx *ctx, double *ux, double *uy, double *uz, const double *eref,
                      int nshells);
 
