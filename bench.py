@@ -346,7 +346,8 @@ def ensemble_arm(args, wl, world, rank, local):
                               "achieved": step_gbs, "peak": peak, "unit": "GB/s",
                               "frac": step_gbs / peak, "peak_source": peak_kind,
                               "note": "bytes of the RK3 step alone; the shell forcing "
-                                      "(6 extra 3-D transforms per member-step) is "
+                                      "(direct low-mode sums: one read and one update "
+                                      "pass per component per member-step) is "
                                       "extra work inside the timed region"},
             "clocks": clk,
         }

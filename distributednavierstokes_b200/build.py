@@ -15,7 +15,7 @@ CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libdnsb.so")
 SOURCES = ["dnsb.cu"]
 HEADERS = ["common.cuh", "fft.cuh", "fft4.cuh", "spectral.cuh", "spectral4.cuh", "stencil.cuh",
-           "tma.cuh", "ysolve.cuh", "gradmom.cuh", "zyz.cuh", "spsolver.cuh"]
+           "tma.cuh", "ysolve.cuh", "gradmom.cuh", "zyz.cuh", "spsolver.cuh", "lowshells.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

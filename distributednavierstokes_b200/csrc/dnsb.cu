@@ -36,6 +36,7 @@
 #include "gradmom.cuh"
 #include "zyz.cuh"
 #include "spsolver.cuh"
+#include "lowshells.cuh"
 
 using namespace dnsb;
 
@@ -102,6 +103,7 @@ struct dnsb_ctx {
   // scratch
   double2 *S = nullptr;
   double2 *Sx[2] = {nullptr, nullptr};  // spectra of u.y, u.z during a shell clamp
+  double2 *lsA = nullptr, *lsB = nullptr, *lsG = nullptr, *lsH = nullptr;  // low-shell clamp scratch
   double *work = nullptr;
   double *ycin = nullptr;  // c' entering each y-chunk, per (kx, kz) line
   double *r = nullptr;
@@ -1085,10 +1087,26 @@ __global__ void k_clamp_factors(const double *E, const double *eref, double *f, 
 
 // the shell-clamp reference table on the device (synchronous; skipped when
 // it is already there, so that a captured clamp never synchronises)
+// the clamp of shells 0..nb-1 by partial Fourier sums (lowshells.cuh)
+bool clamp_direct(const dnsb_ctx *c, int nb) {
+  const Geo &g = c->g;
+  const int KM = nb - 1;
+  return nb <= LS_KX && 2 * KM < g.nx && 2 * KM < g.ny && 2 * KM < g.nz;
+}
+
 int upload_eref(dnsb_ctx *c, const double *eref, int nb) {
-  if (!c->Sx[0]) {  // the clamp keeps all three spectra (first clamp only)
-    const size_t nspec = (size_t)c->g.nkx * c->g.ny * c->g.nz;
-    int rc;
+  const Geo &g = c->g;
+  int rc;
+  if (clamp_direct(c, nb)) {
+    if (!c->lsA) {  // scratch for the largest direct case (first clamp only)
+      if ((rc = dalloc(c, &c->lsA, (size_t)3 * LS_KX * g.ny * g.nz)) ||
+          (rc = dalloc(c, &c->lsB, (size_t)3 * LS_KX * g.nz * LS_KY)) ||
+          (rc = dalloc(c, &c->lsG, (size_t)3 * LS_KX * LS_KY * LS_KY)) ||
+          (rc = dalloc(c, &c->lsH, (size_t)3 * LS_KX * LS_KY * g.nz)))
+        return rc;
+    }
+  } else if (!c->Sx[0]) {  // the transform clamp keeps all three spectra
+    const size_t nspec = (size_t)g.nkx * g.ny * g.nz;
     if ((rc = dalloc(c, &c->Sx[0], nspec)) || (rc = dalloc(c, &c->Sx[1], nspec))) return rc;
   }
   if (c->eref_host.size() == (size_t)nb && std::equal(eref, eref + nb, c->eref_host.begin())) return 0;
@@ -1648,6 +1666,23 @@ int dnsb_shell_clamp(dnsb_ctx *c, double *ux, double *uy, double *uz, const doub
   const int nb = std::min(nshells, c->nshell_max);
   double *E = c->shellbuf, *f = E + c->nshell_max, *er = f + c->nshell_max;
   if ((rc = upload_eref(c, eref, nb))) return rc;
+  if (clamp_direct(c, nb)) {
+    const Geo &g = c->g;
+    const int KM = nb - 1;
+    const unsigned lines = (unsigned)(((long long)g.ny * g.nz + LS_LINES - 1) / LS_LINES);
+    k_ls_xsums<<<lines, 32 * LS_LINES, 0, c->stream>>>(g, cf(ux, uy, uz), KM, c->lsA);
+    CKL(c);
+    k_ls_ysums<<<(unsigned)(3 * (KM + 1) * g.nz), 128, 0, c->stream>>>(g, c->lsA, KM, c->lsB);
+    CKL(c);
+    k_ls_zsums<<<(unsigned)(3 * (KM + 1) * (2 * KM + 1)), 128, 0, c->stream>>>(g, c->lsB, KM, c->lsG);
+    CKL(c);
+    k_ls_modes<<<1, 1024, 0, c->stream>>>(g, KM, c->lsG, c->lsH, E, er, f, nb);
+    CKL(c);
+    k_ls_correct<<<lines, 32 * LS_LINES, 0, c->stream>>>(g, ff(ux, uy, uz), KM, c->lsH);
+    CKL(c);
+    c->umax_for[0] = c->umax_for[1] = c->umax_for[2] = nullptr;
+    return 0;
+  }
   double *u[3] = {ux, uy, uz};
   return shell_clamp_dev(c, u, E, er, f, nb);
 }

@@ -93,13 +93,15 @@ def test_shell_energies_and_rescale(oracle_mod, D, n):
         assert np.array_equal(ud[c][0], ud[c][-2]) and np.array_equal(ud[c][:, :, -1], ud[c][:, :, 1])
 
 
-def test_forced_run_matches_oracle(oracle_mod, D):
+# shells below 4 take the direct partial-sum clamp, (1, 3, 4) the transform one
+@pytest.mark.parametrize("shells", [(1, 2), (2, 3), (1, 3, 4)])
+def test_forced_run_matches_oracle(oracle_mod, D, shells):
     n = (18, 18, 18)
     so, s = oracle_mod.Setup(n, visc=5e-3), D.setup(n=n, visc=5e-3)
     uo = so.random_field(so.vectorfield(), totalenergy=0.4, kpeak=2, seed=7)
     u = D.random_field(D.vectorfield(s), s, totalenergy=0.4, kpeak=2, seed=7)
-    fo = so.shellforcing(uo, shells=(1, 2))
-    f = D.shellforcing(u, s, shells=(1, 2))
+    fo = so.shellforcing(uo, shells=shells)
+    f = D.shellforcing(u, s, shells=shells)
     assert np.allclose(f.eref, fo.eref, rtol=1e-12, atol=0)
     so.solve(uo, (0.0, 0.05), dt=0.01, forcing=fo)
     st = D.solve(u=u, setup=s, tlims=(0.0, 0.05), dt=0.01, forcing=f)
@@ -107,8 +109,11 @@ def test_forced_run_matches_oracle(oracle_mod, D):
     ud = host(u)
     for c in "xyz":
         assert rel(ud[c], uo[c]) < 1e-11
-    assert np.allclose(D.shell_energies(u, s, (1, 2)), f.eref, rtol=1e-13, atol=0)
+    assert np.allclose(D.shell_energies(u, s, shells), f.eref, rtol=1e-13, atol=0)
     assert D.maxdiv(u, s) < 1e-12
+    ud = host(u)
+    for c in "xyz":  # ghost images rewritten by the clamp
+        assert np.array_equal(ud[c][0], ud[c][-2]) and np.array_equal(ud[c][:, :, -1], ud[c][:, :, 1])
 
 
 def test_shells_need_periodic_box(D):
