@@ -208,8 +208,10 @@ int dnsb_les_cube(dnsb_ctx *ctx, const double *ux, const double *uy, const doubl
  * hold none), shells with eref[s] < 0 are not forced.  Energies, factors
  * and the rescale stay on the device (no host synchronisation once eref
  * is uploaded; a changed eref is uploaded synchronously, and the first call
- * allocates two spectrum buffers that the context keeps: make it outside a
- * stream capture).  Each component is transformed once and back. */
+ * allocates scratch that the context keeps: make it outside a stream
+ * capture).  With nshells <= 4 the modes are formed by direct partial
+ * Fourier sums (one read and one update pass per component); otherwise
+ * each component is transformed once and back. */
 int dnsb_shell_clamp(dnsb_ctx *ctx, double *ux, double *uy, double *uz, const double *eref,
                      int nshells);
 
