@@ -121,6 +121,7 @@ struct dnsb_ctx {
   int *deverr = nullptr;               // device-side error word (bounded waits)
   int use_tma = 1;                     // persistent TMA-pipelined z-FFT
   int zyz_c = 0;                       // CTAs per cluster of k_zyz (0: three kernels)
+  int zyz_mode = 1;                    // 1: k_zyz (32-row chunks), 2: k_zyz2 (16-row chunks)
   int nkx_active = 0;                  // z-FFTs on kx < nkx_active only (0: all; spectral solver)
   int x1 = 0, x2 = 0, z1 = 0, z2 = 0;  // four-step splits of nx/2 and nz (0: generic kernels)
   int L4z = 8;                         // lines per CTA of the z-FFT
@@ -749,10 +750,12 @@ int launch_irfftx(dnsb_ctx *c, int mode, double *out) {
   return 0;
 }
 
-// k_zyz for this context's z split: one cluster of zyz_c CTAs per kx plane
+// k_zyz (mode 1) or k_zyz2 (mode 2) for this context's z split: one cluster
+// of zyz_c CTAs per kx plane
 template <int N1, int N2>
 cudaError_t launch_zyz_as(dnsb_ctx *c, bool query, int *nclusters) {
   const Geo &g = c->g;
+  const bool two = c->zyz_mode == 2;
   cudaLaunchConfig_t cfg = {};
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -760,16 +763,16 @@ cudaError_t launch_zyz_as(dnsb_ctx *c, bool query, int *nclusters) {
   attr[0].val.clusterDim.y = 1;
   attr[0].val.clusterDim.z = 1;
   cfg.gridDim = dim3((unsigned)(g.nkx * c->zyz_c));
-  cfg.blockDim = dim3(ZYZ_THREADS);
-  cfg.dynamicSmemBytes = zyz_smem<N1, N2>();
+  cfg.blockDim = dim3(two ? ZYZ2_THREADS : ZYZ_THREADS);
+  cfg.dynamicSmemBytes = two ? zyz2_smem<N1, N2>() : zyz_smem<N1, N2>();
   cfg.stream = c->stream;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  if (query) return cudaOccupancyMaxActiveClusters(nclusters, k_zyz<N1, N2>, &cfg);
-  return cudaLaunchKernelEx(&cfg, k_zyz<N1, N2>, g, c->S, (const double *)c->ycin,
-                            (const double *)c->ay, (const double *)c->by, (const double *)c->cy,
-                            (const double *)c->lam1, (const double *)c->lam3,
-                            (const double2 *)c->twz);
+  auto kern = two ? k_zyz2<N1, N2> : k_zyz<N1, N2>;
+  if (query) return cudaOccupancyMaxActiveClusters(nclusters, kern, &cfg);
+  return cudaLaunchKernelEx(&cfg, kern, g, c->S, (const double *)c->ycin, (const double *)c->ay,
+                            (const double *)c->by, (const double *)c->cy, (const double *)c->lam1,
+                            (const double *)c->lam3, (const double2 *)c->twz);
 }
 
 cudaError_t launch_zyz_split(dnsb_ctx *c, bool query, int *nclusters) {
@@ -778,19 +781,42 @@ cudaError_t launch_zyz_split(dnsb_ctx *c, bool query, int *nclusters) {
   return cudaErrorInvalidValue;
 }
 
+template <class K>
+int allow_cluster_kernel(dnsb_ctx *c, K kern, size_t smem, bool nonportable) {
+  int rc = allow_smem(c, kern, smem);
+  if (rc) return rc;
+  if (nonportable &&
+      cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+    cudaGetLastError();
+    return -1;  // not available: the caller falls back
+  }
+  return 0;
+}
+
 // Chooses the fused z-FFT / y-solve / inverse z-FFT kernel where it applies:
 // walls, nz in {256, 384} (four-step 16 x 16 / 16 x 24), ny a multiple of
-// 32 with at most 8 chunks, and a cluster of that size can be resident.
-int setup_zyz(dnsb_ctx *c) {
+// the chunk rows (32 for mode 1, 16 for mode 2) with at most 8 (16) chunks,
+// and a cluster of that size can be resident.
+int setup_zyz(dnsb_ctx *c, int mode) {
   const Geo &g = c->g;
   c->zyz_c = 0;
+  c->zyz_mode = mode == 2 ? 2 : 1;
   if (!(c->z1 == 16 && (c->z2 == 24 || c->z2 == 16))) return 0;
-  if (g.ny % ZYZ_ROWS != 0 || g.ny / ZYZ_ROWS > ZYZ_MAXC) return 0;
+  const int rows = c->zyz_mode == 2 ? ZYZ2_ROWS : ZYZ_ROWS;
+  const int maxc = c->zyz_mode == 2 ? ZYZ2_MAXC : ZYZ_MAXC;
+  if (g.ny % rows != 0 || g.ny / rows > maxc) return 0;
+  const int C = g.ny / rows;
   int rc;
-  if (c->z2 == 24) rc = allow_smem(c, k_zyz<16, 24>, zyz_smem<16, 24>());
-  else rc = allow_smem(c, k_zyz<16, 16>, zyz_smem<16, 16>());
+  if (c->zyz_mode == 2) {
+    rc = c->z2 == 24 ? allow_cluster_kernel(c, k_zyz2<16, 24>, zyz2_smem<16, 24>(), C > 8)
+                     : allow_cluster_kernel(c, k_zyz2<16, 16>, zyz2_smem<16, 16>(), C > 8);
+    if (rc < 0) return 0;
+  } else {
+    rc = c->z2 == 24 ? allow_smem(c, k_zyz<16, 24>, zyz_smem<16, 24>())
+                     : allow_smem(c, k_zyz<16, 16>, zyz_smem<16, 16>());
+  }
   if (rc) return rc;
-  c->zyz_c = g.ny / ZYZ_ROWS;
+  c->zyz_c = C;
   int n = 0;
   if (launch_zyz_split(c, true, &n) != cudaSuccess || n < 1) {
     cudaGetLastError();  // the query's error is not the context's
@@ -1350,7 +1376,8 @@ int dnsb_create(const dnsb_grid *gr, int device, void *stream, dnsb_ctx **out) {
   if (g.wall && ythomas_rows(ny) == 0 && (rc = dalloc(c, &c->work, nspec))) return bail(rc);
   // the fused z-FFT / y-solve / inverse z-FFT is opt-in: at 384 x 256 x 384
   // it measured 0.44-0.46 ms against 0.43 ms for the three kernels
-  if (g.wall && !c->use_tma && envint("DNSB_ZYZ", 0) != 0 && (rc = setup_zyz(c))) return bail(rc);
+  if (g.wall && !c->use_tma && envint("DNSB_ZYZ", 0) != 0 && (rc = setup_zyz(c, envint("DNSB_ZYZ", 0))))
+    return bail(rc);
   if (g.wall && (c->zyz_c || ythomas_rows(ny) != 0)) {
 #define YTS(MR)                                                                                    \
   if (ythomas_rows(ny) == MR && (rc = allow_smem(c, k_ythomas<MR>, ythomas_smem(MR)))) return bail(rc);
@@ -1359,7 +1386,8 @@ int dnsb_create(const dnsb_grid *gr, int device, void *stream, dnsb_ctx **out) {
     const long long nl = (long long)g.nkx * nz;
     if ((rc = dalloc(c, &c->ycin, (size_t)nl * TY_CHUNKS))) return bail(rc);
     k_ythomas_entries<<<(unsigned)((nl + 127) / 128), 128, 0, c->stream>>>(
-        g, c->zyz_c ? ZYZ_ROWS : ythomas_rows(ny), c->ycin, c->ay, c->by, c->cy, c->lam1, c->lam3);
+        g, c->zyz_c ? (c->zyz_mode == 2 ? ZYZ2_ROWS : ZYZ_ROWS) : ythomas_rows(ny), c->ycin, c->ay,
+        c->by, c->cy, c->lam1, c->lam3);
     if (cudaGetLastError() != cudaSuccess) {
       fail(c, DNSB_ECUDA, "launch of the y-solve table kernel failed");
       return bail(DNSB_ECUDA);

@@ -228,4 +228,219 @@ __global__ void __launch_bounds__(ZYZ_THREADS, 1)
   cluster_wait();
 }
 
+
+// ---- two CTAs per SM: 16-row chunks, clusters of ny/16 (up to 16, the
+// non-portable size), 192 threads.  The rows are stored without padding
+// (16 x nz complex = 96 KB at nz = 384) under a rotation swizzle: element
+// (k1, k2) of a row sits at k1 N2 + (k2 + k1) mod N2, which keeps the runs
+// of the second four-step pass on distinct banks; the twiddles are read
+// from global memory (L1-resident) and the forward and backward chunk maps
+// share one buffer behind an extra cluster barrier, so that two CTAs fit in
+// one SM's shared memory and their load, transform and solve phases
+// overlap.  Same algorithm and results as k_zyz.
+constexpr int ZYZ2_ROWS = 16;
+constexpr int ZYZ2_THREADS = 192;  // two z-lines per thread in the Thomas phase
+constexpr int ZYZ2_MAXC = 16;
+
+template <int N1, int N2>
+constexpr size_t zyz2_smem() {
+  return sizeof(double2) * (size_t)ZYZ2_ROWS * N1 * N2 + sizeof(double) * 3 * (size_t)N1 * N2;
+}
+
+template <int N1, int N2>
+__global__ void __launch_bounds__(ZYZ2_THREADS, 2)
+    k_zyz2(Geo g, double2 *__restrict__ S, const double *__restrict__ cin,
+           const double *__restrict__ ay, const double *__restrict__ by,
+           const double *__restrict__ cy, const double *__restrict__ lam1,
+           const double *__restrict__ lam3, const double2 *__restrict__ tw) {
+  namespace cg = cooperative_groups;
+  constexpr int N = N1 * N2;  // nz
+  constexpr int R = ZYZ2_ROWS;
+  constexpr int LPT = (N + ZYZ2_THREADS - 1) / ZYZ2_THREADS;  // lines per thread (2 at 384)
+  static_assert(LPT <= 2, "at most two lines per thread");
+  extern __shared__ __align__(16) double2 zsm2[];
+  double2 *pl = zsm2;                               // [R][N], swizzled
+  double *mp = reinterpret_cast<double *>(pl + R * N);  // [3][N] chunk maps
+  auto pos = [](int k1, int k2) { int r = k2 + k1; r -= r >= N2 ? N2 : 0; return k1 * N2 + r; };
+  cg::cluster_group cl = cg::this_cluster();
+  const int C = (int)cl.num_blocks();
+  const int c = (int)cl.block_rank();
+  const int kx = blockIdx.x / C;
+  const int j0 = c * R;
+  double2 *src = S + ((long long)kx * g.ny + j0) * N;
+
+  // forward z-FFT step 1: N1-point transforms from HBM into the swizzled rows
+  for (int it = threadIdx.x; it < R * N2; it += blockDim.x) {
+    const int l = it / N2, j2 = it - l * N2;
+    const double2 *line = src + (long long)l * N;
+    double2 v[N1];
+#pragma unroll
+    for (int j1 = 0; j1 < N1; j1++) v[j1] = line[j1 * N2 + j2];
+    reg_fft<N1, false>(v, tw, N2);
+    double2 *row = pl + l * N;
+#pragma unroll
+    for (int k1 = 0; k1 < N1; k1++) row[pos(k1, j2)] = k1 == 0 ? v[0] : cmul(v[k1], __ldg(tw + j2 * k1));
+  }
+  __syncthreads();
+  // step 2 in place: pos(k1, k2) of a row holds X[k1 + N1 k2]
+  for (int it = threadIdx.x; it < R * N1; it += blockDim.x) {
+    const int l = it / N1, k1 = it - l * N1;
+    double2 *row = pl + l * N;
+    double2 v[N2];
+#pragma unroll
+    for (int j2 = 0; j2 < N2; j2++) v[j2] = row[pos(k1, j2)];
+    reg_fft<N2, false>(v, tw, N1);
+#pragma unroll
+    for (int k2 = 0; k2 < N2; k2++) row[pos(k1, k2)] = v[k2];
+  }
+  __syncthreads();
+
+  // Thomas along y: this CTA is chunk c of every line; thread t owns the
+  // lines at row positions t and t + blockDim.x
+  {
+    int p[LPT], kz[LPT];
+    bool act[LPT];
+    double lam[LPT], cprev[LPT];
+    bool pin[LPT];
+#pragma unroll
+    for (int q = 0; q < LPT; q++) {
+      p[q] = threadIdx.x + q * ZYZ2_THREADS;
+      act[q] = p[q] < N;
+      const int pp = act[q] ? p[q] : 0;
+      const int k1 = pp / N2;
+      int k2 = pp - k1 * N2 - k1;
+      while (k2 < 0) k2 += N2;
+      kz[q] = k1 + N1 * k2;
+      lam[q] = __ldg(lam1 + kx) + __ldg(lam3 + kz[q]);
+      pin[q] = lam[q] == 0.0;
+      cprev[q] = act[q] ? __ldg(cin + ((long long)kx * N + kz[q]) * TY_CHUNKS + c) : 0.0;
+    }
+    double ib[LPT][R];
+    double2 z[LPT];
+    double G[LPT];
+#pragma unroll
+    for (int q = 0; q < LPT; q++) { z[q] = make_double2(0.0, 0.0); G[q] = 1.0; }
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+      const int j = j0 + r;
+      const double a0 = __ldg(ay + j), b0 = __ldg(by + j), c0 = __ldg(cy + j);
+#pragma unroll
+      for (int q = 0; q < LPT; q++) {
+        const bool p0 = pin[q] && j == 0;
+        const double a = p0 ? 0.0 : a0, b = p0 ? 1.0 : b0 + lam[q], cc = p0 ? 0.0 : c0;
+        const double rb = 1.0 / (b - a * cprev[q]);
+        cprev[q] = cc * rb;
+        ib[q][r] = rb;
+        const double2 d = p0 ? make_double2(0.0, 0.0) : pl[r * N + (act[q] ? p[q] : 0)];
+        z[q] = make_double2((d.x - a * z[q].x) * rb, (d.y - a * z[q].y) * rb);
+        G[q] *= -a * rb;
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < LPT; q++)
+      if (act[q]) { mp[p[q]] = z[q].x; mp[N + p[q]] = z[q].y; mp[2 * N + p[q]] = G[q]; }
+    cl.sync();
+    double2 dp[LPT];
+#pragma unroll
+    for (int q = 0; q < LPT; q++) {
+      dp[q] = make_double2(0.0, 0.0);
+      if (act[q])
+        for (int i = 0; i < c; i++) {
+          const double *m = cl.map_shared_rank(mp, i);
+          const double gi = m[2 * N + p[q]];
+          dp[q] = make_double2(fma(gi, dp[q].x, m[p[q]]), fma(gi, dp[q].y, m[N + p[q]]));
+        }
+    }
+    cluster_arrive();  // forward maps read; the buffer is reused below
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+      const int j = j0 + r;
+      const double a0 = __ldg(ay + j);
+#pragma unroll
+      for (int q = 0; q < LPT; q++) {
+        const bool p0 = pin[q] && j == 0;
+        const double a = p0 ? 0.0 : a0;
+        double2 *x = pl + r * N + (act[q] ? p[q] : 0);
+        const double2 d = p0 ? make_double2(0.0, 0.0) : *x;
+        dp[q] = make_double2((d.x - a * dp[q].x) * ib[q][r], (d.y - a * dp[q].y) * ib[q][r]);
+        if (act[q]) *x = dp[q];
+      }
+    }
+    double2 y[LPT];
+    double Hh[LPT];
+#pragma unroll
+    for (int q = 0; q < LPT; q++) { y[q] = make_double2(0.0, 0.0); Hh[q] = 1.0; }
+#pragma unroll
+    for (int r = R - 1; r >= 0; r--) {
+      const int j = j0 + r;
+      const double c0 = __ldg(cy + j);
+#pragma unroll
+      for (int q = 0; q < LPT; q++) {
+        const double cpr = ((pin[q] && j == 0) ? 0.0 : c0) * ib[q][r];
+        const double2 d = pl[r * N + (act[q] ? p[q] : 0)];
+        y[q] = make_double2(d.x - cpr * y[q].x, d.y - cpr * y[q].y);
+        Hh[q] *= -cpr;
+      }
+    }
+    cluster_wait();  // every peer has read the forward maps
+#pragma unroll
+    for (int q = 0; q < LPT; q++)
+      if (act[q]) { mp[p[q]] = y[q].x; mp[N + p[q]] = y[q].y; mp[2 * N + p[q]] = Hh[q]; }
+    cl.sync();
+    double2 xn[LPT];
+#pragma unroll
+    for (int q = 0; q < LPT; q++) {
+      xn[q] = make_double2(0.0, 0.0);
+      if (act[q])
+        for (int i = C - 1; i > c; i--) {
+          const double *m = cl.map_shared_rank(mp, i);
+          const double hi = m[2 * N + p[q]];
+          xn[q] = make_double2(fma(hi, xn[q].x, m[p[q]]), fma(hi, xn[q].y, m[N + p[q]]));
+        }
+    }
+    cluster_arrive();  // peers' maps read: they may exit once everyone has arrived
+#pragma unroll
+    for (int r = R - 1; r >= 0; r--) {
+      const int j = j0 + r;
+      const double c0 = __ldg(cy + j);
+#pragma unroll
+      for (int q = 0; q < LPT; q++) {
+        const double cpr = ((pin[q] && j == 0) ? 0.0 : c0) * ib[q][r];
+        double2 *x = pl + r * N + (act[q] ? p[q] : 0);
+        const double2 d = *x;
+        xn[q] = make_double2(d.x - cpr * xn[q].x, d.y - cpr * xn[q].y);
+        if (act[q]) *x = xn[q];
+      }
+    }
+  }
+  __syncthreads();
+
+  // inverse z-FFT: step 1 in place per row run, step 2 to HBM (x 1/nz)
+  for (int it = threadIdx.x; it < R * N1; it += blockDim.x) {
+    const int l = it / N1, k1 = it - l * N1;
+    double2 *row = pl + l * N;
+    double2 v[N2];
+#pragma unroll
+    for (int k2 = 0; k2 < N2; k2++) v[k2] = row[pos(k1, k2)];
+    reg_fft<N2, true>(v, tw, N1);
+#pragma unroll
+    for (int j2 = 0; j2 < N2; j2++)
+      row[pos(k1, j2)] = (k1 == 0 || j2 == 0) ? v[j2] : cmul(v[j2], cconj(__ldg(tw + j2 * k1)));
+  }
+  __syncthreads();
+  const double sc = 1.0 / N;
+  for (int it = threadIdx.x; it < R * N2; it += blockDim.x) {
+    const int l = it / N2, j2 = it - l * N2;
+    const double2 *row = pl + l * N;
+    double2 v[N1];
+#pragma unroll
+    for (int k1 = 0; k1 < N1; k1++) v[k1] = row[pos(k1, j2)];
+    reg_fft<N1, true>(v, tw, N2);
+    double2 *line = src + (long long)l * N;
+#pragma unroll
+    for (int j1 = 0; j1 < N1; j1++) line[j1 * N2 + j2] = cscale(v[j1], sc);
+  }
+  cluster_wait();
+}
+
 }  // namespace dnsb

@@ -228,14 +228,16 @@ ZYZ = {
 }
 
 
+@pytest.mark.parametrize("mode", ["1", "2"])
 @pytest.mark.parametrize("cfg", list(ZYZ))
-def test_fused_poisson_kernel(oracle_mod, D, cfg, monkeypatch):
-    """With DNSB_ZYZ=1 the fused kernel runs (and the three-kernel path does
-    not) where it applies; the Poisson solve, the projection and one RK3
-    step agree with the oracle."""
+def test_fused_poisson_kernel(oracle_mod, D, cfg, mode, monkeypatch):
+    """With DNSB_ZYZ=1 (32-row chunks, one CTA per SM) or 2 (16-row chunks,
+    two CTAs per SM, clusters up to 16) the fused kernel runs (and the
+    three-kernel path does not) where it applies; the Poisson solve, the
+    projection and one RK3 step agree with the oracle."""
     from distributednavierstokes_b200 import _lib
 
-    monkeypatch.setenv("DNSB_ZYZ", "1")
+    monkeypatch.setenv("DNSB_ZYZ", mode)
     so, sd = both(oracle_mod, D, **ZYZ[cfg])
     lib = _lib.load()
     lib.dnsb_profile(sd.ctx, 1)
