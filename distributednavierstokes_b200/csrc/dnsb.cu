@@ -98,6 +98,10 @@ struct dnsb_ctx {
   int fuse = 1;       // fused projection + momentum between implicit stages
   double *pn = nullptr;  // pressure after stage 1 when fused
   dim3 tgrid, tblock;
+  // z-planes per CTA of the fused projection + momentum: 32 measured 1.5 %
+  // faster than 16 and 64 at 384x256x384 (its prologue projects two planes)
+  int gm_planes = 32;
+  dim3 gmgrid;
 
   dim3 cgrid, cblock;  // launch shape of the per-cell step kernels
   // scratch
@@ -917,8 +921,8 @@ int do_step(dnsb_ctx *c, double *ux, double *uy, double *uz, double *p, double *
         const double *pin = s == 0 ? p : c->pn;
         double *pout = s == 0 ? c->pn : p;
         LAUNCH(c, DNSB_KIND_GRADMOM,
-               k_gradmom_march<<<c->tgrid, c->tblock, GRADMOM_SMEM, c->stream>>>(
-                   g, cf(ux, uy, uz), delta, pin, pout, 1.0 / adt, ff(qx, qy, qz),
+               k_gradmom_march<<<c->gmgrid, c->tblock, GRADMOM_SMEM, c->stream>>>(
+                   g, c->gm_planes, cf(ux, uy, uz), delta, pin, pout, 1.0 / adt, ff(qx, qy, qz),
                    ff(c->V[0], c->V[1], c->V[2]), A1, dt, B1, al1 * dt, c->ymet,
                    al1 * dt * g.visc / 2));
       } else {
@@ -1315,6 +1319,8 @@ int dnsb_create(const dnsb_grid *gr, int device, void *stream, dnsb_ctx **out) {
     c->fuse = envint("DNSB_FUSE", 1) != 0;
     c->tblock = dim3(MC_X, MC_Y, 1);
     c->tgrid = dim3((nx + MC_X - 1) / MC_X, (ny + MC_Y - 1) / MC_Y, (nz + MC_Z - 1) / MC_Z);
+    c->gm_planes = std::max(4, std::min(256, envint("DNSB_GMZ", c->gm_planes)));
+    c->gmgrid = dim3(c->tgrid.x, c->tgrid.y, (nz + c->gm_planes - 1) / c->gm_planes);
   }
   c->smem_rx = sizeof(double2) * (2 * (size_t)c->Lx * (M + 1) + M + (M + 1));
   c->smem_ix = sizeof(double2) * (2 * (size_t)c->Lx * (M + 2) + M + (M + 1));

@@ -33,11 +33,12 @@ constexpr int GP_X = MC_X + 4, GP_Y = MC_Y + 3, GP_N = GP_X * GP_Y;
 // Reads u* (ux, uy, uz after the Crank-Nicolson solve of stage s), delta,
 // p_in (lagged pressure before stage s's update), q; writes p_out =
 // p_in + delta * radt on the interior with ghost images, q, and V (the
-// Crank-Nicolson right-hand side of stage s+1, as k_momentum<IMPLICIT>).
+// Crank-Nicolson right-hand side of stage s+1, as k_momentum<IMPLICIT>);
+// each CTA walks `planes` z-planes (grid z = ceil(nz / planes)).
 // p_out must not alias p_in (other CTAs stage p_in while this one writes).
 // 3 CTAs of 256 per SM (80 registers, no spills; faster than 2)
 __global__ void __launch_bounds__(MC_X *MC_Y, 3)
-    k_gradmom_march(Geo g, CFields3 us, const double *__restrict__ delta,
+    k_gradmom_march(Geo g, int planes, CFields3 us, const double *__restrict__ delta,
                     const double *__restrict__ p_in, double *__restrict__ p_out, double radt,
                     Fields3 q, Fields3 out, double A, double dt, double B, double adt,
                     const double2 *__restrict__ ymet, double theta) {
@@ -50,7 +51,7 @@ __global__ void __launch_bounds__(MC_X *MC_Y, 3)
   const int tid = tx + MC_X * ty;
   constexpr int NT = MC_X * MC_Y;
   const int I0 = blockIdx.x * MC_X + 1, J0 = blockIdx.y * MC_Y + 1;
-  const int K0 = blockIdx.z * MC_Z + 1, K1 = min(g.nz, K0 + MC_Z - 1);
+  const int K0 = blockIdx.z * planes + 1, K1 = min(g.nz, K0 + planes - 1);
   const bool wall = g.wall;
   constexpr int CH = GP_X / 2;
   static_assert(GP_Y * CH <= NT, "one staging chunk per thread and field plane");
