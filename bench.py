@@ -13,6 +13,10 @@ ydiffusion = :implicit, CFL 0.8, initial condition = a Reichardt mean
 profile (Re_tau = 395) plus seeded splitmix64 noise of amplitude 0.2.
 Synthetic data of that shape: the reference publishes no dataset.
 
+The line also carries `fft_vs_cufft`: cuFFT (torch.fft) timed on the
+shapes of the four Poisson transforms beside the library's own kernels
+(--no-cufft skips it).
+
 Prints ONE JSON line on rank 0.  Under torchrun (N > 1) each rank advances
 an independent replica (the single-GPU step does not shard without the
 multi-GPU transposes; weak scaling, no collective in the data path).
@@ -527,6 +531,9 @@ def b200_arm(args, wl, world, rank, local):
     step_bytes = wl["bytes_per_cell_step"] * cells
     step_gbs = step_bytes / (ms / args.steps / 1e3) / 1e9
 
+    fftcmp = None
+    if rank == 0 and not args.no_cufft and "div_rfft_x" in kinds:
+        fftcmp = cufft_leg(s, dev, kinds)
     e2e_line = None
     if not args.no_e2e:
         e2e_line = e2e_leg(lib, s, host_ic, wl, args, world, dev, cells, G)
@@ -561,6 +568,7 @@ def b200_arm(args, wl, world, rank, local):
                               "achieved": step_gbs, "peak": peak, "unit": "GB/s",
                               "frac": step_gbs / peak},
             "kernels": per_kernel,
+            "fft_vs_cufft": fftcmp,
             "gpu_launches": launches,
             "clocks": clk,
             "cpu_baseline": cpu,
@@ -569,6 +577,57 @@ def b200_arm(args, wl, world, rank, local):
     s.close()
     if world > 1:
         torch.distributed.destroy_process_group()
+
+
+def cufft_leg(s, dev, kinds, reps=20):
+    """cuFFT (through torch.fft, a library) on the shapes of the Poisson
+    solve's four transforms, timed beside the library's own kernels.  Each
+    cuFFT transform runs along the contiguous axis of its own tensor, its
+    best case: no transposed spectrum, no fused divergence, no ghost images.
+    The library's x-transform also forms the divergence from the three
+    velocity fields and writes the kz-fastest spectrum; its inverse writes
+    the ghosted pressure with its images."""
+    import torch
+
+    nx, ny, nz = s.n
+    stream = torch.cuda.current_stream(dev)
+    gen = torch.Generator(device=dev).manual_seed(0)
+    r = torch.randn((nz, ny, nx), dtype=torch.float64, device=dev, generator=gen)
+    sx = torch.fft.rfft(r, dim=2)                                   # (nz, ny, nx/2+1)
+    sz = torch.randn((nx // 2 + 1, ny, nz), dtype=torch.complex128, device=dev,
+                     generator=gen)                                 # kz fastest
+
+    def timed(fn):
+        for _ in range(3):
+            fn()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        return e0.elapsed_time(e1) / reps
+
+    cu = {"rfft_x": timed(lambda: torch.fft.rfft(r, dim=2)),
+          "fft_z": timed(lambda: torch.fft.fft(sz, dim=2)),
+          "ifft_z": timed(lambda: torch.fft.ifft(sz, dim=2)),
+          "irfft_x": timed(lambda: torch.fft.irfft(sx, n=nx, dim=2))}
+    cu["total"] = sum(cu.values())
+    own = {}
+    for k in ("div_rfft_x", "fft_z", "ifft_z", "irfft_x"):
+        t, n = kinds.get(k, (0.0, 0))
+        if n:
+            own[k] = t / n
+    if len(own) == 4:
+        own["total"] = sum(own.values())
+    del r, sx, sz
+    torch.cuda.empty_cache()
+    return {"shape": [nx, ny, nz], "cufft_ms": cu, "dnsb_ms": own,
+            "timing": f"CUDA events, {reps} calls after 3 (cuFFT); live event pairs of the "
+                      "timed steps (library)",
+            "note": "cuFFT via torch.fft along the contiguous axis of separate tensors "
+                    "(complex128 / float64): no transposes, divergence or ghost images"}
 
 
 def e2e_leg(lib, s, host_ic, wl, args, world, dev, cells, G):
@@ -627,6 +686,8 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cufft", action="store_true",
+                    help="skip timing cuFFT beside the library's transforms")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "b200" else args.warmup
     wl = WORKLOADS[args.workload]
