@@ -516,11 +516,13 @@ def b200_arm(args, wl, world, rank, local):
     t_dom, n_dom = kinds[dom]
     bytes_launch = passes(dom, s.imexy, spec, fused) * cells * 8
     achieved = bytes_launch / (t_dom / n_dom / 1e3) / 1e9
-    traffic = None
+    traffic = step_traffic = None
     tpath = os.path.join(ROOT, "profiles", f"traffic_{args.workload}.json")
     if os.path.exists(tpath):
         with open(tpath) as f:
-            traffic = json.load(f).get(dom)
+            tj = json.load(f)
+        traffic = tj.get(dom)
+        step_traffic = tj.get("_step_dram_bytes_per_cell_step")
     per_kernel = {}
     for k, (t, n) in kinds.items():
         if n == 0:
@@ -566,7 +568,13 @@ def b200_arm(args, wl, world, rank, local):
                                    % (ms_profiled / args.steps)},
             "step_roofline": {"bytes_per_cell_step": wl["bytes_per_cell_step"],
                               "achieved": step_gbs, "peak": peak, "unit": "GB/s",
-                              "frac": step_gbs / peak},
+                              "frac": step_gbs / peak,
+                              # ncu DRAM bytes of one whole step per cell-step
+                              # (a smaller grid; writes still in L2 at kernel
+                              # ends not counted) and the fraction at that figure
+                              "dram_bytes_per_cell_step": step_traffic,
+                              "dram_frac": (step_traffic * cells / (ms / args.steps / 1e3)
+                                            / 1e9 / peak) if step_traffic else None},
             "kernels": per_kernel,
             "fft_vs_cufft": fftcmp,
             "gpu_launches": launches,
