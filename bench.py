@@ -173,9 +173,23 @@ def dist_init():
 
 # ------------------------------------------------------------------ CPU arm
 
-def cpu_oracle_run(wl, nsteps, nwarm, dt=None):
+def cpu_model():
+    """The host CPU's model name (/proc/cpuinfo), or the platform string."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or platform.machine()
+
+
+def cpu_oracle_run(wl, nsteps, nwarm, dt=None, per_step=None):
     """Advance the CPU oracle nwarm + nsteps steps; returns (seconds for
-    nsteps, threads, dt used)."""
+    nsteps, threads, dt used).  per_step, a list, receives each timed step's
+    seconds."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
 
@@ -202,8 +216,18 @@ def cpu_oracle_run(wl, nsteps, nwarm, dt=None):
         s.step(u, p, q, delta, dt)
     t0 = time.perf_counter()
     for _ in range(nsteps):
+        t1 = time.perf_counter()
         s.step(u, p, q, delta, dt)
+        if per_step is not None:
+            per_step.append(time.perf_counter() - t1)
     return time.perf_counter() - t0, threads, dt
+
+
+def step_stats(per_step):
+    """min / median / mean seconds of the timed CPU steps."""
+    v = sorted(per_step)
+    return {"min": v[0], "median": v[len(v) // 2] if len(v) % 2 else 0.5 * (v[len(v) // 2 - 1] + v[len(v) // 2]),
+            "mean": sum(v) / len(v)}
 
 
 REF_MAX_STEPS = 10
@@ -216,7 +240,8 @@ def reference_arm(args, wl, world, rank):
     # a bounded sample: at most REF_MAX_STEPS full-grid steps are timed (about
     # 2 s each on 16 host cores), so that any --steps K finishes in minutes
     n_run = max(1, min(args.steps, REF_MAX_STEPS))
-    secs, threads, _ = cpu_oracle_run(wl, n_run, min(args.warmup, 1))
+    per = []
+    secs, threads, _ = cpu_oracle_run(wl, n_run, min(args.warmup, 1), per_step=per)
     value = cells * n_run / secs
     line = {
         "metric": "DNS cell-steps/s (FP64)", "impl": "reference", "value": value,
@@ -226,6 +251,7 @@ def reference_arm(args, wl, world, rank):
         "config": {"workload": args.workload, "grid": list(wl["n"]),
                    "ydiffusion": wl["ydiffusion"], "parallelism": "host cores (OpenMP)"},
         "cpu_baseline": {"value": value, "unit": "cell-steps/s", "cores": threads, "kind": "port",
+                         "cpu_model": cpu_model(), "step_seconds": step_stats(per),
                          "sample": f"{n_run} timed RK3 steps of the full grid (of the "
                                    f"{args.steps} requested) after {min(args.warmup, 1)} warm-up "
                                    "step (C/OpenMP restatement of the Julia reference; "
@@ -541,9 +567,10 @@ def b200_arm(args, wl, world, rank, local):
         e2e_line = e2e_leg(lib, s, host_ic, wl, args, world, dev, cells, G)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        secs, threads, _ = cpu_oracle_run(wl, args.cpu_steps, 1)
+        per = []
+        secs, threads, _ = cpu_oracle_run(wl, args.cpu_steps, 1, per_step=per)
         cpu = {"value": cells * args.cpu_steps / secs, "unit": "cell-steps/s", "cores": threads,
-               "kind": "port",
+               "kind": "port", "cpu_model": cpu_model(), "step_seconds": step_stats(per),
                "sample": f"{args.cpu_steps} RK3 steps of the full {nx}x{ny}x{nz} grid after 1 "
                          "warm-up step, CPU oracle (C/OpenMP restatement of the Julia "
                          "reference) on all host threads"}
@@ -691,7 +718,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="channel384_implicit", choices=list(WORKLOADS))
-    ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--cpu-steps", type=int, default=5,
+                    help="timed full-grid CPU oracle steps of the cpu_baseline (about 2 s each)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cufft", action="store_true",
