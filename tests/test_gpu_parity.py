@@ -296,13 +296,16 @@ def test_one_step_production_lengths(oracle_mod, D, cfg):
     assert D.maxdiv(ud, sd) < 1e-12
 
 
-@pytest.mark.parametrize("planes", ["5", "40"])
+@pytest.mark.parametrize("planes,pipe", [("5", "0"), ("40", "0"), ("5", "1"), ("7", "1"),
+                                         ("32", "1")])
 @pytest.mark.parametrize("cfg", ["channel_implicit", "nx384_nz384"])
-def test_fused_projection_momentum_planes(oracle_mod, D, cfg, planes, monkeypatch):
+def test_fused_projection_momentum_planes(oracle_mod, D, cfg, planes, pipe, monkeypatch):
     """The fused projection + momentum kernel with other z-planes per CTA
-    (DNSB_GMZ; 5 and 40 leave a shorter last column at nz = 384 and at the
-    small channel): one semi-implicit step agrees with the oracle."""
+    (DNSB_GMZ; 5, 7 and 40 leave a shorter last column, 7 a single-plane one
+    at nz = 8) and its one-barrier pipelined variant (DNSB_GMPIPE=1): one
+    semi-implicit step agrees with the oracle."""
     monkeypatch.setenv("DNSB_GMZ", planes)
+    monkeypatch.setenv("DNSB_GMPIPE", pipe)
     kw = CONFIGS.get(cfg) or PRODUCTION[cfg]
     so, sd = both(oracle_mod, D, **kw)
     u = rand_fields(so)
