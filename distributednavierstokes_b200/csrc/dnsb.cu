@@ -132,6 +132,9 @@ struct dnsb_ctx {
   int nkx_active = 0;                  // z-FFTs on kx < nkx_active only (0: all; spectral solver)
   int x1 = 0, x2 = 0, z1 = 0, z2 = 0;  // four-step splits of nx/2 and nz (0: generic kernels)
   int L4z = 8;                         // lines per CTA of the z-FFT
+  // divergence x-FFT with its output pass in registers (3 % faster at
+  // 384x256x384 than the separate shared-memory pass)
+  int rx_post = 1;
   size_t smem_rx4 = 0, smem_ix4 = 0, smem_z4 = 0;
   int nsm = 148;
   size_t smem_zt = 0;
@@ -613,7 +616,9 @@ int launch_rfftx4(dnsb_ctx *c, int mode, const double *a, const double *b, const
   dim3 grid(g.ny * ((g.nz + RFX_L - 1) / RFX_L));
 #define RF4(A, B)                                                                                  \
   if (c->x1 == A && c->x2 == B) {                                                                  \
-    if (mode == RIN_DIVERGENCE)                                                                    \
+    if (mode == RIN_DIVERGENCE && c->rx_post)                                                      \
+      LAUNCH(c, DNSB_KIND_RFFTX, k_rfftx4<A, B, RFX_L, RIN_DIVERGENCE, true><<<grid, F4_THREADS, c->smem_rx4, c->stream>>>(g, c->S, a, b, cc, c->twM, c->twN)); \
+    else if (mode == RIN_DIVERGENCE)                                                               \
       LAUNCH(c, DNSB_KIND_RFFTX, k_rfftx4<A, B, RFX_L, RIN_DIVERGENCE><<<grid, F4_THREADS, c->smem_rx4, c->stream>>>(g, c->S, a, b, cc, c->twM, c->twN)); \
     else if (mode == RIN_REAL)                                                                     \
       LAUNCH(c, DNSB_KIND_RFFTX, k_rfftx4<A, B, RFX_L, RIN_REAL><<<grid, F4_THREADS, c->smem_rx4, c->stream>>>(g, c->S, a, b, cc, c->twM, c->twN)); \
@@ -666,6 +671,7 @@ template <int A, int B>
 int allow_fft4(dnsb_ctx *c) {
   int rc;
   if ((rc = allow_smem(c, k_rfftx4<A, B, RFX_L, RIN_DIVERGENCE>, c->smem_rx4)) ||
+      (rc = allow_smem(c, k_rfftx4<A, B, RFX_L, RIN_DIVERGENCE, true>, c->smem_rx4)) ||
       (rc = allow_smem(c, k_rfftx4<A, B, RFX_L, RIN_REAL>, c->smem_rx4)) ||
       (rc = allow_smem(c, k_rfftx4<A, B, RFX_L, RIN_FIELD>, c->smem_rx4)) ||
       (rc = allow_smem(c, k_rfftx4<A, B, RFX_L, RIN_PRODUCT>, c->smem_rx4)) ||
@@ -1336,11 +1342,12 @@ int dnsb_create(const dnsb_grid *gr, int device, void *stream, dnsb_ctx **out) {
   if (envint("DNSB_FFT4", 1) != 0) {
     int a = 0, b = 0;
     c->L4z = std::max(1, envint("DNSB_L4Z", 8));
+    c->rx_post = envint("DNSB_RXPOST", c->rx_post) != 0;
     if (fft4_split(M, a, b)) {
       c->x1 = a;
       c->x2 = b;
       const size_t pitch = b % 2 == 0 ? b + 1 : b;
-      c->smem_rx4 = sizeof(double2) * ((size_t)RFX_L * a * pitch + (size_t)RFX_L * (M + 1) + M + (M + 1));
+      c->smem_rx4 = sizeof(double2) * ((size_t)RFX_L * (a * pitch + 1) + (size_t)RFX_L * (M + 1) + M + (M + 1));
       c->smem_ix4 = sizeof(double2) * ((size_t)IRX_L * (M + 2) + (size_t)IRX_L * a * pitch + M + (M + 1));
     }
     if (fft4_split(nz, a, b)) {

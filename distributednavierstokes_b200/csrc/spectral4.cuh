@@ -43,7 +43,15 @@ __global__ void __launch_bounds__(F4_THREADS, 2) k_fftz4(Geo g, double2 *__restr
 // threads with batched loads, then transformed.  M = N1*N2 = nx/2.
 // 3 CTAs per SM (80 registers; the small spill costs less than the third
 // CTA gains: 0.377-0.384 ms against 0.392-0.398 ms at 2 CTAs, 384^2 x 256)
-template <int N1, int N2, int L, int INMODE>
+// POST: the second FFT pass forms the real-transform output X[k] (which
+// needs Z[k] and Z[M-k]) in registers and stores it, instead of writing Z
+// back to shared memory for a separate pass.  Its thread (line l, column
+// k1) holds Z[k1 + N1 k2], k2 = 0..N2-1; Z[M - k1 - N1 k2] is element
+// N2-1-k2 of column N1-k1, so columns k1 and N1-k1 share a warp (8 lines x
+// 4 columns per warp) and swap it with one shuffle; columns 0 and N1/2 are
+// their own partners.  The transpose buffer rows carry one pad value
+// (N1*P + 1 per line) so those 8 lines read distinct banks.
+template <int N1, int N2, int L, int INMODE, bool POST = false>
 __global__ void __launch_bounds__(F4_THREADS, 3) k_rfftx4(Geo g, double2 *__restrict__ S,
                                                           const double *__restrict__ in0,
                                                           const double *__restrict__ in1,
@@ -52,9 +60,11 @@ __global__ void __launch_bounds__(F4_THREADS, 3) k_rfftx4(Geo g, double2 *__rest
                                                           const double2 *__restrict__ twN) {
   constexpr int M = N1 * N2;
   constexpr int ls = M + 1;
+  constexpr int P = fft4_pitch<N2>();
+  constexpr int LS1 = N1 * P + 1;  // transpose-buffer stride per line
   extern __shared__ double2 smem[];
   double2 *buf = smem;
-  double2 *res = buf + fft4_buf<N1, N2>(L);
+  double2 *res = buf + L * LS1;
   double2 *tw = res + L * ls;
   double2 *tn = tw + M;
   const int ngrp = (g.nz + L - 1) / L;
@@ -103,6 +113,59 @@ __global__ void __launch_bounds__(F4_THREADS, 3) k_rfftx4(Geo g, double2 *__rest
         res[l * ls + m] = z;
       });
   __syncthreads();
+  if (POST) {
+    static_assert(!POST || (L == 8 && N1 % 4 == 0 && 8 * N1 <= F4_THREADS),
+                  "8 lines x 4 columns per warp");
+    // step 1: N1-point transforms of the stride-N2 subsequences
+    for (int it = threadIdx.x; it < L * N2; it += blockDim.x) {
+      const int l = it / N2, j2 = it - l * N2;
+      double2 v[N1];
+#pragma unroll
+      for (int j1 = 0; j1 < N1; j1++) v[j1] = res[l * ls + j1 * N2 + j2];
+      reg_fft<N1, false>(v, tw, N2);
+      double2 *row = buf + l * LS1 + j2;
+#pragma unroll
+      for (int k1 = 0; k1 < N1; k1++) row[k1 * P] = k1 == 0 ? v[0] : cmul(v[k1], tw[j2 * k1]);
+    }
+    __syncthreads();
+    // step 2 with the output pass, on N1/4 warps
+    if (threadIdx.x < 8 * N1) {
+      const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+      const int l = lane & 7, qd = lane >> 3;
+      const int a = 2 * w + (qd >> 1);
+      const int k1 = (w == 0 && qd == 1) ? N1 / 2 : ((qd & 1) ? N1 - a : a);
+      const bool self0 = k1 == 0, selfh = k1 == N1 / 2;
+      const double2 *col = buf + l * LS1 + k1 * P;
+      double2 v[N2];
+#pragma unroll
+      for (int j2 = 0; j2 < N2; j2++) v[j2] = col[j2];
+      reg_fft<N2, false>(v, tw, N1);
+      const int Lv = min(L, g.nz - k0);
+      const bool store = l < Lv;
+#pragma unroll
+      for (int k2 = 0; k2 < N2; k2++) {
+        const double2 mine = v[N2 - 1 - k2];
+        double2 other;
+        other.x = __shfl_xor_sync(0xffffffffu, mine.x, 8);
+        other.y = __shfl_xor_sync(0xffffffffu, mine.y, 8);
+        const double2 zm = self0 ? v[(N2 - k2) % N2] : (selfh ? mine : other);
+        const int kx = k1 + N1 * k2;
+        const double2 zk = v[k2], zc = cconj(zm);
+        const double2 e = make_double2(0.5 * (zk.x + zc.x), 0.5 * (zk.y + zc.y));
+        const double2 d = csub(zk, zc);
+        const double2 o = make_double2(0.5 * d.y, -0.5 * d.x);
+        if (store) S[sidx(g, kx, j, k0 + l)] = cadd(e, cmul(tn[kx], o));
+        if (self0 && k2 == 0 && store) {  // kx = M from Z[0]
+          const double2 z0c = cconj(zk);
+          const double2 e0 = make_double2(0.5 * (zk.x + z0c.x), 0.5 * (zk.y + z0c.y));
+          const double2 d0 = csub(zk, z0c);
+          const double2 o0 = make_double2(0.5 * d0.y, -0.5 * d0.x);
+          S[sidx(g, M, j, k0 + l)] = cadd(e0, cmul(tn[M], o0));
+        }
+      }
+    }
+    return;
+  }
   // step 1 reads res, step 2 (after the barrier inside) overwrites it
   fft4_lines<N1, N2, false>([&](int l, int m) { return res[l * ls + m]; },
                             [&](int l, int e, double2 v) { res[l * ls + e] = v; }, buf, L, tw);
