@@ -135,6 +135,7 @@ struct dnsb_ctx {
   // divergence x-FFT with its output pass in registers (3 % faster at
   // 384x256x384 than the separate shared-memory pass)
   int rx_post = 1;
+  int ix_pairs = 0;  // inverse x-FFT with the pair pre-processing in its first pass
   size_t smem_rx4 = 0, smem_ix4 = 0, smem_z4 = 0;
   int nsm = 148;
   size_t smem_zt = 0;
@@ -641,7 +642,8 @@ int launch_irfftx4(dnsb_ctx *c, int mode, double *out) {
     if (mode == ROUT_INTERIOR)                                                                     \
       LAUNCH(c, DNSB_KIND_IRFFTX, k_irfftx4<A, B, IRX_L, ROUT_INTERIOR><<<grid, F4_THREADS, c->smem_ix4, c->stream>>>(g, c->S, out, c->twM, c->twN)); \
     else if (mode == ROUT_IMAGES)                                                                  \
-      LAUNCH(c, DNSB_KIND_IRFFTX, k_irfftx4<A, B, IRX_L, ROUT_IMAGES><<<grid, F4_THREADS, c->smem_ix4, c->stream>>>(g, c->S, out, c->twM, c->twN)); \
+      { if (c->ix_pairs) LAUNCH(c, DNSB_KIND_IRFFTX, k_irfftx4<A, B, IRX_L, ROUT_IMAGES, true><<<grid, F4_THREADS, c->smem_ix4, c->stream>>>(g, c->S, out, c->twM, c->twN)); \
+        else LAUNCH(c, DNSB_KIND_IRFFTX, k_irfftx4<A, B, IRX_L, ROUT_IMAGES><<<grid, F4_THREADS, c->smem_ix4, c->stream>>>(g, c->S, out, c->twM, c->twN)); } \
     else                                                                                           \
       LAUNCH(c, DNSB_KIND_IRFFTX, k_irfftx4<A, B, IRX_L, ROUT_REAL><<<grid, F4_THREADS, c->smem_ix4, c->stream>>>(g, c->S, out, c->twM, c->twN)); \
     return 0;                                                                                      \
@@ -677,6 +679,7 @@ int allow_fft4(dnsb_ctx *c) {
       (rc = allow_smem(c, k_rfftx4<A, B, RFX_L, RIN_PRODUCT>, c->smem_rx4)) ||
       (rc = allow_smem(c, k_irfftx4<A, B, IRX_L, ROUT_INTERIOR>, c->smem_ix4)) ||
       (rc = allow_smem(c, k_irfftx4<A, B, IRX_L, ROUT_IMAGES>, c->smem_ix4)) ||
+      (rc = allow_smem(c, k_irfftx4<A, B, IRX_L, ROUT_IMAGES, true>, c->smem_ix4)) ||
       (rc = allow_smem(c, k_irfftx4<A, B, IRX_L, ROUT_REAL>, c->smem_ix4)) ||
       (rc = allow_smem(c, k_fftz4<A, B, false>, c->smem_z4)) ||
       (rc = allow_smem(c, k_fftz4<A, B, true>, c->smem_z4)))
@@ -1343,12 +1346,13 @@ int dnsb_create(const dnsb_grid *gr, int device, void *stream, dnsb_ctx **out) {
     int a = 0, b = 0;
     c->L4z = std::max(1, envint("DNSB_L4Z", 8));
     c->rx_post = envint("DNSB_RXPOST", c->rx_post) != 0;
+    c->ix_pairs = envint("DNSB_IXPAIRS", c->ix_pairs) != 0;
     if (fft4_split(M, a, b)) {
       c->x1 = a;
       c->x2 = b;
       const size_t pitch = b % 2 == 0 ? b + 1 : b;
       c->smem_rx4 = sizeof(double2) * ((size_t)RFX_L * (a * pitch + 1) + (size_t)RFX_L * (M + 1) + M + (M + 1));
-      c->smem_ix4 = sizeof(double2) * ((size_t)IRX_L * (M + 2) + (size_t)IRX_L * a * pitch + M + (M + 1));
+      c->smem_ix4 = sizeof(double2) * ((size_t)IRX_L * (M + 2) + (size_t)IRX_L * (a * pitch + 1) + M + (M + 1));
     }
     if (fft4_split(nz, a, b)) {
       c->z1 = a;

@@ -187,7 +187,13 @@ __global__ void __launch_bounds__(F4_THREADS, 3) k_rfftx4(Geo g, double2 *__rest
 // (row j, kz = k0..k0+L-1; Lv valid) of X are in zb (pitch M+2).  The pairs
 // (k, M-k) are pre-processed in place, then the four-step inverse writes
 // the field in its step 2 (OUTMODE as in k_irfftx).  Ends with a barrier.
-template <int N1, int N2, int OUTMODE>
+// PAIRS (L = 16, N2 % 4 == 0): the pre-processing runs inside the first
+// FFT pass instead of as a pass of its own.  Thread (line l, column j2)
+// needs X[j1 N2 + j2] and X[M - j1 N2 - j2], which is element N1-1-j1 of
+// column N2-j2; columns j2 and N2-j2 share a warp (8 lines x 4 columns) and
+// swap those values by shuffle; columns 0 and N2/2 are their own partners.
+// The transpose buffer then has N1*P + 1 values per line.
+template <int N1, int N2, int OUTMODE, bool PAIRS = false>
 __device__ __forceinline__ void irfftx4_tile(const Geo &g, double2 *zb, int L, int Lv, int j,
                                              int k0, double *__restrict__ out, double2 *buf,
                                              const double2 *tw, const double2 *tn) {
@@ -196,7 +202,7 @@ __device__ __forceinline__ void irfftx4_tile(const Geo &g, double2 *zb, int L, i
   // Z[k] = E[k] + i O[k], E = (X[k] + conj X[M-k])/2,
   // O = (X[k] - conj X[M-k]) conj(w^k)/2; one thread per pair (k, M-k)
   constexpr int half = M / 2 + 1;
-  for (int t = threadIdx.x; t < L * half; t += blockDim.x) {
+  for (int t = threadIdx.x; !PAIRS && t < L * half; t += blockDim.x) {
     const int l = t / half, k = t - l * half;
     double2 *X = zb + l * ls;
     if (k == 0) {
@@ -219,7 +225,6 @@ __device__ __forceinline__ void irfftx4_tile(const Geo &g, double2 *zb, int L, i
       }
     }
   }
-  __syncthreads();
   const double sc = 1.0 / M;
   const int J = j + 1;
   const bool row_edge = (J == 1) | (J >= g.ny - 1);
@@ -227,9 +232,7 @@ __device__ __forceinline__ void irfftx4_tile(const Geo &g, double2 *zb, int L, i
     const int K = k0 + l + 1;
     return row_edge | (K == 1) | (K == g.nz);
   };
-  fft4_lines<N1, N2, true>(
-      [&](int l, int e) { return zb[l * ls + e]; },
-      [&](int l, int m, double2 z) {
+  auto store = [&](int l, int m, double2 z) {
         if (l >= Lv) return;
         const double x0 = z.x * sc, x1 = z.y * sc;
         const int K = k0 + l + 1;
@@ -250,12 +253,71 @@ __device__ __forceinline__ void irfftx4_tile(const Geo &g, double2 *zb, int L, i
             store_images_core(out, g.nx, g.ny, g.nz, g.NX, g.NY, g.wall, 2 * m + 2, J, K, x1, STAG_P);
           }
         }
-      },
-      buf, L, tw);
+      };
+  if (!PAIRS) {
+    __syncthreads();
+    fft4_lines<N1, N2, true>([&](int l, int e) { return zb[l * ls + e]; }, store, buf, L, tw);
+    return;
+  }
+  static_assert(!PAIRS || N2 % 4 == 0, "columns in pairs, 4 per warp");
+  constexpr int P = fft4_pitch<N2>();
+  constexpr int LS1 = N1 * P + 1;
+  // step 1: 8 lines x 4 columns per warp, L/8 groups of N2/4 warps
+  for (int it = threadIdx.x; it < 8 * N2 * (L / 8); it += blockDim.x) {
+    const int lane = it & 31, w = it >> 5;
+    const int grp = w / (N2 / 4), wg = w - grp * (N2 / 4);
+    const int l = grp * 8 + (lane & 7), qd = lane >> 3;
+    const int a = 2 * wg + (qd >> 1);
+    const int j2 = (wg == 0 && qd == 1) ? N2 / 2 : ((qd & 1) ? N2 - a : a);
+    const bool self0 = j2 == 0, selfh = j2 == N2 / 2;
+    const double2 *X = zb + l * ls;
+    double2 x[N1];
+#pragma unroll
+    for (int j1 = 0; j1 < N1; j1++) x[j1] = X[j1 * N2 + j2];
+    const double2 xM = X[M];
+    double2 v[N1];
+#pragma unroll
+    for (int j1 = 0; j1 < N1; j1++) {
+      const double2 mine = x[N1 - 1 - j1];
+      double2 other;
+      other.x = __shfl_xor_sync(0xffffffffu, mine.x, 8);
+      other.y = __shfl_xor_sync(0xffffffffu, mine.y, 8);
+      const int k = j1 * N2 + j2;
+      const double2 a0 = x[j1];
+      if (self0 && j1 == 0) {  // k = 0 pairs with X[M]
+        v[0] = make_double2(0.5 * (a0.x + xM.x), 0.5 * (a0.x - xM.x));
+        continue;
+      }
+      const double2 b = self0 ? x[(N1 - j1) % N1] : (selfh ? mine : other);
+      const double2 bc = cconj(b);
+      const double2 e = cscale(cadd(a0, bc), 0.5);
+      const double2 o = cmul(cscale(csub(a0, bc), 0.5), cconj(tn[k]));
+      v[j1] = make_double2(e.x - o.y, e.y + o.x);
+    }
+    reg_fft<N1, true>(v, tw, N2);
+    double2 *row = buf + l * LS1 + j2;
+#pragma unroll
+    for (int k1 = 0; k1 < N1; k1++) row[k1 * P] = k1 == 0 ? v[0] : cmul(v[k1], cconj(tw[j2 * k1]));
+  }
+  __syncthreads();
+  // step 2 as in fft4_lines
+  for (int it = threadIdx.x; it < L * N1; it += blockDim.x) {
+    const int l = it / N1, k1 = it - l * N1;
+    double2 v[N2];
+    const double2 *col = buf + l * LS1 + k1 * P;
+#pragma unroll
+    for (int j2 = 0; j2 < N2; j2++) v[j2] = col[j2];
+    reg_fft<N2, true>(v, tw, N1);
+#pragma unroll
+    for (int k2 = 0; k2 < N2; k2++) store(l, k1 + N1 * k2, v[k2]);
+  }
+  __syncthreads();
 }
 
 // Inverse real FFT along x, one tile of L lines per CTA.
-template <int N1, int N2, int L, int OUTMODE>
+// PAIRS: the pair pre-processing inside the first FFT pass (irfftx4_tile),
+// where N2 % 4 == 0 and L % 8 == 0; elsewhere the separate pass.
+template <int N1, int N2, int L, int OUTMODE, bool PAIRS = false>
 __global__ void __launch_bounds__(F4_THREADS, 2) k_irfftx4(Geo g, const double2 *__restrict__ S,
                                                            double *__restrict__ out,
                                                            const double2 *__restrict__ twM,
@@ -265,7 +327,7 @@ __global__ void __launch_bounds__(F4_THREADS, 2) k_irfftx4(Geo g, const double2 
   extern __shared__ double2 smem[];
   double2 *zb = smem;
   double2 *buf = zb + L * ls;
-  double2 *tw = buf + fft4_buf<N1, N2>(L);
+  double2 *tw = buf + L * (N1 * fft4_pitch<N2>() + 1);
   double2 *tn = tw + M;
   const int ngrp = (g.nz + L - 1) / L;
   const int grp = blockIdx.x % ngrp;
@@ -285,7 +347,8 @@ __global__ void __launch_bounds__(F4_THREADS, 2) k_irfftx4(Geo g, const double2 
         zb[l * ls + kx] = v;
       });
   __syncthreads();
-  irfftx4_tile<N1, N2, OUTMODE>(g, zb, L, Lv, j, k0, out, buf, tw, tn);
+  irfftx4_tile<N1, N2, OUTMODE, PAIRS && N2 % 4 == 0 && L % 8 == 0>(g, zb, L, Lv, j, k0, out,
+                                                                      buf, tw, tn);
 }
 
 }  // namespace dnsb

@@ -323,14 +323,17 @@ def test_fused_projection_momentum_planes(oracle_mod, D, cfg, planes, pipe, monk
     assert rel(N(pd), p) <= 1e-10
 
 
-@pytest.mark.parametrize("post", ["1", "0"])
+@pytest.mark.parametrize("post,pairs", [("1", "0"), ("0", "0"), ("1", "1")])
 @pytest.mark.parametrize("nx", [64, 384])
-def test_rfftx_output_pass_in_registers(oracle_mod, D, nx, post, monkeypatch):
+def test_rfftx_output_pass_in_registers(oracle_mod, D, nx, post, pairs, monkeypatch):
     """The divergence x-FFT with its output pass in registers (the default)
-    and with the separate shared-memory pass (DNSB_RXPOST=0), at the splits
-    8 x 4 and 16 x 12; nz = 12 leaves a short last group of lines: Poisson
-    solve, projection and one step agree with the oracle."""
+    and with the separate shared-memory pass (DNSB_RXPOST=0), and the
+    inverse x-FFT with its pair pre-processing inside the first FFT pass
+    (DNSB_IXPAIRS=1), at the splits 8 x 4 and 16 x 12; nz = 12 leaves a
+    short last group of lines: Poisson solve, projection and one step agree
+    with the oracle."""
     monkeypatch.setenv("DNSB_RXPOST", post)
+    monkeypatch.setenv("DNSB_IXPAIRS", pairs)
     kw = dict(n=(nx, 8, 12), lims=((0, 4 * math.pi), (-1, 1), (0, 4 * math.pi / 3)),
               bc=("periodic", "wall", "periodic"), stretch=R.tanhstretch(1.5),
               visc=1 / 395, bodyforce=(1.0, 0.0, 0.0), ydiffusion="implicit")
