@@ -240,12 +240,16 @@ def reference_arm(args, wl, world, rank):
     # a bounded sample: at most REF_MAX_STEPS full-grid steps are timed (about
     # 2 s each on 16 host cores), so that any --steps K finishes in minutes
     n_run = max(1, min(args.steps, REF_MAX_STEPS))
+    n_warm = min(args.warmup, 1)
     per = []
-    secs, threads, _ = cpu_oracle_run(wl, n_run, min(args.warmup, 1), per_step=per)
+    secs, threads, _ = cpu_oracle_run(wl, n_run, n_warm, per_step=per)
     value = cells * n_run / secs
+    # "steps" / "warmup" are the counts this run executed (a bounded sample of
+    # the requested ones, which are reported beside them)
     line = {
         "metric": "DNS cell-steps/s (FP64)", "impl": "reference", "value": value,
-        "unit": "cell-steps/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "unit": "cell-steps/s", "n_gpus": args.gpus, "steps": n_run, "warmup": n_warm,
+        "requested": {"steps": args.steps, "warmup": args.warmup},
         "ms_per_step": 1e3 * secs / n_run, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": args.workload, "grid": list(wl["n"]),

@@ -39,6 +39,7 @@ SIGNATURES = {
     "dnsb_last_error": (ctypes.c_char_p, [P]),
     "dnsb_set_stream": (c_int, [P, P]),
     "dnsb_sync": (c_int, [P]),
+    "dnsb_set_wait_limit": (c_int, [P, ctypes.c_ulong]),
     "dnsb_fill_ghosts": (c_int, [P, P, c_int]),
     "dnsb_divergence": (c_int, [P, P, P, P, P]),
     "dnsb_momentum": (c_int, [P, P, P, P, P, P, P, c_double, c_double]),

@@ -1,0 +1,613 @@
+// cnn.cuh -- tensor-core kernels of the sub-filter-stress CNN closure.
+//
+// The network (no counterpart in the reference, which has no learned
+// closure): 4 layers of 3x3x3 convolutions, channels 3 -> 32 -> 32 -> 32 ->
+// 6, bias, exact GELU after the first three, periodic padding on the full
+// field.  Every convolution is an implicit GEMM on the 5th-generation tensor
+// cores: BF16 operands staged in shared memory by TMA, FP32 accumulators in
+// tensor memory (tcgen05.mma, cta_group::1, M = 128), read back with
+// tcgen05.ld for a fused epilogue.
+//
+// Activation layout ("chunked voxels"): a volume of P x P x Pz voxels per
+// sample; channels in chunks of 8 BF16 values (16 bytes); element
+// [b][chunk][z][y][x][8].  Every layer of a network lives in the same
+// geometry (same P, Pz): layer L's output occupies the box [0, Do)^3, Do =
+// P - 2L, and the input voxel of output (x, y, z) for tap (dx, dy, dz) is
+// (x + s + dx, y + s + dy, z + s + dz) with s = 0 (forward, "valid"
+// convolution) or s = -2 (the transposed convolution of the backward pass;
+// the box of the input is surrounded by zeros).  Voxels outside an output's
+// box hold zeros: the buffers are cleared once and every kernel writes zeros
+// at the positions of its tiles that are outside the box.
+//
+// Forward / transposed convolution (k_conv): one tile = 128 consecutive
+// positions f = y*P + x of one plane of one sample (rows of the GEMM).  With
+// the input patch of that tile staged as whole rows [chunk][dz][row][x][16 B]
+// (one 5-D TMA box: 8 channels x P x R rows x 3 planes x CI chunks), the 128
+// GEMM rows of every tap are 128 consecutive 16-byte rows of the patch:
+// tap (dx, dy, dz) starts at patch offset x0 + s + dx + (dy + e) P, e = 1 for
+// s < 0 (one extra row below the tile so that offsets stay >= 0).  So the A
+// operand of each tap is a K-major canonical layout without swizzle (8-row
+// core matrices of 128 contiguous bytes, SBO = 128 B, LBO = the chunk
+// stride), addressed by its start alone: no im2col copy.  Positions with
+// x >= Do inside a row compute garbage that the epilogue replaces by zeros.
+// B (the weights, N = output channels) is resident in shared memory for the
+// whole persistent CTA, packed in the K-major core-matrix order.
+//
+// Weight gradient (k_wgrad): D[(tap slot j, ci)][co] = sum_o h[o + t_j][ci]
+// g[o][co] over the output positions o (the GEMM's K).  Both operands are
+// MN-major canonical layouts without swizzle, straight from the chunked
+// activations: a K-block of 64 positions of one plane is one TMA box
+// [chunk][64][16 B] per tap; 128 / (8 CI) taps fill the 128 rows (the slot
+// after the last real tap holds ones, which makes that row the bias
+// gradient).  Split-K partials are reduced in a fixed order.
+//
+// Warp roles of both kernels (192 threads): warp 0 issues the TMA copies,
+// warp 1 owns the tensor memory and issues the MMAs (one thread), warps 2-5
+// run the epilogue (warp w reads TMEM lanes 32 (w % 4) .. + 31).  Every
+// mbarrier wait is bounded; a wait that runs out raises the CTA's abort flag
+// and the global error word, every role leaves its loop, the copies and MMAs
+// in flight are waited for (bounded), the tensor memory is freed and the CTA
+// returns.
+#pragma once
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace dnsb {
+namespace cnn {
+
+constexpr int NTHREADS = 192;
+constexpr int NTAPS = 27;
+constexpr int TILE_M = 128;
+constexpr int WG_K = 64;          // positions per weight-gradient K-block
+constexpr int WG_STAGES = 4;
+constexpr int CV_STAGES = 2;
+enum { DEVERR_CNN_TIMEOUT = 2 };
+
+enum Mode { FWD_GELU = 0, FWD_LOSS = 1, FWD_INFER = 2, DGRAD = 3 };
+
+// ----------------------------------------------------------- PTX helpers --
+
+__device__ __forceinline__ uint32_t saddr(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mb_init(uint64_t *b, uint32_t n) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(saddr(b)), "r"(n) : "memory");
+}
+__device__ __forceinline__ void mb_expect(uint64_t *b, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(saddr(b)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void mb_arrive(uint64_t *b) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(saddr(b)) : "memory");
+}
+__device__ __forceinline__ bool mb_try(uint64_t *b, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(saddr(b)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// bounded wait; gives up early once the CTA's abort flag is raised
+__device__ __forceinline__ bool mb_wait(uint64_t *b, uint32_t parity, unsigned limit,
+                                        volatile int *abort_flag) {
+  for (unsigned it = 0; it < limit; it++) {
+    if (mb_try(b, parity)) return true;
+    if ((it & 255) == 255 && *abort_flag) return false;
+  }
+  return false;
+}
+__device__ __forceinline__ void tma5(void *dst, const CUtensorMap *m, int c0, int c1, int c2, int c3,
+                                     int c4, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(
+          saddr(dst)),
+      "l"(m), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(saddr(bar))
+      : "memory");
+}
+__device__ __forceinline__ void tma4(void *dst, const CUtensorMap *m, int c0, int c1, int c2, int c3,
+                                     uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(
+          saddr(dst)),
+      "l"(m), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(saddr(bar))
+      : "memory");
+}
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          saddr(dst)),
+      "l"(src), "r"(bytes), "r"(saddr(bar))
+      : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+// shared-memory matrix descriptor, no swizzle (layout type 0), version 1
+__device__ __forceinline__ uint64_t sdesc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46);
+}
+// instruction descriptor of kind::f16: BF16 x BF16 -> FP32, M = 128
+__host__ __device__ constexpr uint32_t idesc_bf16(int n, bool a_mn, bool b_mn) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((a_mn ? 1u : 0u) << 15) | ((b_mn ? 1u : 0u) << 16) |
+         ((uint32_t)(n >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+}
+__device__ __forceinline__ void mma_bf16(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc,
+                                         uint32_t accumulate) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(
+          d),
+      "l"(a), "l"(b), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+__device__ __forceinline__ void mma_commit(uint64_t *bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                   saddr(bar))
+               : "memory");
+}
+__device__ __forceinline__ void tmem_alloc(uint32_t *slot, uint32_t ncols) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(saddr(slot)),
+               "r"(ncols)
+               : "memory");
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_free(uint32_t taddr, uint32_t ncols) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols)
+               : "memory");
+}
+// 32 lanes x N columns of FP32 (this warp's lane quarter), into v[0..N)
+template <int N>
+__device__ __forceinline__ void tmem_ld(uint32_t taddr, float *v);
+template <>
+__device__ __forceinline__ void tmem_ld<16>(uint32_t taddr, float *v) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
+}
+template <>
+__device__ __forceinline__ void tmem_ld<32>(uint32_t taddr, float *v) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]),
+        "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]),
+        "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 32; i++) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ float gelu_f(float z) {
+  return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f));
+}
+__device__ __forceinline__ float gelu_grad_f(float z) {
+  return 0.5f * (1.0f + erff(z * 0.70710678118654752f)) +
+         z * expf(-0.5f * z * z) * 0.39894228040143268f;
+}
+
+__device__ __forceinline__ uint4 pack8(const float *v) {
+  uint4 o;
+  __nv_bfloat162 t;
+  t = __floats2bfloat162_rn(v[0], v[1]);
+  o.x = *reinterpret_cast<uint32_t *>(&t);
+  t = __floats2bfloat162_rn(v[2], v[3]);
+  o.y = *reinterpret_cast<uint32_t *>(&t);
+  t = __floats2bfloat162_rn(v[4], v[5]);
+  o.z = *reinterpret_cast<uint32_t *>(&t);
+  t = __floats2bfloat162_rn(v[6], v[7]);
+  o.w = *reinterpret_cast<uint32_t *>(&t);
+  return o;
+}
+__device__ __forceinline__ void unpack8(uint4 q, float *v) {
+  const uint32_t w[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    v[2 * i] = __uint_as_float(w[i] << 16);
+    v[2 * i + 1] = __uint_as_float(w[i] & 0xFFFF0000u);
+  }
+}
+
+// ------------------------------------------------------------ geometry --
+
+struct ConvArgs {
+  int P, Pz, B;        // volume pitch (x, y), planes, samples
+  int Do;              // output box side
+  int s, e, R;         // input offset (0 / -2), extra patch row, patch rows
+  int tpp;             // tiles per plane: ceil(Do * P / 128)
+  int ntiles;          // B * Do * tpp
+  uint32_t stage_bytes;  // CI * 3 * R * P * 16
+  uint32_t w_bytes;      // 27 * CI * CO * 128
+  unsigned wait_limit;
+  const uint4 *wpack;    // packed weights (B operand), w_bytes
+  const float *bias;     // Cout values (forward modes)
+  uint4 *out;            // [b][CO][Pz][P^2] x 16 B (FWD_GELU, FWD_LOSS, DGRAD)
+  uint4 *zout;           // FWD_GELU: the pre-activation, same layout
+  const uint4 *zin;      // DGRAD: the pre-activation of the output's layer
+  const float4 *target;  // FWD_LOSS: [b][Pz][P^2][8] floats
+  float loss_scale;      // FWD_LOSS: 2 / count
+  float *loss_part;      // FWD_LOSS: one partial sum per CTA
+  double *infer_out;     // FWD_INFER: 6 arrays of Do^3 values ([z][y][x])
+  const float *oscale;   // FWD_INFER: per-component output scale
+  int *err;
+};
+
+// Forward / transposed convolution, CI input chunks, CO output chunks
+// (N = 8 CO GEMM columns), persistent over tiles.
+template <int CI, int CO, int MODE>
+__global__ void __launch_bounds__(NTHREADS, 1)
+    k_conv(const __grid_constant__ CUtensorMap tin, const ConvArgs a) {
+  constexpr int N = 8 * CO;
+  constexpr uint32_t NCOLS = 2 * N < 32 ? 32 : 2 * N;  // two accumulators
+  extern __shared__ __align__(1024) unsigned char smem[];
+  unsigned char *wsm = smem;
+  unsigned char *stg = smem + a.w_bytes;
+  uint64_t *bars = reinterpret_cast<uint64_t *>(stg + CV_STAGES * a.stage_bytes);
+  uint64_t *full = bars, *empty = bars + 2, *tfull = bars + 4, *tempty = bars + 6, *wbar = bars + 8;
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + 9);
+  volatile int *abort_flag = reinterpret_cast<volatile int *>(bars + 10);
+  float *lsum = reinterpret_cast<float *>(bars + 11);  // 4 floats
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < 2; i++) {
+      mb_init(&full[i], 1);
+      mb_init(&empty[i], 1);
+      mb_init(&tfull[i], 1);
+      mb_init(&tempty[i], 4);
+    }
+    mb_init(wbar, 1);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) tmem_alloc(tslot, NCOLS);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tbase = *tslot;
+  const int P2 = a.P * a.P;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      // weights once, then the patch of every tile
+      mb_expect(wbar, a.w_bytes);
+      bulk_load(wsm, a.wpack, a.w_bytes, wbar);
+      int i = 0, last_s = -1, last_ph = 0, prev_s = -1, prev_ph = 0;
+      for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x, i++) {
+        const int s = i & 1, ph = (i >> 1) & 1;
+        if (*abort_flag || !mb_wait(&empty[s], ph ^ 1, a.wait_limit, abort_flag)) {
+          *abort_flag = 1;
+          atomicExch(a.err, DEVERR_CNN_TIMEOUT);
+          break;
+        }
+        const int j = t % a.tpp, rest = t / a.tpp;
+        const int z = rest % a.Do, b = rest / a.Do;
+        const int f0 = j * TILE_M, y0 = f0 / a.P;
+        mb_expect(&full[s], a.stage_bytes);
+        tma5(stg + s * a.stage_bytes, &tin, 0, 0, y0 + a.s - a.e, z + a.s, b * CI, &full[s]);
+        prev_s = last_s;
+        prev_ph = last_ph;
+        last_s = s;
+        last_ph = ph;
+      }
+      // the copies issued last land before the CTA may leave
+      if (last_s >= 0) mb_wait(&full[last_s], last_ph, a.wait_limit, abort_flag);
+      if (prev_s >= 0) mb_wait(&full[prev_s], prev_ph, a.wait_limit, abort_flag);
+      mb_wait(wbar, 0, a.wait_limit, abort_flag);
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      constexpr uint32_t idesc = idesc_bf16(N, false, false);
+      const uint32_t wb = saddr(wsm);
+      const uint32_t plane = (uint32_t)a.R * a.P * 16;
+      const uint32_t cstride = 3 * plane;
+      int i = 0, last_a = -1, last_aph = 0;
+      bool ok = mb_wait(wbar, 0, a.wait_limit, abort_flag);
+      for (int t = blockIdx.x; ok && t < a.ntiles; t += gridDim.x, i++) {
+        const int s = i & 1, ph = (i >> 1) & 1;
+        const int ac = i & 1, aph = (i >> 1) & 1;
+        if (*abort_flag || !mb_wait(&tempty[ac], aph ^ 1, a.wait_limit, abort_flag) ||
+            !mb_wait(&full[s], ph, a.wait_limit, abort_flag)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const int j = t % a.tpp;
+        const int x0 = (j * TILE_M) % a.P;
+        const uint32_t sb = saddr(stg + s * a.stage_bytes);
+        const uint32_t dacc = tbase + (uint32_t)(ac * N);
+#pragma unroll 1
+        for (int tap = 0; tap < NTAPS; tap++) {
+          const int dz = tap / 9, dy = (tap / 3) % 3, dx = tap % 3;
+          const uint32_t off = (uint32_t)(x0 + a.s + dx + (dy + a.e) * a.P) * 16u;
+#pragma unroll
+          for (int k = 0; k < CI / 2; k++) {
+            const uint64_t ad = sdesc(sb + (uint32_t)(2 * k) * cstride + dz * plane + off, cstride, 128);
+            const uint64_t bd = sdesc(wb + (uint32_t)((tap * CI + 2 * k) * CO) * 128u, CO * 128u, 128);
+            mma_bf16(dacc, ad, bd, idesc, (tap | k) != 0);
+          }
+        }
+        mma_commit(&empty[s]);
+        mma_commit(&tfull[ac]);
+        last_a = ac;
+        last_aph = aph;
+      }
+      if (!ok) {
+        *abort_flag = 1;
+        atomicExch(a.err, DEVERR_CNN_TIMEOUT);
+      }
+      // the MMAs issued last complete before the tensor memory is freed
+      if (last_a >= 0) mb_wait(&tfull[last_a], last_aph, a.wait_limit, abort_flag);
+    }
+  } else {
+    // epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31
+    const int q = warp & 3;
+    const int m = q * 32 + lane;
+    float lacc = 0.f;
+    int i = 0;
+    for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x, i++) {
+      const int ac = i & 1, aph = (i >> 1) & 1;
+      if (*abort_flag || !mb_wait(&tfull[ac], aph, a.wait_limit, abort_flag)) {
+        *abort_flag = 1;
+        atomicExch(a.err, DEVERR_CNN_TIMEOUT);
+        break;
+      }
+      tc_fence_after();
+      float v[N];
+      tmem_ld<N>(tbase + ((uint32_t)(q * 32) << 16) + (uint32_t)(ac * N), v);
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mb_arrive(&tempty[ac]);
+      const int j = t % a.tpp, rest = t / a.tpp;
+      const int z = rest % a.Do, b = rest / a.Do;
+      const int f = j * TILE_M + m;
+      if (f >= P2) continue;
+      const int x = f % a.P, y = f / a.P;
+      const bool valid = x < a.Do && y < a.Do;
+      const long long vox = (long long)z * P2 + f;
+      if (MODE == FWD_GELU) {
+#pragma unroll
+        for (int c = 0; c < CO; c++) {
+          float zv[8], hv[8];
+#pragma unroll
+          for (int k = 0; k < 8; k++) {
+            const float zz = valid ? v[8 * c + k] + __ldg(a.bias + 8 * c + k) : 0.f;
+            zv[k] = zz;
+            hv[k] = valid ? gelu_f(zz) : 0.f;
+          }
+          const long long o = ((long long)(b * CO + c) * a.Pz) * P2 + vox;
+          a.zout[o] = pack8(zv);
+          a.out[o] = pack8(hv);
+        }
+      } else if (MODE == FWD_LOSS) {
+        // 6 output components in chunk 0 (N = 16: chunk 1 stays zero)
+        float tv[8];
+        if (valid) {
+          const float4 *tp = a.target + ((long long)b * a.Pz * P2 + vox) * 2;
+          const float4 t0 = tp[0], t1 = tp[1];
+          tv[0] = t0.x; tv[1] = t0.y; tv[2] = t0.z; tv[3] = t0.w;
+          tv[4] = t1.x; tv[5] = t1.y; tv[6] = 0.f; tv[7] = 0.f;
+        }
+        float gv[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+          float g = 0.f;
+          if (valid && k < 6) {
+            const float d = v[k] + __ldg(a.bias + k) - tv[k];
+            lacc += d * d;
+            g = a.loss_scale * d;
+          }
+          gv[k] = g;
+        }
+        const long long o = ((long long)(b * CO) * a.Pz) * P2 + vox;
+        a.out[o] = pack8(gv);
+      } else if (MODE == FWD_INFER) {
+        if (valid) {
+          const long long n3 = (long long)a.Do * a.Do * a.Do;
+          const long long o = ((long long)z * a.Do + y) * a.Do + x;
+#pragma unroll
+          for (int k = 0; k < 6; k++)
+            a.infer_out[k * n3 + o] = (double)((v[k] + __ldg(a.bias + k)) * __ldg(a.oscale + k));
+        }
+      } else {  // DGRAD: g = dL/dh * gelu'(z) of the output's layer
+#pragma unroll
+        for (int c = 0; c < CO; c++) {
+          const long long o = ((long long)(b * CO + c) * a.Pz) * P2 + vox;
+          float gv[8];
+          if (valid) {
+            float zv[8];
+            unpack8(a.zin[o], zv);
+#pragma unroll
+            for (int k = 0; k < 8; k++) gv[k] = v[8 * c + k] * gelu_grad_f(zv[k]);
+          } else {
+#pragma unroll
+            for (int k = 0; k < 8; k++) gv[k] = 0.f;
+          }
+          a.out[o] = pack8(gv);
+        }
+      }
+    }
+    if (MODE == FWD_LOSS) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) lacc += __shfl_xor_sync(0xffffffffu, lacc, o);
+      if (lane == 0) lsum[warp - 2] = lacc;
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (MODE == FWD_LOSS && threadIdx.x == 0)
+    a.loss_part[blockIdx.x] = (lsum[0] + lsum[1]) + (lsum[2] + lsum[3]);
+  if (warp == 1) {
+    tc_fence_after();
+    tmem_free(tbase, NCOLS);
+  }
+}
+
+// ------------------------------------------------------ weight gradient --
+
+struct WgradArgs {
+  int P, Pz, B;     // volume geometry
+  int Do;           // output box side (of g)
+  int kpp;          // K-blocks per plane: ceil(Do * P / 64)
+  int nk;           // B * Do * kpp
+  int ngroups;      // ceil(27 / G) tap groups
+  int nsplit;       // K splits (grid = ngroups * nsplit)
+  int ones_slot;    // slot of the last group holding ones (bias row)
+  uint32_t a_bytes, stage_bytes;
+  unsigned wait_limit;
+  float *partial;   // [split][group][128][N]
+  int *err;
+};
+
+// h: CI chunks (A operand, tap-shifted), g: CO chunks (B operand).
+template <int CI, int CO>
+__global__ void __launch_bounds__(NTHREADS, 1)
+    k_wgrad(const __grid_constant__ CUtensorMap th, const __grid_constant__ CUtensorMap tg,
+            const WgradArgs a) {
+  constexpr int N = 8 * CO;
+  constexpr int G = 16 / CI;             // tap slots per group (M = 128 rows)
+  constexpr uint32_t NCOLS = N < 32 ? 32 : N;
+  constexpr uint32_t SLOT = CI * WG_K * 16;  // bytes of one tap slot
+  extern __shared__ __align__(1024) unsigned char smem[];
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem + WG_STAGES * a.stage_bytes);
+  uint64_t *full = bars, *empty = bars + WG_STAGES, *done = bars + 2 * WG_STAGES;
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + 2 * WG_STAGES + 1);
+  volatile int *abort_flag = reinterpret_cast<volatile int *>(bars + 2 * WG_STAGES + 2);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int grp = blockIdx.x % a.ngroups, split = blockIdx.x / a.ngroups;
+  const int tap0 = grp * G;
+  const int ntap = min(G, NTAPS - tap0);
+  const bool ones = grp == a.ngroups - 1 && a.ones_slot < G;
+  const int k0 = (int)((long long)a.nk * split / a.nsplit);
+  const int k1 = (int)((long long)a.nk * (split + 1) / a.nsplit);
+
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < WG_STAGES; i++) {
+      mb_init(&full[i], 1);
+      mb_init(&empty[i], 1);
+    }
+    mb_init(done, 1);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (ones) {
+    // the slot after the last tap: BF16 ones, in every stage, never copied over
+    const uint32_t one2 = 0x3F803F80u;
+    for (int st = 0; st < WG_STAGES; st++) {
+      uint32_t *p = reinterpret_cast<uint32_t *>(smem + st * a.stage_bytes + a.ones_slot * SLOT);
+      for (int i = threadIdx.x; i < (int)(SLOT / 4); i += NTHREADS) p[i] = one2;
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  if (warp == 1) tmem_alloc(tslot, NCOLS);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tbase = *tslot;
+  const int P2 = a.P * a.P;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      const uint32_t bytes = (uint32_t)ntap * SLOT + (uint32_t)CO * WG_K * 16;
+      int i = 0, issued = 0;
+      for (int k = k0; k < k1; k++, i++) {
+        const int s = i % WG_STAGES, ph = (i / WG_STAGES) & 1;
+        if (*abort_flag || !mb_wait(&empty[s], ph ^ 1, a.wait_limit, abort_flag)) {
+          *abort_flag = 1;
+          atomicExch(a.err, DEVERR_CNN_TIMEOUT);
+          break;
+        }
+        const int jb = k % a.kpp, rest = k / a.kpp;
+        const int z = rest % a.Do, b = rest / a.Do;
+        const int f0 = jb * WG_K;
+        unsigned char *st = smem + s * a.stage_bytes;
+        mb_expect(&full[s], bytes);
+        for (int j = 0; j < ntap; j++) {
+          const int tap = tap0 + j;
+          const int dz = tap / 9, dy = (tap / 3) % 3, dx = tap % 3;
+          tma4(st + j * SLOT, &th, 0, f0 + dx + dy * a.P, z + dz, b * CI, &full[s]);
+        }
+        tma4(st + a.a_bytes, &tg, 0, f0, z, b * CO, &full[s]);
+        issued = i + 1;
+      }
+      // let the last copies of every stage land before leaving
+      for (int i2 = issued - WG_STAGES < 0 ? 0 : issued - WG_STAGES; i2 < issued; i2++)
+        mb_wait(&full[i2 % WG_STAGES], (i2 / WG_STAGES) & 1, a.wait_limit, abort_flag);
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      constexpr uint32_t idesc = idesc_bf16(N, true, true);
+      int i = 0;
+      bool ok = true, any = false;
+      for (int k = k0; k < k1; k++, i++) {
+        const int s = i % WG_STAGES, ph = (i / WG_STAGES) & 1;
+        if (*abort_flag || !mb_wait(&full[s], ph, a.wait_limit, abort_flag)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t sa = saddr(smem + s * a.stage_bytes);
+        const uint32_t sb = sa + a.a_bytes;
+#pragma unroll
+        for (int kk = 0; kk < WG_K / 16; kk++) {
+          // MN-major, no swizzle: SBO = stride of 8-element MN groups (1 KB),
+          // LBO = stride of 8-row K groups (128 B)
+          const uint64_t ad = sdesc(sa + kk * 256, 128, WG_K * 16);
+          const uint64_t bd = sdesc(sb + kk * 256, 128, WG_K * 16);
+          mma_bf16(tbase, ad, bd, idesc, (i | kk) != 0);
+        }
+        mma_commit(&empty[s]);
+        any = true;
+      }
+      if (!ok) {
+        *abort_flag = 1;
+        atomicExch(a.err, DEVERR_CNN_TIMEOUT);
+      }
+      if (any) mma_commit(done);
+      else mb_arrive(done);
+    }
+  } else {
+    const int q = warp & 3;
+    const int m = q * 32 + lane;
+    const bool ok = mb_wait(done, 0, a.wait_limit, abort_flag) && !*abort_flag;
+    if (!ok) {
+      *abort_flag = 1;
+      atomicExch(a.err, DEVERR_CNN_TIMEOUT);
+    }
+    tc_fence_after();
+    float v[N];
+    tmem_ld<N>(tbase + ((uint32_t)(q * 32) << 16), v);
+    float *dst = a.partial + (((long long)split * a.ngroups + grp) * 128 + m) * N;
+    const bool empty_range = k1 <= k0;
+#pragma unroll
+    for (int c = 0; c < N; c += 4)
+      *reinterpret_cast<float4 *>(dst + c) =
+          empty_range || !ok ? make_float4(0.f, 0.f, 0.f, 0.f)
+                             : make_float4(v[c], v[c + 1], v[c + 2], v[c + 3]);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    tmem_free(tbase, NCOLS);
+  }
+}
+
+}  // namespace cnn
+}  // namespace dnsb

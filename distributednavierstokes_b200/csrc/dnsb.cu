@@ -126,6 +126,7 @@ struct dnsb_ctx {
   double2 *cube = nullptr;             // LES cubes of the filtered-field sampler
   size_t cube_cap = 0;
   int *deverr = nullptr;               // device-side error word (bounded waits)
+  unsigned wait_limit = DNSB_WAIT_LIMIT;  // polls per device-side wait
   int use_tma = 1;                     // persistent TMA-pipelined z-FFT
   int zyz_c = 0;                       // CTAs per cluster of k_zyz (0: three kernels)
   int zyz_mode = 1;                    // 1: k_zyz (32-row chunks), 2: k_zyz2 (16-row chunks)
@@ -717,8 +718,8 @@ int launch_fftz(dnsb_ctx *c, bool inv) {
   if (c->use_tma) {
     const long long ngroups = (nlines + c->Lz - 1) / c->Lz;
     dim3 grid((unsigned)std::min<long long>(ngroups, 2LL * c->nsm));
-    if (inv) LAUNCH(c, DNSB_KIND_IFFTZ, k_fftz_tma<true><<<grid, SPEC_THREADS, c->smem_zt, c->stream>>>(g, c->S, c->pz, c->Lz, c->twz, c->deverr));
-    else LAUNCH(c, DNSB_KIND_FFTZ, k_fftz_tma<false><<<grid, SPEC_THREADS, c->smem_zt, c->stream>>>(g, c->S, c->pz, c->Lz, c->twz, c->deverr));
+    if (inv) LAUNCH(c, DNSB_KIND_IFFTZ, k_fftz_tma<true><<<grid, SPEC_THREADS, c->smem_zt, c->stream>>>(g, c->S, c->pz, c->Lz, c->twz, c->deverr, c->wait_limit));
+    else LAUNCH(c, DNSB_KIND_FFTZ, k_fftz_tma<false><<<grid, SPEC_THREADS, c->smem_zt, c->stream>>>(g, c->S, c->pz, c->Lz, c->twz, c->deverr, c->wait_limit));
     return 0;
   }
   dim3 grid((unsigned)((nlines + c->Lz - 1) / c->Lz));
@@ -1465,6 +1466,12 @@ void dnsb_destroy(dnsb_ctx *c) {
 int dnsb_set_stream(dnsb_ctx *c, void *stream) {
   if (!c) return DNSB_EINVAL;
   c->stream = (cudaStream_t)stream;
+  return 0;
+}
+
+int dnsb_set_wait_limit(dnsb_ctx *c, unsigned long polls) {
+  if (!c) return DNSB_EINVAL;
+  c->wait_limit = polls == 0 ? 0u : (unsigned)std::min<unsigned long>(polls, 0xffffffffUL);
   return 0;
 }
 
@@ -2562,24 +2569,36 @@ static_assert(kNoAllocBytes < (28LL << 20), "the fixed scratch stays modest (abo
 
 __device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
 
-// host staging for the per-call tables (static: the entry point allocates
-// nothing, host or device; overlapping calls race anyway)
+// Host staging for the tables and, per device, the grid whose tables the
+// device copy holds (static: the entry point allocates nothing, host or
+// device).  g_noalloc_mu serialises the set-up and the table uploads of
+// all host threads; the kernels are enqueued outside it.
 double h_tab[4 * (kNoAllocMaxN + 2) + 6 * kNoAllocMaxN];
 double2 h_tw[3 * kNoAllocMaxN + 1];
 
 constexpr int kMaxDevices = 64;
-double *g_noalloc_ptr[kMaxDevices] = {};
+struct NoAllocDev {
+  void *ptr;        // device address of g_noalloc_scratch (attributes set for it)
+  bool have_grid;   // the device tables hold the grid below
+  int nx, ny, nz, bc;
+  double dx, dz;
+  double dy[kNoAllocMaxN + 2], dyu[kNoAllocMaxN + 2];
+};
+NoAllocDev g_noalloc_dev[kMaxDevices];
+std::mutex g_noalloc_mu;
 
-// once per device, with that device current: the device address of the
-// scratch array (in host code the symbol is only a stand-in) and the
-// shared-memory limits of the kernels used
+// With g_noalloc_mu held and device dev current: the device address of the
+// scratch array (in host code the symbol is only a stand-in), resolved on
+// every call so that a reset device gets its new address, and the
+// shared-memory limits of the kernels used, set again when it changes.
 int noalloc_setup(int dev, double **out) {
   if (dev < 0 || dev >= kMaxDevices) return fail(nullptr, DNSB_EUNSUP, "device index %d out of range", dev);
-  if (!g_noalloc_ptr[dev]) {
-    void *ptr = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
-    if (e != cudaSuccess || !ptr)
-      return fail(nullptr, DNSB_ECUDA, "cudaGetSymbolAddress(scratch): %s", cudaGetErrorString(e));
+  void *ptr = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+  if (e != cudaSuccess || !ptr)
+    return fail(nullptr, DNSB_ECUDA, "cudaGetSymbolAddress(scratch): %s", cudaGetErrorString(e));
+  NoAllocDev &d = g_noalloc_dev[dev];
+  if (d.ptr != ptr) {
     const int big = 200 * 1024;
     cudaError_t a = cudaSuccess;
     a = a != cudaSuccess ? a : raise_smem(dev, k_rfftx<RIN_REAL>, big);
@@ -2589,10 +2608,20 @@ int noalloc_setup(int dev, double **out) {
     a = a != cudaSuccess ? a : raise_smem(dev, k_irfftx<ROUT_INTERIOR>, big);
     if (a != cudaSuccess)
       return fail(nullptr, DNSB_ECUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(a));
-    g_noalloc_ptr[dev] = (double *)ptr;
+    d.ptr = ptr;
+    d.have_grid = false;  // a new address: the tables must be uploaded again
   }
-  *out = g_noalloc_ptr[dev];
+  *out = (double *)ptr;
   return 0;
+}
+
+// Does the device copy of the tables already describe this grid?
+bool noalloc_same_grid(const NoAllocDev &d, const dnsb_grid *gr) {
+  if (!d.have_grid || d.nx != gr->nx || d.ny != gr->ny || d.nz != gr->nz || d.bc != gr->bc_y ||
+      d.dx != gr->dx || d.dz != gr->dz)
+    return false;
+  return std::memcmp(d.dy, gr->dy, sizeof(double) * (gr->ny + 2)) == 0 &&
+         std::memcmp(d.dyu, gr->dyu, sizeof(double) * (gr->ny + 2)) == 0;
 }
 
 }  // namespace
@@ -2619,53 +2648,66 @@ extern "C" int dnsb_poisson_noalloc(const dnsb_grid *gr, const double *r, double
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return fail(nullptr, DNSB_ECUDA, "cudaGetDevice failed");
   double *base = nullptr;
-  int rc = noalloc_setup(dev, &base);
-  if (rc) return rc;
   cudaStream_t st = (cudaStream_t)stream;
-
+  double *tabs = nullptr;
+  double2 *tws = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    int rc = noalloc_setup(dev, &base);
+    if (rc) return rc;
+    tabs = base + 3 * kNoAllocMaxSpec;  // after S (2*spec) and work (spec): 4*(N+2) + 6*N doubles
+    tws = reinterpret_cast<double2 *>(tabs + 4 * (kNoAllocMaxN + 2) + 6 * kNoAllocMaxN);
+    NoAllocDev &d = g_noalloc_dev[dev];
+    if (!noalloc_same_grid(d, gr)) {
+      // tables, computed exactly as in dnsb_create (plan_poisson, griddata)
+      double *dy = h_tab, *dyu = dy + (ny + 2), *rdy = dyu + (ny + 2), *rdyu = rdy + (ny + 2);
+      double *lam1 = rdyu + (ny + 2), *lam2 = lam1 + (M + 1), *lam3 = lam2 + ny;
+      double *ay = lam3 + nz, *by = ay + ny, *cy = by + ny;
+      const long long ntab = (cy + ny) - h_tab;
+      for (int J = 0; J < ny + 2; J++) {
+        dy[J] = gr->dy[J];
+        dyu[J] = gr->dyu[J];
+        rdy[J] = 1.0 / dy[J];
+        rdyu[J] = 1.0 / dyu[J];
+      }
+      for (int k = 1; k <= M + 1; k++) lam1[k - 1] = modlam(k, nx, gr->dx);
+      for (int k = 1; k <= nz; k++) lam3[k - 1] = modlam(k, nz, gr->dz);
+      for (int k = 1; k <= ny; k++) lam2[k - 1] = modlam(k, ny, dy[1]);
+      for (int j = 1; j <= ny; j++) {
+        double a = 0.0, cc = 0.0;
+        if (wall) {
+          a = j == 1 ? 0.0 : 1 / (dy[j] * dyu[j - 1]);
+          cc = j == ny ? 0.0 : 1 / (dy[j] * dyu[j]);
+        }
+        ay[j - 1] = a;
+        cy[j - 1] = cc;
+        by[j - 1] = -(a + cc);
+      }
+      double2 *twM = h_tw, *twN = twM + M, *twz = twN + (M + 1), *twy = twz + nz;
+      const long long ntw = (twy + ny) - h_tw;
+      for (int t = 0; t < M; t++) twM[t] = unit_root(t, M);
+      for (int t = 0; t <= M; t++) twN[t] = unit_root(t, nx);
+      for (int t = 0; t < nz; t++) twz[t] = unit_root(t, nz);
+      for (int t = 0; t < ny; t++) twy[t] = unit_root(t, ny);
+      d.have_grid = false;
+      cudaError_t e = cudaMemcpyAsync(tabs, h_tab, ntab * sizeof(double), cudaMemcpyHostToDevice, st);
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(tws, h_tw, ntw * sizeof(double2), cudaMemcpyHostToDevice, st);
+      if (e != cudaSuccess) return fail(nullptr, DNSB_ECUDA, "table upload: %s", cudaGetErrorString(e));
+      // the static host staging is reused by the next upload: wait for the copies
+      if ((e = cudaStreamSynchronize(st)) != cudaSuccess)
+        return fail(nullptr, DNSB_ECUDA, "%s", cudaGetErrorString(e));
+      d.nx = nx; d.ny = ny; d.nz = nz; d.bc = gr->bc_y;
+      d.dx = gr->dx; d.dz = gr->dz;
+      std::memcpy(d.dy, gr->dy, sizeof(double) * (ny + 2));
+      std::memcpy(d.dyu, gr->dyu, sizeof(double) * (ny + 2));
+      d.have_grid = true;
+    }
+  }
   // carve the scratch array
   double2 *S = reinterpret_cast<double2 *>(base);
   double *work = base + 2 * kNoAllocMaxSpec;
-  double *tabs = work + kNoAllocMaxSpec;  // 4*(N+2) + 6*N doubles, then twiddles
-  double2 *tws = reinterpret_cast<double2 *>(tabs + 4 * (kNoAllocMaxN + 2) + 6 * kNoAllocMaxN);
-
-  // tables, computed exactly as in dnsb_create (plan_poisson, griddata)
-  double *dy = h_tab, *dyu = dy + (ny + 2), *rdy = dyu + (ny + 2), *rdyu = rdy + (ny + 2);
-  double *lam1 = rdyu + (ny + 2), *lam2 = lam1 + (M + 1), *lam3 = lam2 + ny;
-  double *ay = lam3 + nz, *by = ay + ny, *cy = by + ny;
-  const long long ntab = (cy + ny) - h_tab;
-  for (int J = 0; J < ny + 2; J++) {
-    dy[J] = gr->dy[J];
-    dyu[J] = gr->dyu[J];
-    rdy[J] = 1.0 / dy[J];
-    rdyu[J] = 1.0 / dyu[J];
-  }
-  for (int k = 1; k <= M + 1; k++) lam1[k - 1] = modlam(k, nx, gr->dx);
-  for (int k = 1; k <= nz; k++) lam3[k - 1] = modlam(k, nz, gr->dz);
-  for (int k = 1; k <= ny; k++) lam2[k - 1] = modlam(k, ny, dy[1]);
-  for (int j = 1; j <= ny; j++) {
-    double a = 0.0, cc = 0.0;
-    if (wall) {
-      a = j == 1 ? 0.0 : 1 / (dy[j] * dyu[j - 1]);
-      cc = j == ny ? 0.0 : 1 / (dy[j] * dyu[j]);
-    }
-    ay[j - 1] = a;
-    cy[j - 1] = cc;
-    by[j - 1] = -(a + cc);
-  }
-  double2 *twM = h_tw, *twN = twM + M, *twz = twN + (M + 1), *twy = twz + nz;
-  const long long ntw = (twy + ny) - h_tw;
-  for (int t = 0; t < M; t++) twM[t] = unit_root(t, M);
-  for (int t = 0; t <= M; t++) twN[t] = unit_root(t, nx);
-  for (int t = 0; t < nz; t++) twz[t] = unit_root(t, nz);
-  for (int t = 0; t < ny; t++) twy[t] = unit_root(t, ny);
-  cudaError_t e = cudaMemcpyAsync(tabs, h_tab, ntab * sizeof(double), cudaMemcpyHostToDevice, st);
-  if (e == cudaSuccess)
-    e = cudaMemcpyAsync(tws, h_tw, ntw * sizeof(double2), cudaMemcpyHostToDevice, st);
-  if (e != cudaSuccess) return fail(nullptr, DNSB_ECUDA, "table upload: %s", cudaGetErrorString(e));
-  // the static host staging is reused by the next call: wait for the copies
-  if ((e = cudaStreamSynchronize(st)) != cudaSuccess)
-    return fail(nullptr, DNSB_ECUDA, "%s", cudaGetErrorString(e));
+  cudaError_t e = cudaSuccess;
 
   Geo g{};
   g.nx = nx; g.ny = ny; g.nz = nz;

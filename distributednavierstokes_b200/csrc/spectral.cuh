@@ -129,13 +129,15 @@ __global__ void __launch_bounds__(SPEC_THREADS, 3) k_fftz(Geo g, double2 *__rest
 // half of a double-buffered staging area while the current tile is
 // transformed.  The first radix stage reads the staging buffer, the middle
 // stages ping-pong in shared memory, the last stage writes HBM directly.
-// On a (bounded) wait timeout the kernel records err and stops after its
-// in-flight copy has landed.
+// Every thread waits for the tile at most wait_limit polls; if any thread
+// ran out, the whole CTA (a uniform decision, __syncthreads_or) records err,
+// lets the copies it has in flight land (drained with DNSB_WAIT_LIMIT polls
+// by thread 0) and returns, so no bulk copy outlives its CTA.
 template <bool INV>
 __global__ void __launch_bounds__(SPEC_THREADS, 2) k_fftz_tma(Geo g, double2 *__restrict__ S,
                                                              FFTPlan plan, int L,
                                                              const double2 *__restrict__ twz,
-                                                             int *err) {
+                                                             int *err, unsigned wait_limit) {
   extern __shared__ __align__(128) double2 smem[];
   const int n = g.nz;
   const int ls = n + 1;
@@ -170,8 +172,14 @@ __global__ void __launch_bounds__(SPEC_THREADS, 2) k_fftz_tma(Geo g, double2 *__
       fence_proxy_async_smem();  // the previous readers of this buffer are past a barrier
       issue(nxt, cur ^ 1);
     }
-    if (!mbar_wait(&bar[cur], (it >> 1) & 1, err)) {
-      if (nxt < ngroups) mbar_wait(&bar[cur ^ 1], ((it + 1) >> 1) & 1, nullptr);
+    const bool ok = mbar_wait_n(&bar[cur], (it >> 1) & 1, wait_limit);
+    if (__syncthreads_or(!ok)) {
+      if (threadIdx.x == 0) {
+        atomicExch(err, DEVERR_TMA_TIMEOUT);
+        mbar_wait_n(&bar[cur], (it >> 1) & 1, DNSB_WAIT_LIMIT);
+        if (nxt < ngroups) mbar_wait_n(&bar[cur ^ 1], ((it + 1) >> 1) & 1, DNSB_WAIT_LIMIT);
+      }
+      __syncthreads();
       return;
     }
     const double2 *st = cur ? stage1 : stage0;

@@ -3,8 +3,9 @@
 // A persistent CTA prefetches the next tile of lines with one
 // cp.async.bulk (global -> shared, completion counted on an mbarrier)
 // while it transforms the current one.  No multicast is used anywhere.
-// Every wait is bounded: after DNSB_WAIT_LIMIT polls the kernel records an
-// error code in a global word and the caller returns.
+// Every wait is bounded: after a caller-given number of polls the kernel
+// records an error code in a global word and returns; DNSB_WAIT_LIMIT is the
+// default limit and the one used to drain copies still in flight.
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -58,11 +59,11 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
   return ok != 0;
 }
 
-// bounded wait; returns false (and records err) when the limit is hit
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *err) {
-  for (unsigned it = 0; it < DNSB_WAIT_LIMIT; it++)
+// bounded wait of the calling thread: at most `limit` polls (0: none);
+// returns false when they ran out
+__device__ __forceinline__ bool mbar_wait_n(uint64_t *bar, uint32_t parity, unsigned limit) {
+  for (unsigned it = 0; it < limit; it++)
     if (mbar_try_wait(bar, parity)) return true;
-  if (err) atomicExch(err, DEVERR_TMA_TIMEOUT);
   return false;
 }
 

@@ -69,7 +69,16 @@ void dnsb_destroy(dnsb_ctx *ctx);
  * ctx is NULL). */
 const char *dnsb_last_error(const dnsb_ctx *ctx);
 int dnsb_set_stream(dnsb_ctx *ctx, void *stream);
+/* Synchronises the context's stream; returns DNSB_ECUDA if a kernel's
+ * bounded device-side wait ran out since the last check (and clears it). */
 int dnsb_sync(dnsb_ctx *ctx);
+/* Poll limit of every device-side wait of this context's kernels (default
+ * 2^26; 0 makes every such wait give up at once).  The only device-side
+ * waits are the mbarrier waits of the opt-in persistent TMA z-transform
+ * (DNSB_TMA=1); a wait that runs out makes its CTA drain its copies in
+ * flight and return, and the next dnsb_sync reports it.  The reference's
+ * FV path has no device-side waits (no counterpart). */
+int dnsb_set_wait_limit(dnsb_ctx *ctx, unsigned long polls);
 
 /* exchange_halo!(φ, stag, setup), single rank (src/halo.jl:81-126). */
 int dnsb_fill_ghosts(dnsb_ctx *ctx, double *phi, int stag);
@@ -228,11 +237,17 @@ int dnsb_shell_clamp(dnsb_ctx *ctx, double *ux, double *uy, double *uz, const do
  * grids are rejected with DNSB_EUNSUP.  r (ghost-free nx*ny*nz) and p
  * (ghosted; its interior is written, no halos) are the caller's device
  * arrays on the current device; work is enqueued on `stream`.  The first
- * call on a device resolves the scratch array's device address
- * (cudaGetSymbolAddress) and sets kernel attributes, so make that first call
- * before any stream capture.  Every call reuses the same scratch (nothing in
- * it needs to start at zero; each call rewrites what it reads): calls that
- * overlap on the GPU (other streams, other host threads) race.  Errors are
+ * call on a device sets up: it resolves the scratch array's device address
+ * (cudaGetSymbolAddress), sets kernel attributes and uploads the grid's
+ * tables from host memory, synchronising `stream`; make that first call
+ * before any stream capture.  A later call whose grid (sizes, boundary,
+ * spacings, dy, dyu) differs from the previous call's on that device
+ * uploads the tables again and synchronises `stream` as well; a call with
+ * the same grid only enqueues its five kernels.  Every call reuses the same
+ * scratch (nothing in it needs to start at zero; each call rewrites what it
+ * reads): calls that overlap on the GPU (other streams, other host threads)
+ * race.  The transforms are those of dnsb_poisson's Stockham path; with
+ * walls the y-solve is the one-thread-per-line Thomas kernel.  Errors are
  * reported by dnsb_last_error(NULL). */
 int dnsb_poisson_noalloc(const dnsb_grid *grid, const double *r, double *p, void *stream);
 

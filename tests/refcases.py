@@ -125,3 +125,39 @@ RUNCASE_IC = dict(
 TG_IC = dict(x=lambda x, y, z: math.sin(x) * math.cos(y),
              y=lambda x, y, z: -math.cos(x) * math.sin(y))
 """Taylor-Green field (test/serialtests.jl:85-90)."""
+
+
+def _rel(a, b):
+    return float(np.max(np.abs(a - b))) / max(float(np.max(np.abs(b))), 1e-300)
+
+
+def pressure_sensitivity(so, u0, p0, dt, seed=1):
+    """Relative change of the oracle's one-step pressure when its initial
+    velocity u0 (with lagged pressure p0) is perturbed by Gaussian relative
+    noise of 4e-16 (about 4 ulp)."""
+    rng = np.random.default_rng(seed)
+
+    def run(u):
+        u = {c: np.array(u[c]) for c in "xyz"}
+        so.exchange_halo(u)
+        p = p0.copy()
+        q = so.vectorfield()
+        d = so.scalarfield() if so.imexy else p
+        so.step(u, p, q, d, dt)
+        return p
+
+    pa = run(u0)
+    pb = run({c: u0[c] * (1 + 4e-16 * rng.standard_normal(u0[c].shape)) for c in "xyz"})
+    return _rel(pb, pa)
+
+
+def check_pressure(err, so, u0, p0, dt):
+    """The one-step pressure error err (relative, max-norm) is <= 1e-12, or
+    <= 2x the oracle's own sensitivity where that is larger: the pressure
+    solves a Poisson problem whose right-hand side, the divergence of the
+    intermediate velocity, is a difference of nearly equal fluxes, so the
+    round-off of u is amplified in p by the grid's conditioning."""
+    if err <= 1e-12:
+        return
+    sens = pressure_sensitivity(so, u0, p0, dt)
+    assert err <= 2 * sens, f"pressure error {err:.3e} > 1e-12 and > 2 x oracle sensitivity {sens:.3e}"

@@ -5,7 +5,14 @@ and known-answer tests run on the GPU path.
 Tolerances (FP64): operators and one RK3 step agree with the oracle to
 <= 1e-12 relative (max-norm, relative to the field's max); 100 steps of the
 64^3 channel to <= 1e-9; halo fills are exact; divergence after projection
-< 1e-12 as in the reference.
+< 1e-12 as in the reference.  The pressure after one step is held to
+1e-12 too, or to twice the oracle's own change under a 4-ulp perturbation
+of its initial velocity where that is larger (check_pressure): the step's
+pressure solves a Poisson problem whose right-hand side is the divergence
+of the intermediate velocity, a difference of nearly equal fluxes, so
+round-off of u is amplified in p by the grid's conditioning (on the 256-row
+tanh(1.5) channel both the device-vs-oracle difference and the oracle's own
+sensitivity are about 1.0e-12 to 1.7e-12; everywhere else <= 2.6e-13).
 """
 import ctypes
 import math
@@ -62,6 +69,10 @@ def rand_fields(so, seed=42):
 
 def to_dev(D, u):
     return D.VectorField(x=T(u["x"]), y=T(u["y"]), z=T(u["z"]))
+
+
+check_pressure = R.check_pressure
+
 
 
 CONFIGS = {
@@ -187,12 +198,13 @@ def test_one_step(oracle_mod, D, cfg):
     delta = so.scalarfield() if so.imexy else p
     deltad = D.scalarfield(sd) if sd.imexy else pd
     dt = 0.5 * so.cfl_timestep(u, 0.5)
+    u0, p0 = {c: u[c].copy() for c in "xyz"}, p.copy()
     so.step(u, p, q, delta, dt)
     D.step(ud, pd, qd, deltad, sd, dt)
     for c in "xyz":
         assert rel(N(ud[c]), u[c]) <= TOL_STEP, c
         assert rel(N(qd[c]), q[c]) <= 1e-11, c
-    assert rel(N(pd), p) <= 1e-10
+    check_pressure(rel(N(pd), p), so, u0, p0, dt)
     assert D.maxdiv(ud, sd) < 1e-12
 
 
@@ -287,12 +299,13 @@ def test_one_step_production_lengths(oracle_mod, D, cfg):
     q, qd = so.vectorfield(), D.vectorfield(sd)
     delta, deltad = so.scalarfield(), D.scalarfield(sd)
     dt = 0.5 * so.cfl_timestep(u, 0.5)
+    u0, p0 = {c: u[c].copy() for c in "xyz"}, p.copy()
     so.step(u, p, q, delta, dt)
     D.step(ud, pd, qd, deltad, sd, dt)
     for c in "xyz":
         assert rel(N(ud[c]), u[c]) <= TOL_STEP, c
         assert rel(N(qd[c]), q[c]) <= 1e-11, c
-    assert rel(N(pd), p) <= 1e-10
+    check_pressure(rel(N(pd), p), so, u0, p0, dt)
     assert D.maxdiv(ud, sd) < 1e-12
 
 
@@ -315,12 +328,13 @@ def test_fused_projection_momentum_planes(oracle_mod, D, cfg, planes, pipe, monk
     q, qd = so.vectorfield(), D.vectorfield(sd)
     delta, deltad = so.scalarfield(), D.scalarfield(sd)
     dt = 0.5 * so.cfl_timestep(u, 0.5)
+    u0, p0 = {c: u[c].copy() for c in "xyz"}, p.copy()
     so.step(u, p, q, delta, dt)
     D.step(ud, pd, qd, deltad, sd, dt)
     for c in "xyz":
         assert rel(N(ud[c]), u[c]) <= TOL_STEP, c
         assert rel(N(qd[c]), q[c]) <= 1e-11, c
-    assert rel(N(pd), p) <= 1e-10
+    check_pressure(rel(N(pd), p), so, u0, p0, dt)
 
 
 @pytest.mark.parametrize("post,pairs", [("1", "0"), ("0", "0"), ("1", "1")])
@@ -381,12 +395,13 @@ def test_one_step_unaligned_fields(oracle_mod, D, cfg):
     delta = so.scalarfield() if so.imexy else p
     deltad = D.scalarfield(sd) if sd.imexy else pd
     dt = 0.5 * so.cfl_timestep(u, 0.5)
+    u0, p0 = {c: u[c].copy() for c in "xyz"}, p.copy()
     so.step(u, p, q, delta, dt)
     D.step(ud, pd, qd, deltad, sd, dt)
     for c in "xyz":
         assert rel(N(ud[c]), u[c]) <= TOL_STEP, c
         assert rel(N(qd[c]), q[c]) <= 1e-11, c
-    assert rel(N(pd), p) <= 1e-10
+    check_pressure(rel(N(pd), p), so, u0, p0, dt)
 
 
 def _c1_ic(O, D, n, ydiff="explicit", amp=0.1, visc=1 / 180):
