@@ -100,6 +100,31 @@ SIGNATURES = {
     "dnsb_spectral_phaserandomize": (c_int, [P, P, ctypes.c_ulonglong]),
 }
 
+# include/dnsb_cnn.h
+SIGNATURES.update({
+    "dnsb_cnn_create": (c_int, [c_int, P, c_int, c_int, c_int, ctypes.POINTER(c_void_p)]),
+    "dnsb_cnn_destroy": (None, [P]),
+    "dnsb_cnn_last_error": (ctypes.c_char_p, [P]),
+    "dnsb_cnn_set_stream": (c_int, [P, P]),
+    "dnsb_cnn_sync": (c_int, [P]),
+    "dnsb_cnn_launch_count": (c_long, [P]),
+    "dnsb_cnn_param_count": (c_int, [P]),
+    "dnsb_cnn_init": (c_int, [P, ctypes.c_ulonglong]),
+    "dnsb_cnn_set_params": (c_int, [P, P]),
+    "dnsb_cnn_get_params": (c_int, [P, P]),
+    "dnsb_cnn_set_scales": (c_int, [P, P, P]),
+    "dnsb_cnn_set_dataset": (c_int, [P, P, c_int, c_int]),
+    "dnsb_cnn_train": (c_int, [P, c_int, ctypes.c_float, ctypes.c_ulonglong]),
+    "dnsb_cnn_steps": (c_int, [P, ctypes.POINTER(c_long)]),
+    "dnsb_cnn_losses": (c_int, [P, P, c_long, c_long]),
+    "dnsb_cnn_batch": (c_int, [P, P, P, c_int, ctypes.c_float, P, P]),
+    "dnsb_cnn_infer_cells": (c_int, [P, P, P]),
+    "dnsb_cnn_infer": (c_int, [P, P, P, P, P]),
+    "dnsb_cnn_profile": (c_int, [P, c_int]),
+    "dnsb_cnn_profile_read": (c_int, [P, c_int, ctypes.POINTER(c_double), ctypes.POINTER(c_long),
+                                      ctypes.POINTER(c_double)]),
+})
+
 KINDS = ["momentum", "cn_solve", "div_rfft_x", "fft_z", "y_solve", "ifft_z", "irfft_x",
          "grad_update", "other", "grad_momentum", "fft_z_y_solve"]
 
@@ -133,3 +158,10 @@ def check(rc, ctx=None):
         msg = load().dnsb_last_error(ctx)
         msg = msg.decode() if msg else ""
         raise DNSBError(f"libdnsb: {ERRORS.get(rc, rc)}: {msg}")
+
+
+def check_cnn(rc, cnn=None):
+    if rc != DNSB_OK:
+        msg = load().dnsb_cnn_last_error(cnn)
+        msg = msg.decode() if msg else ""
+        raise DNSBError(f"libdnsb (closure): {ERRORS.get(rc, rc)}: {msg}")

@@ -232,7 +232,8 @@ struct ConvArgs {
   int s, e, R;         // input offset (0 / -2), extra patch row, patch rows
   int tpp;             // tiles per plane: ceil(Do * P / 128)
   int ntiles;          // B * Do * tpp
-  uint32_t stage_bytes;  // CI * 3 * R * P * 16
+  uint32_t box_bytes;    // CI * 3 * R * P * 16 (one TMA box)
+  uint32_t stage_bytes;  // stage stride: box_bytes rounded up to 1 KB
   uint32_t w_bytes;      // 27 * CI * CO * 128
   unsigned wait_limit;
   const uint4 *wpack;    // packed weights (B operand), w_bytes
@@ -255,7 +256,9 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     k_conv(const __grid_constant__ CUtensorMap tin, const ConvArgs a) {
   constexpr int N = 8 * CO;
   constexpr uint32_t NCOLS = 2 * N < 32 ? 32 : 2 * N;  // two accumulators
-  extern __shared__ __align__(1024) unsigned char smem[];
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  // 1 KB-aligned base (TMA destinations; the host adds 1 KB of slack)
+  unsigned char *smem = smem_raw + ((1024u - (saddr(smem_raw) & 1023u)) & 1023u);
   unsigned char *wsm = smem;
   unsigned char *stg = smem + a.w_bytes;
   uint64_t *bars = reinterpret_cast<uint64_t *>(stg + CV_STAGES * a.stage_bytes);
@@ -299,7 +302,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         const int j = t % a.tpp, rest = t / a.tpp;
         const int z = rest % a.Do, b = rest / a.Do;
         const int f0 = j * TILE_M, y0 = f0 / a.P;
-        mb_expect(&full[s], a.stage_bytes);
+        mb_expect(&full[s], a.box_bytes);
         tma5(stg + s * a.stage_bytes, &tin, 0, 0, y0 + a.s - a.e, z + a.s, b * CI, &full[s]);
         prev_s = last_s;
         prev_ph = last_ph;
@@ -484,7 +487,8 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   constexpr int G = 16 / CI;             // tap slots per group (M = 128 rows)
   constexpr uint32_t NCOLS = N < 32 ? 32 : N;
   constexpr uint32_t SLOT = CI * WG_K * 16;  // bytes of one tap slot
-  extern __shared__ __align__(1024) unsigned char smem[];
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char *smem = smem_raw + ((1024u - (saddr(smem_raw) & 1023u)) & 1023u);
   uint64_t *bars = reinterpret_cast<uint64_t *>(smem + WG_STAGES * a.stage_bytes);
   uint64_t *full = bars, *empty = bars + WG_STAGES, *done = bars + 2 * WG_STAGES;
   uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + 2 * WG_STAGES + 1);
