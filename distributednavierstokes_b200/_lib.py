@@ -47,6 +47,7 @@ SIGNATURES = {
     "dnsb_poisson": (c_int, [P, P, P]),
     "dnsb_project": (c_int, [P, P, P, P, P]),
     "dnsb_imex_update": (c_int, [P, P, P, P, P, P, P, P, c_double, c_double, c_double]),
+    "dnsb_sfs_stage": (c_int, [P, P, P, P, P, P, P, P, c_double, c_double]),
     "dnsb_step": (c_int, [P, P, P, P, P, P, P, P, P, c_double]),
     "dnsb_cfl": (c_int, [P, P, P, P, c_double, c_int, ctypes.POINTER(c_double)]),
     "dnsb_solve": (c_int, [P, P, P, P, P, P, P, P, P, c_double, c_double, c_double, c_double,

@@ -1540,6 +1540,85 @@ int dnsb_project(dnsb_ctx *c, double *ux, double *uy, double *uz, double *psi) {
   return do_project(c, ux, uy, uz, psi);
 }
 
+// One explicit Runge-Kutta stage update with a sub-filter-stress closure on
+// a periodic box (no counterpart in the reference): after momentum! has set
+// q <- A q + dt F(u), add dt f_sfs to q, f_sfs = -div(tau) on the staggered
+// faces, then u += B q (the explicit stage of step!, src/timestep.jl:52-57).
+// tau holds 6 cell-centred components [xx, yy, zz, xy, yz, zx] of nx*ny*nz
+// values (x fastest).  Normal stresses are differenced across the face
+// (the two cells it separates); shear stresses are averaged onto the cell
+// edges (four cells) and differenced across the face's cell in the
+// transverse direction.  tau == NULL: the plain stage update.
+__global__ void k_sfs_stage(Geo g, const double *__restrict__ tau, Fields3 q, Fields3 u, double dt,
+                            double B) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  if (i >= g.nx || j >= g.ny) return;
+  const int I = i + 1, J = j + 1, K = k + 1;
+  const long long n3 = (long long)g.nx * g.ny * g.nz;
+  double f[3] = {0.0, 0.0, 0.0};
+  if (tau) {
+    auto T = [&](int c, int a, int b, int d) {  // component c at cell (a, b, d), periodic
+      a = (a + g.nx) % g.nx;
+      b = (b + g.ny) % g.ny;
+      d = (d + g.nz) % g.nz;
+      return __ldg(tau + c * n3 + ((long long)d * g.ny + b) * g.nx + a);
+    };
+    const double rdy = g.rdy[J], rdyu = g.rdyu[J];
+    // x-face between cells i, i+1
+    {
+      const double dxx = (T(0, i + 1, j, k) - T(0, i, j, k)) * g.rdx;
+      const double en = 0.25 * (T(3, i, j, k) + T(3, i + 1, j, k) + T(3, i, j + 1, k) + T(3, i + 1, j + 1, k));
+      const double es = 0.25 * (T(3, i, j, k) + T(3, i + 1, j, k) + T(3, i, j - 1, k) + T(3, i + 1, j - 1, k));
+      const double eu = 0.25 * (T(5, i, j, k) + T(5, i + 1, j, k) + T(5, i, j, k + 1) + T(5, i + 1, j, k + 1));
+      const double ed = 0.25 * (T(5, i, j, k) + T(5, i + 1, j, k) + T(5, i, j, k - 1) + T(5, i + 1, j, k - 1));
+      f[0] = -(dxx + (en - es) * rdy + (eu - ed) * g.rdz);
+    }
+    // y-face between cells j, j+1
+    {
+      const double dyy = (T(1, i, j + 1, k) - T(1, i, j, k)) * rdyu;
+      const double ee = 0.25 * (T(3, i, j, k) + T(3, i, j + 1, k) + T(3, i + 1, j, k) + T(3, i + 1, j + 1, k));
+      const double ew = 0.25 * (T(3, i, j, k) + T(3, i, j + 1, k) + T(3, i - 1, j, k) + T(3, i - 1, j + 1, k));
+      const double eu = 0.25 * (T(4, i, j, k) + T(4, i, j + 1, k) + T(4, i, j, k + 1) + T(4, i, j + 1, k + 1));
+      const double ed = 0.25 * (T(4, i, j, k) + T(4, i, j + 1, k) + T(4, i, j, k - 1) + T(4, i, j + 1, k - 1));
+      f[1] = -((ee - ew) * g.rdx + dyy + (eu - ed) * g.rdz);
+    }
+    // z-face between cells k, k+1
+    {
+      const double dzz = (T(2, i, j, k + 1) - T(2, i, j, k)) * g.rdz;
+      const double ee = 0.25 * (T(5, i, j, k) + T(5, i, j, k + 1) + T(5, i + 1, j, k) + T(5, i + 1, j, k + 1));
+      const double ew = 0.25 * (T(5, i, j, k) + T(5, i, j, k + 1) + T(5, i - 1, j, k) + T(5, i - 1, j, k + 1));
+      const double en = 0.25 * (T(4, i, j, k) + T(4, i, j, k + 1) + T(4, i, j + 1, k) + T(4, i, j + 1, k + 1));
+      const double es = 0.25 * (T(4, i, j, k) + T(4, i, j, k + 1) + T(4, i, j - 1, k) + T(4, i, j - 1, k + 1));
+      f[2] = -((ee - ew) * g.rdx + (en - es) * rdy + dzz);
+    }
+  }
+  const int c0 = gidx(g, I, J, K);
+  double *qs[3] = {q.x, q.y, q.z};
+  double *us[3] = {u.x, u.y, u.z};
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    const double qn = qs[c][c0] + dt * f[c];
+    qs[c][c0] = qn;
+    store_img(us[c], g, I, J, K, us[c][c0] + B * qn, c);
+  }
+}
+
+int dnsb_sfs_stage(dnsb_ctx *c, const double *tau, double *qx, double *qy, double *qz, double *ux,
+                   double *uy, double *uz, double dt, double B) {
+  if (!c || !qx || !qy || !qz || !ux || !uy || !uz)
+    return c ? fail(c, DNSB_EINVAL, "null field") : DNSB_EINVAL;
+  if (c->g.wall) return fail(c, DNSB_EINVAL, "the closure stage needs a periodic box");
+  if (ensure_device(c)) return DNSB_ECUDA;
+  k_sfs_stage<<<cell_grid(c->g), cell_block, 0, c->stream>>>(c->g, tau, ff(qx, qy, qz),
+                                                             ff(ux, uy, uz), dt, B);
+  CKL(c);
+  c->launches++;
+  c->umax_for[0] = c->umax_for[1] = c->umax_for[2] = nullptr;
+  return 0;
+}
+
 int dnsb_imex_update(dnsb_ctx *c, double *ux, double *uy, double *uz, const double *qx,
                      const double *qy, const double *qz, const double *p, double B, double alpha,
                      double dt) {

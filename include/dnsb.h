@@ -103,6 +103,17 @@ int dnsb_poisson(dnsb_ctx *ctx, const double *r, double *p);
  * halos. */
 int dnsb_project(dnsb_ctx *ctx, double *ux, double *uy, double *uz, double *psi);
 
+/* The explicit stage of step! (src/timestep.jl:52-57, after momentum!
+ * set q <- A q + dt F(u)) with a sub-filter-stress closure, on a periodic
+ * box: q += dt f, f = -div(tau) on the staggered faces (normal stresses
+ * differenced across each face, shear stresses averaged onto the cell
+ * edges), then u += B q with the ghost images of u rewritten.  tau: DEVICE
+ * [6][nz][ny][nx] cell-centred components xx, yy, zz, xy, yz, zx (e.g.
+ * from dnsb_cnn_infer); NULL gives the plain stage update.  The closure is
+ * the north star's addition; the reference has no SFS model. */
+int dnsb_sfs_stage(dnsb_ctx *ctx, const double *tau, double *qx, double *qy, double *qz,
+                   double *ux, double *uy, double *uz, double dt, double B);
+
 /* imex_update!(u, q, p, B, α, Δt, setup) (src/ydiffusion.jl:119-154). */
 int dnsb_imex_update(dnsb_ctx *ctx, double *ux, double *uy, double *uz, const double *qx,
                      const double *qy, const double *qz, const double *p, double B,
