@@ -2,7 +2,8 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
                     [--workload channel384_implicit|channel256_implicit|
-                                channel64_explicit|ensemble64_periodic]
+                                channel64_explicit|ensemble64_periodic|les64_cnn|
+                                spectral256_hit]
 
 One "step" is one full RK3 time step (3 stages: momentum, semi-implicit
 wall-normal Crank-Nicolson, FFT/Thomas projection, lagged-pressure update)
@@ -54,6 +55,16 @@ WORKLOADS = {
     "ensemble64_periodic": dict(
         members=64, sizes=(32, 48, 64, 96, 128), visc=(1e-3, 1e-2), cfl=0.5, energy=0.5,
         kpeak=4.0, forced_shells=(1, 2), ydiffusion="explicit", bytes_per_cell_step=792.0),
+    # the closure study: 256^3 periodic FV DNS (nu = 5e-4, random-phase
+    # E(k) ~ k^4 exp(-2 (k/4)^2) field, shell-clamp forcing of shells 1-2)
+    # to t = 10 with 200 filtered pairs (Gaussian width 4 dx_DNS onto 64^3);
+    # the CNN trained on them (20k Adam steps, lr 1e-3, batches of 8 crops
+    # of 32^3); then the CNN-closed and the unclosed 64^3 LES and the DNS
+    # itself advanced from t = 10 for 5 time units and compared
+    "les64_cnn": dict(
+        closure=True, n_dns=256, M=64, visc=5e-4, energy=0.5, kpeak=4.0, shells=(1, 2),
+        t_train=10.0, nsnap=200, t_les=5.0, nsample=10, cfl=0.5, train_steps=20000, lr=1e-3,
+        batch=8, crop=32),
     # the pseudo-spectral solver on a 256^3 periodic cube (nu = 5e-4, kcut 85):
     # random-phase E(k) ~ k^4 exp(-2 (k/4)^2) initial field, shell-clamp
     # forcing of shells 1-2 after every step, CFL-adaptive Wray steps
@@ -452,6 +463,73 @@ def spectral_arm(args, wl, world, rank, local):
     s.close()
 
 
+def closure_arm(args, wl, world, rank, local):
+    """The closure study (les_closure.pipeline): the headline is the
+    simulated time per second of the CNN-closed 64^3 LES over that of the
+    256^3 DNS on the same GPU, both device-timed over the same 5 time units,
+    reported beside the LES's filtered energy-spectrum error for k <= 64/3
+    against the filtered DNS (and the unclosed LES's, the fallback).  Runs
+    on rank 0; other ranks only join the barrier (replicas, no collective
+    on the data path)."""
+    import torch
+
+    from distributednavierstokes_b200 import les_closure
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    keys = ("n_dns", "M", "visc", "energy", "kpeak", "shells", "t_train", "nsnap", "t_les", "nsample",
+            "cfl", "train_steps", "lr", "batch", "crop")
+    kw = {k: wl[k] for k in keys}
+    if args.train_steps is not None:
+        kw["train_steps"] = args.train_steps
+    clocks = ClockSampler(local)
+    clocks.start()
+    t0 = time.perf_counter()
+    res = les_closure.pipeline(device=dev, log=(lambda m: print(m, file=sys.stderr, flush=True)), **kw)
+    wall = time.perf_counter() - t0
+    clk = clocks.stop()
+    if rank != 0:
+        return
+    les = res["les"]
+    tr = res["training"]
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except Exception:
+        pass
+    bf16 = float(peaks.get("bf16_tflops_sustained", 1418.6))
+    line = {
+        "metric": "CNN-LES vs 256^3 DNS simulated-time/s ratio (64^3 LES, E(k) error for k <= kcut)",
+        "value": les["speedup_cnn_vs_dns"], "unit": "x", "n_gpus": 1, "steps": les["steps"]["les_cnn"],
+        "warmup": 0, "ms_per_step": les["device_ms"]["les_cnn"] / max(les["steps"]["les_cnn"], 1),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64 flow, bf16/fp32 network",
+        "data": "synthetic: the library's own DNS (random-phase initial field, seed 0, shell forcing)",
+        "config": {"workload": args.workload, **res["config"]},
+        "les": {k: v for k, v in les.items() if k != "samples"},
+        "les_samples": [{k: v for k, v in r.items() if not k.startswith("E_")} for r in les["samples"]],
+        "spectra_final": {k: les["samples"][-1][k] for k in ("E_dns", "E_cnn", "E_plain")},
+        "training": tr,
+        "dataset": res["dataset"],
+        "roofline": {"bound": "tensor", "kernel": "training step (all tensor-core kernels)",
+                     "achieved": tr["tflops"], "peak": bf16, "unit": "TFLOP/s",
+                     "frac": (tr["tflops"] or 0) / bf16, "traffic": None,
+                     "peak_source": "measured (sustained cuBLAS bf16)" if peaks else "fallback",
+                     "note": "algorithmic FLOPs (2 x 27 x cin x cout per output voxel and "
+                             "pass) over the CUDA-event time of the training loop"},
+        "e2e": {"value": les["speedup_cnn_vs_dns"], "unit": "x", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 8,
+                "note": "device-resident state; the CFL step size (8 bytes) is read back every "
+                        "step, inside the timed region, for both the LES and the DNS"},
+        "gpu_launches": res.get("closure_launches"),
+        "wall_s": wall,
+        "clocks": clk,
+        "cpu_baseline": None,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def b200_arm(args, wl, world, rank, local):
     import ctypes
 
@@ -726,13 +804,22 @@ def main():
                     help="timed full-grid CPU oracle steps of the cpu_baseline (about 2 s each)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--train-steps", type=int, default=None,
+                    help="closure workload: Adam steps (default: the workload's 20000)")
     ap.add_argument("--no-cufft", action="store_true",
                     help="skip timing cuFFT beside the library's transforms")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "b200" else args.warmup
     wl = WORKLOADS[args.workload]
     world, rank, local = dist_init()
-    if wl.get("spectral"):
+    if wl.get("closure"):
+        if args.impl == "reference":
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "unavailable":
+                                  "the reference has no learned closure or LES path"}), flush=True)
+        else:
+            closure_arm(args, wl, world, rank, local)
+    elif wl.get("spectral"):
         if args.impl == "reference":
             if rank == 0:
                 print(json.dumps({"impl": "reference", "unavailable":

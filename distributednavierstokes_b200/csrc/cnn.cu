@@ -34,7 +34,7 @@ constexpr int CICH[NL] = {2, 4, 4, 4};  // input chunks of 8 channels (3 -> 16 p
 constexpr int COCH[NL] = {4, 4, 4, 2};  // output chunks (6 -> 16 padded)
 constexpr int HALO = 4;
 constexpr long LOSS_CAP = 1L << 18;     // loss history ring
-constexpr unsigned WAIT_LIMIT = 1u << 22;
+constexpr unsigned WAIT_LIMIT = 1u << 21;   // polls of up to 1 us each
 constexpr int MAX_SMEM = 227 * 1024;
 
 typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
@@ -400,40 +400,58 @@ int patch_rows(int P, int s, int e) {
   return (int)(M / P) + 1;
 }
 
-int make_map5(dnsb_cnn *c, CUtensorMap *m, void *base, int P, int chunks, int B, int R) {
+// The chunked-voxel tensors are described with 8-byte elements so that the
+// innermost box dimension is a whole x-row (16 P bytes) or a whole run of
+// positions (1 KB): TMA moves long rows instead of 16-byte pieces.  The
+// copy is byte-exact (no conversion; out-of-bounds elements read as zero).
+// Conv plane: dims {2P (x and 8 channels), P (y), P (z), chunks * B}, box
+// {2P, R, 1, chunks} -> shared memory [chunk][row][x][16 B] (one ring slot).
+int make_map_patch(dnsb_cnn *c, CUtensorMap *m, void *base, int P, int chunks, int B, int R) {
   EncodeTiledFn enc = encode_fn();
   if (!enc) return cfail(c, DNSB_ECUDA, "cuTensorMapEncodeTiled is not available");
-  if (P > 256 || R > 256 || chunks > 256) return cfail(c, DNSB_EUNSUP, "TMA box beyond 256 (P %d, R %d)", P, R);
-  const cuuint64_t dims[5] = {8, (cuuint64_t)P, (cuuint64_t)P, (cuuint64_t)P, (cuuint64_t)chunks * B};
-  const cuuint64_t strides[4] = {16, 16ull * P, 16ull * P * P, 16ull * P * P * P};
-  const cuuint32_t box[5] = {8, (cuuint32_t)P, (cuuint32_t)R, 3, (cuuint32_t)chunks};
-  const cuuint32_t es[5] = {1, 1, 1, 1, 1};
-  const CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, base, dims, strides, box, es,
-                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                         CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  if (r != CUDA_SUCCESS) return cfail(c, DNSB_ECUDA, "cuTensorMapEncodeTiled (5-D) failed: %d", (int)r);
-  return 0;
-}
-
-int make_map4(dnsb_cnn *c, CUtensorMap *m, void *base, int P, int chunks, int B) {
-  EncodeTiledFn enc = encode_fn();
-  if (!enc) return cfail(c, DNSB_ECUDA, "cuTensorMapEncodeTiled is not available");
-  const cuuint64_t dims[4] = {8, (cuuint64_t)P * P, (cuuint64_t)P, (cuuint64_t)chunks * B};
-  const cuuint64_t strides[3] = {16, 16ull * P * P, 16ull * P * P * P};
-  const cuuint32_t box[4] = {8, (cuuint32_t)WG_K, 1, (cuuint32_t)chunks};
+  if (2 * P > 256 || R > 256 || chunks > 256) return cfail(c, DNSB_EUNSUP, "TMA box beyond 256 (P %d, R %d)", P, R);
+  const cuuint64_t dims[4] = {2ull * P, (cuuint64_t)P, (cuuint64_t)P, (cuuint64_t)chunks * B};
+  const cuuint64_t strides[3] = {16ull * P, 16ull * P * P, 16ull * P * P * P};
+  const cuuint32_t box[4] = {(cuuint32_t)(2 * P), (cuuint32_t)R, 1, (cuuint32_t)chunks};
   const cuuint32_t es[4] = {1, 1, 1, 1};
-  const CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, base, dims, strides, box, es,
+  const CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_UINT64, 4, base, dims, strides, box, es,
                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                          CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  if (r != CUDA_SUCCESS) return cfail(c, DNSB_ECUDA, "cuTensorMapEncodeTiled (4-D) failed: %d", (int)r);
+  if (r != CUDA_SUCCESS) return cfail(c, DNSB_ECUDA, "cuTensorMapEncodeTiled (patch) failed: %d", (int)r);
   return 0;
 }
 
-size_t conv_smem(int ci, int co, int P, int R, uint32_t *stage, uint32_t *wbytes, uint32_t *box) {
-  *box = (uint32_t)ci * 3 * R * P * 16;
-  *stage = (*box + 1023) & ~1023u;
+// Weight-gradient runs: dims {2 P^2 (positions and 8 channels), P (z),
+// chunks * B}, box {2 WG_K, 1, chunks} -> shared memory [chunk][WG_K][16 B].
+int make_map_run(dnsb_cnn *c, CUtensorMap *m, void *base, int P, int chunks, int B) {
+  EncodeTiledFn enc = encode_fn();
+  if (!enc) return cfail(c, DNSB_ECUDA, "cuTensorMapEncodeTiled is not available");
+  const cuuint64_t dims[3] = {2ull * P * P, (cuuint64_t)P, (cuuint64_t)chunks * B};
+  const cuuint64_t strides[2] = {16ull * P * P, 16ull * P * P * P};
+  const cuuint32_t box[3] = {2 * WG_K, 1, (cuuint32_t)chunks};
+  const cuuint32_t es[3] = {1, 1, 1};
+  const CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_UINT64, 3, base, dims, strides, box, es,
+                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                         CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return cfail(c, DNSB_ECUDA, "cuTensorMapEncodeTiled (run) failed: %d", (int)r);
+  return 0;
+}
+
+constexpr int RING_MAX = 12, RING_MIN = 4;
+constexpr size_t CONV_EXTRA = 512 + 1024;  // barriers, and alignment slack
+
+// shared memory of a convolution with the largest plane ring that fits
+// (at most RING_MAX slots); 0 when not even RING_MIN slots fit
+size_t conv_smem(int ci, int co, int P, int R, int *nslot, uint32_t *slot, uint32_t *stride,
+                 uint32_t *wbytes) {
+  *slot = (uint32_t)ci * R * P * 16;
+  *stride = (*slot + 1023) & ~1023u;
   *wbytes = 27u * ci * co * 128;
-  return (size_t)*wbytes + 2 * (size_t)*stage + 256 + 1024;
+  const long room = (long)MAX_SMEM - (long)*wbytes - (long)CONV_EXTRA;
+  const int n = (int)std::min<long>(RING_MAX, room / (long)*stride);
+  *nslot = n;
+  if (n < RING_MIN) return 0;
+  return (size_t)*wbytes + (size_t)n * *stride + CONV_EXTRA;
 }
 
 template <int CI, int CO, int MODE>
@@ -470,19 +488,19 @@ int alloc_volume(dnsb_cnn *c, Volume &V, int side, int B, bool training) {
     return cfail(c, DNSB_EUNSUP, "side %d too small: the 128-position tiles need %d patch rows", side,
                  std::max(V.Rf, V.Rb));
   {
-    uint32_t st, wb, bx;
-    const size_t need = std::max(conv_smem(4, 4, P, V.Rf, &st, &wb, &bx),
-                                 training ? conv_smem(4, 4, P, V.Rb, &st, &wb, &bx) : 0);
-    if (need > (size_t)MAX_SMEM)
-      return cfail(c, DNSB_EUNSUP, "side %d too large: a convolution tile needs %zu bytes of shared memory",
-                   side, need);
+    int ns;
+    uint32_t sl, st, wb;
+    if (!conv_smem(4, 4, P, V.Rf, &ns, &sl, &st, &wb) ||
+        (training && !conv_smem(4, 4, P, V.Rb, &ns, &sl, &st, &wb)))
+      return cfail(c, DNSB_EUNSUP, "side %d too large: a convolution's plane ring (%d slots of %u bytes) "
+                   "does not fit in shared memory", side, RING_MIN, sl);
   }
   for (int L = 0; L < NL; L++) {
-    if ((rc = make_map5(c, &V.fwd[L], V.in[L], P, CICH[L], B, V.Rf))) return rc;
+    if ((rc = make_map_patch(c, &V.fwd[L], V.in[L], P, CICH[L], B, V.Rf))) return rc;
     if (training) {
-      if ((rc = make_map4(c, &V.flatA[L], V.in[L], P, CICH[L], B))) return rc;
-      if ((rc = make_map4(c, &V.flatB[L], V.gz[L], P, COCH[L], B))) return rc;
-      if (L > 0 && (rc = make_map5(c, &V.bwd[L], V.gz[L], P, COCH[L], B, V.Rb))) return rc;
+      if ((rc = make_map_run(c, &V.flatA[L], V.in[L], P, CICH[L], B))) return rc;
+      if ((rc = make_map_run(c, &V.flatB[L], V.gz[L], P, COCH[L], B))) return rc;
+      if (L > 0 && (rc = make_map_patch(c, &V.bwd[L], V.gz[L], P, COCH[L], B, V.Rb))) return rc;
     }
   }
   return 0;
@@ -514,9 +532,9 @@ void prof_end(dnsb_cnn *c, Prof &p) {
   c->prof_pending.push_back(p);
 }
 
-int grid_for(dnsb_cnn *c, const void *kernel, size_t smem, long work) {
+int grid_for(dnsb_cnn *c, const void *kernel, size_t smem, long work, int threads) {
   int per = 1;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, NTHREADS, smem) != cudaSuccess || per < 1) {
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, smem) != cudaSuccess || per < 1) {
     cudaGetLastError();
     per = 1;
   }
@@ -539,7 +557,8 @@ int run_conv(dnsb_cnn *c, Volume &V, int L, const CUtensorMap &map, bool transpo
   a.Do = transposed ? V.P - 2 * L : V.P - 2 * (L + 1);
   a.tpp = (a.Do * a.P + TILE_M - 1) / TILE_M;
   a.ntiles = V.B * a.Do * a.tpp;
-  const size_t smem = conv_smem(CI, CO, a.P, a.R, &a.stage_bytes, &a.w_bytes, &a.box_bytes);
+  const size_t smem = conv_smem(CI, CO, a.P, a.R, &a.nslot, &a.slot_bytes, &a.slot_stride, &a.w_bytes);
+  if (!smem) return cfail(c, DNSB_EUNSUP, "convolution plane ring does not fit in shared memory");
   a.wait_limit = WAIT_LIMIT;
   a.wpack = reinterpret_cast<const uint4 *>(transposed ? c->packs.d[L] : c->packs.f[L]);
   a.bias = c->params + LAYOUT.b[L];
@@ -554,7 +573,7 @@ int run_conv(dnsb_cnn *c, Volume &V, int L, const CUtensorMap &map, bool transpo
   a.err = c->deverr;
   int rc = setup_conv_attr<CI, CO, MODE>(c, smem);
   if (rc) return rc;
-  const int grid = grid_for(c, (const void *)k_conv<CI, CO, MODE>, smem, a.ntiles);
+  const int grid = grid_for(c, (const void *)k_conv<CI, CO, MODE>, smem, a.ntiles, CONV_THREADS);
   if (MODE == FWD_LOSS) {
     if (grid > c->loss_nparts) return cfail(c, DNSB_EUNSUP, "loss partials: grid %d > %d", grid, c->loss_nparts);
     c->loss_nparts_used = grid;
@@ -562,7 +581,7 @@ int run_conv(dnsb_cnn *c, Volume &V, int L, const CUtensorMap &map, bool transpo
   const double flops = 2.0 * 27 * CIN[L] * COUT[L] * V.B * pow((double)(V.P - 2 * (L + 1)), 3);
   Prof p;
   prof_begin(c, p, kind, flops);
-  k_conv<CI, CO, MODE><<<grid, NTHREADS, smem, c->stream>>>(map, a);
+  k_conv<CI, CO, MODE><<<grid, CONV_THREADS, smem, c->stream>>>(map, a);
   prof_end(c, p);
   CC(c, cudaGetLastError());
   return 0;

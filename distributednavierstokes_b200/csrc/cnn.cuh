@@ -2,7 +2,7 @@
 //
 // The network (no counterpart in the reference, which has no learned
 // closure): 4 layers of 3x3x3 convolutions, channels 3 -> 32 -> 32 -> 32 ->
-// 6, bias, exact GELU after the first three, periodic padding on the full
+// 6, bias, GELU (tanh form) after the first three, periodic padding on the full
 // field.  Every convolution is an implicit GEMM on the 5th-generation tensor
 // cores: BF16 operands staged in shared memory by TMA, FP32 accumulators in
 // tensor memory (tcgen05.mma, cta_group::1, M = 128), read back with
@@ -22,7 +22,7 @@
 // Forward / transposed convolution (k_conv): one tile = 128 consecutive
 // positions f = y*P + x of one plane of one sample (rows of the GEMM).  With
 // the input patch of that tile staged as whole rows [chunk][dz][row][x][16 B]
-// (one 5-D TMA box: 8 channels x P x R rows x 3 planes x CI chunks), the 128
+// (one 4-D TMA box: x-rows of 16 P bytes x R rows x 3 planes x CI chunks), the 128
 // GEMM rows of every tap are 128 consecutive 16-byte rows of the patch:
 // tap (dx, dy, dz) starts at patch offset x0 + s + dx + (dy + e) P, e = 1 for
 // s < 0 (one extra row below the tile so that offsets stay >= 0).  So the A
@@ -37,7 +37,7 @@
 // g[o][co] over the output positions o (the GEMM's K).  Both operands are
 // MN-major canonical layouts without swizzle, straight from the chunked
 // activations: a K-block of 64 positions of one plane is one TMA box
-// [chunk][64][16 B] per tap; 128 / (8 CI) taps fill the 128 rows (the slot
+// [chunk][1 KB run] per tap; 128 / (8 CI) taps fill the 128 rows (the slot
 // after the last real tap holds ones, which makes that row the bias
 // gradient).  Split-K partials are reduced in a fixed order.
 //
@@ -57,7 +57,8 @@
 namespace dnsb {
 namespace cnn {
 
-constexpr int NTHREADS = 192;
+constexpr int NTHREADS = 192;       // weight gradient: TMA, MMA, 4 epilogue warps
+constexpr int CONV_THREADS = 320;   // convolution: TMA, MMA, 8 epilogue warps
 constexpr int NTAPS = 27;
 constexpr int TILE_M = 128;
 constexpr int WG_K = 64;          // positions per weight-gradient K-block
@@ -91,21 +92,34 @@ __device__ __forceinline__ bool mb_try(uint64_t *b, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// bounded wait; gives up early once the CTA's abort flag is raised
+// try_wait that may suspend the thread for up to `ns` nanoseconds while the
+// phase is incomplete (returns as soon as it completes)
+__device__ __forceinline__ bool mb_try_sleep(uint64_t *b, uint32_t parity, uint32_t ns) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(saddr(b)), "r"(parity), "r"(ns)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait: at most `limit` polls, each suspending up to 1 us (so a
+// waiting role takes no issue slots from the working warps); gives up
+// early once the CTA's abort flag is raised.
 __device__ __forceinline__ bool mb_wait(uint64_t *b, uint32_t parity, unsigned limit,
                                         volatile int *abort_flag) {
   for (unsigned it = 0; it < limit; it++) {
-    if (mb_try(b, parity)) return true;
-    if ((it & 255) == 255 && *abort_flag) return false;
+    if (mb_try_sleep(b, parity, 1000)) return true;
+    if ((it & 15) == 15 && *abort_flag) return false;
   }
   return false;
 }
-__device__ __forceinline__ void tma5(void *dst, const CUtensorMap *m, int c0, int c1, int c2, int c3,
-                                     int c4, uint64_t *bar) {
+__device__ __forceinline__ void tma3(void *dst, const CUtensorMap *m, int c0, int c1, int c2,
+                                     uint64_t *bar) {
   asm volatile(
-      "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(
           saddr(dst)),
-      "l"(m), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(saddr(bar))
+      "l"(m), "r"(c0), "r"(c1), "r"(c2), "r"(saddr(bar))
       : "memory");
 }
 __device__ __forceinline__ void tma4(void *dst, const CUtensorMap *m, int c0, int c1, int c2, int c3,
@@ -194,12 +208,21 @@ __device__ __forceinline__ void tmem_ld<32>(uint32_t taddr, float *v) {
   for (int i = 0; i < 32; i++) v[i] = __uint_as_float(r[i]);
 }
 
-__device__ __forceinline__ float gelu_f(float z) {
-  return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f));
+// GELU in its tanh form, 0.5 z (1 + tanh(u)) with u = sqrt(2/pi) (z +
+// 0.044715 z^3), written as z sigma(2u) (sigma(x) = 1 / (1 + e^-x)) with the
+// hardware exponential: a handful of instructions, about 1e-7 relative.
+constexpr float GELU_C = 0.7978845608028654f;  // sqrt(2 / pi)
+constexpr float GELU_A = 0.044715f;
+__device__ __forceinline__ float sigmoid2u(float z) {
+  const float u2 = 2.f * GELU_C * fmaf(GELU_A * z, z * z, z);
+  return __frcp_rn(1.f + __expf(-u2));
 }
+__device__ __forceinline__ float gelu_f(float z) { return z * sigmoid2u(z); }
+// d/dz [z sigma(2u)] = sigma + z sigma (1 - sigma) 2 u'(z)
 __device__ __forceinline__ float gelu_grad_f(float z) {
-  return 0.5f * (1.0f + erff(z * 0.70710678118654752f)) +
-         z * expf(-0.5f * z * z) * 0.39894228040143268f;
+  const float sg = sigmoid2u(z);
+  const float du2 = 2.f * GELU_C * fmaf(3.f * GELU_A * z, z, 1.f);
+  return fmaf(z * sg * (1.f - sg), du2, sg);
 }
 
 __device__ __forceinline__ uint4 pack8(const float *v) {
@@ -231,9 +254,10 @@ struct ConvArgs {
   int Do;              // output box side
   int s, e, R;         // input offset (0 / -2), extra patch row, patch rows
   int tpp;             // tiles per plane: ceil(Do * P / 128)
-  int ntiles;          // B * Do * tpp
-  uint32_t box_bytes;    // CI * 3 * R * P * 16 (one TMA box)
-  uint32_t stage_bytes;  // stage stride: box_bytes rounded up to 1 KB
+  int ntiles;          // B * tpp * Do output tiles, z fastest
+  int nslot;           // input planes held in the shared-memory ring
+  uint32_t slot_bytes;   // one input plane: CI * R * P * 16 (one TMA box)
+  uint32_t slot_stride;  // slot_bytes rounded up to 1 KB
   uint32_t w_bytes;      // 27 * CI * CO * 128
   unsigned wait_limit;
   const uint4 *wpack;    // packed weights (B operand), w_bytes
@@ -250,30 +274,42 @@ struct ConvArgs {
 };
 
 // Forward / transposed convolution, CI input chunks, CO output chunks
-// (N = 8 CO GEMM columns), persistent over tiles.
+// (N = 8 CO GEMM columns).  Tiles are numbered z fastest (tile = ((b tpp) +
+// j) Do + z) and every CTA takes one contiguous range of them, marching up
+// z: the input planes z+s .. z+s+2 of a tile sit in a ring of nslot
+// shared-memory slots, so a tile loads one new plane (three at the start
+// of a column) and the planes are released to the producer after their
+// last use.
 template <int CI, int CO, int MODE>
-__global__ void __launch_bounds__(NTHREADS, 1)
+__global__ void __launch_bounds__(CONV_THREADS, 1)
     k_conv(const __grid_constant__ CUtensorMap tin, const ConvArgs a) {
   constexpr int N = 8 * CO;
   constexpr uint32_t NCOLS = 2 * N < 32 ? 32 : 2 * N;  // two accumulators
+  constexpr int MAXSLOT = 12;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   // 1 KB-aligned base (TMA destinations; the host adds 1 KB of slack)
   unsigned char *smem = smem_raw + ((1024u - (saddr(smem_raw) & 1023u)) & 1023u);
   unsigned char *wsm = smem;
-  unsigned char *stg = smem + a.w_bytes;
-  uint64_t *bars = reinterpret_cast<uint64_t *>(stg + CV_STAGES * a.stage_bytes);
-  uint64_t *full = bars, *empty = bars + 2, *tfull = bars + 4, *tempty = bars + 6, *wbar = bars + 8;
-  uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + 9);
-  volatile int *abort_flag = reinterpret_cast<volatile int *>(bars + 10);
-  float *lsum = reinterpret_cast<float *>(bars + 11);  // 4 floats
+  unsigned char *ring = smem + a.w_bytes;
+  uint64_t *bars = reinterpret_cast<uint64_t *>(ring + a.nslot * a.slot_stride);
+  uint64_t *full = bars, *empty = bars + MAXSLOT, *tfull = bars + 2 * MAXSLOT,
+           *tempty = bars + 2 * MAXSLOT + 2, *wbar = bars + 2 * MAXSLOT + 4;
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + 2 * MAXSLOT + 5);
+  volatile int *abort_flag = reinterpret_cast<volatile int *>(bars + 2 * MAXSLOT + 6);
+  float *lsum = reinterpret_cast<float *>(bars + 2 * MAXSLOT + 7);  // 8 floats
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  // this CTA's tiles
+  const int t0 = (int)((long long)a.ntiles * blockIdx.x / gridDim.x);
+  const int t1 = (int)((long long)a.ntiles * (blockIdx.x + 1) / gridDim.x);
 
   if (threadIdx.x == 0) {
-    for (int i = 0; i < 2; i++) {
+    for (int i = 0; i < a.nslot; i++) {
       mb_init(&full[i], 1);
       mb_init(&empty[i], 1);
+    }
+    for (int i = 0; i < 2; i++) {
       mb_init(&tfull[i], 1);
-      mb_init(&tempty[i], 4);
+      mb_init(&tempty[i], 8);
     }
     mb_init(wbar, 1);
     *abort_flag = 0;
@@ -288,66 +324,84 @@ __global__ void __launch_bounds__(NTHREADS, 1)
 
   if (warp == 0) {
     if (lane == 0) {
-      // weights once, then the patch of every tile
+      // weights once, then the input planes of the tiles in order
       mb_expect(wbar, a.w_bytes);
       bulk_load(wsm, a.wpack, a.w_bytes, wbar);
-      int i = 0, last_s = -1, last_ph = 0, prev_s = -1, prev_ph = 0;
-      for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x, i++) {
-        const int s = i & 1, ph = (i >> 1) & 1;
-        if (*abort_flag || !mb_wait(&empty[s], ph ^ 1, a.wait_limit, abort_flag)) {
-          *abort_flag = 1;
-          atomicExch(a.err, DEVERR_CNN_TIMEOUT);
-          break;
+      int g = 0;
+      bool ok = true;
+      for (int t = t0; ok && t < t1; t++) {
+        const int z = t % a.Do, rest = t / a.Do;
+        const int j = rest % a.tpp, b = rest / a.tpp;
+        const int y0 = (j * TILE_M) / a.P;
+        const bool fresh = t == t0 || z == 0;
+        for (int zp = fresh ? 0 : 2; zp < 3; zp++, g++) {
+          const int sl = g % a.nslot, ph = (g / a.nslot) & 1;
+          if (*abort_flag || !mb_wait(&empty[sl], ph ^ 1, a.wait_limit, abort_flag)) {
+            ok = false;
+            break;
+          }
+          mb_expect(&full[sl], a.slot_bytes);
+          tma4(ring + sl * a.slot_stride, &tin, 0, y0 + a.s - a.e, z + a.s + zp, b * CI, &full[sl]);
         }
-        const int j = t % a.tpp, rest = t / a.tpp;
-        const int z = rest % a.Do, b = rest / a.Do;
-        const int f0 = j * TILE_M, y0 = f0 / a.P;
-        mb_expect(&full[s], a.box_bytes);
-        tma5(stg + s * a.stage_bytes, &tin, 0, 0, y0 + a.s - a.e, z + a.s, b * CI, &full[s]);
-        prev_s = last_s;
-        prev_ph = last_ph;
-        last_s = s;
-        last_ph = ph;
+      }
+      if (!ok) {
+        *abort_flag = 1;
+        atomicExch(a.err, DEVERR_CNN_TIMEOUT);
       }
       // the copies issued last land before the CTA may leave
-      if (last_s >= 0) mb_wait(&full[last_s], last_ph, a.wait_limit, abort_flag);
-      if (prev_s >= 0) mb_wait(&full[prev_s], prev_ph, a.wait_limit, abort_flag);
+      for (int g2 = g - a.nslot < 0 ? 0 : g - a.nslot; g2 < g; g2++)
+        mb_wait(&full[g2 % a.nslot], (g2 / a.nslot) & 1, a.wait_limit, abort_flag);
       mb_wait(wbar, 0, a.wait_limit, abort_flag);
     }
   } else if (warp == 1) {
     if (lane == 0) {
       constexpr uint32_t idesc = idesc_bf16(N, false, false);
-      const uint32_t wb = saddr(wsm);
-      const uint32_t plane = (uint32_t)a.R * a.P * 16;
-      const uint32_t cstride = 3 * plane;
-      int i = 0, last_a = -1, last_aph = 0;
+      // Descriptors are built once; per MMA only the start-address field
+      // (bits 0-13, 16-byte units) moves, by an offset added to the whole
+      // 64-bit word (starts stay below 256 KB, so the field never carries).
+      const uint32_t cstride_u = (uint32_t)a.R * a.P;  // chunk stride in a slot, 16-byte units
+      const uint64_t bdesc0 = sdesc(saddr(wsm), CO * 128u, 128);
+      const uint64_t adesc_st = sdesc(0, cstride_u * 16u, 128);  // start 0
+      const uint32_t ring_u = saddr(ring) >> 4, stride_u = a.slot_stride >> 4;
+      uint32_t yrow[3];  // (dy + e) P, 16-byte units
+#pragma unroll
+      for (int q = 0; q < 3; q++) yrow[q] = (uint32_t)((q + a.e) * a.P);
+      int g = 0, i = 0, last_a = -1, last_aph = 0;
       bool ok = mb_wait(wbar, 0, a.wait_limit, abort_flag);
-      for (int t = blockIdx.x; ok && t < a.ntiles; t += gridDim.x, i++) {
-        const int s = i & 1, ph = (i >> 1) & 1;
+      for (int t = t0; ok && t < t1; t++, i++) {
+        const int z = t % a.Do, j = (t / a.Do) % a.tpp;
+        const bool fresh = t == t0 || z == 0;
+        const bool last = t == t1 - 1 || z == a.Do - 1;
         const int ac = i & 1, aph = (i >> 1) & 1;
-        if (*abort_flag || !mb_wait(&tempty[ac], aph ^ 1, a.wait_limit, abort_flag) ||
-            !mb_wait(&full[s], ph, a.wait_limit, abort_flag)) {
+        for (int q = fresh ? 0 : 2; q < 3 && ok; q++, g++)
+          ok = !*abort_flag && mb_wait(&full[g % a.nslot], (g / a.nslot) & 1, a.wait_limit, abort_flag);
+        if (!ok || *abort_flag || !mb_wait(&tempty[ac], aph ^ 1, a.wait_limit, abort_flag)) {
           ok = false;
           break;
         }
         tc_fence_after();
-        const int j = t % a.tpp;
         const int x0 = (j * TILE_M) % a.P;
-        const uint32_t sb = saddr(stg + s * a.stage_bytes);
-        const uint32_t dacc = tbase + (uint32_t)(ac * N);
-#pragma unroll 1
-        for (int tap = 0; tap < NTAPS; tap++) {
-          const int dz = tap / 9, dy = (tap / 3) % 3, dx = tap % 3;
-          const uint32_t off = (uint32_t)(x0 + a.s + dx + (dy + a.e) * a.P) * 16u;
+        uint64_t ab[3];  // planes z+s, z+s+1, z+s+2 are the last three loaded
 #pragma unroll
-          for (int k = 0; k < CI / 2; k++) {
-            const uint64_t ad = sdesc(sb + (uint32_t)(2 * k) * cstride + dz * plane + off, cstride, 128);
-            const uint64_t bd = sdesc(wb + (uint32_t)((tap * CI + 2 * k) * CO) * 128u, CO * 128u, 128);
-            mma_bf16(dacc, ad, bd, idesc, (tap | k) != 0);
-          }
+        for (int dz = 0; dz < 3; dz++)
+          ab[dz] = adesc_st + (uint64_t)(ring_u + (uint32_t)((g - 3 + dz) % a.nslot) * stride_u +
+                                         (uint32_t)(x0 + a.s));
+        const uint32_t dacc = tbase + (uint32_t)(ac * N);
+#pragma unroll
+        for (int tap = 0; tap < NTAPS; tap++) {
+          const uint64_t at = ab[tap / 9] + (uint64_t)(yrow[(tap / 3) % 3] + (uint32_t)(tap % 3));
+#pragma unroll
+          for (int k = 0; k < CI / 2; k++)
+            mma_bf16(dacc, at + (uint64_t)(2 * k) * cstride_u,
+                     bdesc0 + (uint64_t)((tap * CI + 2 * k) * CO * 8), idesc, (tap | k) != 0 ? 1u : 0u);
         }
-        mma_commit(&empty[s]);
         mma_commit(&tfull[ac]);
+        // release the planes this tile used for the last time
+        mma_commit(&empty[(g - 3) % a.nslot]);
+        if (last) {
+          mma_commit(&empty[(g - 2) % a.nslot]);
+          mma_commit(&empty[(g - 1) % a.nslot]);
+        }
         last_a = ac;
         last_aph = aph;
       }
@@ -359,12 +413,26 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       if (last_a >= 0) mb_wait(&tfull[last_a], last_aph, a.wait_limit, abort_flag);
     }
   } else {
-    // epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31
-    const int q = warp & 3;
+    // epilogue: 8 warps; warp w reads TMEM lanes 32 (w % 4) .. + 31, the
+    // first four columns 0-15, the other four 16-31 (N = 32); with N = 16
+    // the second four only release the accumulator
+    const int e = warp - 2, q = warp & 3, half = e >> 2;
+    const bool active = CO == 4 || half == 0;
     const int m = q * 32 + lane;
+    constexpr int NB = CO == 4 ? 16 : 8;   // outputs this warp writes per row
+    float br[NB], osc[6];
+#pragma unroll
+    for (int k = 0; k < NB; k++)
+      br[k] = (MODE != DGRAD && active && (CO == 4 || k < 6)) ? __ldg(a.bias + 16 * half + k) : 0.f;
+#pragma unroll
+    for (int k = 0; k < 6; k++) osc[k] = MODE == FWD_INFER ? __ldg(a.oscale + k) : 0.f;
     float lacc = 0.f;
+    // the tile's (b, j, z) and this thread's position, updated as z marches
+    int z = t0 % a.Do, j = (t0 / a.Do) % a.tpp, b = t0 / (a.Do * a.tpp);
+    int f = 0, x = 0, y = 0;
+    bool fresh = true;
     int i = 0;
-    for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x, i++) {
+    for (int t = t0; t < t1; t++, i++) {
       const int ac = i & 1, aph = (i >> 1) & 1;
       if (*abort_flag || !mb_wait(&tfull[ac], aph, a.wait_limit, abort_flag)) {
         *abort_flag = 1;
@@ -372,72 +440,84 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         break;
       }
       tc_fence_after();
-      float v[N];
-      tmem_ld<N>(tbase + ((uint32_t)(q * 32) << 16) + (uint32_t)(ac * N), v);
+      float v[16];
+      if (active) tmem_ld<16>(tbase + ((uint32_t)(q * 32) << 16) + (uint32_t)(ac * N + 16 * half), v);
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mb_arrive(&tempty[ac]);
-      const int j = t % a.tpp, rest = t / a.tpp;
-      const int z = rest % a.Do, b = rest / a.Do;
-      const int f = j * TILE_M + m;
-      if (f >= P2) continue;
-      const int x = f % a.P, y = f / a.P;
+      if (fresh) {
+        f = j * TILE_M + m;
+        x = f % a.P;
+        y = f / a.P;
+        fresh = false;
+      }
+      const int zc = z, bc = b;
+      if (++z == a.Do) {  // next column
+        z = 0;
+        fresh = true;
+        if (++j == a.tpp) {
+          j = 0;
+          b++;
+        }
+      }
+      if (!active || f >= P2) continue;
       const bool valid = x < a.Do && y < a.Do;
-      const long long vox = (long long)z * P2 + f;
+      const long long vox = (long long)zc * P2 + f;
       if (MODE == FWD_GELU) {
 #pragma unroll
-        for (int c = 0; c < CO; c++) {
+        for (int cc = 0; cc < 2; cc++) {
+          const int c = 2 * half + cc;
           float zv[8], hv[8];
 #pragma unroll
           for (int k = 0; k < 8; k++) {
-            const float zz = valid ? v[8 * c + k] + __ldg(a.bias + 8 * c + k) : 0.f;
+            const float zz = valid ? v[8 * cc + k] + br[8 * cc + k] : 0.f;
             zv[k] = zz;
-            hv[k] = valid ? gelu_f(zz) : 0.f;
+            hv[k] = gelu_f(zz);
           }
-          const long long o = ((long long)(b * CO + c) * a.Pz) * P2 + vox;
+          const long long o = ((long long)(bc * CO + c) * a.Pz) * P2 + vox;
           a.zout[o] = pack8(zv);
           a.out[o] = pack8(hv);
         }
       } else if (MODE == FWD_LOSS) {
         // 6 output components in chunk 0 (N = 16: chunk 1 stays zero)
-        float tv[8];
+        float tv[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
         if (valid) {
-          const float4 *tp = a.target + ((long long)b * a.Pz * P2 + vox) * 2;
-          const float4 t0 = tp[0], t1 = tp[1];
-          tv[0] = t0.x; tv[1] = t0.y; tv[2] = t0.z; tv[3] = t0.w;
-          tv[4] = t1.x; tv[5] = t1.y; tv[6] = 0.f; tv[7] = 0.f;
+          const float4 *tp = a.target + ((long long)bc * a.Pz * P2 + vox) * 2;
+          const float4 t0v = tp[0], t1v = tp[1];
+          tv[0] = t0v.x; tv[1] = t0v.y; tv[2] = t0v.z; tv[3] = t0v.w;
+          tv[4] = t1v.x; tv[5] = t1v.y;
         }
         float gv[8];
 #pragma unroll
         for (int k = 0; k < 8; k++) {
           float g = 0.f;
           if (valid && k < 6) {
-            const float d = v[k] + __ldg(a.bias + k) - tv[k];
+            const float d = v[k] + br[k] - tv[k];
             lacc += d * d;
             g = a.loss_scale * d;
           }
           gv[k] = g;
         }
-        const long long o = ((long long)(b * CO) * a.Pz) * P2 + vox;
+        const long long o = ((long long)(bc * CO) * a.Pz) * P2 + vox;
         a.out[o] = pack8(gv);
       } else if (MODE == FWD_INFER) {
         if (valid) {
           const long long n3 = (long long)a.Do * a.Do * a.Do;
-          const long long o = ((long long)z * a.Do + y) * a.Do + x;
+          const long long o = ((long long)zc * a.Do + y) * a.Do + x;
 #pragma unroll
-          for (int k = 0; k < 6; k++)
-            a.infer_out[k * n3 + o] = (double)((v[k] + __ldg(a.bias + k)) * __ldg(a.oscale + k));
+          for (int k = 0; k < 6; k++) a.infer_out[k * n3 + o] = (double)((v[k] + br[k]) * osc[k]);
         }
       } else {  // DGRAD: g = dL/dh * gelu'(z) of the output's layer
 #pragma unroll
-        for (int c = 0; c < CO; c++) {
-          const long long o = ((long long)(b * CO + c) * a.Pz) * P2 + vox;
+        for (int cc = 0; cc < 2; cc++) {
+          const int c = 2 * half + cc;
+          const long long o = ((long long)(bc * CO + c) * a.Pz) * P2 + vox;
           float gv[8];
           if (valid) {
             float zv[8];
             unpack8(a.zin[o], zv);
 #pragma unroll
-            for (int k = 0; k < 8; k++) gv[k] = v[8 * c + k] * gelu_grad_f(zv[k]);
+            for (int k = 0; k < 8; k++) gv[k] = v[8 * cc + k] * gelu_grad_f(zv[k]);
           } else {
 #pragma unroll
             for (int k = 0; k < 8; k++) gv[k] = 0.f;
@@ -449,13 +529,13 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     if (MODE == FWD_LOSS) {
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) lacc += __shfl_xor_sync(0xffffffffu, lacc, o);
-      if (lane == 0) lsum[warp - 2] = lacc;
+      if (lane == 0) lsum[e] = lacc;
     }
   }
   tc_fence_before();
   __syncthreads();
   if (MODE == FWD_LOSS && threadIdx.x == 0)
-    a.loss_part[blockIdx.x] = (lsum[0] + lsum[1]) + (lsum[2] + lsum[3]);
+    a.loss_part[blockIdx.x] = (lsum[0] + lsum[1]) + (lsum[2] + lsum[3]);  // the four half-0 warps
   if (warp == 1) {
     tc_fence_after();
     tmem_free(tbase, NCOLS);
@@ -545,9 +625,9 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         for (int j = 0; j < ntap; j++) {
           const int tap = tap0 + j;
           const int dz = tap / 9, dy = (tap / 3) % 3, dx = tap % 3;
-          tma4(st + j * SLOT, &th, 0, f0 + dx + dy * a.P, z + dz, b * CI, &full[s]);
+          tma3(st + j * SLOT, &th, 2 * (f0 + dx + dy * a.P), z + dz, b * CI, &full[s]);
         }
-        tma4(st + a.a_bytes, &tg, 0, f0, z, b * CO, &full[s]);
+        tma3(st + a.a_bytes, &tg, 2 * f0, z, b * CO, &full[s]);
         issued = i + 1;
       }
       // let the last copies of every stage land before leaving

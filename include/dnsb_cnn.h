@@ -9,7 +9,7 @@
  * library's own DNS (dnsb_les_cube + the host half of the sampler).
  *
  * The network: 4 convolution layers, 3x3x3 kernels, channels 3 -> 32 -> 32
- * -> 32 -> 6, bias, exact GELU after the first three, periodic padding on
+ * -> 32 -> 6, bias, GELU (tanh form) after the first three, periodic padding on
  * the full periodic field.  BF16 weights / activations / gradients, FP32
  * accumulation on the tensor cores (tcgen05.mma, accumulators in tensor
  * memory, operands staged by TMA), FP32 master weights and Adam state.

@@ -9,8 +9,9 @@ kernels implement, restated in float64 numpy with the same storage
 roundings, so that the two can be compared:
 
 * 4 convolution layers, 3x3x3 kernels, channels 3 -> 32 -> 32 -> 32 -> 6,
-  bias on every layer, exact GELU (0.5 z (1 + erf(z / sqrt 2))) after the
-  first three;
+  bias on every layer, GELU in its tanh form
+  (0.5 z (1 + tanh(sqrt(2/pi) (z + 0.044715 z^3))), evaluated as z sigma(2u))
+  after the first three;
 * periodic padding on the full periodic field.  Training crops carry a halo
   of 4 cells taken from their periodic parent field and the layers are
   "valid" convolutions (each shrinks the box by 2), so a crop's outputs are
@@ -47,17 +48,27 @@ def f32(x):
     return np.asarray(x, dtype=np.float32).astype(np.float64)
 
 
-def _erf(x):
-    from scipy.special import erf
-    return erf(x)
+GELU_C = math.sqrt(2.0 / math.pi)
+GELU_A = 0.044715
+
+
+def _sigmoid2u(z):
+    u2 = 2.0 * GELU_C * (z + GELU_A * z ** 3)
+    return 1.0 / (1.0 + np.exp(-u2))
 
 
 def gelu(z):
-    return 0.5 * z * (1.0 + _erf(z / math.sqrt(2.0)))
+    """GELU in its tanh form: 0.5 z (1 + tanh(sqrt(2/pi) (z + 0.044715 z^3)))
+    = z sigma(2u)."""
+    with np.errstate(over="ignore"):
+        return z * _sigmoid2u(z)
 
 
 def gelu_grad(z):
-    return 0.5 * (1.0 + _erf(z / math.sqrt(2.0))) + z * np.exp(-0.5 * z * z) / math.sqrt(2 * math.pi)
+    with np.errstate(over="ignore"):
+        sg = _sigmoid2u(z)
+    du2 = 2.0 * GELU_C * (1.0 + 3.0 * GELU_A * z * z)
+    return sg + z * sg * (1.0 - sg) * du2
 
 
 def init_params(seed=0, channels=CHANNELS):
