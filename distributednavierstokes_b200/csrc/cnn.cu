@@ -477,10 +477,6 @@ int alloc_volume(dnsb_cnn *c, Volume &V, int side, int B, bool training) {
     for (int L = 0; L < NL; L++)
       if ((rc = dal(c, &V.gz[L], (size_t)B * COCH[L] * P3))) return rc;
     if ((rc = dal(c, &V.tgt, (size_t)B * P3 * 2))) return rc;
-  } else {
-    // inference keeps no pre-activations: one scratch for all three
-    if ((rc = dal(c, &V.z[0], (size_t)B * 4 * P3))) return rc;
-    V.z[1] = V.z[2] = V.z[0];
   }
   V.Rf = patch_rows(P, 0, 0);
   V.Rb = patch_rows(P, -2, 1);
@@ -947,9 +943,10 @@ static int infer_common(dnsb_cnn *c, const double *v, const double *ux, const do
   k_infer_in<<<(unsigned)((P3 + 255) / 256), 256, 0, c->stream>>>(v, ux, uy, uz, V.side, V.P, c->scales, V.in[0]);
   prof_end(c, p);
   CC(c, cudaGetLastError());
-  if ((rc = run_conv<2, 4, FWD_GELU>(c, V, 0, V.fwd[0], false, V.in[1], V.z[0], nullptr, nullptr, 0)) ||
-      (rc = run_conv<4, 4, FWD_GELU>(c, V, 1, V.fwd[1], false, V.in[2], V.z[1], nullptr, nullptr, 0)) ||
-      (rc = run_conv<4, 4, FWD_GELU>(c, V, 2, V.fwd[2], false, V.in[3], V.z[2], nullptr, nullptr, 0)) ||
+  // inference keeps no pre-activations (zout = nullptr)
+  if ((rc = run_conv<2, 4, FWD_GELU>(c, V, 0, V.fwd[0], false, V.in[1], nullptr, nullptr, nullptr, 0)) ||
+      (rc = run_conv<4, 4, FWD_GELU>(c, V, 1, V.fwd[1], false, V.in[2], nullptr, nullptr, nullptr, 0)) ||
+      (rc = run_conv<4, 4, FWD_GELU>(c, V, 2, V.fwd[2], false, V.in[3], nullptr, nullptr, nullptr, 0)) ||
       (rc = run_conv<4, 2, FWD_INFER>(c, V, 3, V.fwd[3], false, nullptr, nullptr, nullptr, tau, 0)))
     return rc;
   return 0;

@@ -215,7 +215,7 @@ constexpr float GELU_C = 0.7978845608028654f;  // sqrt(2 / pi)
 constexpr float GELU_A = 0.044715f;
 __device__ __forceinline__ float sigmoid2u(float z) {
   const float u2 = 2.f * GELU_C * fmaf(GELU_A * z, z * z, z);
-  return __frcp_rn(1.f + __expf(-u2));
+  return __fdividef(1.f, 1.f + __expf(-u2));  // 0 once e^-u2 overflows
 }
 __device__ __forceinline__ float gelu_f(float z) { return z * sigmoid2u(z); }
 // d/dz [z sigma(2u)] = sigma + z sigma (1 - sigma) 2 u'(z)
@@ -284,7 +284,8 @@ template <int CI, int CO, int MODE>
 __global__ void __launch_bounds__(CONV_THREADS, 1)
     k_conv(const __grid_constant__ CUtensorMap tin, const ConvArgs a) {
   constexpr int N = 8 * CO;
-  constexpr uint32_t NCOLS = 2 * N < 32 ? 32 : 2 * N;  // two accumulators
+  constexpr int NACC = 4;                               // accumulators in flight
+  constexpr uint32_t NCOLS = NACC * N;                  // 64 or 128 columns
   constexpr int MAXSLOT = 12;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   // 1 KB-aligned base (TMA destinations; the host adds 1 KB of slack)
@@ -293,10 +294,10 @@ __global__ void __launch_bounds__(CONV_THREADS, 1)
   unsigned char *ring = smem + a.w_bytes;
   uint64_t *bars = reinterpret_cast<uint64_t *>(ring + a.nslot * a.slot_stride);
   uint64_t *full = bars, *empty = bars + MAXSLOT, *tfull = bars + 2 * MAXSLOT,
-           *tempty = bars + 2 * MAXSLOT + 2, *wbar = bars + 2 * MAXSLOT + 4;
-  uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + 2 * MAXSLOT + 5);
-  volatile int *abort_flag = reinterpret_cast<volatile int *>(bars + 2 * MAXSLOT + 6);
-  float *lsum = reinterpret_cast<float *>(bars + 2 * MAXSLOT + 7);  // 8 floats
+           *tempty = bars + 2 * MAXSLOT + NACC, *wbar = bars + 2 * MAXSLOT + 2 * NACC;
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + 2 * MAXSLOT + 2 * NACC + 1);
+  volatile int *abort_flag = reinterpret_cast<volatile int *>(bars + 2 * MAXSLOT + 2 * NACC + 2);
+  float *lsum = reinterpret_cast<float *>(bars + 2 * MAXSLOT + 2 * NACC + 3);  // 8 floats
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   // this CTA's tiles
   const int t0 = (int)((long long)a.ntiles * blockIdx.x / gridDim.x);
@@ -307,9 +308,9 @@ __global__ void __launch_bounds__(CONV_THREADS, 1)
       mb_init(&full[i], 1);
       mb_init(&empty[i], 1);
     }
-    for (int i = 0; i < 2; i++) {
+    for (int i = 0; i < NACC; i++) {
       mb_init(&tfull[i], 1);
-      mb_init(&tempty[i], 8);
+      mb_init(&tempty[i], 4);
     }
     mb_init(wbar, 1);
     *abort_flag = 0;
@@ -372,7 +373,7 @@ __global__ void __launch_bounds__(CONV_THREADS, 1)
         const int z = t % a.Do, j = (t / a.Do) % a.tpp;
         const bool fresh = t == t0 || z == 0;
         const bool last = t == t1 - 1 || z == a.Do - 1;
-        const int ac = i & 1, aph = (i >> 1) & 1;
+        const int ac = i % NACC, aph = (i / NACC) & 1;
         for (int q = fresh ? 0 : 2; q < 3 && ok; q++, g++)
           ok = !*abort_flag && mb_wait(&full[g % a.nslot], (g / a.nslot) & 1, a.wait_limit, abort_flag);
         if (!ok || *abort_flag || !mb_wait(&tempty[ac], aph ^ 1, a.wait_limit, abort_flag)) {
@@ -413,19 +414,18 @@ __global__ void __launch_bounds__(CONV_THREADS, 1)
       if (last_a >= 0) mb_wait(&tfull[last_a], last_aph, a.wait_limit, abort_flag);
     }
   } else {
-    // epilogue: 8 warps; warp w reads TMEM lanes 32 (w % 4) .. + 31, the
-    // first four columns 0-15, the other four 16-31 (N = 32); with N = 16
-    // the second four only release the accumulator
-    const int e = warp - 2, q = warp & 3, half = e >> 2;
-    const bool active = CO == 4 || half == 0;
+    // epilogue: two groups of 4 warps take alternate tiles (group e / 4 the
+    // tiles with local index i % 2 == e / 4); warp w reads TMEM lanes
+    // 32 (w % 4) .. + 31, all N columns of its tile
+    const int e = warp - 2, q = warp & 3, grp = e >> 2;
     const int m = q * 32 + lane;
-    constexpr int NB = CO == 4 ? 16 : 8;   // outputs this warp writes per row
+    constexpr int NB = CO == 4 ? 32 : 8;   // outputs written per row
     float br[NB], osc[6];
 #pragma unroll
-    for (int k = 0; k < NB; k++)
-      br[k] = (MODE != DGRAD && active && (CO == 4 || k < 6)) ? __ldg(a.bias + 16 * half + k) : 0.f;
+    for (int k = 0; k < NB; k++) br[k] = (MODE != DGRAD && (CO == 4 || k < 6)) ? __ldg(a.bias + k) : 0.f;
 #pragma unroll
     for (int k = 0; k < 6; k++) osc[k] = MODE == FWD_INFER ? __ldg(a.oscale + k) : 0.f;
+    const bool store_z = a.zout != nullptr;
     float lacc = 0.f;
     // the tile's (b, j, z) and this thread's position, updated as z marches
     int z = t0 % a.Do, j = (t0 / a.Do) % a.tpp, b = t0 / (a.Do * a.tpp);
@@ -433,18 +433,21 @@ __global__ void __launch_bounds__(CONV_THREADS, 1)
     bool fresh = true;
     int i = 0;
     for (int t = t0; t < t1; t++, i++) {
-      const int ac = i & 1, aph = (i >> 1) & 1;
-      if (*abort_flag || !mb_wait(&tfull[ac], aph, a.wait_limit, abort_flag)) {
-        *abort_flag = 1;
-        atomicExch(a.err, DEVERR_CNN_TIMEOUT);
-        break;
+      const bool mine = (i & 1) == grp;
+      const int ac = i % NACC, aph = (i / NACC) & 1;
+      float v[N];
+      if (mine) {
+        if (*abort_flag || !mb_wait(&tfull[ac], aph, a.wait_limit, abort_flag)) {
+          *abort_flag = 1;
+          atomicExch(a.err, DEVERR_CNN_TIMEOUT);
+          break;
+        }
+        tc_fence_after();
+        tmem_ld<N>(tbase + ((uint32_t)(q * 32) << 16) + (uint32_t)(ac * N), v);
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mb_arrive(&tempty[ac]);
       }
-      tc_fence_after();
-      float v[16];
-      if (active) tmem_ld<16>(tbase + ((uint32_t)(q * 32) << 16) + (uint32_t)(ac * N + 16 * half), v);
-      tc_fence_before();
-      __syncwarp();
-      if (lane == 0) mb_arrive(&tempty[ac]);
       if (fresh) {
         f = j * TILE_M + m;
         x = f % a.P;
@@ -460,22 +463,21 @@ __global__ void __launch_bounds__(CONV_THREADS, 1)
           b++;
         }
       }
-      if (!active || f >= P2) continue;
+      if (!mine || f >= P2) continue;
       const bool valid = x < a.Do && y < a.Do;
       const long long vox = (long long)zc * P2 + f;
       if (MODE == FWD_GELU) {
 #pragma unroll
-        for (int cc = 0; cc < 2; cc++) {
-          const int c = 2 * half + cc;
+        for (int c = 0; c < CO; c++) {
           float zv[8], hv[8];
 #pragma unroll
           for (int k = 0; k < 8; k++) {
-            const float zz = valid ? v[8 * cc + k] + br[8 * cc + k] : 0.f;
+            const float zz = valid ? v[8 * c + k] + br[8 * c + k] : 0.f;
             zv[k] = zz;
             hv[k] = gelu_f(zz);
           }
           const long long o = ((long long)(bc * CO + c) * a.Pz) * P2 + vox;
-          a.zout[o] = pack8(zv);
+          if (store_z) a.zout[o] = pack8(zv);
           a.out[o] = pack8(hv);
         }
       } else if (MODE == FWD_LOSS) {
@@ -509,15 +511,14 @@ __global__ void __launch_bounds__(CONV_THREADS, 1)
         }
       } else {  // DGRAD: g = dL/dh * gelu'(z) of the output's layer
 #pragma unroll
-        for (int cc = 0; cc < 2; cc++) {
-          const int c = 2 * half + cc;
+        for (int c = 0; c < CO; c++) {
           const long long o = ((long long)(bc * CO + c) * a.Pz) * P2 + vox;
           float gv[8];
           if (valid) {
             float zv[8];
             unpack8(a.zin[o], zv);
 #pragma unroll
-            for (int k = 0; k < 8; k++) gv[k] = v[8 * cc + k] * gelu_grad_f(zv[k]);
+            for (int k = 0; k < 8; k++) gv[k] = v[8 * c + k] * gelu_grad_f(zv[k]);
           } else {
 #pragma unroll
             for (int k = 0; k < 8; k++) gv[k] = 0.f;
@@ -535,7 +536,8 @@ __global__ void __launch_bounds__(CONV_THREADS, 1)
   tc_fence_before();
   __syncthreads();
   if (MODE == FWD_LOSS && threadIdx.x == 0)
-    a.loss_part[blockIdx.x] = (lsum[0] + lsum[1]) + (lsum[2] + lsum[3]);  // the four half-0 warps
+    a.loss_part[blockIdx.x] = ((lsum[0] + lsum[1]) + (lsum[2] + lsum[3])) +
+                              ((lsum[4] + lsum[5]) + (lsum[6] + lsum[7]));
   if (warp == 1) {
     tc_fence_after();
     tmem_free(tbase, NCOLS);
