@@ -934,8 +934,10 @@ int do_step(dnsb_ctx *c, double *ux, double *uy, double *uz, double *p, double *
         const double *pin = s == 0 ? p : c->pn;
         double *pout = s == 0 ? c->pn : p;
         LAUNCH(c, DNSB_KIND_GRADMOM,
-               (c->gm_pipe ? k_gradmom_pipe : k_gradmom_march)<<<
-                   c->gmgrid, c->tblock, c->gm_pipe ? GRADMOM_PIPE_SMEM : GRADMOM_SMEM, c->stream>>>(
+               (c->gm_pipe == 2 ? k_gradmom_deep : c->gm_pipe ? k_gradmom_pipe : k_gradmom_march)<<<
+                   c->gmgrid, c->tblock,
+                   c->gm_pipe == 2 ? GRADMOM_DEEP_SMEM : c->gm_pipe ? GRADMOM_PIPE_SMEM : GRADMOM_SMEM,
+                   c->stream>>>(
                    g, c->gm_planes, cf(ux, uy, uz), delta, pin, pout, 1.0 / adt, ff(qx, qy, qz),
                    ff(c->V[0], c->V[1], c->V[2]), A1, dt, B1, al1 * dt, c->ymet,
                    al1 * dt * g.visc / 2));
@@ -1334,7 +1336,7 @@ int dnsb_create(const dnsb_grid *gr, int device, void *stream, dnsb_ctx **out) {
     c->tblock = dim3(MC_X, MC_Y, 1);
     c->tgrid = dim3((nx + MC_X - 1) / MC_X, (ny + MC_Y - 1) / MC_Y, (nz + MC_Z - 1) / MC_Z);
     c->gm_planes = std::max(4, std::min(256, envint("DNSB_GMZ", c->gm_planes)));
-    c->gm_pipe = envint("DNSB_GMPIPE", c->gm_pipe) != 0;
+    c->gm_pipe = std::max(0, std::min(2, envint("DNSB_GMPIPE", c->gm_pipe)));
     c->gmgrid = dim3(c->tgrid.x, c->tgrid.y, (nz + c->gm_planes - 1) / c->gm_planes);
   }
   c->smem_rx = sizeof(double2) * (2 * (size_t)c->Lx * (M + 1) + M + (M + 1));
@@ -1431,7 +1433,8 @@ int dnsb_create(const dnsb_grid *gr, int device, void *stream, dnsb_ctx **out) {
   if (c->implicit && c->fuse) {
     if ((rc = dalloc(c, &c->pn, G))) return bail(rc);
     if ((rc = allow_smem(c, k_gradmom_march, GRADMOM_SMEM)) ||
-        (rc = allow_smem(c, k_gradmom_pipe, GRADMOM_PIPE_SMEM)))
+        (rc = allow_smem(c, k_gradmom_pipe, GRADMOM_PIPE_SMEM)) ||
+        (rc = allow_smem(c, k_gradmom_deep, GRADMOM_DEEP_SMEM)))
       return bail(rc);
   }
   if (cudaMemset(c->deverr, 0, 4 * sizeof(int)) != cudaSuccess) {

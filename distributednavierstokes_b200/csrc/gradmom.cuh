@@ -425,4 +425,192 @@ __global__ void __launch_bounds__(MC_X *MC_Y, 3)
 // Dynamic shared memory of k_gradmom_pipe.
 constexpr size_t GRADMOM_PIPE_SMEM = sizeof(double) * (2 * 3 + 3 + 5 + 3 * 3) * GP_N;
 
+// k_gradmom_deep: k_gradmom_pipe with the raw data staged two planes ahead
+// instead of one.  Iteration K waits for the copies issued in iteration K-2
+// (cp.async.wait_group 1 leaves the previous iteration's in flight) and
+// issues u* of K+4, delta of K+5 and p of K+3, so two planes of loads are
+// in flight per CTA; the ring slots are indexed by plane number (u* 3,
+// p 4, delta 6, projected u 3 x 3 components: 88.7 KB, 2 CTAs per SM).
+constexpr int GD_US = 3, GD_P = 4, GD_D = 6, GD_UN = 3;
+__global__ void __launch_bounds__(MC_X *MC_Y, 2)
+    k_gradmom_deep(Geo g, int planes, CFields3 us, const double *__restrict__ delta,
+                   const double *__restrict__ p_in, double *__restrict__ p_out, double radt,
+                   Fields3 q, Fields3 out, double A, double dt, double B, double adt,
+                   const double2 *__restrict__ ymet, double theta) {
+  extern __shared__ __align__(16) double gsm[];
+  double *ustar = gsm;                       // [GD_US][3][GP_N]
+  double *pold = ustar + GD_US * 3 * GP_N;   // [GD_P][GP_N]
+  double *dl = pold + GD_P * GP_N;           // [GD_D][GP_N]
+  double *unew = dl + GD_D * GP_N;           // [GD_UN][3][GP_N]
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int tid = tx + MC_X * ty;
+  const int I0 = blockIdx.x * MC_X + 1, J0 = blockIdx.y * MC_Y + 1;
+  const int K0 = blockIdx.z * planes + 1, K1 = min(g.nz, K0 + planes - 1);
+  const bool wall = g.wall;
+  constexpr int CH = GP_X / 2;
+  const long long plane = (long long)g.NX * g.NY;
+  bool stage = tid < GP_Y * CH;
+  int goff = 0, soff = 0;
+  if (stage) {
+    const int ch = tid % CH, hy = tid / CH;
+    int x = I0 - 1 + 2 * ch, y = J0 - 1 + hy;
+    if (x >= g.NX) x -= g.nx;
+    if (y >= g.NY) {
+      if (wall) stage = false;
+      y -= g.ny;
+    }
+    if (x + 1 >= g.NX || y >= g.NY) stage = false;
+    goff = x + g.NX * y;
+    soff = 2 * ch + GP_X * hy;
+  }
+  auto box = [&](const double *f, int z, double *dst) {
+    if (z >= g.NZ) z -= g.nz;
+    if (stage) cp_async16(dst + soff, f + (plane * z + goff));
+  };
+  auto us_slot = [&](int z) { return ustar + (z % GD_US) * 3 * GP_N; };
+  auto p_slot = [&](int z) { return pold + (z % GD_P) * GP_N; };
+  auto d_slot = [&](int z) { return dl + (z % GD_D) * GP_N; };
+  auto un_slot = [&](int z) { return unew + (z % GD_UN) * 3 * GP_N; };
+  auto issue_us = [&](int z) {
+    double *s = us_slot(z);
+    box(us.x, z, s);
+    box(us.y, z, s + GP_N);
+    box(us.z, z, s + 2 * GP_N);
+  };
+  constexpr int HX = MC_X + 2, HY = MC_Y + 2;
+  __shared__ int rsrc[3][HY];
+  __shared__ double rsgn[3][HY], rg[HY];
+  if (tid < 3 * HY) {
+    const int c = tid / HY, hy = tid - c * HY;
+    const int y = J0 - 1 + hy;
+    int hs = hy;
+    double sgn = y <= g.NY - 1 ? 1.0 : 0.0;
+    if (wall && sgn != 0.0) {
+      if (c == STAG_Y) {
+        if (y == 0 || y == g.ny) sgn = 0.0;
+        else if (y == g.ny + 1) { hs = hy - 2; sgn = -1.0; }
+      } else {
+        if (y == 0) { hs = 1; sgn = -1.0; }
+        else if (y == g.ny + 1) { hs = hy - 1; sgn = -1.0; }
+      }
+    }
+    rsrc[c][hy] = hs;
+    rsgn[c][hy] = sgn;
+    if (c == STAG_Y) rg[hy] = sgn != 0.0 ? __ldg(g.rdyu + (J0 - 1 + hs)) : 0.0;
+  }
+  const bool plain = wall ? (J0 >= 2 && J0 + MC_Y <= g.ny - 1) : (J0 + MC_Y <= g.ny + 1);
+  // projected u of plane z from its u* and delta of z and z+1
+  auto project_plane = [&](int z) {
+    const double *su = us_slot(z), *d0 = d_slot(z), *d1 = d_slot(z + 1);
+    double *dst = un_slot(z);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+#pragma unroll
+      for (int ry = 0; ry < 2; ry++) {
+        const int hy = ty + ry * MC_Y;
+        if (hy >= HY) continue;
+        const int srow = GP_X * (plain ? hy : rsrc[c][hy]);
+        const double sgn = plain ? 1.0 : rsgn[c][hy];
+        const double gy = c == STAG_Y ? rg[hy] : 0.0;
+#pragma unroll
+        for (int rx = 0; rx < 2; rx++) {
+          const int hx = tx + rx * MC_X;
+          if (hx >= HX) continue;
+          const int a = hx + srow;
+          double v;
+          if (c == STAG_X) v = su[a] - (d0[a + 1] - d0[a]) * g.rdx;
+          else if (c == STAG_Y) v = su[GP_N + a] - (d0[a + GP_X] - d0[a]) * gy;
+          else v = su[2 * GP_N + a] - (d1[a] - d0[a]) * g.rdz;
+          dst[c * GP_N + hx + GP_X * hy] = plain ? v : sgn * v;
+        }
+      }
+    }
+  };
+  // prologue: project K0-1, K0, K0+1; then two sets of raw data in flight:
+  // (u* K0+2, delta K0+3, p K0+1) and (u* K0+3, delta K0+4, p K0+2)
+  issue_us(K0 - 1);
+  box(delta, K0 - 1, d_slot(K0 - 1));
+  box(delta, K0, d_slot(K0));
+  cp_async_commit();
+  cp_async_wait<0>();
+  __syncthreads();
+  project_plane(K0 - 1);
+  issue_us(K0);
+  box(delta, K0 + 1, d_slot(K0 + 1));
+  box(p_in, K0, p_slot(K0));
+  cp_async_commit();
+  cp_async_wait<0>();
+  __syncthreads();
+  project_plane(K0);
+  __syncthreads();     // every thread is done with u* of K0-1 (slot of K0+2)
+  issue_us(K0 + 1);
+  box(delta, K0 + 2, d_slot(K0 + 2));
+  cp_async_commit();
+  cp_async_wait<0>();
+  __syncthreads();
+  project_plane(K0 + 1);
+  __syncthreads();     // projected K0-1, K0, K0+1 complete; u* of K0 free
+  if (K0 + 1 <= K1) {
+    issue_us(K0 + 2);
+    box(delta, K0 + 3, d_slot(K0 + 3));
+  }
+  box(p_in, K0 + 1, p_slot(K0 + 1));
+  cp_async_commit();
+  if (K0 + 2 <= K1) {
+    issue_us(K0 + 3);
+    box(delta, K0 + 4, d_slot(K0 + 4));
+  }
+  if (K0 + 1 <= K1) box(p_in, K0 + 2, p_slot(K0 + 2));
+  cp_async_commit();
+  const int I = I0 + tx, J = J0 + ty;
+  const bool inside = I <= g.nx && J <= g.ny;
+  constexpr int SY = GP_X;
+  const int h = (tx + 1) + SY * (ty + 1);
+  // plane K0-1 as seen from the first cell: centre values and u_z east/north
+  const double *um1 = un_slot(K0 - 1);
+  double bx0 = um1[h], by0 = um1[GP_N + h], bz0 = um1[2 * GP_N + h];
+  double bzE = um1[2 * GP_N + h + 1], bzN = um1[2 * GP_N + h + SY];
+  for (int K = K0; K <= K1; K++) {
+    MomNb nb;
+    const int c0 = gidx(g, inside ? I : 1, inside ? J : 1, K);
+    nb.qx0 = inside ? q.x[c0] : 0.0;
+    nb.qy0 = inside ? q.y[c0] : 0.0;
+    nb.qz0 = inside ? q.z[c0] : 0.0;
+    cp_async_wait<1>();  // the set of iteration K-2: u* K+2, delta K+3, p K+1
+    __syncthreads();     // ... for every thread; projected K+1 complete; slots of K-1 free
+    if (K + 1 <= K1) project_plane(K + 2);
+    if (K + 3 <= K1) {   // raw data two iterations ahead
+      issue_us(K + 4);
+      box(delta, K + 5, d_slot(K + 5));
+    }
+    if (K + 2 <= K1) box(p_in, K + 3, p_slot(K + 3));
+    cp_async_commit();
+    if (inside) {
+      const double *pk = p_slot(K) + h, *pk1 = p_slot(K + 1) + h;
+      const double *dk = d_slot(K) + h, *dk1 = d_slot(K + 1) + h;
+      nb.p0 = pk[0] + dk[0] * radt;
+      nb.pE = pk[1] + dk[1] * radt;
+      nb.pN = pk[SY] + dk[SY] * radt;
+      nb.pT = pk1[0] + dk1[0] * radt;
+      const double *cx = un_slot(K) + h, *tx_ = un_slot(K + 1) + h;
+      const double *cy = cx + GP_N, *ty_ = tx_ + GP_N;
+      const double *cz = cx + 2 * GP_N, *tz_ = tx_ + 2 * GP_N;
+      nb.ux0 = cx[0]; nb.uxE = cx[1]; nb.uxW = cx[-1]; nb.uxN = cx[SY]; nb.uxS = cx[-SY];
+      nb.uxT = tx_[0]; nb.uxB = bx0; nb.uxWN = cx[SY - 1]; nb.uxWT = tx_[-1];
+      nb.uy0 = cy[0]; nb.uyE = cy[1]; nb.uyW = cy[-1]; nb.uyN = cy[SY]; nb.uyS = cy[-SY];
+      nb.uyT = ty_[0]; nb.uyB = by0; nb.uySE = cy[1 - SY]; nb.uyST = ty_[-SY];
+      nb.uz0 = cz[0]; nb.uzE = cz[1]; nb.uzW = cz[-1]; nb.uzN = cz[SY]; nb.uzS = cz[-SY];
+      nb.uzT = tz_[0]; nb.uzB = bz0; nb.uzEB = bzE; nb.uzNB = bzN;
+      bx0 = nb.ux0; by0 = nb.uy0; bz0 = nb.uz0; bzE = nb.uzE; bzN = nb.uzN;
+      const MomCell m = mom_compute<MOM_IMPLICIT>(g, J, nb, A, dt, B, adt, 1, ymet, theta);
+      mom_store<MOM_IMPLICIT>(g, I, J, K, m, q, out);
+      store_img(p_out, g, I, J, K, nb.p0, STAG_P);
+    }
+  }
+  cp_async_wait<0>();
+}
+
+// Dynamic shared memory of k_gradmom_deep.
+constexpr size_t GRADMOM_DEEP_SMEM = sizeof(double) * (GD_US * 3 + GD_P + GD_D + GD_UN * 3) * GP_N;
+
 }  // namespace dnsb

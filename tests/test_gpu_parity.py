@@ -310,13 +310,14 @@ def test_one_step_production_lengths(oracle_mod, D, cfg):
 
 
 @pytest.mark.parametrize("planes,pipe", [("5", "0"), ("40", "0"), ("5", "1"), ("7", "1"),
-                                         ("32", "1")])
+                                         ("32", "1"), ("5", "2"), ("7", "2"), ("32", "2")])
 @pytest.mark.parametrize("cfg", ["channel_implicit", "nx384_nz384"])
 def test_fused_projection_momentum_planes(oracle_mod, D, cfg, planes, pipe, monkeypatch):
     """The fused projection + momentum kernel with other z-planes per CTA
     (DNSB_GMZ; 5, 7 and 40 leave a shorter last column, 7 a single-plane one
-    at nz = 8) and its one-barrier pipelined variant (DNSB_GMPIPE=1): one
-    semi-implicit step agrees with the oracle."""
+    at nz = 8), its one-barrier pipelined variant (DNSB_GMPIPE=1) and the
+    variant that stages two planes ahead (DNSB_GMPIPE=2): one semi-implicit
+    step agrees with the oracle."""
     monkeypatch.setenv("DNSB_GMZ", planes)
     monkeypatch.setenv("DNSB_GMPIPE", pipe)
     kw = CONFIGS.get(cfg) or PRODUCTION[cfg]
