@@ -314,11 +314,21 @@ def ensemble_arm(args, wl, world, rank, local):
     viscs = np.exp(rng.uniform(lo, hi, size=wl["members"]))
     owner = partition_members([int(n) ** 3 for n in ns], world)
     total_cells = int(sum(int(n) ** 3 for n in ns))
+    tunings, tune_report = {}, None
+    if not args.no_autotune:
+        from distributednavierstokes_b200 import autotune
+
+        t0 = time.perf_counter()
+        tunings, rep = autotune.tune_sizes(sorted(set(int(n) for n in ns)), device=dev)
+        tune_report = {"seconds": time.perf_counter() - t0,
+                       "choices": {str(n): {"tuning": r["tuning"], "ms_per_step": r["ms_per_step"],
+                                            "default_ms_per_step": r["tried"].get("default"),
+                                            "cached": r["cached"]} for n, r in rep.items()}}
     setups, states, dts, forcings = [], [], [], []
     for i, (n, nu) in enumerate(zip(ns, viscs)):
         if owner[i] != rank:
             continue
-        s = dns.setup(n=(int(n),) * 3, visc=float(nu), device=dev)
+        s = dns.setup(n=(int(n),) * 3, visc=float(nu), device=dev, tuning=tunings.get(int(n)))
         # random-phase E(k) ~ k^4 exp(-2 (k/k0)^2) initial field, seed = member id
         u = dns.random_field(dns.vectorfield(s), s, totalenergy=wl["energy"], kpeak=wl["kpeak"],
                              seed=i)
@@ -358,6 +368,41 @@ def ensemble_arm(args, wl, world, rank, local):
     ms_seq = ev0.elapsed_time(ev1)
     for (u, _, _, _), s in zip(states, setups):
         assert dns.maxdiv(u, s) < 1e-10, "ensemble member lost incompressibility"
+    # member-by-member check: the ensemble (tuned members, one graph launch)
+    # against every member stepped and forced alone on a default setup, from
+    # the same initial fields, args.verify_steps steps
+    verify = None
+    if args.verify_steps > 0:
+        ver_e, ver_a, ver_f = [], [], []
+        mine = [i for i in range(len(ns)) if owner[i] == rank]
+        for k, i in enumerate(mine):
+            s = setups[k]
+            u = dns.random_field(dns.vectorfield(s), s, totalenergy=wl["energy"], kpeak=wl["kpeak"],
+                                 seed=i)
+            sa = dns.setup(n=s.n, visc=s.visc, device=dev)
+            ua = dns.vectorfield(sa)
+            for c in "xyz":
+                ua[c].copy_(u[c])
+            ver_e.append((u, dns.scalarfield(s), dns.vectorfield(s), None))
+            ver_a.append((sa, ua, dns.scalarfield(sa), dns.vectorfield(sa)))
+            ver_f.append(forcings[k])
+        E.run(ver_e, dts, args.verify_steps)
+        for (sa, ua, pa, qa), dt, f in zip(ver_a, dts, ver_f):
+            for _ in range(args.verify_steps):
+                dns.step(ua, pa, qa, None, sa, dt)
+                f(ua, sa)
+        torch.cuda.synchronize(dev)
+        worst, identical = 0.0, 0
+        for (u, _, _, _), (sa, ua, _, _) in zip(ver_e, ver_a):
+            d = max(float((u[c] - ua[c]).abs().max()) / max(float(ua[c].abs().max()), 1e-300)
+                    for c in "xyz")
+            worst = max(worst, d)
+            identical += int(all(torch.equal(u[c], ua[c]) for c in "xyz"))
+            sa.close()
+        verify = {"steps": args.verify_steps, "members": len(ver_e), "bit_identical": identical,
+                  "max_rel_diff": worst,
+                  "note": "ensemble (autotuned members, one graph launch) vs each member stepped "
+                          "and forced alone with dnsb_step on a default setup"}
     E.close()
     if world > 1:
         t = torch.tensor([ms, ms_seq], device=dev, dtype=torch.float64)
@@ -381,9 +426,11 @@ def ensemble_arm(args, wl, world, rank, local):
             "config": {"workload": args.workload, "members": wl["members"],
                        "sizes": sorted(set(int(n) for n in ns)), "total_cells": cells,
                        "visc_range": list(wl["visc"]),
-                       "parallelism": "1 GPU, one CUDA graph" if world == 1 else
+                       "parallelism": "1 GPU, one launch of one CUDA graph for all steps" if world == 1 else
                        f"members partitioned over {world} GPUs (no collective on the data path), "
-                       "one CUDA graph per GPU"},
+                       "one CUDA graph launch per GPU"},
+            "autotune": tune_report,
+            "member_check": verify,
             "sequential": {"value": cells * args.steps / (ms_seq / 1e3), "unit": "cell-steps/s",
                            "ms_per_step": ms_seq / args.steps,
                            "note": "the same members stepped one after another on one stream"},
@@ -804,6 +851,10 @@ def main():
                     help="timed full-grid CPU oracle steps of the cpu_baseline (about 2 s each)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="ensemble workload: default launch shapes instead of autotuned ones")
+    ap.add_argument("--verify-steps", type=int, default=500,
+                    help="ensemble workload: steps of the member-by-member check (0: skip)")
     ap.add_argument("--train-steps", type=int, default=None,
                     help="closure workload: Adam steps (default: the workload's 20000)")
     ap.add_argument("--no-cufft", action="store_true",

@@ -31,10 +31,18 @@ class dnsb_grid(ctypes.Structure):
     ]
 
 
+class dnsb_tuning(ctypes.Structure):
+    _fields_ = [("lines_x", c_int), ("lines_z", c_int), ("lines_y", c_int), ("lines_z4", c_int),
+                ("cell_bx", c_int), ("cell_by", c_int), ("gm_planes", c_int)]
+
+
 # name -> (restype, argtypes); every symbol declared in include/dnsb.h
 SIGNATURES = {
     "dnsb_version": (c_int, []),
     "dnsb_create": (c_int, [ctypes.POINTER(dnsb_grid), c_int, P, ctypes.POINTER(c_void_p)]),
+    "dnsb_create_tuned": (c_int, [ctypes.POINTER(dnsb_grid), ctypes.POINTER(dnsb_tuning), c_int, P,
+                                  ctypes.POINTER(c_void_p)]),
+    "dnsb_get_tuning": (c_int, [P, ctypes.POINTER(dnsb_tuning)]),
     "dnsb_destroy": (None, [P]),
     "dnsb_last_error": (ctypes.c_char_p, [P]),
     "dnsb_set_stream": (c_int, [P, P]),
@@ -73,6 +81,8 @@ SIGNATURES = {
     "dnsb_poisson_noalloc": (c_int, [ctypes.POINTER(dnsb_grid), P, P, P]),
     "dnsb_ensemble_create": (c_int, [c_int, ctypes.POINTER(dnsb_grid), c_int, P,
                                      ctypes.POINTER(c_void_p)]),
+    "dnsb_ensemble_create_tuned": (c_int, [c_int, ctypes.POINTER(dnsb_grid), ctypes.POINTER(dnsb_tuning),
+                                           c_int, P, ctypes.POINTER(c_void_p)]),
     "dnsb_ensemble_destroy": (None, [P]),
     "dnsb_ensemble_last_error": (ctypes.c_char_p, [P]),
     "dnsb_ensemble_member": (P, [P, c_int]),

@@ -69,7 +69,8 @@ class Setup:
     """The reference's setup NamedTuple (src/setup.jl:34-113), single rank,
     holding the libdnsb context (plans, coefficient tables, scratch)."""
 
-    def __init__(self, n, lims, bc, stretch, visc, bodyforce, ydiffusion, order, device):
+    def __init__(self, n, lims, bc, stretch, visc, bodyforce, ydiffusion, order, device,
+                 tuning=None):
         self.n = tuple(int(v) for v in n)
         self.lims = tuple((float(a), float(b)) for a, b in lims)
         self.bc = tuple(bc)
@@ -100,17 +101,25 @@ class Setup:
         for i in range(3):
             g.bodyforce[i] = self.bodyforce[i]
         self._grid = g  # (with _dy_c, _dyu_c) also describes the setup to an Ensemble
+        self._tuning = make_tuning(tuning)
         ctx = ctypes.c_void_p()
         with torch.cuda.device(self.device):
             stream = torch.cuda.current_stream(self.device).cuda_stream
-            rc = lib.dnsb_create(ctypes.byref(g), self.device.index or 0,
-                                 ctypes.c_void_p(stream), ctypes.byref(ctx))
+            rc = lib.dnsb_create_tuned(ctypes.byref(g), ctypes.byref(self._tuning),
+                                       self.device.index or 0, ctypes.c_void_p(stream),
+                                       ctypes.byref(ctx))
         if rc != 0:
             raise _lib.DNSBError(f"setup failed: {lib.dnsb_last_error(None).decode()}")
         self._ctx = ctx
         nx, ny, nz = self.n
         # setup.poisson.r: the real input/output buffer of poisson!
         self.poisson = {"r": torch.zeros((nz, ny, nx), dtype=torch.float64, device=self.device)}
+
+    def tuning(self):
+        """The launch shapes in effect (dnsb_get_tuning), as a dict."""
+        t = _lib.dnsb_tuning()
+        check(_lib.load().dnsb_get_tuning(self.ctx, ctypes.byref(t)), self._ctx)
+        return {k: getattr(t, k) for k, _ in _lib.dnsb_tuning._fields_}
 
     # -------------------------------------------------------------- grid
     def _griddata(self, stretch):
@@ -183,10 +192,22 @@ def griddata(n, lims, bc, stretch=None):
     )
 
 
+def make_tuning(tuning):
+    """dnsb_tuning from a dict of its fields (missing / None: 0 = default)."""
+    t = _lib.dnsb_tuning()
+    for k, v in dict(tuning or {}).items():
+        if k not in dict(_lib.dnsb_tuning._fields_):
+            raise ValueError(f"unknown tuning field {k}")
+        setattr(t, k, int(v or 0))
+    return t
+
+
 def setup(*, n, lims=((0.0, 2 * math.pi),) * 3, bc=("periodic", "periodic", "periodic"),
           stretch=None, visc=1e-3, bodyforce=(0.0, 0.0, 0.0), procgrid=None,
-          ydiffusion="explicit", mpibuf="auto", order=2, device=None, T=torch.float64):
-    """setup(; n, kwargs...) (src/setup.jl:34-113) on one GPU."""
+          ydiffusion="explicit", mpibuf="auto", order=2, device=None, T=torch.float64,
+          tuning=None):
+    """setup(; n, kwargs...) (src/setup.jl:34-113) on one GPU.  `tuning` (not
+    in the reference): launch shapes, a dict of dnsb_tuning fields."""
     bc = tuple(b.lstrip(":") if isinstance(b, str) else b for b in bc)
     if not (bc[0] == bc[2] == "periodic"):
         raise ValueError("x and z must be periodic")
@@ -206,7 +227,7 @@ def setup(*, n, lims=((0.0, 2 * math.pi),) * 3, bc=("periodic", "periodic", "per
         raise ValueError("implicit y-diffusion requires bc[2] == :wall")
     if device is None:
         device = torch.device("cuda", torch.cuda.current_device())
-    return Setup(n, lims, bc, stretch, visc, bodyforce, ydiffusion, order, device)
+    return Setup(n, lims, bc, stretch, visc, bodyforce, ydiffusion, order, device, tuning)
 
 
 # ----------------------------------------------------------------- fields
@@ -419,9 +440,10 @@ class Ensemble:
     """A batched ensemble of independent setups (no counterpart in the
     reference: the north star's ensemble of periodic boxes of uneven sizes and
     viscosities).  run() advances every member nsteps RK3 steps of a fixed
-    step through one CUDA graph (one step of all members, captured once,
-    member branches concurrent); the result equals stepping each member
-    alone with step()."""
+    step in one launch of a CUDA graph (a conditional while loop over one
+    step of all members, member branches concurrent; captured once); the
+    result equals stepping each member alone with step().  Members take the
+    launch shapes of their setups (setup(..., tuning=...))."""
 
     def __init__(self, setups):
         self.setups = list(setups)
@@ -433,11 +455,13 @@ class Ensemble:
         self.device = dev
         lib = _lib.load()
         grids = (_lib.dnsb_grid * len(self.setups))(*[s._grid for s in self.setups])
+        # each member takes its setup's launch shapes
+        tunings = (_lib.dnsb_tuning * len(self.setups))(*[s._tuning for s in self.setups])
         ens = ctypes.c_void_p()
         with torch.cuda.device(dev):
             stream = torch.cuda.current_stream(dev).cuda_stream
-            rc = lib.dnsb_ensemble_create(len(self.setups), grids, dev.index or 0,
-                                          ctypes.c_void_p(stream), ctypes.byref(ens))
+            rc = lib.dnsb_ensemble_create_tuned(len(self.setups), grids, tunings, dev.index or 0,
+                                                ctypes.c_void_p(stream), ctypes.byref(ens))
         if rc != 0:
             raise _lib.DNSBError(f"ensemble failed: {lib.dnsb_ensemble_last_error(None).decode()}")
         self._ens = ens

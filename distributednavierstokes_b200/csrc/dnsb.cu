@@ -1182,7 +1182,17 @@ int dnsb_version(void) { return DNSB_VERSION; }
 const char *dnsb_last_error(const dnsb_ctx *ctx) { return ctx ? ctx->err.c_str() : g_create_err; }
 
 int dnsb_create(const dnsb_grid *gr, int device, void *stream, dnsb_ctx **out) {
+  return dnsb_create_tuned(gr, nullptr, device, stream, out);
+}
+
+int dnsb_create_tuned(const dnsb_grid *gr, const dnsb_tuning *tun, int device, void *stream,
+                      dnsb_ctx **out) {
   if (!gr || !out) return fail(nullptr, DNSB_EINVAL, "null argument");
+  if (tun && (tun->lines_x < 0 || tun->lines_z < 0 || tun->lines_y < 0 || tun->lines_z4 < 0 ||
+              tun->cell_bx < 0 || tun->cell_by < 0 || tun->gm_planes < 0))
+    return fail(nullptr, DNSB_EINVAL, "tuning values must be >= 0 (0: default)");
+  // an explicit tuning value wins over the DNSB_* environment default
+  auto tuned = [&](int v, const char *env, int dflt) { return v > 0 ? v : envint(env, dflt); };
   *out = nullptr;
   const int nx = gr->nx, ny = gr->ny, nz = gr->nz;
   if (nx < 2 || ny < 2 || nz < 1 || nx % 2)
@@ -1321,13 +1331,20 @@ int dnsb_create(const dnsb_grid *gr, int device, void *stream, dnsb_ctx **out) {
   // DNSB_LX / DNSB_LZ / DNSB_LY / DNSB_CELL_BLOCK ("32x8") override them
   auto pow2floor = [](int v) { int p = 1; while (2 * p <= v) p *= 2; return p; };
   const int budget = 100 * 1024 / (2 * (int)sizeof(double2));  // complex per buffer
-  c->Lx = pow2floor(std::max(1, std::min({std::max(1, envint("DNSB_LX", 8)), nz, budget / (M + 2)})));
-  c->Lz = std::max(1, std::min(std::max(1, envint("DNSB_LZ", 4)), budget / (nz + 1)));
-  c->Ly = pow2floor(std::max(1, std::min({std::max(1, envint("DNSB_LY", 8)), nz, budget / ny})));
+  c->Lx = pow2floor(std::max(1, std::min({std::max(1, tuned(tun ? tun->lines_x : 0, "DNSB_LX", 8)),
+                                            nz, budget / (M + 2)})));
+  c->Lz = std::max(1, std::min(std::max(1, tuned(tun ? tun->lines_z : 0, "DNSB_LZ", 4)), budget / (nz + 1)));
+  c->Ly = pow2floor(std::max(1, std::min({std::max(1, tuned(tun ? tun->lines_y : 0, "DNSB_LY", 8)),
+                                            nz, budget / ny})));
   {
     int bx = 64, by = 2;
     const char *e = getenv("DNSB_CELL_BLOCK");
-    if (e && sscanf(e, "%dx%d", &bx, &by) == 2 && bx > 0 && by > 0 && bx * by <= 256 && bx % 32 == 0) {
+    if (tun && tun->cell_bx > 0 && tun->cell_by > 0) {
+      bx = tun->cell_bx;
+      by = tun->cell_by;
+      if (bx * by > 256 || bx % 32 != 0)
+        return bail(fail(c, DNSB_EINVAL, "cell block %dx%d: need a multiple of 32 wide, <= 256 threads", bx, by));
+    } else if (e && sscanf(e, "%dx%d", &bx, &by) == 2 && bx > 0 && by > 0 && bx * by <= 256 && bx % 32 == 0) {
     } else { bx = 64; by = 2; }
     c->cblock = dim3(bx, by, 1);
     c->cgrid = dim3((nx + bx - 1) / bx, (ny + by - 1) / by, nz);
@@ -1335,7 +1352,7 @@ int dnsb_create(const dnsb_grid *gr, int device, void *stream, dnsb_ctx **out) {
     c->fuse = envint("DNSB_FUSE", 1) != 0;
     c->tblock = dim3(MC_X, MC_Y, 1);
     c->tgrid = dim3((nx + MC_X - 1) / MC_X, (ny + MC_Y - 1) / MC_Y, (nz + MC_Z - 1) / MC_Z);
-    c->gm_planes = std::max(4, std::min(256, envint("DNSB_GMZ", c->gm_planes)));
+    c->gm_planes = std::max(4, std::min(256, tuned(tun ? tun->gm_planes : 0, "DNSB_GMZ", c->gm_planes)));
     c->gm_pipe = std::max(0, std::min(2, envint("DNSB_GMPIPE", c->gm_pipe)));
     c->gmgrid = dim3(c->tgrid.x, c->tgrid.y, (nz + c->gm_planes - 1) / c->gm_planes);
   }
@@ -1347,7 +1364,7 @@ int dnsb_create(const dnsb_grid *gr, int device, void *stream, dnsb_ctx **out) {
   // four-step kernels for the lengths with a register split (DNSB_FFT4=0: off)
   if (envint("DNSB_FFT4", 1) != 0) {
     int a = 0, b = 0;
-    c->L4z = std::max(1, envint("DNSB_L4Z", 8));
+    c->L4z = std::max(1, tuned(tun ? tun->lines_z4 : 0, "DNSB_L4Z", 8));
     c->rx_post = envint("DNSB_RXPOST", c->rx_post) != 0;
     c->ix_pairs = envint("DNSB_IXPAIRS", c->ix_pairs) != 0;
     if (fft4_split(M, a, b)) {
@@ -1469,6 +1486,18 @@ void dnsb_destroy(dnsb_ctx *c) {
 int dnsb_set_stream(dnsb_ctx *c, void *stream) {
   if (!c) return DNSB_EINVAL;
   c->stream = (cudaStream_t)stream;
+  return 0;
+}
+
+int dnsb_get_tuning(const dnsb_ctx *c, dnsb_tuning *t) {
+  if (!c || !t) return DNSB_EINVAL;
+  t->lines_x = c->Lx;
+  t->lines_z = c->Lz;
+  t->lines_y = c->Ly;
+  t->lines_z4 = c->L4z;
+  t->cell_bx = (int)c->cblock.x;
+  t->cell_by = (int)c->cblock.y;
+  t->gm_planes = c->gm_planes;
   return 0;
 }
 
@@ -1971,6 +2000,13 @@ int dnsb_solve_host(dnsb_ctx *c, double *ux, double *uy, double *uz, double *p, 
 }
 
 // ---------------------------------------------------------------- ensembles
+// The last node of the ensemble's loop body: one step done; loop again
+// while steps are left.
+__global__ void k_ens_countdown(cudaGraphConditionalHandle cond, long long *left) {
+  const long long n = --(*left);
+  cudaGraphSetConditional(cond, n > 0 ? 1u : 0u);
+}
+
 // Members are ordinary contexts with their own streams.  One RK3 step of all
 // members is captured from an internal origin stream (capture cannot start
 // on the legacy default stream a caller may pass): fork event -> member
@@ -1987,6 +2023,7 @@ struct dnsb_ensemble {
   cudaEvent_t fork = nullptr, in = nullptr, out = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
+  long long *counter = nullptr;            // device: steps left in the while loop
   std::vector<double *> key_fields;
   std::vector<double> key_dts;
   std::vector<std::vector<double>> eref;  // per member: shell-clamp table (empty: no forcing)
@@ -2024,12 +2061,18 @@ void dnsb_ensemble_destroy(dnsb_ensemble *e) {
   if (e->fork) cudaEventDestroy(e->fork);
   if (e->in) cudaEventDestroy(e->in);
   if (e->out) cudaEventDestroy(e->out);
+  if (e->counter) cudaFree(e->counter);
   if (e->origin) cudaStreamDestroy(e->origin);
   delete e;
 }
 
 int dnsb_ensemble_create(int n, const dnsb_grid *grids, int device, void *stream,
                          dnsb_ensemble **out) {
+  return dnsb_ensemble_create_tuned(n, grids, nullptr, device, stream, out);
+}
+
+int dnsb_ensemble_create_tuned(int n, const dnsb_grid *grids, const dnsb_tuning *tunings,
+                               int device, void *stream, dnsb_ensemble **out) {
   if (!out || !grids || n <= 0) return efail(nullptr, DNSB_EINVAL, "need n >= 1 grids and an output");
   *out = nullptr;
   if (cudaSetDevice(device) != cudaSuccess)
@@ -2045,6 +2088,7 @@ int dnsb_ensemble_create(int n, const dnsb_grid *grids, int device, void *stream
     return rc;
   };
   if (cudaStreamCreateWithFlags(&e->origin, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaMalloc(&e->counter, sizeof(long long)) != cudaSuccess ||
       cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&e->in, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&e->out, cudaEventDisableTiming) != cudaSuccess)
@@ -2059,7 +2103,7 @@ int dnsb_ensemble_create(int n, const dnsb_grid *grids, int device, void *stream
       return bail(DNSB_ECUDA, "member event creation failed");
     e->done.push_back(ev);
     dnsb_ctx *c = nullptr;
-    const int rc = dnsb_create(&grids[i], device, st, &c);
+    const int rc = dnsb_create_tuned(&grids[i], tunings ? &tunings[i] : nullptr, device, st, &c);
     if (rc) {
       char msg[600];
       snprintf(msg, sizeof msg, "member %d: %.480s", i, g_create_err);
@@ -2111,8 +2155,35 @@ int dnsb_ensemble_run(dnsb_ensemble *e, double *const *fields, const double *dts
   if (nsteps == 0) return 0;
   if (!e->exec || f != e->key_fields || d != e->key_dts) {
     ens_drop_graph(e);
-    if (cudaStreamBeginCapture(e->origin, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+    // The executable graph is [while (steps left) { one RK3 step of every
+    // member (fork/join over the member streams, each followed by its
+    // forcing); count down }]: one graph launch runs all nsteps steps.
+    cudaGraph_t graph = nullptr;
+    cudaGraphConditionalHandle cond;
+    cudaGraphNode_t wnode;
+    cudaGraphNodeParams wp = {};
+    if (cudaGraphCreate(&graph, 0) != cudaSuccess)
+      return efail(e, DNSB_ECUDA, "graph creation failed");
+    e->graph = graph;
+    // the loop condition starts at 1 on every launch: a launch runs >= 1 step
+    if (cudaGraphConditionalHandleCreate(&cond, graph, 1, cudaGraphCondAssignDefault) != cudaSuccess) {
+      ens_drop_graph(e);
+      return efail(e, DNSB_ECUDA, "conditional handle creation failed");
+    }
+    wp.type = cudaGraphNodeTypeConditional;
+    wp.conditional.handle = cond;
+    wp.conditional.type = cudaGraphCondTypeWhile;
+    wp.conditional.size = 1;
+    if (cudaGraphAddNode(&wnode, graph, nullptr, 0, &wp) != cudaSuccess) {
+      ens_drop_graph(e);
+      return efail(e, DNSB_ECUDA, "conditional node creation failed");
+    }
+    cudaGraph_t body = wp.conditional.phGraph_out[0];
+    if (cudaStreamBeginCaptureToGraph(e->origin, body, nullptr, nullptr, 0,
+                                      cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+      ens_drop_graph(e);
       return efail(e, DNSB_ECUDA, "stream capture could not start");
+    }
     int rc = 0;
     cudaEventRecord(e->fork, e->origin);
     for (int i = 0; i < n && !rc; i++) {
@@ -2133,15 +2204,17 @@ int dnsb_ensemble_run(dnsb_ensemble *e, double *const *fields, const double *dts
       cudaEventRecord(e->done[i], e->ms[i]);
       cudaStreamWaitEvent(e->origin, e->done[i], 0);
     }
-    cudaGraph_t graph = nullptr;
-    const cudaError_t ce = cudaStreamEndCapture(e->origin, &graph);
+    if (!rc) k_ens_countdown<<<1, 1, 0, e->origin>>>(cond, e->counter);
+    cudaGraph_t captured = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(e->origin, &captured);
     if (rc) {
-      if (graph) cudaGraphDestroy(graph);
+      ens_drop_graph(e);
       return rc;
     }
-    if (ce != cudaSuccess || !graph)
+    if (ce != cudaSuccess) {
+      ens_drop_graph(e);
       return efail(e, DNSB_ECUDA, "stream capture failed: %s", cudaGetErrorString(ce));
-    e->graph = graph;
+    }
     if (cudaGraphInstantiate(&e->exec, e->graph, 0) != cudaSuccess) {
       ens_drop_graph(e);
       return efail(e, DNSB_ECUDA, "graph instantiation failed");
@@ -2151,11 +2224,15 @@ int dnsb_ensemble_run(dnsb_ensemble *e, double *const *fields, const double *dts
   }
   cudaEventRecord(e->in, e->stream);
   cudaStreamWaitEvent(e->origin, e->in, 0);
-  for (long s = 0; s < nsteps; s++)
-    if (cudaGraphLaunch(e->exec, e->origin) != cudaSuccess)
-      return efail(e, DNSB_ECUDA, "graph launch failed");
+  // steps for the loop (the counter is read by the graph's countdown kernel)
+  const long long steps = nsteps;
+  if (cudaMemcpyAsync(e->counter, &steps, sizeof steps, cudaMemcpyHostToDevice, e->origin) != cudaSuccess)
+    return efail(e, DNSB_ECUDA, "step count upload failed");
+  if (cudaGraphLaunch(e->exec, e->origin) != cudaSuccess)
+    return efail(e, DNSB_ECUDA, "graph launch failed");
   cudaEventRecord(e->out, e->origin);
   cudaStreamWaitEvent(e->stream, e->out, 0);
+  // (a copy from pageable memory is staged before cudaMemcpyAsync returns)
   const cudaError_t le = cudaGetLastError();
   if (le != cudaSuccess) return efail(e, DNSB_ECUDA, "%s", cudaGetErrorString(le));
   return 0;

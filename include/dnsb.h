@@ -57,6 +57,20 @@ typedef struct {
 
 typedef struct dnsb_ctx dnsb_ctx;
 
+/* Launch shapes of a context (no counterpart in the reference; the
+ * autotuner of the batched ensemble picks them per grid).  0 keeps the
+ * default (or the DNSB_* environment override): lines per CTA of the
+ * Stockham x-, z- and y-transforms and of the four-step z-transform, the
+ * block shape of the per-cell kernels (cell_bx a multiple of 32,
+ * cell_bx * cell_by <= 256), z-planes per CTA of the fused projection +
+ * momentum.  Results do not depend on them (every line and cell is computed
+ * by the same arithmetic). */
+typedef struct {
+  int lines_x, lines_z, lines_y, lines_z4;
+  int cell_bx, cell_by;
+  int gm_planes;
+} dnsb_tuning;
+
 /* Library version (DNSB_VERSION). */
 int dnsb_version(void);
 
@@ -64,6 +78,12 @@ int dnsb_version(void);
  * plan_ydiffusion (src/ydiffusion.jl:54-68).  `stream` is a cudaStream_t
  * (NULL = legacy default stream) on device `device`. */
 int dnsb_create(const dnsb_grid *grid, int device, void *stream, dnsb_ctx **out);
+/* dnsb_create with explicit launch shapes (tuning may be NULL); the shapes
+ * in effect (after the clamps to the grid) are read back by
+ * dnsb_get_tuning. */
+int dnsb_create_tuned(const dnsb_grid *grid, const dnsb_tuning *tuning, int device, void *stream,
+                      dnsb_ctx **out);
+int dnsb_get_tuning(const dnsb_ctx *ctx, dnsb_tuning *out);
 void dnsb_destroy(dnsb_ctx *ctx);
 /* Message of the last failed call on ctx (or of the last failed create when
  * ctx is NULL). */
@@ -266,15 +286,21 @@ int dnsb_poisson_noalloc(const dnsb_grid *grid, const double *r, double *p, void
  * ensemble of the north star): n independent members, each a context of its
  * own grid and viscosity with its own stream.  dnsb_ensemble_run advances
  * every member nsteps RK3 steps with a fixed step dts[i] (dnsb_step on each
- * member): one step of all members is captured once into a CUDA graph whose
- * member branches run concurrently (fork/join from the caller's stream) and
- * the graph is replayed nsteps times on that stream.  fields holds 8 device
- * pointers per member: ux, uy, uz, p, qx, qy, qz, delta (delta NULL for an
- * explicit member).  The graph is re-captured when the pointers or steps
- * change.  Results equal those of stepping each member alone. */
+ * member) in ONE graph launch: the graph is a conditional while loop whose
+ * body is one step of all members (member branches concurrent, fork/join
+ * from an internal stream ordered after and before the caller's stream)
+ * followed by a countdown kernel.  fields holds 8 device pointers per
+ * member: ux, uy, uz, p, qx, qy, qz, delta (delta NULL for an explicit
+ * member).  The graph is captured again only when the pointers, steps or
+ * forcing change (the step count is a device counter, set per call).
+ * Results equal those of stepping each member alone.
+ * dnsb_ensemble_create_tuned takes one launch-shape tuning per member
+ * (NULL: defaults). */
 typedef struct dnsb_ensemble dnsb_ensemble;
 int dnsb_ensemble_create(int n, const dnsb_grid *grids, int device, void *stream,
                          dnsb_ensemble **out);
+int dnsb_ensemble_create_tuned(int n, const dnsb_grid *grids, const dnsb_tuning *tunings,
+                               int device, void *stream, dnsb_ensemble **out);
 void dnsb_ensemble_destroy(dnsb_ensemble *ens);
 const char *dnsb_ensemble_last_error(const dnsb_ensemble *ens);
 /* Context of member i (for the per-member calls: cfl, noise, project, ...). */

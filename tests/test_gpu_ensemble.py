@@ -133,3 +133,72 @@ def test_forced_ensemble_equals_members_alone(D):
     for c in "xyz":
         assert torch.equal(ens_states[0][0][c], ref[0][0][c])
     E.close()
+
+
+def test_launch_shapes_do_not_change_results(D):
+    """A setup created with other launch shapes (dnsb_create_tuned) steps to
+    the same bits as the default one; the shapes in effect read back."""
+    kw = dict(n=(24, 16, 32), visc=3e-3)
+    s0 = D.setup(**kw)
+    tun = dict(lines_x=2, lines_y=2, lines_z=1, lines_z4=2, cell_bx=32, cell_by=8)
+    s1 = D.setup(**kw, tuning=tun)
+    t = s1.tuning()
+    assert t["cell_bx"] == 32 and t["cell_by"] == 8 and t["lines_z4"] == 2
+    u0 = D.random_field(D.vectorfield(s0), s0, totalenergy=0.5, kpeak=3, seed=4)
+    u1 = D.vectorfield(s1)
+    for c in "xyz":
+        u1[c].copy_(u0[c])
+    dt = 0.5 * D.cfl_timestep(u0, s0, 0.5)
+    for s, u in ((s0, u0), (s1, u1)):
+        p, q = D.scalarfield(s), D.vectorfield(s)
+        for _ in range(3):
+            D.step(u, p, q, None, s, dt)
+    torch.cuda.synchronize()
+    for c in "xyz":
+        assert torch.equal(u0[c], u1[c]), c
+    with pytest.raises(Exception):
+        D.setup(**kw, tuning=dict(cell_bx=48, cell_by=2))   # not a multiple of 32
+    s0.close()
+    s1.close()
+
+
+def test_autotuner_picks_valid_shapes(D, tmp_path):
+    """The coordinate-descent autotuner on a small box returns shapes that
+    the library accepts, caches them, and reads the cache back."""
+    from distributednavierstokes_b200 import autotune
+
+    cache = str(tmp_path / "tuning.json")
+    out, rep = autotune.tune_sizes([16], cache=cache)
+    assert 16 in out and not rep[16]["cached"] and rep[16]["ms_per_step"] > 0
+    s = D.setup(n=(16, 16, 16), visc=1e-2, tuning=out[16])
+    s.close()
+    out2, rep2 = autotune.tune_sizes([16], cache=cache)
+    assert rep2[16]["cached"] and out2[16] == out[16]
+
+
+def test_tuned_ensemble_one_launch_many_steps(D):
+    """Members with their own launch shapes in the ensemble; 7 steps in one
+    graph launch equal 7 steps of each member alone (bit for bit)."""
+    kws = [dict(n=(16, 16, 16), visc=1e-2), dict(n=(32, 32, 32), visc=2e-3)]
+    tuns = [dict(lines_z4=4, lines_y=4), dict(cell_bx=32, cell_by=4, lines_x=4)]
+    setups = [D.setup(**kw, tuning=t) for kw, t in zip(kws, tuns)]
+    alone = [D.setup(**kw) for kw in kws]
+    ens_states, ref, dts = [], [], []
+    for i, (s, sa) in enumerate(zip(setups, alone)):
+        u = D.random_field(D.vectorfield(s), s, totalenergy=0.5, kpeak=3, seed=20 + i)
+        ua = D.vectorfield(sa)
+        for c in "xyz":
+            ua[c].copy_(u[c])
+        ens_states.append(_as_fields(D, (u, D.scalarfield(s), D.vectorfield(s), None)))
+        ref.append(_as_fields(D, (ua, D.scalarfield(sa), D.vectorfield(sa), None)))
+        dts.append(0.5 * D.cfl_timestep(u, s, 0.5))
+    E = D.Ensemble(setups)
+    E.run(ens_states, dts, 7)
+    for st, s, dt in zip(ref, alone, dts):
+        for _ in range(7):
+            D.step(st[0], st[1], st[2], st[1], s, dt)
+    torch.cuda.synchronize()
+    for i, (a, b) in enumerate(zip(ens_states, ref)):
+        for c in "xyz":
+            assert torch.equal(a[0][c], b[0][c]), (i, c)
+    E.close()
