@@ -54,6 +54,12 @@ SIGNATURES = {
     "dnsb_pressuregrad": (c_int, [P, P, P, c_int, c_double]),
     "dnsb_poisson": (c_int, [P, P, P]),
     "dnsb_project": (c_int, [P, P, P, P, P]),
+    "dnsb_poisson_x": (c_int, [P, P]),
+    "dnsb_poisson_zy": (c_int, [P, P, c_int, c_int]),
+    "dnsb_poisson_xinv": (c_int, [P, P]),
+    "dnsb_spectrum": (c_int, [P, ctypes.POINTER(c_void_p), ctypes.POINTER(c_int), ctypes.POINTER(c_int),
+                              ctypes.POINTER(c_int)]),
+    "dnsb_zblock_copy": (c_int, [P, P, P, c_int, c_int, c_int, c_int, c_int, c_int, c_int]),
     "dnsb_imex_update": (c_int, [P, P, P, P, P, P, P, P, c_double, c_double, c_double]),
     "dnsb_sfs_stage": (c_int, [P, P, P, P, P, P, P, P, c_double, c_double]),
     "dnsb_step": (c_int, [P, P, P, P, P, P, P, P, P, c_double]),

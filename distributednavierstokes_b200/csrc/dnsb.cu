@@ -1566,6 +1566,90 @@ int dnsb_poisson(dnsb_ctx *c, const double *r, double *p) {
   return poisson_from_spectrum(c, ROUT_INTERIOR, p);
 }
 
+// ---------------------------------------------- z-slab decomposition ---
+// The pieces of poisson! between which a z-slab decomposition (the
+// reference's (P,1) process grid: z split over ranks, transpose.jl:47-122)
+// redistributes the spectrum: the real x-transform of a rank's planes into
+// its context's spectrum ([kx][j][z], z fastest), the z-transform, y-solve
+// and inverse z-transform of a kx-slab holding every z (on a context of the
+// global grid, whose plans and tables it uses), and the inverse
+// x-transform back into a rank's pressure.
+
+__global__ void k_zblock_copy(double2 *__restrict__ dst, const double2 *__restrict__ src, int nkx,
+                              int ny, int nz_dst, int z_dst, int nz_src, int z_src, int nz_copy) {
+  const long long n = (long long)nkx * ny * nz_copy;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int z = (int)(t % nz_copy);
+    const long long line = t / nz_copy;  // kx * ny + j
+    dst[line * nz_dst + z_dst + z] = src[line * nz_src + z_src + z];
+  }
+}
+
+int dnsb_poisson_x(dnsb_ctx *c, const double *r) {
+  if (!c || !r) return c ? fail(c, DNSB_EINVAL, "null field") : DNSB_EINVAL;
+  if (ensure_device(c)) return DNSB_ECUDA;
+  return launch_rfftx(c, RIN_REAL, r, nullptr, nullptr);
+}
+
+int dnsb_poisson_xinv(dnsb_ctx *c, double *p) {
+  if (!c || !p) return c ? fail(c, DNSB_EINVAL, "null field") : DNSB_EINVAL;
+  if (ensure_device(c)) return DNSB_ECUDA;
+  return launch_irfftx(c, ROUT_IMAGES, p);
+}
+
+int dnsb_poisson_zy(dnsb_ctx *c, void *S, int kx0, int nkx) {
+  if (!c || !S) return c ? fail(c, DNSB_EINVAL, "null spectrum") : DNSB_EINVAL;
+  if (kx0 < 0 || nkx < 1 || kx0 + nkx > c->g.nkx)
+    return fail(c, DNSB_EINVAL, "kx-slab %d..%d outside 0..%d", kx0, kx0 + nkx - 1, c->g.nkx - 1);
+  if (ensure_device(c)) return DNSB_ECUDA;
+  // run the three launches on the caller's slab: the spectrum, the kx count
+  // and the kx-indexed tables point at the slab for the duration
+  double2 *S0 = c->S;
+  const int nkx0 = c->g.nkx, act0 = c->nkx_active;
+  double *lam1_0 = c->lam1, *ycin0 = c->ycin;
+  c->S = (double2 *)S;
+  c->g.nkx = nkx;
+  c->nkx_active = 0;
+  c->lam1 = lam1_0 + kx0;
+  if (ycin0) c->ycin = ycin0 + (long long)kx0 * c->g.nz * TY_CHUNKS;
+  int rc = launch_fftz(c, false);
+  if (!rc) rc = launch_ysolve(c);
+  if (!rc) rc = launch_fftz(c, true);
+  c->S = S0;
+  c->g.nkx = nkx0;
+  c->nkx_active = act0;
+  c->lam1 = lam1_0;
+  c->ycin = ycin0;
+  return rc;
+}
+
+int dnsb_spectrum(dnsb_ctx *c, void **S, int *nkx, int *ny, int *nz) {
+  if (!c || !S) return DNSB_EINVAL;
+  *S = c->S;
+  if (nkx) *nkx = c->g.nkx;
+  if (ny) *ny = c->g.ny;
+  if (nz) *nz = c->g.nz;
+  return 0;
+}
+
+int dnsb_zblock_copy(dnsb_ctx *c, void *dst, const void *src, int nkx, int ny, int nz_dst, int z_dst,
+                     int nz_src, int z_src, int nz_copy) {
+  if (!c || !dst || !src) return c ? fail(c, DNSB_EINVAL, "null buffer") : DNSB_EINVAL;
+  if (nkx < 0 || ny < 0 || nz_copy < 0 || z_dst < 0 || z_src < 0 || z_dst + nz_copy > nz_dst ||
+      z_src + nz_copy > nz_src)
+    return fail(c, DNSB_EINVAL, "z-block outside its lines");
+  if (ensure_device(c)) return DNSB_ECUDA;
+  const long long n = (long long)nkx * ny * nz_copy;
+  if (n == 0) return 0;
+  const unsigned blocks = (unsigned)std::min<long long>((n + 255) / 256, 8LL * 148);
+  k_zblock_copy<<<blocks, 256, 0, c->stream>>>((double2 *)dst, (const double2 *)src, nkx, ny, nz_dst,
+                                               z_dst, nz_src, z_src, nz_copy);
+  CKL(c);
+  c->launches++;
+  return 0;
+}
+
 int dnsb_project(dnsb_ctx *c, double *ux, double *uy, double *uz, double *psi) {
   if (!c || !ux || !uy || !uz || !psi) return c ? fail(c, DNSB_EINVAL, "null field") : DNSB_EINVAL;
   if (ensure_device(c)) return DNSB_ECUDA;
@@ -1641,7 +1725,7 @@ int dnsb_sfs_stage(dnsb_ctx *c, const double *tau, double *qx, double *qy, doubl
                    double *uy, double *uz, double dt, double B) {
   if (!c || !qx || !qy || !qz || !ux || !uy || !uz)
     return c ? fail(c, DNSB_EINVAL, "null field") : DNSB_EINVAL;
-  if (c->g.wall) return fail(c, DNSB_EINVAL, "the closure stage needs a periodic box");
+  if (c->g.wall && tau) return fail(c, DNSB_EINVAL, "the closure stage needs a periodic box");
   if (ensure_device(c)) return DNSB_ECUDA;
   k_sfs_stage<<<cell_grid(c->g), cell_block, 0, c->stream>>>(c->g, tau, ff(qx, qy, qz),
                                                              ff(ux, uy, uz), dt, B);

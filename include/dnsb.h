@@ -119,6 +119,31 @@ int dnsb_pressuregrad(dnsb_ctx *ctx, double *phi, const double *p, int c, double
  * (the reference's setup.poisson.r): writes the interior of p, no halos. */
 int dnsb_poisson(dnsb_ctx *ctx, const double *r, double *p);
 
+/* z-slab decomposition (the reference's (P,1) process grid, z split over
+ * ranks; transpose.jl:47-122 redistributes the spectrum between the FFT
+ * directions): poisson! (src/poisson.jl:147-161) in three pieces between
+ * which the caller moves the spectrum across ranks.
+ * dnsb_poisson_x: rfft in x of the ghost-free local r (nx*ny*nz_local) into
+ *   the context's spectrum, layout [kx][j][z] (z fastest), nx/2+1 kx planes;
+ * dnsb_poisson_zy: on a context of the GLOBAL grid, the z-transform, the
+ *   y-solve (solve_y!, poisson.jl:122-140, with the kx-dependent tables
+ *   offset to kx0) and the inverse z-transform of the caller's kx-slab S
+ *   holding planes kx0..kx0+nkx-1 with every z: [kx-kx0][j][z];
+ * dnsb_poisson_xinv: the normalised inverse x-transform of the context's
+ *   spectrum into p's interior with its x and y images (z ghosts are the
+ *   caller's halo exchange);
+ * dnsb_spectrum: the context's spectrum buffer and its dims;
+ * dnsb_zblock_copy: dst[kx][j][z_dst + z] = src[kx][j][z_src + z] for
+ *   z < nz_copy (complex values; lines of nz_dst and nz_src), the pack /
+ *   unpack of the spectrum transposes.  Asynchronous on the context's
+ *   stream. */
+int dnsb_poisson_x(dnsb_ctx *ctx, const double *r);
+int dnsb_poisson_zy(dnsb_ctx *ctx, void *S, int kx0, int nkx);
+int dnsb_poisson_xinv(dnsb_ctx *ctx, double *p);
+int dnsb_spectrum(dnsb_ctx *ctx, void **S, int *nkx, int *ny, int *nz);
+int dnsb_zblock_copy(dnsb_ctx *ctx, void *dst, const void *src, int nkx, int ny, int nz_dst,
+                     int z_dst, int nz_src, int z_src, int nz_copy);
+
 /* project!(u, ψ, setup) (src/timestep.jl:25-31): u and ψ leave with valid
  * halos. */
 int dnsb_project(dnsb_ctx *ctx, double *ux, double *uy, double *uz, double *psi);
@@ -129,8 +154,9 @@ int dnsb_project(dnsb_ctx *ctx, double *ux, double *uy, double *uz, double *psi)
  * differenced across each face, shear stresses averaged onto the cell
  * edges), then u += B q with the ghost images of u rewritten.  tau: DEVICE
  * [6][nz][ny][nx] cell-centred components xx, yy, zz, xy, yz, zx (e.g.
- * from dnsb_cnn_infer); NULL gives the plain stage update.  The closure is
- * the north star's addition; the reference has no SFS model. */
+ * from dnsb_cnn_infer; periodic boxes only); NULL gives the plain stage
+ * update (any box).  The closure is the north star's addition; the
+ * reference has no SFS model. */
 int dnsb_sfs_stage(dnsb_ctx *ctx, const double *tau, double *qx, double *qy, double *qz,
                    double *ux, double *uy, double *uz, double dt, double B);
 

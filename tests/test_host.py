@@ -157,3 +157,81 @@ def test_ensemble_partition_balanced_and_deterministic():
         assert sorted(set(owner)) == list(range(world))
         loads = [sum(c for c, o in zip(cells, owner) if o == r) for r in range(world)]
         assert max(loads) - min(loads) <= max(cells)
+
+
+def _slab_data_movement_rank(rank, world, port, errq):
+    """One gloo rank of test_slab_exchanges_gloo."""
+    import os
+    import types
+
+    import torch
+    import torch.distributed as dist
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    try:
+        import datetime
+
+        dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+        from distributednavierstokes_b200 import slab
+
+        comm = slab.TorchComm()
+        nx, ny, nz = 6, 3, 8
+        nkx_all, nzl = nx // 2 + 1, nz // world
+        kx0, nkx = slab.split(nkx_all, world)[rank]
+        part = types.SimpleNamespace(rank=rank, nzl=nzl, k0=rank * nzl, nkx_all=nkx_all, kx0=kx0, nkx=nkx,
+                                     ny=ny, nz=nz)
+        # the spectrum of global plane z at (kx, j): (1000 kx + 10 j + z, -z)
+        kx = torch.arange(nkx_all, dtype=torch.float64)[:, None, None]
+        j = torch.arange(ny, dtype=torch.float64)[None, :, None]
+        z = torch.arange(part.k0, part.k0 + nzl, dtype=torch.float64)[None, None, :]
+        S = torch.stack([(1000 * kx + 10 * j + z).expand(nkx_all, ny, nzl), (-z).expand(nkx_all, ny, nzl)],
+                        dim=-1).contiguous()
+        part.S = S.view(-1)
+        part.St = torch.zeros(nkx * ny * nz * 2, dtype=torch.float64)
+        part.rbuf = torch.zeros(nkx * ny * nzl * 2, dtype=torch.float64)
+        parts = {rank: part}
+        slab.to_kx(parts, comm)
+        St = part.St.view(nkx, ny, nz, 2)
+        kxs = torch.arange(kx0, kx0 + nkx, dtype=torch.float64)[:, None, None]
+        zs = torch.arange(nz, dtype=torch.float64)[None, None, :]
+        assert torch.equal(St[..., 0], (1000 * kxs + 10 * j + zs).expand(nkx, ny, nz))
+        assert torch.equal(St[..., 1], (-zs).expand(nkx, ny, nz))
+        ref = part.S.clone()
+        part.S.zero_()
+        slab.from_kx(parts, comm)
+        assert torch.equal(part.S, ref)
+        # halos: field value = global plane index of each interior plane
+        f = torch.zeros((nzl + 2, 2, 2), dtype=torch.float64)
+        for k in range(nzl):
+            f[k + 1] = part.k0 + k
+        slab.halo_z(parts, comm, lambda p: [f])
+        assert float(f[0].max()) == (part.k0 - 1) % nz and float(f[-1].max()) == (part.k0 + nzl) % nz
+        dist.destroy_process_group()
+    except BaseException as e:  # noqa: BLE001
+        errq.put(f"rank {rank}: {type(e).__name__}: {e}")
+        raise
+
+
+def test_slab_exchanges_gloo():
+    """The z-slab decomposition's data movement on two gloo ranks (CPU): the
+    spectrum transposes z-slabs -> kx-slabs -> z-slabs and the periodic
+    z-halo exchange place every value where the (P,1) layout wants it."""
+    import multiprocessing as mp
+    import socket
+
+    ctx = mp.get_context("spawn")
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    errq = ctx.Queue()
+    procs = [ctx.Process(target=_slab_data_movement_rank, args=(r, 2, port, errq)) for r in range(2)]
+    for pr in procs:
+        pr.start()
+    for pr in procs:
+        pr.join(120)
+    errs = []
+    while not errq.empty():
+        errs.append(errq.get())
+    assert not errs, errs
+    assert all(pr.exitcode == 0 for pr in procs), [pr.exitcode for pr in procs]
