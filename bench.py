@@ -18,9 +18,11 @@ The line also carries `fft_vs_cufft`: cuFFT (torch.fft) timed on the
 shapes of the four Poisson transforms beside the library's own kernels
 (--no-cufft skips it).
 
-Prints ONE JSON line on rank 0.  Under torchrun (N > 1) each rank advances
-an independent replica (the single-GPU step does not shard without the
-multi-GPU transposes; weak scaling, no collective in the data path).
+Prints ONE JSON line on rank 0.  Under torchrun (N > 1) the channel is
+decomposed over the ranks in z-slabs (the reference's (P,1) process grid:
+z-halos and the Poisson solve's spectrum transposes over NCCL
+point-to-point; strong scaling); --replicas runs independent replicas
+instead (weak scaling, no collective on the data path).
 --impl reference times the CPU oracle (a C/OpenMP restatement of the
 reference's Julia path; the Julia reference cannot run here) on the host
 cores, on rank 0 only.
@@ -577,6 +579,89 @@ def closure_arm(args, wl, world, rank, local):
     print(json.dumps(line), flush=True)
 
 
+def slab_arm(args, wl, world, rank, local):
+    """The production channel decomposed over the ranks (strong scaling):
+    z-slabs of nz / world planes, z-halos and the Poisson solve's spectrum
+    transposes over NCCL point-to-point (slab.py, the reference's (P,1)
+    process grid).  Every rank builds the global initial field on its GPU
+    and keeps its slab."""
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    import distributednavierstokes_b200 as dns
+    from distributednavierstokes_b200 import slab
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+    comm = slab.TorchComm()
+    kw = dict(n=wl["n"], stretch=tanhstretch(1.5), visc=wl["visc"], ydiffusion=wl["ydiffusion"], **COMMON)
+    sg = dns.setup(device=dev, **kw)
+    u = dns.vectorfield(sg)
+    dns.velocityfield(u, sg, x=mean_profile(wl))
+    for c in "xyz":
+        dns.noise(u[c], c, sg, 0, wl["amp"])
+    dns.exchange_halo(u, sg)
+    delta = dns.scalarfield(sg)
+    dns.project(u, delta, sg)
+    parts, _ = slab.make_parts(comm, kw, device=dev)
+    part = parts[rank]
+    us = {c: slab.scatter(parts, u[c])[rank] for c in "xyz"}
+    del u, delta
+    uu = dns.VectorField(x=us["x"], y=us["y"], z=us["z"])
+    st = (uu, dns.scalarfield(part.s), dns.vectorfield(part.s), dns.scalarfield(part.s))
+    nx, ny, nz = wl["n"]
+    cells = nx * ny * nz
+
+    def one_step():
+        dt = slab.cfl_timestep(parts, comm, lambda p: st[0], wl["cfl"])
+        slab.step(parts, comm, lambda p: st, dt)
+
+    for _ in range(args.warmup):
+        one_step()
+    torch.cuda.synchronize(dev)
+    dist.barrier()
+    torch.cuda.synchronize(dev)
+    clocks = ClockSampler(local)
+    clocks.start()
+    stream = torch.cuda.current_stream(dev)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        one_step()
+    ev1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms = ev0.elapsed_time(ev1)
+    clk = clocks.stop()
+    t = torch.tensor([ms], device=dev, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t.item())
+    md = slab.maxdiv(parts, comm, lambda p: st[0])
+    dist.barrier()
+    if rank == 0:
+        peak, peak_kind = measured_peaks()
+        value = cells * args.steps / (ms / 1e3)
+        print(json.dumps({
+            "metric": "DNS cell-steps/s (FP64)", "value": value, "unit": "cell-steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": args.workload, "grid": [nx, ny, nz], "ydiffusion": wl["ydiffusion"],
+                       "cfl": wl["cfl"], "parallelism": f"z-slabs over {world} GPUs (NCCL halos and "
+                                                        "spectrum transposes)"},
+            "maxdiv": md, "clocks": clk,
+            "step_roofline": {"bytes_per_cell_step": wl["bytes_per_cell_step"],
+                              "achieved": wl["bytes_per_cell_step"] * value / 1e9 / world, "peak": peak,
+                              "unit": "GB/s per GPU", "peak_source": peak_kind},
+            "e2e": None, "gpu_launches": None, "cpu_baseline": None}), flush=True)
+    for p in parts.values():
+        p.close()
+    sg.close()
+    dist.destroy_process_group()
+
+
 def b200_arm(args, wl, world, rank, local):
     import ctypes
 
@@ -851,6 +936,8 @@ def main():
                     help="timed full-grid CPU oracle steps of the cpu_baseline (about 2 s each)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--replicas", action="store_true",
+                    help="under torchrun: independent replicas per GPU instead of the z-slab decomposition")
     ap.add_argument("--no-autotune", action="store_true",
                     help="ensemble workload: default launch shapes instead of autotuned ones")
     ap.add_argument("--verify-steps", type=int, default=500,
@@ -888,6 +975,8 @@ def main():
             ensemble_arm(args, wl, world, rank, local)
     elif args.impl == "reference":
         reference_arm(args, wl, world, rank)
+    elif world > 1 and not args.replicas:
+        slab_arm(args, wl, world, rank, local)
     else:
         b200_arm(args, wl, world, rank, local)
 

@@ -54,6 +54,7 @@ SIGNATURES = {
     "dnsb_pressuregrad": (c_int, [P, P, P, c_int, c_double]),
     "dnsb_poisson": (c_int, [P, P, P]),
     "dnsb_project": (c_int, [P, P, P, P, P]),
+    "dnsb_axpy": (c_int, [P, P, P, c_double]),
     "dnsb_poisson_x": (c_int, [P, P]),
     "dnsb_poisson_zy": (c_int, [P, P, c_int, c_int]),
     "dnsb_poisson_xinv": (c_int, [P, P]),

@@ -1586,6 +1586,22 @@ __global__ void k_zblock_copy(double2 *__restrict__ dst, const double2 *__restri
   }
 }
 
+__global__ void k_axpy_interior(Geo g, double *__restrict__ y, const double *__restrict__ x, double a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i >= g.nx || j >= g.ny) return;
+  const int c0 = gidx(g, i + 1, j + 1, blockIdx.z + 1);
+  y[c0] += a * x[c0];
+}
+
+int dnsb_axpy(dnsb_ctx *c, double *y, const double *x, double a) {
+  if (!c || !y || !x) return c ? fail(c, DNSB_EINVAL, "null field") : DNSB_EINVAL;
+  if (ensure_device(c)) return DNSB_ECUDA;
+  k_axpy_interior<<<cell_grid(c->g), cell_block, 0, c->stream>>>(c->g, y, x, a);
+  CKL(c);
+  c->launches++;
+  return 0;
+}
+
 int dnsb_poisson_x(dnsb_ctx *c, const double *r) {
   if (!c || !r) return c ? fail(c, DNSB_EINVAL, "null field") : DNSB_EINVAL;
   if (ensure_device(c)) return DNSB_ECUDA;

@@ -275,17 +275,34 @@ def project(parts, comm, u_of, psi_of):
 
 
 def step(parts, comm, state_of, dt):
-    """step!(u, p, q, delta, setup, dt) (src/timestep.jl:41-63), explicit
-    y-diffusion, over the slabs; state_of(part) -> (u, p, q)."""
+    """step!(u, p, q, delta, setup, dt) (src/timestep.jl:41-63) over the
+    slabs; state_of(part) -> (u, p, q) or (u, p, q, delta).  Explicit
+    y-diffusion: u += B q, halo, projection into p.  Semi-implicit: the
+    Crank-Nicolson update (imex_update!, y-lines whole on every rank), halo,
+    projection into delta, p += delta / (alpha dt), halo of p."""
     from .les_closure import sfs_stage
 
-    for A, B in zip(api.RK3["A"], api.RK3["B"]):
+    lib = _lib.load()
+    one = next(iter(parts.values()))
+    for A, B, al in zip(api.RK3["A"], api.RK3["B"], api.RK3["alpha"]):
         for p in parts.values():
-            u, _, q = state_of(p)
+            st = state_of(p)
+            u, pr, q = st[0], st[1], st[2]
             api.momentum(q, u, A, dt, p.s)
-            sfs_stage(None, q, u, dt, B, p.s)
+            if p.s.imexy:
+                api.imex_update(u, q, pr, B, al, dt, p.s)
+            else:
+                sfs_stage(None, q, u, dt, B, p.s)
         halo_z(parts, comm, lambda p: [state_of(p)[0][c] for c in "xyz"])
-        project(parts, comm, lambda p: state_of(p)[0], lambda p: state_of(p)[1])
+        if one.s.imexy:
+            project(parts, comm, lambda p: state_of(p)[0], lambda p: state_of(p)[3])
+            for p in parts.values():
+                st = state_of(p)
+                check(lib.dnsb_axpy(p.s.ctx, api._ptr(st[1]), api._ptr(st[3]), 1.0 / (al * dt)), p.s._ctx)
+                api.exchange_halo(st[1], "p", p.s)
+            halo_z(parts, comm, lambda p: [state_of(p)[1]])
+        else:
+            project(parts, comm, lambda p: state_of(p)[0], lambda p: state_of(p)[1])
 
 
 def cfl_timestep(parts, comm, u_of, cfl):

@@ -137,6 +137,10 @@ int dnsb_poisson(dnsb_ctx *ctx, const double *r, double *p);
  *   z < nz_copy (complex values; lines of nz_dst and nz_src), the pack /
  *   unpack of the spectrum transposes.  Asynchronous on the context's
  *   stream. */
+/* y += a x on the interior cells of two ghosted fields (the lagged-pressure
+ * update p += delta / (alpha dt) of step!, src/timestep.jl:49-52, when the
+ * stage is assembled from the pieces above); halos are the caller's. */
+int dnsb_axpy(dnsb_ctx *ctx, double *y, const double *x, double a);
 int dnsb_poisson_x(dnsb_ctx *ctx, const double *r);
 int dnsb_poisson_zy(dnsb_ctx *ctx, void *S, int kx0, int nkx);
 int dnsb_poisson_xinv(dnsb_ctx *ctx, double *p);
