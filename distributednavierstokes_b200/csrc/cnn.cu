@@ -71,14 +71,19 @@ struct Layout {
 };
 const Layout LAYOUT;
 
-// element offsets (BF16) of the packed B operands of layer L
+// element offsets (BF16) of the packed B operands of layer L: per (dz, dy)
+// pair g and K chunk, the N = 3 x 8 NCH rows (dx, output channel) of 8 K
+// values each, in the K-major core-matrix order of the convolution kernel
+// (tap t = 3 g + dx; the transposed convolution reads tap 26 - t).
 __host__ __device__ inline long pack_fwd(int L, int t, int co, int ci) {
   const int cich = L == 0 ? 2 : 4, coch = L == 3 ? 2 : 4;
-  return (((long)t * cich + ci / 8) * coch + co / 8) * 64 + (co % 8) * 8 + ci % 8;
+  const int g = t / 3, dx = t % 3;
+  return (((long)g * cich + ci / 8) * (3 * coch) + dx * coch + co / 8) * 64 + (co % 8) * 8 + ci % 8;
 }
 __host__ __device__ inline long pack_bwd(int L, int t, int co, int ci) {
   const int cich = L == 0 ? 2 : 4, coch = L == 3 ? 2 : 4;
-  return (((long)(26 - t) * coch + co / 8) * cich + ci / 8) * 64 + (ci % 8) * 8 + co % 8;
+  const int g = (26 - t) / 3, dx = (26 - t) % 3;
+  return (((long)g * coch + co / 8) * (3 * cich) + dx * cich + ci / 8) * 64 + (ci % 8) * 8 + co % 8;
 }
 
 struct KernelLayout {  // passed by value to the element-wise kernels
@@ -394,9 +399,9 @@ int deverr_check(dnsb_cnn *c) {
   return 0;
 }
 
-// patch rows of a tile: offsets x0 + s + dx + (dy + e) P + m, m < 128
+// patch rows of a tile: offsets x0 + s + (dy + e) P + m, x0 < P, m < 128
 int patch_rows(int P, int s, int e) {
-  const long M = (long)(P - 1) + (TILE_M - 1) + (2 + s) + (long)(2 + e) * P;
+  const long M = (long)(P - 1) + (TILE_M - 1) + s + (long)(2 + e) * P;
   return (int)(M / P) + 1;
 }
 
@@ -438,7 +443,7 @@ int make_map_run(dnsb_cnn *c, CUtensorMap *m, void *base, int P, int chunks, int
 }
 
 constexpr int RING_MAX = 12, RING_MIN = 4;
-constexpr size_t CONV_EXTRA = 512 + 1024;  // barriers, and alignment slack
+constexpr size_t CONV_EXTRA = CONV_BARS + CONV_XBUF + 1024;  // barriers, exchange, alignment slack
 
 // shared memory of a convolution with the largest plane ring that fits
 // (at most RING_MAX slots); 0 when not even RING_MIN slots fit
@@ -551,7 +556,7 @@ int run_conv(dnsb_cnn *c, Volume &V, int L, const CUtensorMap &map, bool transpo
   // output box of a forward layer L: P - 2 (L+1); of the transposed one: the
   // box of layer L's input (layer L-1's output)
   a.Do = transposed ? V.P - 2 * L : V.P - 2 * (L + 1);
-  a.tpp = (a.Do * a.P + TILE_M - 1) / TILE_M;
+  a.tpp = (a.Do * a.P + TILE_OUT - 1) / TILE_OUT;
   a.ntiles = V.B * a.Do * a.tpp;
   const size_t smem = conv_smem(CI, CO, a.P, a.R, &a.nslot, &a.slot_bytes, &a.slot_stride, &a.w_bytes);
   if (!smem) return cfail(c, DNSB_EUNSUP, "convolution plane ring does not fit in shared memory");

@@ -23,15 +23,17 @@
 // positions f = y*P + x of one plane of one sample (rows of the GEMM).  With
 // the input patch of that tile staged as whole rows [chunk][dz][row][x][16 B]
 // (one 4-D TMA box: x-rows of 16 P bytes x R rows x 3 planes x CI chunks), the 128
-// GEMM rows of every tap are 128 consecutive 16-byte rows of the patch:
-// tap (dx, dy, dz) starts at patch offset x0 + s + dx + (dy + e) P, e = 1 for
-// s < 0 (one extra row below the tile so that offsets stay >= 0).  So the A
-// operand of each tap is a K-major canonical layout without swizzle (8-row
-// core matrices of 128 contiguous bytes, SBO = 128 B, LBO = the chunk
-// stride), addressed by its start alone: no im2col copy.  Positions with
+// GEMM rows of every (dy, dz) tap pair are 128 consecutive 16-byte rows of
+// the patch starting at offset x0 + s + (dy + e) P, e = 1 for s < 0 (one
+// extra row below the tile so that offsets stay >= 0).  So the A operand is a
+// K-major canonical layout without swizzle (8-row core matrices of 128
+// contiguous bytes, SBO = 128 B, LBO = the chunk stride), addressed by its
+// start alone: no im2col copy.  The three x-taps are columns of the GEMM
+// (N = 3 x output channels), and the epilogue adds row m + dx of column
+// block dx into output m, so a tile yields 126 outputs.  Positions with
 // x >= Do inside a row compute garbage that the epilogue replaces by zeros.
-// B (the weights, N = output channels) is resident in shared memory for the
-// whole persistent CTA, packed in the K-major core-matrix order.
+// B (the weights) is resident in shared memory for the whole persistent
+// CTA, packed in the K-major core-matrix order.
 //
 // Weight gradient (k_wgrad): D[(tap slot j, ci)][co] = sum_o h[o + t_j][ci]
 // g[o][co] over the output positions o (the GEMM's K).  Both operands are
@@ -41,9 +43,11 @@
 // after the last real tap holds ones, which makes that row the bias
 // gradient).  Split-K partials are reduced in a fixed order.
 //
-// Warp roles of both kernels (192 threads): warp 0 issues the TMA copies,
-// warp 1 owns the tensor memory and issues the MMAs (one thread), warps 2-5
-// run the epilogue (warp w reads TMEM lanes 32 (w % 4) .. + 31).  Every
+// Warp roles: warp 0 issues the TMA copies, warp 1 owns the tensor memory
+// and issues the MMAs (one thread), the other warps run the epilogue (warp
+// w reads TMEM lanes 32 (w % 4) .. + 31): warps 2-5 of the weight gradient
+// (192 threads), two groups of four (warps 2-5, 6-9) taking alternate tiles
+// of the convolution (320 threads).  Every
 // mbarrier wait is bounded; a wait that runs out raises the CTA's abort flag
 // and the global error word, every role leaves its loop, the copies and MMAs
 // in flight are waited for (bounded), the tensor memory is freed and the CTA
@@ -58,9 +62,13 @@ namespace dnsb {
 namespace cnn {
 
 constexpr int NTHREADS = 192;       // weight gradient: TMA, MMA, 4 epilogue warps
-constexpr int CONV_THREADS = 320;   // convolution: TMA, MMA, 8 epilogue warps
+constexpr int CONV_GROUPS = 4;      // convolution epilogue: groups of 4 warps taking tiles in turn
+constexpr int CONV_THREADS = 64 + 128 * CONV_GROUPS;  // TMA, MMA, epilogue warps
 constexpr int NTAPS = 27;
-constexpr int TILE_M = 128;
+constexpr int TILE_M = 128;      // GEMM rows (positions) of a convolution tile
+constexpr int TILE_OUT = 126;    // outputs of a convolution tile (rows m, m + 1, m + 2 feed output m)
+constexpr int CONV_BARS = 512;   // bytes of barriers and flags after the plane ring
+constexpr int CONV_XBUF = CONV_GROUPS * 2 * 3 * 3 * 32 * 4;  // lane-quarter boundary exchange, bytes
 constexpr int WG_K = 64;          // positions per weight-gradient K-block
 constexpr int WG_STAGES = 4;
 constexpr int CV_STAGES = 2;
@@ -113,6 +121,16 @@ __device__ __forceinline__ bool mb_wait(uint64_t *b, uint32_t parity, unsigned l
     if ((it & 15) == 15 && *abort_flag) return false;
   }
   return false;
+}
+// named barrier over `n` threads that also ORs a predicate across them
+__device__ __forceinline__ bool bar_or(int id, int n, bool pred) {
+  uint32_t r;
+  asm volatile(
+      "{\n .reg .pred p, q;\n setp.ne.u32 p, %1, 0;\n barrier.red.or.pred q, %2, %3, p;\n selp.u32 %0, 1, 0, q;\n}\n"
+      : "=r"(r)
+      : "r"((uint32_t)pred), "r"(id), "r"(n)
+      : "memory");
+  return r != 0;
 }
 __device__ __forceinline__ void tma3(void *dst, const CUtensorMap *m, int c0, int c1, int c2,
                                      uint64_t *bar) {
@@ -208,6 +226,24 @@ __device__ __forceinline__ void tmem_ld<32>(uint32_t taddr, float *v) {
   for (int i = 0; i < 32; i++) v[i] = __uint_as_float(r[i]);
 }
 
+// three 32-lane x 8-column loads (columns c0, c1, c2) and one wait, into v[0..24)
+__device__ __forceinline__ void tmem_ld3x8(uint32_t c0, uint32_t c1, uint32_t c2, float *v) {
+  uint32_t r[24];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%24];\n"
+      "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%8,%9,%10,%11,%12,%13,%14,%15}, [%25];\n"
+      "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%16,%17,%18,%19,%20,%21,%22,%23}, [%26];\n"
+      "tcgen05.wait::ld.sync.aligned;"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]),
+        "=r"(r[21]), "=r"(r[22]), "=r"(r[23])
+      : "r"(c0), "r"(c1), "r"(c2)
+      : "memory");
+#pragma unroll
+  for (int i = 0; i < 24; i++) v[i] = __uint_as_float(r[i]);
+}
+
 // GELU in its tanh form, 0.5 z (1 + tanh(u)) with u = sqrt(2/pi) (z +
 // 0.044715 z^3), written as z sigma(2u) (sigma(x) = 1 / (1 + e^-x)) with the
 // hardware exponential: a handful of instructions, about 1e-7 relative.
@@ -273,20 +309,32 @@ struct ConvArgs {
   int *err;
 };
 
-// Forward / transposed convolution, CI input chunks, CO output chunks
-// (N = 8 CO GEMM columns).  Tiles are numbered z fastest (tile = ((b tpp) +
-// j) Do + z) and every CTA takes one contiguous range of them, marching up
-// z: the input planes z+s .. z+s+2 of a tile sit in a ring of nslot
-// shared-memory slots, so a tile loads one new plane (three at the start
-// of a column) and the planes are released to the producer after their
-// last use.
+// Forward / transposed convolution, CI input chunks (the GEMM's K, 16
+// channels per MMA), CO output chunks.  One MMA covers the three x-taps of
+// a (dz, dy) pair: its N = 3 * 8 CO columns are (dx, output channel), so
+// D[m][(dx, c)] = sum over (dz, dy, ci) of in[m + x0 + s + (dy + e) P, plane
+// z + s + dz][ci] W[dz, dy, dx][c][ci], and the convolution at position m
+// is D[m][(0, c)] + D[m + 1][(1, c)] + D[m + 2][(2, c)].  The epilogue forms
+// that sum with warp shuffles (rows of a TMEM lane quarter are the lanes
+// of one warp) and, for the two rows that cross into the next quarter,
+// through shared memory; a tile of 128 rows thus yields TILE_OUT = 126
+// outputs and costs 9 CI / 2 MMAs of N = 24 CO instead of 27 CI / 2 of N =
+// 8 CO (the tensor core takes about as long for N = 96 as for N = 32).
+// Tiles are numbered z fastest (tile = ((b tpp) + j) Do + z) and every CTA
+// takes one contiguous range of them, marching up z: the input planes
+// z+s .. z+s+2 of a tile sit in a ring of nslot shared-memory slots, so a
+// tile loads one new plane (three at the start of a column) and the planes
+// are released to the producer after their last use.
 template <int CI, int CO, int MODE>
 __global__ void __launch_bounds__(CONV_THREADS, 1)
     k_conv(const __grid_constant__ CUtensorMap tin, const ConvArgs a) {
-  constexpr int N = 8 * CO;
+  constexpr int NW = 8 * CO;                            // outputs per position
+  constexpr int N = 3 * NW;                             // MMA columns: 96 or 48
   constexpr int NACC = 4;                               // accumulators in flight
-  constexpr uint32_t NCOLS = NACC * N;                  // 64 or 128 columns
+  constexpr uint32_t ACC_STRIDE = N <= 64 ? 64 : 128;   // TMEM columns per accumulator
+  constexpr uint32_t NCOLS = NACC * ACC_STRIDE;         // 256 or 512 columns
   constexpr int MAXSLOT = 12;
+  constexpr int XB = 3 * 3 * NW;                        // exchange floats per group and buffer
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   // 1 KB-aligned base (TMA destinations; the host adds 1 KB of slack)
   unsigned char *smem = smem_raw + ((1024u - (saddr(smem_raw) & 1023u)) & 1023u);
@@ -297,7 +345,11 @@ __global__ void __launch_bounds__(CONV_THREADS, 1)
            *tempty = bars + 2 * MAXSLOT + NACC, *wbar = bars + 2 * MAXSLOT + 2 * NACC;
   uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + 2 * MAXSLOT + 2 * NACC + 1);
   volatile int *abort_flag = reinterpret_cast<volatile int *>(bars + 2 * MAXSLOT + 2 * NACC + 2);
-  float *lsum = reinterpret_cast<float *>(bars + 2 * MAXSLOT + 2 * NACC + 3);  // 8 floats
+  float *lsum = reinterpret_cast<float *>(bars + 2 * MAXSLOT + 2 * NACC + 3);  // 16 floats
+  float *bsm = reinterpret_cast<float *>(reinterpret_cast<unsigned char *>(bars) + 352);  // 32 biases
+  // boundary rows handed between TMEM lane quarters: [group][buffer][quarter
+  // 1..3][3][NW] (row 32q: x-shift 1 and 2, row 32q + 1: x-shift 2)
+  float *xbuf = reinterpret_cast<float *>(reinterpret_cast<unsigned char *>(bars) + CONV_BARS);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   // this CTA's tiles
   const int t0 = (int)((long long)a.ntiles * blockIdx.x / gridDim.x);
@@ -317,6 +369,7 @@ __global__ void __launch_bounds__(CONV_THREADS, 1)
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 1) tmem_alloc(tslot, NCOLS);
+  if (warp == 2) bsm[lane] = MODE != DGRAD && lane < (CO == 4 ? 32 : 6) ? __ldg(a.bias + lane) : 0.f;
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
@@ -333,7 +386,7 @@ __global__ void __launch_bounds__(CONV_THREADS, 1)
       for (int t = t0; ok && t < t1; t++) {
         const int z = t % a.Do, rest = t / a.Do;
         const int j = rest % a.tpp, b = rest / a.tpp;
-        const int y0 = (j * TILE_M) / a.P;
+        const int y0 = (j * TILE_OUT) / a.P;
         const bool fresh = t == t0 || z == 0;
         for (int zp = fresh ? 0 : 2; zp < 3; zp++, g++) {
           const int sl = g % a.nslot, ph = (g / a.nslot) & 1;
@@ -361,7 +414,7 @@ __global__ void __launch_bounds__(CONV_THREADS, 1)
       // (bits 0-13, 16-byte units) moves, by an offset added to the whole
       // 64-bit word (starts stay below 256 KB, so the field never carries).
       const uint32_t cstride_u = (uint32_t)a.R * a.P;  // chunk stride in a slot, 16-byte units
-      const uint64_t bdesc0 = sdesc(saddr(wsm), CO * 128u, 128);
+      const uint64_t bdesc0 = sdesc(saddr(wsm), 3 * CO * 128u, 128);
       const uint64_t adesc_st = sdesc(0, cstride_u * 16u, 128);  // start 0
       const uint32_t ring_u = saddr(ring) >> 4, stride_u = a.slot_stride >> 4;
       uint32_t yrow[3];  // (dy + e) P, 16-byte units
@@ -381,20 +434,20 @@ __global__ void __launch_bounds__(CONV_THREADS, 1)
           break;
         }
         tc_fence_after();
-        const int x0 = (j * TILE_M) % a.P;
+        const int x0 = (j * TILE_OUT) % a.P;
         uint64_t ab[3];  // planes z+s, z+s+1, z+s+2 are the last three loaded
 #pragma unroll
         for (int dz = 0; dz < 3; dz++)
           ab[dz] = adesc_st + (uint64_t)(ring_u + (uint32_t)((g - 3 + dz) % a.nslot) * stride_u +
                                          (uint32_t)(x0 + a.s));
-        const uint32_t dacc = tbase + (uint32_t)(ac * N);
+        const uint32_t dacc = tbase + (uint32_t)ac * ACC_STRIDE;
 #pragma unroll
-        for (int tap = 0; tap < NTAPS; tap++) {
-          const uint64_t at = ab[tap / 9] + (uint64_t)(yrow[(tap / 3) % 3] + (uint32_t)(tap % 3));
+        for (int zy = 0; zy < 9; zy++) {
+          const uint64_t at = ab[zy / 3] + (uint64_t)yrow[zy % 3];
 #pragma unroll
           for (int k = 0; k < CI / 2; k++)
             mma_bf16(dacc, at + (uint64_t)(2 * k) * cstride_u,
-                     bdesc0 + (uint64_t)((tap * CI + 2 * k) * CO * 8), idesc, (tap | k) != 0 ? 1u : 0u);
+                     bdesc0 + (uint64_t)((zy * CI + 2 * k) * 3 * CO * 8), idesc, (zy | k) != 0 ? 1u : 0u);
         }
         mma_commit(&tfull[ac]);
         // release the planes this tile used for the last time
@@ -414,42 +467,78 @@ __global__ void __launch_bounds__(CONV_THREADS, 1)
       if (last_a >= 0) mb_wait(&tfull[last_a], last_aph, a.wait_limit, abort_flag);
     }
   } else {
-    // epilogue: two groups of 4 warps take alternate tiles (group e / 4 the
-    // tiles with local index i % 2 == e / 4); warp w reads TMEM lanes
-    // 32 (w % 4) .. + 31, all N columns of its tile
+    // epilogue: CONV_GROUPS groups of 4 warps take the tiles in turn (group
+    // e / 4 the tiles with local index i % CONV_GROUPS == e / 4); warp w
+    // reads TMEM lanes 32 (w % 4) .. + 31 (rows m = 32 (w % 4) + lane of its
+    // tile), 8 columns of each x-shift at a time
     const int e = warp - 2, q = warp & 3, grp = e >> 2;
     const int m = q * 32 + lane;
-    constexpr int NB = CO == 4 ? 32 : 8;   // outputs written per row
-    float br[NB], osc[6];
-#pragma unroll
-    for (int k = 0; k < NB; k++) br[k] = (MODE != DGRAD && (CO == 4 || k < 6)) ? __ldg(a.bias + k) : 0.f;
+    const float keep1 = lane < 31 ? 1.f : 0.f, keep2 = lane < 30 ? 1.f : 0.f;
+    float osc[6];
 #pragma unroll
     for (int k = 0; k < 6; k++) osc[k] = MODE == FWD_INFER ? __ldg(a.oscale + k) : 0.f;
     const bool store_z = a.zout != nullptr;
+    float *xg = xbuf + grp * 2 * XB;
     float lacc = 0.f;
     // the tile's (b, j, z) and this thread's position, updated as z marches
     int z = t0 % a.Do, j = (t0 / a.Do) % a.tpp, b = t0 / (a.Do * a.tpp);
     int f = 0, x = 0, y = 0;
     bool fresh = true;
-    int i = 0;
+    int i = 0, own = 0;
     for (int t = t0; t < t1; t++, i++) {
-      const bool mine = (i & 1) == grp;
+      const bool mine = (i % CONV_GROUPS) == grp;
       const int ac = i % NACC, aph = (i / NACC) & 1;
-      float v[N];
+      float v[NW];
       if (mine) {
-        if (*abort_flag || !mb_wait(&tfull[ac], aph, a.wait_limit, abort_flag)) {
+        float *xw = xg + (own & 1) * XB;
+        bool ok = !*abort_flag && mb_wait(&tfull[ac], aph, a.wait_limit, abort_flag);
+        ok = __all_sync(0xffffffffu, ok);
+        if (ok) {
+          tc_fence_after();
+          const uint32_t ta = tbase + ((uint32_t)(q * 32) << 16) + (uint32_t)ac * ACC_STRIDE;
+#pragma unroll
+          for (int c = 0; c < CO; c++) {
+            float d[24];  // columns 8c.. of x-shift 0, 1, 2
+            tmem_ld3x8(ta + 8 * c, ta + NW + 8 * c, ta + 2 * NW + 8 * c, d);
+            if (q > 0 && lane < 2) {
+              float *xs = xw + 3 * (q - 1) * NW + 8 * c;
+#pragma unroll
+              for (int k = 0; k < 8; k++) {
+                if (lane == 0) {
+                  xs[k] = d[8 + k];
+                  xs[NW + k] = d[16 + k];
+                } else {
+                  xs[2 * NW + k] = d[16 + k];
+                }
+              }
+            }
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+              const float s1 = __shfl_down_sync(0xffffffffu, d[8 + k], 1);
+              const float s2 = __shfl_down_sync(0xffffffffu, d[16 + k], 2);
+              v[8 * c + k] = fmaf(s2, keep2, fmaf(s1, keep1, d[k]));
+            }
+          }
+          tc_fence_before();
+          __syncwarp();
+          if (lane == 0) mb_arrive(&tempty[ac]);
+        }
+        // the group's four warps agree on going on, and the boundary rows
+        // written above are visible after this barrier
+        if (bar_or(1 + grp, 128, !ok)) {
           *abort_flag = 1;
           atomicExch(a.err, DEVERR_CNN_TIMEOUT);
           break;
         }
-        tc_fence_after();
-        tmem_ld<N>(tbase + ((uint32_t)(q * 32) << 16) + (uint32_t)(ac * N), v);
-        tc_fence_before();
-        __syncwarp();
-        if (lane == 0) mb_arrive(&tempty[ac]);
+        if (q < 3 && lane >= 30) {
+          const float *xr = xw + 3 * q * NW;  // quarter q + 1's rows
+#pragma unroll
+          for (int c = 0; c < NW; c++) v[c] += lane == 31 ? xr[c] + xr[2 * NW + c] : xr[NW + c];
+        }
+        own++;
       }
       if (fresh) {
-        f = j * TILE_M + m;
+        f = j * TILE_OUT + m;
         x = f % a.P;
         y = f / a.P;
         fresh = false;
@@ -463,7 +552,7 @@ __global__ void __launch_bounds__(CONV_THREADS, 1)
           b++;
         }
       }
-      if (!mine || f >= P2) continue;
+      if (!mine || m >= TILE_OUT || f >= P2) continue;
       const bool valid = x < a.Do && y < a.Do;
       const long long vox = (long long)zc * P2 + f;
       if (MODE == FWD_GELU) {
@@ -472,7 +561,7 @@ __global__ void __launch_bounds__(CONV_THREADS, 1)
           float zv[8], hv[8];
 #pragma unroll
           for (int k = 0; k < 8; k++) {
-            const float zz = valid ? v[8 * c + k] + br[8 * c + k] : 0.f;
+            const float zz = valid ? v[8 * c + k] + bsm[8 * c + k] : 0.f;
             zv[k] = zz;
             hv[k] = gelu_f(zz);
           }
@@ -494,7 +583,7 @@ __global__ void __launch_bounds__(CONV_THREADS, 1)
         for (int k = 0; k < 8; k++) {
           float g = 0.f;
           if (valid && k < 6) {
-            const float d = v[k] + br[k] - tv[k];
+            const float d = v[k] + bsm[k] - tv[k];
             lacc += d * d;
             g = a.loss_scale * d;
           }
@@ -507,7 +596,7 @@ __global__ void __launch_bounds__(CONV_THREADS, 1)
           const long long n3 = (long long)a.Do * a.Do * a.Do;
           const long long o = ((long long)zc * a.Do + y) * a.Do + x;
 #pragma unroll
-          for (int k = 0; k < 6; k++) a.infer_out[k * n3 + o] = (double)((v[k] + br[k]) * osc[k]);
+          for (int k = 0; k < 6; k++) a.infer_out[k * n3 + o] = (double)((v[k] + bsm[k]) * osc[k]);
         }
       } else {  // DGRAD: g = dL/dh * gelu'(z) of the output's layer
 #pragma unroll
@@ -535,9 +624,11 @@ __global__ void __launch_bounds__(CONV_THREADS, 1)
   }
   tc_fence_before();
   __syncthreads();
-  if (MODE == FWD_LOSS && threadIdx.x == 0)
-    a.loss_part[blockIdx.x] = ((lsum[0] + lsum[1]) + (lsum[2] + lsum[3])) +
-                              ((lsum[4] + lsum[5]) + (lsum[6] + lsum[7]));
+  if (MODE == FWD_LOSS && threadIdx.x == 0) {
+    float l = 0.f;
+    for (int k = 0; k < 4 * CONV_GROUPS; k++) l += lsum[k];
+    a.loss_part[blockIdx.x] = l;
+  }
   if (warp == 1) {
     tc_fence_after();
     tmem_free(tbase, NCOLS);
