@@ -138,6 +138,9 @@ SIGNATURES.update({
     "dnsb_cnn_batch": (c_int, [P, P, P, c_int, ctypes.c_float, P, P]),
     "dnsb_cnn_infer_cells": (c_int, [P, P, P]),
     "dnsb_cnn_infer": (c_int, [P, P, P, P, P]),
+    "dnsb_les_step": (c_int, [P, P, P, P, P, P, P, P, P, P, c_double]),
+    "dnsb_les_advance": (c_int, [P, P, P, P, P, P, P, P, P, P, c_double, c_double, c_double, P, c_int,
+                                 ctypes.POINTER(c_double), ctypes.POINTER(c_long)]),
     "dnsb_cnn_profile": (c_int, [P, c_int]),
     "dnsb_cnn_profile_read": (c_int, [P, c_int, ctypes.POINTER(c_double), ctypes.POINTER(c_long),
                                       ctypes.POINTER(c_double)]),

@@ -27,6 +27,7 @@
 #include <vector>
 
 #include "../../include/dnsb.h"
+#include "../../include/dnsb_cnn.h"
 #include "common.cuh"
 #include "fft.cuh"
 #include "spectral.cuh"
@@ -1748,6 +1749,54 @@ int dnsb_sfs_stage(dnsb_ctx *c, const double *tau, double *qx, double *qy, doubl
   CKL(c);
   c->launches++;
   c->umax_for[0] = c->umax_for[1] = c->umax_for[2] = nullptr;
+  return 0;
+}
+
+int dnsb_les_step(dnsb_ctx *c, dnsb_cnn *cnn, double *ux, double *uy, double *uz, double *p,
+                  double *qx, double *qy, double *qz, double *tau, double dt) {
+  if (!c || !ux || !uy || !uz || !p || !qx || !qy || !qz)
+    return c ? fail(c, DNSB_EINVAL, "null field") : DNSB_EINVAL;
+  if (cnn && !tau) return fail(c, DNSB_EINVAL, "a closure needs the tau buffer");
+  if (!(dt > 0) || !std::isfinite(dt)) return fail(c, DNSB_EINVAL, "dt must be positive and finite");
+  if (c->implicit) return fail(c, DNSB_EINVAL, "the LES step is explicit (ydiffusion = :explicit)");
+  if (ensure_device(c)) return DNSB_ECUDA;
+  if (cnn && dnsb_cnn_set_stream(cnn, c->stream))
+    return fail(c, DNSB_ECUDA, "closure: %s", dnsb_cnn_last_error(cnn));
+  for (int s = 0; s < 3; s++) {
+    int rc;
+    if (cnn && (rc = dnsb_cnn_infer(cnn, ux, uy, uz, tau)))
+      return fail(c, rc, "closure: %s", dnsb_cnn_last_error(cnn));
+    if ((rc = dnsb_momentum(c, qx, qy, qz, ux, uy, uz, RK_A[s], dt)) ||
+        (rc = dnsb_sfs_stage(c, cnn ? tau : nullptr, qx, qy, qz, ux, uy, uz, dt, RK_B[s])) ||
+        (rc = dnsb_project(c, ux, uy, uz, p)))
+      return rc;
+  }
+  return 0;
+}
+
+int dnsb_les_advance(dnsb_ctx *c, dnsb_cnn *cnn, double *ux, double *uy, double *uz, double *p,
+                     double *qx, double *qy, double *qz, double *tau, double t0, double t1,
+                     double cfl, const double *eref, int nshells, double *t_out, long *n_out) {
+  if (!c || !ux || !uy || !uz || !p || !qx || !qy || !qz)
+    return c ? fail(c, DNSB_EINVAL, "null field") : DNSB_EINVAL;
+  if (!(cfl > 0) || !std::isfinite(t0) || !std::isfinite(t1))
+    return fail(c, DNSB_EINVAL, "cfl must be positive and the times finite");
+  double t = t0;
+  long n = 0;
+  while (t < t1 - 1e-12 * (std::fabs(t1) + 1)) {
+    double dt = 0;
+    int rc = dnsb_cfl(c, ux, uy, uz, cfl, 0, &dt);
+    if (rc) return rc;
+    dt = std::min(dt, t1 - t);
+    rc = cnn ? dnsb_les_step(c, cnn, ux, uy, uz, p, qx, qy, qz, tau, dt)
+             : dnsb_step(c, ux, uy, uz, p, qx, qy, qz, nullptr, dt);
+    if (rc) return rc;
+    if (eref && nshells > 0 && (rc = dnsb_shell_clamp(c, ux, uy, uz, eref, nshells))) return rc;
+    t += dt;
+    n++;
+  }
+  if (t_out) *t_out = t1;
+  if (n_out) *n_out = n;
   return 0;
 }
 

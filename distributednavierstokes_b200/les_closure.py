@@ -42,31 +42,38 @@ def sfs_stage(tau, q, u, dt, B, s):
 
 def les_step(u, p, q, s, dt, closure=None, tau=None):
     """One explicit RK3 step of step! (src/timestep.jl:41-63) whose stages
-    add the closure's -div(tau(u)); closure None: the plain step."""
-    for A, B in zip(api.RK3["A"], api.RK3["B"]):
-        if closure is not None:
-            closure.infer(u, tau)
-        api.momentum(q, u, A, dt, s)
-        sfs_stage(tau if closure is not None else None, q, u, dt, B, s)
-        api.project(u, p, s)
+    add the closure's -div(tau(u)) (dnsb_les_step: tau(u), momentum!, the
+    stage update, the projection, per stage); closure None: the same stages
+    without tau."""
+    if closure is not None and tau is None:
+        raise ValueError("a closure needs the tau buffer")
+    h = closure.handle if closure is not None else None
+    tp = ctypes.c_void_p(tau.data_ptr()) if closure is not None else None
+    check(_lib.load().dnsb_les_step(s.ctx, h, *api._u3(u), api._ptr(p), *api._u3(q), tp, float(dt)),
+          s._ctx)
     return u
 
 
 def advance(u, p, q, s, t, t_end, cfl, forcing=None, closure=None, tau=None, plain=False):
     """CFL-adaptive steps from t to exactly t_end; returns (t_end, steps).
-    plain: the library's fused step (dnsb_step) instead of les_step."""
-    n = 0
-    while t < t_end - 1e-12 * (abs(t_end) + 1):
-        dt = min(api.cfl_timestep(u, s, cfl), t_end - t)
-        if plain:
-            api.step(u, p, q, None, s, dt)
-        else:
-            les_step(u, p, q, s, dt, closure, tau)
-        if forcing is not None:
-            forcing(u, s)
-        t += dt
-        n += 1
-    return t_end, n
+    With a closure: dnsb_les_step; without (or plain): the library's fused
+    step (dnsb_step), the unclosed fallback.  A shell forcing from
+    api.shellforcing is applied after every step; the whole loop runs in
+    dnsb_les_advance (one call, one synchronisation per step for the CFL
+    maximum)."""
+    if closure is not None and plain:
+        raise ValueError("plain excludes a closure")
+    table = getattr(forcing, "_table", None) if forcing is not None else None
+    if forcing is not None and table is None:
+        raise ValueError("advance takes the forcing of api.shellforcing")
+    h = closure.handle if closure is not None else None
+    tp = ctypes.c_void_p(tau.data_ptr()) if closure is not None else None
+    eref = table.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) if table is not None else None
+    t_out, n_out = ctypes.c_double(), ctypes.c_long()
+    check(_lib.load().dnsb_les_advance(s.ctx, h, *api._u3(u), api._ptr(p), *api._u3(q), tp, float(t),
+                                       float(t_end), float(cfl), eref, len(table) if table is not None else 0,
+                                       ctypes.byref(t_out), ctypes.byref(n_out)), s._ctx)
+    return t_out.value, n_out.value
 
 
 # ------------------------------------------------------------ the pairs

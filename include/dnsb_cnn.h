@@ -32,6 +32,8 @@
 #ifndef DNSB_CNN_H
 #define DNSB_CNN_H
 
+#include "dnsb.h"
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -94,6 +96,25 @@ int dnsb_cnn_batch(dnsb_cnn *cnn, const float *x, const float *t, int nadam, flo
 int dnsb_cnn_infer_cells(dnsb_cnn *cnn, const double *v, double *tau);
 int dnsb_cnn_infer(dnsb_cnn *cnn, const double *ux, const double *uy, const double *uz,
                    double *tau);
+
+/* The closed LES step on a periodic box (an explicit-mode context whose
+ * grid side is the closure's nfield): the RK3 stages of step!
+ * (src/timestep.jl:41-63), each evaluating tau(u) with dnsb_cnn_infer and
+ * adding its -div(tau) in the stage update (dnsb_momentum, dnsb_sfs_stage,
+ * dnsb_project).  tau: DEVICE scratch [6][n][n][n].  cnn NULL: the same
+ * three stages without the closure.  The closure is switched to the
+ * context's stream.  Asynchronous. */
+int dnsb_les_step(dnsb_ctx *ctx, dnsb_cnn *cnn, double *ux, double *uy, double *uz, double *p,
+                  double *qx, double *qy, double *qz, double *tau, double dt);
+/* CFL-adaptive steps from t0 to exactly t1 (cfl_timestep, timestep.jl:69-80,
+ * the last step shortened to land on t1): dnsb_les_step with the closure,
+ * or the library's fused dnsb_step when cnn is NULL (the unclosed
+ * fallback); after each step the shell-energy clamp dnsb_shell_clamp with
+ * the HOST table eref[0..nshells) when eref is not NULL.  Reports t1 and the
+ * number of steps; synchronises once per step (the CFL maximum). */
+int dnsb_les_advance(dnsb_ctx *ctx, dnsb_cnn *cnn, double *ux, double *uy, double *uz, double *p,
+                     double *qx, double *qy, double *qz, double *tau, double t0, double t1,
+                     double cfl, const double *eref, int nshells, double *t_out, long *n_out);
 
 /* Instrumentation: with enable != 0, CUDA events bracket every tensor-core
  * launch; kind 0 = forward convolutions, 1 = transposed (backward-data)

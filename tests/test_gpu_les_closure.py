@@ -134,3 +134,47 @@ def test_small_study_closure_beats_unclosed(M):
     assert les["apriori_rel_mse"] < 0.9
     assert math.isfinite(les["spectrum_err_cnn"]) and math.isfinite(les["spectrum_err_plain"])
     assert les["steps"]["les_cnn"] > 0 and les["steps"]["dns"] > 0
+
+
+def test_les_advance_matches_step_loop(M):
+    """dnsb_les_advance (CFL steps, closure every stage, shell clamp after
+    each step, the last step shortened onto t1) equals the same loop driven
+    step by step from Python; without a closure it runs dnsb_step."""
+    dns, L = M
+    from distributednavierstokes_b200.closure import Closure
+
+    n = 16
+    s = dns.setup(n=(n,) * 3, visc=0.01)
+    cl = Closure(batch=0, crop=0, nfield=n, seed=5)
+    cl.set_scales([2.0, 2.0, 2.0], [0.2] * 6)
+    u = dns.random_field(dns.vectorfield(s), s, totalenergy=0.5, kpeak=3.0, seed=7)
+    forcing = dns.shellforcing(u, s, shells=(1, 2))
+    fields = []
+    for _ in range(4):
+        v = dns.vectorfield(s)
+        for c in "xyz":
+            v[c].copy_(u[c])
+        fields.append(v)
+    tau = torch.zeros((6, n, n, n), dtype=torch.float64, device="cuda")
+    t1 = 0.4
+    for closed, (ua, ub) in ((True, fields[:2]), (False, fields[2:])):
+        p, q = dns.scalarfield(s), dns.vectorfield(s)
+        t_end, steps = L.advance(ua, p, q, s, 0.0, t1, 0.5, forcing, cl if closed else None,
+                                 tau if closed else None)
+        assert t_end == t1 and steps >= 2
+        p2, q2 = dns.scalarfield(s), dns.vectorfield(s)
+        t, k = 0.0, 0
+        while t < t1 - 1e-12 * (abs(t1) + 1):
+            dt = min(dns.cfl_timestep(ub, s, 0.5), t1 - t)
+            if closed:
+                L.les_step(ub, p2, q2, s, dt, cl, tau)
+            else:
+                dns.step(ub, p2, q2, None, s, dt)
+            forcing(ub, s)
+            t += dt
+            k += 1
+        assert k == steps
+        for c in "xyz":
+            assert torch.equal(ua[c], ub[c]), (closed, c)
+    cl.close()
+    s.close()
