@@ -42,9 +42,10 @@ typedef struct dnsb_cnn dnsb_cnn;
 
 /* Training geometry: `batch` crops of side `crop`; inference geometry: a
  * periodic field of side `nfield` (0: none).  Either may be 0 to leave that
- * part out.  Sides from 8 to about 72 (a convolution tile's staged input,
- * two stages of 3 planes x 5-8 rows x (side + 8) voxels x 64 bytes, plus the
- * layer's weights, must fit in shared memory): DNSB_EUNSUP otherwise. */
+ * part out.  Sides from 8 to about 96 (a convolution's ring of at least 4
+ * staged input planes, each 4 chunks x 5-12 rows x (side + 8) voxels x 16
+ * bytes, plus the layer's 55 KB of weights must fit in shared memory):
+ * DNSB_EUNSUP otherwise. */
 int dnsb_cnn_create(int device, void *stream, int batch, int crop, int nfield, dnsb_cnn **out);
 void dnsb_cnn_destroy(dnsb_cnn *cnn);
 const char *dnsb_cnn_last_error(const dnsb_cnn *cnn);
