@@ -38,8 +38,8 @@
 // Weight gradient (k_wgrad): D[(tap slot j, ci)][co] = sum_o h[o + t_j][ci]
 // g[o][co] over the output positions o (the GEMM's K).  Both operands are
 // MN-major canonical layouts without swizzle, straight from the chunked
-// activations: a K-block of 64 positions of one plane is one TMA box
-// [chunk][1 KB run] per tap; 128 / (8 CI) taps fill the 128 rows (the slot
+// activations: a K-block of 128 positions of one plane is one TMA box
+// [chunk][2 KB run] per tap; 128 / (8 CI) taps fill the 128 rows (the slot
 // after the last real tap holds ones, which makes that row the bias
 // gradient).  Split-K partials are reduced in a fixed order.
 //
@@ -69,7 +69,7 @@ constexpr int TILE_M = 128;      // GEMM rows (positions) of a convolution tile
 constexpr int TILE_OUT = 126;    // outputs of a convolution tile (rows m, m + 1, m + 2 feed output m)
 constexpr int CONV_BARS = 512;   // bytes of barriers and flags after the plane ring
 constexpr int CONV_XBUF = CONV_GROUPS * 2 * 3 * 3 * 32 * 4;  // lane-quarter boundary exchange, bytes
-constexpr int WG_K = 64;          // positions per weight-gradient K-block
+constexpr int WG_K = 128;         // positions per weight-gradient K-block (one 2 KB TMA row per chunk)
 constexpr int WG_STAGES = 4;
 constexpr int CV_STAGES = 2;
 enum { DEVERR_CNN_TIMEOUT = 2 };
@@ -697,7 +697,6 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   __syncthreads();
   tc_fence_after();
   const uint32_t tbase = *tslot;
-  const int P2 = a.P * a.P;
 
   if (warp == 0) {
     if (lane == 0) {

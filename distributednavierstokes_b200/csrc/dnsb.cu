@@ -102,6 +102,7 @@ struct dnsb_ctx {
   // z-planes per CTA of the fused projection + momentum: 32 measured 1.5 %
   // faster than 16 and 64 at 384x256x384 (its prologue projects two planes)
   int gm_planes = 32;
+  int mom_planes = MC_Z;  // z planes per CTA of k_momentum_march
   // one-barrier pipelined variant of the fused kernel: 2.5 % faster than
   // the two-barrier k_gradmom_march at 384x256x384
   int gm_pipe = 1;
@@ -289,7 +290,11 @@ int allow_smem(dnsb_ctx *c, K kernel, size_t bytes) {
 
 // ----------------------------------------------------------- reductions --
 
-__global__ void k_maxabs3(Geo g, CFields3 u, unsigned long long *out) {
+// out[0..2]: max |u_c| over the interior (as ordered bits); with deverr,
+// out[3] also receives the device error word (read after every earlier
+// kernel of the stream has finished), so that one copy brings both back.
+__global__ void k_maxabs3(Geo g, CFields3 u, unsigned long long *out, const int *deverr) {
+  if (deverr && blockIdx.x == 0 && threadIdx.x == 0) out[3] = (unsigned long long)(unsigned)*deverr;
   double m[3] = {0, 0, 0};
   const long long n = (long long)g.nx * g.ny * g.nz;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
@@ -897,7 +902,7 @@ int do_step(dnsb_ctx *c, double *ux, double *uy, double *uz, double *p, double *
         LAUNCH(c, DNSB_KIND_MOMENTUM,
                k_momentum_march<MOM_EXPLICIT><<<c->tgrid, c->tblock, 0, c->stream>>>(
                    g, ff(qx, qy, qz), cf(ux, uy, uz), ff(c->W[0], c->W[1], c->W[2]), nullptr, A,
-                   dt, B, 0.0, readq, c->ymet, 0.0));
+                   dt, B, 0.0, readq, c->ymet, 0.0, c->mom_planes));
       else
         LAUNCH(c, DNSB_KIND_MOMENTUM,
                k_momentum<MOM_EXPLICIT><<<c->cgrid, c->cblock, 0, c->stream>>>(
@@ -917,7 +922,7 @@ int do_step(dnsb_ctx *c, double *ux, double *uy, double *uz, double *p, double *
         LAUNCH(c, DNSB_KIND_MOMENTUM,
                k_momentum_march<MOM_IMPLICIT><<<c->tgrid, c->tblock, 0, c->stream>>>(
                    g, ff(qx, qy, qz), cf(ux, uy, uz), ff(c->V[0], c->V[1], c->V[2]), p, A, dt, B,
-                   adt, readq, c->ymet, th));
+                   adt, readq, c->ymet, th, c->mom_planes));
       else
         LAUNCH(c, DNSB_KIND_MOMENTUM,
                k_momentum<MOM_IMPLICIT><<<c->cgrid, c->cblock, 0, c->stream>>>(
@@ -1390,6 +1395,18 @@ int dnsb_create_tuned(const dnsb_grid *gr, const dnsb_tuning *tun, int device, v
     if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && nsm > 0)
       c->nsm = nsm;
   }
+  {
+    // planes per momentum CTA: MC_Z, halved while the grid would give
+    // fewer than two CTAs per SM (small boxes), DNSB_MOMZ overrides
+    const long cols = (long)c->tgrid.x * c->tgrid.y;
+    int mp = envint("DNSB_MOMZ", 0);
+    if (mp <= 0) {
+      mp = MC_Z;
+      while (mp > 2 && cols * ((nz + mp - 1) / mp) < 2L * c->nsm) mp /= 2;
+    }
+    c->mom_planes = std::max(1, std::min(64, mp));
+    c->tgrid.z = (nz + c->mom_planes - 1) / c->mom_planes;
+  }
   if ((c->x1 && (rc = allow_fft4_split(c, c->x1, c->x2))) ||
       (c->z1 && (rc = allow_fft4_split(c, c->z1, c->z2))))
     return bail(rc);
@@ -1540,7 +1557,7 @@ int dnsb_momentum(dnsb_ctx *c, double *qx, double *qy, double *qz, const double 
   if (use_tile(c, ux, uy, uz))
     k_momentum_march<MOM_ONLY><<<c->tgrid, c->tblock, 0, c->stream>>>(
         c->g, ff(qx, qy, qz), cf(ux, uy, uz), ff(nullptr, nullptr, nullptr), nullptr, A, dt, 0.0,
-        0.0, 1, c->ymet, 0.0);
+        0.0, 1, c->ymet, 0.0, c->mom_planes);
   else
     k_momentum<MOM_ONLY><<<cell_grid(c->g), cell_block, 0, c->stream>>>(
         c->g, ff(qx, qy, qz), cf(ux, uy, uz), ff(nullptr, nullptr, nullptr), nullptr, A, dt, 0.0,
@@ -1843,11 +1860,18 @@ int dnsb_cfl(dnsb_ctx *c, const double *ux, const double *uy, const double *uz, 
   unsigned long long *scratch = c->umax + 3 * UMAX_SLOTS;
   if (!cached) {
     CK(c, cudaMemsetAsync(scratch, 0, 3 * sizeof(unsigned long long), c->stream));
-    k_maxabs3<<<RED_BLOCKS, 256, 0, c->stream>>>(c->g, cf(ux, uy, uz), scratch);
+    k_maxabs3<<<RED_BLOCKS, 256, 0, c->stream>>>(c->g, cf(ux, uy, uz), scratch, c->deverr);
     CKL(c);
-    CK(c, cudaMemcpyAsync(c->hostred, scratch, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream));
+    CK(c, cudaMemcpyAsync(c->hostred, scratch, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream));
     CK(c, cudaStreamSynchronize(c->stream));
     memcpy(bits, c->hostred, sizeof bits);
+    unsigned long long e = 0;
+    memcpy(&e, (const char *)c->hostred + 3 * sizeof(unsigned long long), sizeof e);
+    if (e != 0) {
+      cudaMemset(c->deverr, 0, sizeof(int));
+      return fail(c, DNSB_ECUDA, "a device-side wait ran out of its iteration limit (code %d)", (int)e);
+    }
+    return cfl_from_max(c, cfl, bits, dt_out);
   } else {
     CK(c, cudaMemcpyAsync(c->hostumax, c->umax, 3 * UMAX_SLOTS * sizeof(unsigned long long),
                           cudaMemcpyDeviceToHost, c->stream));

@@ -235,7 +235,8 @@ __device__ __forceinline__ void mom_store(const Geo &g, int I, int J, int K, con
 }
 
 // Column of k_momentum_march: MC_X x MC_Y cells per CTA (one thread each)
-// walking MC_Z planes in z.  Planes are staged with a one-cell halo in x
+// walking `planes` planes in z (MC_Z on large grids; fewer where the grid
+// would otherwise leave SMs idle).  Planes are staged with a one-cell halo in x
 // and y in a ring of four.
 constexpr int MC_X = 32, MC_Y = 8, MC_Z = 16;  // measured best of 8-64 planes, 4-8 rows
 constexpr int MP_X = MC_X + 2, MP_Y = MC_Y + 2, MP_N = MP_X * MP_Y;
@@ -251,12 +252,12 @@ template <int MODE>
 __global__ void __launch_bounds__(MC_X *MC_Y, 3)
     k_momentum_march(Geo g, Fields3 q, CFields3 u, Fields3 out, const double *__restrict__ p,
                      double A, double dt, double B, double adt, int readq,
-                     const double2 *__restrict__ ymet, double theta) {
+                     const double2 *__restrict__ ymet, double theta, int planes) {
   __shared__ __align__(16) double ring[4][3][MP_N];
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int tid = tx + MC_X * ty;
   const int I0 = blockIdx.x * MC_X + 1, J0 = blockIdx.y * MC_Y + 1;
-  const int K0 = blockIdx.z * MC_Z + 1, K1 = min(g.nz, K0 + MC_Z - 1);
+  const int K0 = blockIdx.z * planes + 1, K1 = min(g.nz, K0 + planes - 1);
   constexpr int CH = MP_X / 2;  // 16-byte chunks per halo row
   static_assert(MP_Y * CH <= MC_X * MC_Y, "one staging chunk per thread and field plane");
   // this thread's chunk of every staged plane (the same in-plane offset for
