@@ -302,6 +302,7 @@ struct Volume {
   float4 *tgt = nullptr;       // targets (training)
   CUtensorMap fwd[NL], bwd[NL], flatA[NL], flatB[NL];
   int Rf = 0, Rb = 0;          // patch rows of forward / transposed reads
+  int subf = 1, subb = 1;      // 126-output sub-tiles per plane load, forward / transposed
 };
 
 struct Prof {
@@ -399,9 +400,10 @@ int deverr_check(dnsb_cnn *c) {
   return 0;
 }
 
-// patch rows of a tile: offsets x0 + s + (dy + e) P + m, x0 < P, m < 128
-int patch_rows(int P, int s, int e) {
-  const long M = (long)(P - 1) + (TILE_M - 1) + s + (long)(2 + e) * P;
+// patch rows of a tile of `sub` sub-tiles: offsets x0 + s + (dy + e) P + 126 sb
+// + m, x0 < P, sb < sub, m < 128
+int patch_rows(int P, int s, int e, int sub) {
+  const long M = (long)(P - 1) + (long)(sub - 1) * TILE_OUT + (TILE_M - 1) + s + (long)(2 + e) * P;
   return (int)(M / P) + 1;
 }
 
@@ -483,8 +485,17 @@ int alloc_volume(dnsb_cnn *c, Volume &V, int side, int B, bool training) {
       if ((rc = dal(c, &V.gz[L], (size_t)B * COCH[L] * P3))) return rc;
     if ((rc = dal(c, &V.tgt, (size_t)B * P3 * 2))) return rc;
   }
-  V.Rf = patch_rows(P, 0, 0);
-  V.Rb = patch_rows(P, -2, 1);
+  // two sub-tiles per plane load (half the copies per output) where the
+  // wider patch fits the plane and a ring of at least RING_MIN planes
+  {
+    int ns;
+    uint32_t sl, st, wb;
+    const int rf2 = patch_rows(P, 0, 0, 2), rb2 = patch_rows(P, -2, 1, 2);
+    V.subf = rf2 <= P && conv_smem(4, 4, P, rf2, &ns, &sl, &st, &wb) ? 2 : 1;
+    V.subb = rb2 <= P && conv_smem(4, 4, P, rb2, &ns, &sl, &st, &wb) ? 2 : 1;
+  }
+  V.Rf = patch_rows(P, 0, 0, V.subf);
+  V.Rb = patch_rows(P, -2, 1, V.subb);
   if (V.Rf > P || V.Rb > P)
     return cfail(c, DNSB_EUNSUP, "side %d too small: the 128-position tiles need %d patch rows", side,
                  std::max(V.Rf, V.Rb));
@@ -553,10 +564,11 @@ int run_conv(dnsb_cnn *c, Volume &V, int L, const CUtensorMap &map, bool transpo
   a.s = transposed ? -2 : 0;
   a.e = transposed ? 1 : 0;
   a.R = transposed ? V.Rb : V.Rf;
+  a.sub = transposed ? V.subb : V.subf;
   // output box of a forward layer L: P - 2 (L+1); of the transposed one: the
   // box of layer L's input (layer L-1's output)
   a.Do = transposed ? V.P - 2 * L : V.P - 2 * (L + 1);
-  a.tpp = (a.Do * a.P + TILE_OUT - 1) / TILE_OUT;
+  a.tpp = (a.Do * a.P + a.sub * TILE_OUT - 1) / (a.sub * TILE_OUT);
   a.ntiles = V.B * a.Do * a.tpp;
   const size_t smem = conv_smem(CI, CO, a.P, a.R, &a.nslot, &a.slot_bytes, &a.slot_stride, &a.w_bytes);
   if (!smem) return cfail(c, DNSB_EUNSUP, "convolution plane ring does not fit in shared memory");

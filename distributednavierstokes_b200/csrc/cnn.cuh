@@ -289,7 +289,8 @@ struct ConvArgs {
   int P, Pz, B;        // volume pitch (x, y), planes, samples
   int Do;              // output box side
   int s, e, R;         // input offset (0 / -2), extra patch row, patch rows
-  int tpp;             // tiles per plane: ceil(Do * P / 128)
+  int sub;             // 126-output sub-tiles per tile (1 or 2), one plane load each tile
+  int tpp;             // tiles per plane: ceil(Do * P / (126 sub))
   int ntiles;          // B * tpp * Do output tiles, z fastest
   int nslot;           // input planes held in the shared-memory ring
   uint32_t slot_bytes;   // one input plane: CI * R * P * 16 (one TMA box)
@@ -386,7 +387,7 @@ __global__ void __launch_bounds__(CONV_THREADS, 1)
       for (int t = t0; ok && t < t1; t++) {
         const int z = t % a.Do, rest = t / a.Do;
         const int j = rest % a.tpp, b = rest / a.tpp;
-        const int y0 = (j * TILE_OUT) / a.P;
+        const int y0 = (j * a.sub * TILE_OUT) / a.P;
         const bool fresh = t == t0 || z == 0;
         for (int zp = fresh ? 0 : 2; zp < 3; zp++, g++) {
           const int sl = g % a.nslot, ph = (g / a.nslot) & 1;
@@ -422,42 +423,48 @@ __global__ void __launch_bounds__(CONV_THREADS, 1)
       for (int q = 0; q < 3; q++) yrow[q] = (uint32_t)((q + a.e) * a.P);
       int g = 0, i = 0, last_a = -1, last_aph = 0;
       bool ok = mb_wait(wbar, 0, a.wait_limit, abort_flag);
-      for (int t = t0; ok && t < t1; t++, i++) {
+      for (int t = t0; ok && t < t1; t++) {
         const int z = t % a.Do, j = (t / a.Do) % a.tpp;
         const bool fresh = t == t0 || z == 0;
         const bool last = t == t1 - 1 || z == a.Do - 1;
-        const int ac = i % NACC, aph = (i / NACC) & 1;
         for (int q = fresh ? 0 : 2; q < 3 && ok; q++, g++)
           ok = !*abort_flag && mb_wait(&full[g % a.nslot], (g / a.nslot) & 1, a.wait_limit, abort_flag);
-        if (!ok || *abort_flag || !mb_wait(&tempty[ac], aph ^ 1, a.wait_limit, abort_flag)) {
-          ok = false;
-          break;
-        }
-        tc_fence_after();
-        const int x0 = (j * TILE_OUT) % a.P;
+        if (!ok) break;
+        const int f0 = j * a.sub * TILE_OUT;
+        const int x0 = f0 - (f0 / a.P) * a.P;  // the tile's first position in patch row y0
         uint64_t ab[3];  // planes z+s, z+s+1, z+s+2 are the last three loaded
 #pragma unroll
         for (int dz = 0; dz < 3; dz++)
           ab[dz] = adesc_st + (uint64_t)(ring_u + (uint32_t)((g - 3 + dz) % a.nslot) * stride_u +
                                          (uint32_t)(x0 + a.s));
-        const uint32_t dacc = tbase + (uint32_t)ac * ACC_STRIDE;
+        for (int sb = 0; sb < a.sub; sb++, i++) {
+          const int ac = i % NACC, aph = (i / NACC) & 1;
+          if (*abort_flag || !mb_wait(&tempty[ac], aph ^ 1, a.wait_limit, abort_flag)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t dacc = tbase + (uint32_t)ac * ACC_STRIDE;
+          const uint64_t so = (uint64_t)(sb * TILE_OUT);  // the sub-tile's rows, 16-byte units
 #pragma unroll
-        for (int zy = 0; zy < 9; zy++) {
-          const uint64_t at = ab[zy / 3] + (uint64_t)yrow[zy % 3];
+          for (int zy = 0; zy < 9; zy++) {
+            const uint64_t at = ab[zy / 3] + so + (uint64_t)yrow[zy % 3];
 #pragma unroll
-          for (int k = 0; k < CI / 2; k++)
-            mma_bf16(dacc, at + (uint64_t)(2 * k) * cstride_u,
-                     bdesc0 + (uint64_t)((zy * CI + 2 * k) * 3 * CO * 8), idesc, (zy | k) != 0 ? 1u : 0u);
+            for (int k = 0; k < CI / 2; k++)
+              mma_bf16(dacc, at + (uint64_t)(2 * k) * cstride_u,
+                       bdesc0 + (uint64_t)((zy * CI + 2 * k) * 3 * CO * 8), idesc, (zy | k) != 0 ? 1u : 0u);
+          }
+          mma_commit(&tfull[ac]);
+          last_a = ac;
+          last_aph = aph;
         }
-        mma_commit(&tfull[ac]);
+        if (!ok) break;
         // release the planes this tile used for the last time
         mma_commit(&empty[(g - 3) % a.nslot]);
         if (last) {
           mma_commit(&empty[(g - 2) % a.nslot]);
           mma_commit(&empty[(g - 1) % a.nslot]);
         }
-        last_a = ac;
-        last_aph = aph;
       }
       if (!ok) {
         *abort_flag = 1;
@@ -480,67 +487,20 @@ __global__ void __launch_bounds__(CONV_THREADS, 1)
     const bool store_z = a.zout != nullptr;
     float *xg = xbuf + grp * 2 * XB;
     float lacc = 0.f;
-    // the tile's (b, j, z) and this thread's position, updated as z marches
+    // the tile's (b, j, z) and this thread's positions in its sub-tiles,
+    // updated as z marches
     int z = t0 % a.Do, j = (t0 / a.Do) % a.tpp, b = t0 / (a.Do * a.tpp);
-    int f = 0, x = 0, y = 0;
-    bool fresh = true;
+    int fA = 0, xA = 0, yA = 0, fB = 0, xB = 0, yB = 0;
+    bool fresh = true, stop = false;
     int i = 0, own = 0;
-    for (int t = t0; t < t1; t++, i++) {
-      const bool mine = (i % CONV_GROUPS) == grp;
-      const int ac = i % NACC, aph = (i / NACC) & 1;
-      float v[NW];
-      if (mine) {
-        float *xw = xg + (own & 1) * XB;
-        bool ok = !*abort_flag && mb_wait(&tfull[ac], aph, a.wait_limit, abort_flag);
-        ok = __all_sync(0xffffffffu, ok);
-        if (ok) {
-          tc_fence_after();
-          const uint32_t ta = tbase + ((uint32_t)(q * 32) << 16) + (uint32_t)ac * ACC_STRIDE;
-#pragma unroll
-          for (int c = 0; c < CO; c++) {
-            float d[24];  // columns 8c.. of x-shift 0, 1, 2
-            tmem_ld3x8(ta + 8 * c, ta + NW + 8 * c, ta + 2 * NW + 8 * c, d);
-            if (q > 0 && lane < 2) {
-              float *xs = xw + 3 * (q - 1) * NW + 8 * c;
-#pragma unroll
-              for (int k = 0; k < 8; k++) {
-                if (lane == 0) {
-                  xs[k] = d[8 + k];
-                  xs[NW + k] = d[16 + k];
-                } else {
-                  xs[2 * NW + k] = d[16 + k];
-                }
-              }
-            }
-#pragma unroll
-            for (int k = 0; k < 8; k++) {
-              const float s1 = __shfl_down_sync(0xffffffffu, d[8 + k], 1);
-              const float s2 = __shfl_down_sync(0xffffffffu, d[16 + k], 2);
-              v[8 * c + k] = fmaf(s2, keep2, fmaf(s1, keep1, d[k]));
-            }
-          }
-          tc_fence_before();
-          __syncwarp();
-          if (lane == 0) mb_arrive(&tempty[ac]);
-        }
-        // the group's four warps agree on going on, and the boundary rows
-        // written above are visible after this barrier
-        if (bar_or(1 + grp, 128, !ok)) {
-          *abort_flag = 1;
-          atomicExch(a.err, DEVERR_CNN_TIMEOUT);
-          break;
-        }
-        if (q < 3 && lane >= 30) {
-          const float *xr = xw + 3 * q * NW;  // quarter q + 1's rows
-#pragma unroll
-          for (int c = 0; c < NW; c++) v[c] += lane == 31 ? xr[c] + xr[2 * NW + c] : xr[NW + c];
-        }
-        own++;
-      }
+    for (int t = t0; t < t1 && !stop; t++) {
       if (fresh) {
-        f = j * TILE_OUT + m;
-        x = f % a.P;
-        y = f / a.P;
+        fA = j * a.sub * TILE_OUT + m;
+        xA = fA % a.P;
+        yA = fA / a.P;
+        fB = fA + TILE_OUT;
+        xB = fB % a.P;
+        yB = fB / a.P;
         fresh = false;
       }
       const int zc = z, bc = b;
@@ -552,67 +512,122 @@ __global__ void __launch_bounds__(CONV_THREADS, 1)
           b++;
         }
       }
-      if (!mine || m >= TILE_OUT || f >= P2) continue;
-      const bool valid = x < a.Do && y < a.Do;
-      const long long vox = (long long)zc * P2 + f;
-      if (MODE == FWD_GELU) {
+      for (int sb = 0; sb < a.sub; sb++, i++) {
+        const bool mine = (i % CONV_GROUPS) == grp;
+        const int ac = i % NACC, aph = (i / NACC) & 1;
+        float v[NW];
+        if (mine) {
+          float *xw = xg + (own & 1) * XB;
+          bool ok = !*abort_flag && mb_wait(&tfull[ac], aph, a.wait_limit, abort_flag);
+          ok = __all_sync(0xffffffffu, ok);
+          if (ok) {
+            tc_fence_after();
+            const uint32_t ta = tbase + ((uint32_t)(q * 32) << 16) + (uint32_t)ac * ACC_STRIDE;
 #pragma unroll
-        for (int c = 0; c < CO; c++) {
-          float zv[8], hv[8];
+            for (int c = 0; c < CO; c++) {
+              float d[24];  // columns 8c.. of x-shift 0, 1, 2
+              tmem_ld3x8(ta + 8 * c, ta + NW + 8 * c, ta + 2 * NW + 8 * c, d);
+              if (q > 0 && lane < 2) {
+                float *xs = xw + 3 * (q - 1) * NW + 8 * c;
+#pragma unroll
+                for (int k = 0; k < 8; k++) {
+                  if (lane == 0) {
+                    xs[k] = d[8 + k];
+                    xs[NW + k] = d[16 + k];
+                  } else {
+                    xs[2 * NW + k] = d[16 + k];
+                  }
+                }
+              }
+#pragma unroll
+              for (int k = 0; k < 8; k++) {
+                const float s1 = __shfl_down_sync(0xffffffffu, d[8 + k], 1);
+                const float s2 = __shfl_down_sync(0xffffffffu, d[16 + k], 2);
+                v[8 * c + k] = fmaf(s2, keep2, fmaf(s1, keep1, d[k]));
+              }
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mb_arrive(&tempty[ac]);
+          }
+          // the group's four warps agree on going on, and the boundary rows
+          // written above are visible after this barrier
+          if (bar_or(1 + grp, 128, !ok)) {
+            *abort_flag = 1;
+            atomicExch(a.err, DEVERR_CNN_TIMEOUT);
+            stop = true;
+            break;
+          }
+          if (q < 3 && lane >= 30) {
+            const float *xr = xw + 3 * q * NW;  // quarter q + 1's rows
+#pragma unroll
+            for (int c = 0; c < NW; c++) v[c] += lane == 31 ? xr[c] + xr[2 * NW + c] : xr[NW + c];
+          }
+          own++;
+        }
+        const int f = sb ? fB : fA, x = sb ? xB : xA, y = sb ? yB : yA;
+        if (!mine || m >= TILE_OUT || f >= P2) continue;
+        const bool valid = x < a.Do && y < a.Do;
+        const long long vox = (long long)zc * P2 + f;
+        if (MODE == FWD_GELU) {
+#pragma unroll
+          for (int c = 0; c < CO; c++) {
+            float zv[8], hv[8];
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+              const float zz = valid ? v[8 * c + k] + bsm[8 * c + k] : 0.f;
+              zv[k] = zz;
+              hv[k] = gelu_f(zz);
+            }
+            const long long o = ((long long)(bc * CO + c) * a.Pz) * P2 + vox;
+            if (store_z) a.zout[o] = pack8(zv);
+            a.out[o] = pack8(hv);
+          }
+        } else if (MODE == FWD_LOSS) {
+          // 6 output components in chunk 0 (N = 16: chunk 1 stays zero)
+          float tv[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+          if (valid) {
+            const float4 *tp = a.target + ((long long)bc * a.Pz * P2 + vox) * 2;
+            const float4 t0v = tp[0], t1v = tp[1];
+            tv[0] = t0v.x; tv[1] = t0v.y; tv[2] = t0v.z; tv[3] = t0v.w;
+            tv[4] = t1v.x; tv[5] = t1v.y;
+          }
+          float gv[8];
 #pragma unroll
           for (int k = 0; k < 8; k++) {
-            const float zz = valid ? v[8 * c + k] + bsm[8 * c + k] : 0.f;
-            zv[k] = zz;
-            hv[k] = gelu_f(zz);
+            float g = 0.f;
+            if (valid && k < 6) {
+              const float d = v[k] + bsm[k] - tv[k];
+              lacc += d * d;
+              g = a.loss_scale * d;
+            }
+            gv[k] = g;
           }
-          const long long o = ((long long)(bc * CO + c) * a.Pz) * P2 + vox;
-          if (store_z) a.zout[o] = pack8(zv);
-          a.out[o] = pack8(hv);
-        }
-      } else if (MODE == FWD_LOSS) {
-        // 6 output components in chunk 0 (N = 16: chunk 1 stays zero)
-        float tv[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-        if (valid) {
-          const float4 *tp = a.target + ((long long)bc * a.Pz * P2 + vox) * 2;
-          const float4 t0v = tp[0], t1v = tp[1];
-          tv[0] = t0v.x; tv[1] = t0v.y; tv[2] = t0v.z; tv[3] = t0v.w;
-          tv[4] = t1v.x; tv[5] = t1v.y;
-        }
-        float gv[8];
-#pragma unroll
-        for (int k = 0; k < 8; k++) {
-          float g = 0.f;
-          if (valid && k < 6) {
-            const float d = v[k] + bsm[k] - tv[k];
-            lacc += d * d;
-            g = a.loss_scale * d;
-          }
-          gv[k] = g;
-        }
-        const long long o = ((long long)(bc * CO) * a.Pz) * P2 + vox;
-        a.out[o] = pack8(gv);
-      } else if (MODE == FWD_INFER) {
-        if (valid) {
-          const long long n3 = (long long)a.Do * a.Do * a.Do;
-          const long long o = ((long long)zc * a.Do + y) * a.Do + x;
-#pragma unroll
-          for (int k = 0; k < 6; k++) a.infer_out[k * n3 + o] = (double)((v[k] + bsm[k]) * osc[k]);
-        }
-      } else {  // DGRAD: g = dL/dh * gelu'(z) of the output's layer
-#pragma unroll
-        for (int c = 0; c < CO; c++) {
-          const long long o = ((long long)(bc * CO + c) * a.Pz) * P2 + vox;
-          float gv[8];
-          if (valid) {
-            float zv[8];
-            unpack8(a.zin[o], zv);
-#pragma unroll
-            for (int k = 0; k < 8; k++) gv[k] = v[8 * c + k] * gelu_grad_f(zv[k]);
-          } else {
-#pragma unroll
-            for (int k = 0; k < 8; k++) gv[k] = 0.f;
-          }
+          const long long o = ((long long)(bc * CO) * a.Pz) * P2 + vox;
           a.out[o] = pack8(gv);
+        } else if (MODE == FWD_INFER) {
+          if (valid) {
+            const long long n3 = (long long)a.Do * a.Do * a.Do;
+            const long long o = ((long long)zc * a.Do + y) * a.Do + x;
+#pragma unroll
+            for (int k = 0; k < 6; k++) a.infer_out[k * n3 + o] = (double)((v[k] + bsm[k]) * osc[k]);
+          }
+        } else {  // DGRAD: g = dL/dh * gelu'(z) of the output's layer
+#pragma unroll
+          for (int c = 0; c < CO; c++) {
+            const long long o = ((long long)(bc * CO + c) * a.Pz) * P2 + vox;
+            float gv[8];
+            if (valid) {
+              float zv[8];
+              unpack8(a.zin[o], zv);
+#pragma unroll
+              for (int k = 0; k < 8; k++) gv[k] = v[8 * c + k] * gelu_grad_f(zv[k]);
+            } else {
+#pragma unroll
+              for (int k = 0; k < 8; k++) gv[k] = 0.f;
+            }
+            a.out[o] = pack8(gv);
+          }
         }
       }
     }
