@@ -102,6 +102,7 @@ struct dnsb_ctx {
   // z-planes per CTA of the fused projection + momentum: 32 measured 1.5 %
   // faster than 16 and 64 at 384x256x384 (its prologue projects two planes)
   int gm_planes = 32;
+  std::map<const void *, CUtensorMap> gm_maps;  // TMA maps of the fused kernel's staged fields
   int mom_planes = MC_Z;  // z planes per CTA of k_momentum_march
   // one-barrier pipelined variant of the fused kernel: 2.5 % faster than
   // the two-barrier k_gradmom_march at 384x256x384
@@ -864,6 +865,58 @@ int poisson_from_spectrum(dnsb_ctx *c, int outmode, double *out) {
 bool aligned16(const double *q) { return (reinterpret_cast<uintptr_t>(q) & 15) == 0; }
 
 // the z-marching momentum kernel copies 16-byte chunks of the velocity rows
+typedef CUresult (*TmaEncodeFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
+                                const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
+                                const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+TmaEncodeFn tma_encoder() {
+  static TmaEncodeFn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (TmaEncodeFn)p;
+  });
+  return fn;
+}
+
+// The five tensor maps (u*x, u*y, u*z, delta, p_in) of k_gradmom_tma: 3-D
+// FP64 maps of the ghosted field, box GP_X x GP_Y x 1; cached per field
+// pointer.  False (the caller runs k_gradmom_pipe) when a field is not
+// 16-byte aligned, a row is not a multiple of 16 bytes, the last x tile
+// has more wrap columns than the kernel's two registers per thread cover,
+// or the driver has no encoder.
+bool gm_tma_maps(dnsb_ctx *c, CFields3 us, const double *delta, const double *pin,
+                 const CUtensorMap **out) {
+  const Geo &g = c->g;
+  const int nwrap = std::max(0, (int)(c->gmgrid.x - 1) * MC_X + GP_X - g.NX);
+  if (g.NX % 2 || 5 * GP_Y * nwrap > 2 * MC_X * MC_Y) return false;
+  const double *f[5] = {us.x, us.y, us.z, delta, pin};
+  TmaEncodeFn enc = tma_encoder();
+  if (!enc) return false;
+  for (int i = 0; i < 5; i++) {
+    if (!aligned16(f[i])) return false;
+    auto it = c->gm_maps.find(f[i]);
+    if (it == c->gm_maps.end()) {
+      if (c->gm_maps.size() >= 64) c->gm_maps.clear();
+      CUtensorMap m;
+      const cuuint64_t dims[3] = {(cuuint64_t)g.NX, (cuuint64_t)g.NY, (cuuint64_t)g.NZ};
+      const cuuint64_t strides[2] = {8ull * g.NX, 8ull * g.NX * g.NY};
+      const cuuint32_t box[3] = {GP_X, GP_Y, 1}, es[3] = {1, 1, 1};
+      if (enc(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<double *>(f[i]), dims, strides, box, es,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return false;
+      it = c->gm_maps.emplace(f[i], m).first;
+    }
+    out[i] = &it->second;
+  }
+  return true;
+}
+
 bool use_tile(const dnsb_ctx *c, const double *ux, const double *uy, const double *uz) {
   return c->mom_tile && aligned16(ux) && aligned16(uy) && aligned16(uz);
 }
@@ -939,6 +992,14 @@ int do_step(dnsb_ctx *c, double *ux, double *uy, double *uz, double *p, double *
         const double A1 = RK_A[s + 1], B1 = RK_B[s + 1], al1 = RK_AL[s + 1];
         const double *pin = s == 0 ? p : c->pn;
         double *pout = s == 0 ? c->pn : p;
+        const CUtensorMap *mp[5];
+        if (c->gm_pipe == 3 && gm_tma_maps(c, cf(ux, uy, uz), delta, pin, mp))
+          LAUNCH(c, DNSB_KIND_GRADMOM,
+                 k_gradmom_tma<<<c->gmgrid, c->tblock, GRADMOM_TMA_SMEM, c->stream>>>(
+                     *mp[0], *mp[1], *mp[2], *mp[3], *mp[4], g, c->gm_planes, cf(ux, uy, uz), delta,
+                     pin, pout, 1.0 / adt, ff(qx, qy, qz), ff(c->V[0], c->V[1], c->V[2]), A1, dt, B1,
+                     al1 * dt, c->ymet, al1 * dt * g.visc / 2, c->deverr, c->wait_limit));
+        else
         LAUNCH(c, DNSB_KIND_GRADMOM,
                (c->gm_pipe == 2 ? k_gradmom_deep : c->gm_pipe ? k_gradmom_pipe : k_gradmom_march)<<<
                    c->gmgrid, c->tblock,
@@ -1359,7 +1420,7 @@ int dnsb_create_tuned(const dnsb_grid *gr, const dnsb_tuning *tun, int device, v
     c->tblock = dim3(MC_X, MC_Y, 1);
     c->tgrid = dim3((nx + MC_X - 1) / MC_X, (ny + MC_Y - 1) / MC_Y, (nz + MC_Z - 1) / MC_Z);
     c->gm_planes = std::max(4, std::min(256, tuned(tun ? tun->gm_planes : 0, "DNSB_GMZ", c->gm_planes)));
-    c->gm_pipe = std::max(0, std::min(2, envint("DNSB_GMPIPE", c->gm_pipe)));
+    c->gm_pipe = std::max(0, std::min(3, envint("DNSB_GMPIPE", c->gm_pipe)));
     c->gmgrid = dim3(c->tgrid.x, c->tgrid.y, (nz + c->gm_planes - 1) / c->gm_planes);
   }
   c->smem_rx = sizeof(double2) * (2 * (size_t)c->Lx * (M + 1) + M + (M + 1));
@@ -1469,6 +1530,7 @@ int dnsb_create_tuned(const dnsb_grid *gr, const dnsb_tuning *tun, int device, v
     if ((rc = dalloc(c, &c->pn, G))) return bail(rc);
     if ((rc = allow_smem(c, k_gradmom_march, GRADMOM_SMEM)) ||
         (rc = allow_smem(c, k_gradmom_pipe, GRADMOM_PIPE_SMEM)) ||
+        (rc = allow_smem(c, k_gradmom_tma, GRADMOM_TMA_SMEM)) ||
         (rc = allow_smem(c, k_gradmom_deep, GRADMOM_DEEP_SMEM)))
       return bail(rc);
   }

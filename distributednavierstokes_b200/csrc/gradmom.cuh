@@ -18,6 +18,7 @@
 // images already held by u* and delta (one more period is read for the
 // gradient at the last ghost layer), wall images mirror interior rows.
 #pragma once
+#include <cuda.h>
 #include "common.cuh"
 #include "stencil.cuh"
 #include "tma.cuh"
@@ -420,6 +421,269 @@ __global__ void __launch_bounds__(MC_X *MC_Y, 3)
     d[4] = t;
   }
   cp_async_wait<0>();
+}
+
+// staged-plane stride of k_gradmom_tma (doubles): GP_N rounded up to 16
+constexpr int GS = (GP_N + 15) / 16 * 16;
+// Dynamic shared memory of k_gradmom_tma (with 128 bytes of alignment slack).
+constexpr size_t GRADMOM_TMA_SMEM = sizeof(double) * ((size_t)(2 * 3 + 3 + 5) * GS + 3 * 3 * GP_N) + 128;
+static_assert(GS * sizeof(double) % 128 == 0, "TMA destinations 128-byte aligned");
+
+// k_gradmom_tma: k_gradmom_pipe with the raw planes (u*, delta, p) staged
+// by the tensor-memory accelerator instead of per-thread cp.async: per
+// plane one thread issues five 2-D boxes (cp.async.bulk.tensor, one
+// mbarrier phase per batch), the iteration's copies for the next plane are
+// issued before its projection instead of after it, and the wrap columns
+// of the last x tile come from registers loaded one iteration ahead.  Same
+// arithmetic, same shared-memory ring.  A wait that runs out of wait_limit
+// polls records DEVERR_TMA_TIMEOUT in *err and the CTA returns (after
+// waiting, bounded, for its last copies).
+__global__ void __launch_bounds__(MC_X *MC_Y, 3)
+    k_gradmom_tma(const __grid_constant__ CUtensorMap m_usx, const __grid_constant__ CUtensorMap m_usy,
+                  const __grid_constant__ CUtensorMap m_usz, const __grid_constant__ CUtensorMap m_d,
+                  const __grid_constant__ CUtensorMap m_p, Geo g, int planes, CFields3 us,
+                  const double *__restrict__ delta, const double *__restrict__ p_in,
+                  double *__restrict__ p_out, double radt, Fields3 q, Fields3 out, double A, double dt,
+                  double B, double adt, const double2 *__restrict__ ymet, double theta, int *err,
+                  unsigned wait_limit) {
+  // TMA destinations start on 128-byte boundaries: the base is aligned at
+  // run time (the host adds 128 bytes of slack) and the staged planes are
+  // GS >= GP_N doubles apart (GS * 8 a multiple of 128)
+  extern __shared__ __align__(128) double gsm_raw[];
+  double *gsm = gsm_raw + ((128u - (smem_u32(gsm_raw) & 127u)) & 127u) / 8;
+  double *ustar = gsm;                    // [2 slots][3][GS]
+  double *pold = ustar + 2 * 3 * GS;      // [3 slots][GS]
+  double *dl = pold + 3 * GS;             // [5 slots][GS]
+  double *unew = dl + 5 * GS;             // [3 slots][3][GP_N]
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int tid = tx + MC_X * ty;
+  const int I0 = blockIdx.x * MC_X + 1, J0 = blockIdx.y * MC_Y + 1;
+  const int K0 = blockIdx.z * planes + 1, K1 = min(g.nz, K0 + planes - 1);
+  const bool wall = g.wall;
+  const long long plane = (long long)g.NX * g.NY;
+  constexpr int NT = MC_X * MC_Y;
+  constexpr uint32_t BOX_BYTES = GP_X * GP_Y * sizeof(double);
+  // Staging by TMA: thread 0 issues one GP_X x GP_Y box (rows J0-1.., columns
+  // I0-1..) per field plane of a batch, all counted on one mbarrier whose
+  // phase n is batch n.  Rows beyond the array read as zeros (y has walls:
+  // they are never read).  Columns beyond the array are the periodic images
+  // one period on (the last x tile): nwrap columns per row, loaded by
+  // threads into registers when the batch is issued and stored after it
+  // has landed.
+  __shared__ uint64_t gbar;
+  const int nwrap = max(0, I0 - 1 + GP_X - g.NX);
+  int nbq = 0, nbatch = 0;
+  double wv0 = 0.0, wv1 = 0.0;
+  double *wd0 = nullptr, *wd1 = nullptr;
+  // one box of field f at plane z into dst, part of the current batch
+  auto box = [&](const double *f, int z, double *dst) {
+    if (z >= g.NZ) z -= g.nz;
+    if (tid == 0) {
+      const CUtensorMap *m = f == us.x ? &m_usx : f == us.y ? &m_usy : f == us.z ? &m_usz
+                             : f == delta ? &m_d : &m_p;
+      if (nbq == 0) fence_proxy_async_smem();  // the slots' earlier reads (before the last barrier) come first
+      mbar_expect_tx_only(&gbar, BOX_BYTES);
+      tma_load3(dst, m, I0 - 1, J0 - 1, z, &gbar);
+    }
+    // wrap element w = (box, row, column) of this box for w = tid, tid + NT
+    const int per = GP_Y * nwrap, lo = nbq * per;
+#pragma unroll
+    for (int r = 0; r < 2; r++) {
+      const int w = tid + r * NT - lo;
+      if (w >= 0 && w < per) {
+        const int hy = w / nwrap, c = GP_X - nwrap + w % nwrap;
+        const int x = I0 - 1 + c - g.nx, y = J0 - 1 + hy;
+        if (x < g.NX && y < g.NY) {
+          const double v = __ldg(f + (plane * z + x + (long long)g.NX * y));
+          if (r == 0) {
+            wv0 = v;
+            wd0 = dst + c + GP_X * hy;
+          } else {
+            wv1 = v;
+            wd1 = dst + c + GP_X * hy;
+          }
+        }
+      }
+    }
+    nbq++;
+  };
+  // closes the batch of the boxes queued since the last call (one arrival)
+  auto issue_batch = [&]() {
+    if (tid == 0) mbar_arrive(&gbar);
+    nbq = 0;
+    nbatch++;
+  };
+  // waits for the last batch, stores the wrap columns, then the CTA barrier;
+  // false (uniform over the CTA) when a wait ran out: the caller returns
+  auto land_batch = [&]() -> bool {
+    const bool ok = mbar_wait_n(&gbar, (uint32_t)((nbatch - 1) & 1), wait_limit);
+    if (wd0) *wd0 = wv0;
+    if (wd1) *wd1 = wv1;
+    wd0 = wd1 = nullptr;
+    if (__syncthreads_or(!ok)) {
+      if (tid == 0) {
+        atomicExch(err, DEVERR_TMA_TIMEOUT);
+        mbar_wait_n(&gbar, (uint32_t)((nbatch - 1) & 1), DNSB_WAIT_LIMIT);  // drain
+      }
+      return false;
+    }
+    return true;
+  };
+  auto us_slot = [&](int z) { return ustar + (z & 1) * 3 * GS; };
+  auto issue_us = [&](int z) {
+    double *s = us_slot(z);
+    box(us.x, z, s);
+    box(us.y, z, s + GS);
+    box(us.z, z, s + 2 * GS);
+  };
+  constexpr int HX = MC_X + 2, HY = MC_Y + 2;
+  __shared__ int rsrc[3][HY];
+  __shared__ double rsgn[3][HY], rg[HY];
+  if (tid < 3 * HY) {
+    const int c = tid / HY, hy = tid - c * HY;
+    const int y = J0 - 1 + hy;
+    int hs = hy;
+    double sgn = y <= g.NY - 1 ? 1.0 : 0.0;
+    if (wall && sgn != 0.0) {
+      if (c == STAG_Y) {
+        if (y == 0 || y == g.ny) sgn = 0.0;
+        else if (y == g.ny + 1) { hs = hy - 2; sgn = -1.0; }
+      } else {
+        if (y == 0) { hs = 1; sgn = -1.0; }
+        else if (y == g.ny + 1) { hs = hy - 1; sgn = -1.0; }
+      }
+    }
+    rsrc[c][hy] = hs;
+    rsgn[c][hy] = sgn;
+    if (c == STAG_Y) rg[hy] = sgn != 0.0 ? __ldg(g.rdyu + (J0 - 1 + hs)) : 0.0;
+  }
+  const bool plain = wall ? (J0 >= 2 && J0 + MC_Y <= g.ny - 1) : (J0 + MC_Y <= g.ny + 1);
+  // projected u of one plane from its u* and delta of it and the plane above
+  auto project_plane = [&](const double *su, const double *d0, const double *d1, double *dst) {
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+#pragma unroll
+      for (int ry = 0; ry < 2; ry++) {
+        const int hy = ty + ry * MC_Y;
+        if (hy >= HY) continue;
+        const int srow = GP_X * (plain ? hy : rsrc[c][hy]);
+        const double sgn = plain ? 1.0 : rsgn[c][hy];
+        const double gy = c == STAG_Y ? rg[hy] : 0.0;
+#pragma unroll
+        for (int rx = 0; rx < 2; rx++) {
+          const int hx = tx + rx * MC_X;
+          if (hx >= HX) continue;
+          const int a = hx + srow;
+          double v;
+          if (c == STAG_X) v = su[a] - (d0[a + 1] - d0[a]) * g.rdx;
+          else if (c == STAG_Y) v = su[GS + a] - (d0[a + GP_X] - d0[a]) * gy;
+          else v = su[2 * GS + a] - (d1[a] - d0[a]) * g.rdz;
+          dst[c * GP_N + hx + GP_X * hy] = plain ? v : sgn * v;
+        }
+      }
+    }
+  };
+  // rotating slots: d[i] holds delta of plane K+i (i = 0..4), un_* the
+  // projected planes K, K+1, K+2, p_* the lagged pressure of K, K+1, K+2
+  double *d[5] = {dl, dl + GS, dl + 2 * GS, dl + 3 * GS, dl + 4 * GS};
+  double *dm1 = d[4];  // delta of K0-1 in the slot that K0+4 takes later
+  double *un_cur = unew, *un_next = unew + 3 * GP_N, *un_new = unew + 6 * GP_N;
+  double *un_m1 = un_new;  // plane K0-1 in the slot that K0+2 takes later
+  double *p_cur = pold, *p_next = pold + GS, *p_nn = pold + 2 * GS;
+  // prologue: project K0-1, K0, K0+1; raw data of K0+2 in flight
+  if (tid == 0) {
+    mbar_init(&gbar, 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  issue_us(K0 - 1);
+  box(delta, K0 - 1, dm1);
+  box(delta, K0, d[0]);
+  issue_batch();
+  if (!land_batch()) return;
+  project_plane(us_slot(K0 - 1), dm1, d[0], un_m1);
+  issue_us(K0);
+  box(delta, K0 + 1, d[1]);
+  box(p_in, K0, p_cur);
+  issue_batch();
+  if (!land_batch()) return;  // u* of K0 and delta of K0+1 landed
+  project_plane(us_slot(K0), d[0], d[1], un_cur);
+  __syncthreads();     // every thread is done with u* of K0-1
+  issue_us(K0 + 1);
+  box(delta, K0 + 2, d[2]);
+  box(p_in, K0 + 1, p_next);
+  issue_batch();
+  if (!land_batch()) return;
+  project_plane(us_slot(K0 + 1), d[1], d[2], un_next);
+  __syncthreads();     // projected K0-1, K0, K0+1 complete; u* of K0 free
+  const int I = I0 + tx, J = J0 + ty;
+  const bool inside = I <= g.nx && J <= g.ny;
+  constexpr int SY = GP_X;
+  const int h = (tx + 1) + SY * (ty + 1);
+  // plane K0-1 as seen from the first cell: centre values and u_z east/north
+  double bx0 = un_m1[h], by0 = un_m1[GP_N + h], bz0 = un_m1[2 * GP_N + h];
+  double bzE = un_m1[2 * GP_N + h + 1], bzN = un_m1[2 * GP_N + h + SY];
+  if (K0 + 1 <= K1) {
+    issue_us(K0 + 2);
+    box(delta, K0 + 3, d[3]);
+  }
+  issue_batch();
+  for (int K = K0; K <= K1; K++) {
+    MomNb nb;
+    const int c0 = gidx(g, inside ? I : 1, inside ? J : 1, K);
+    nb.qx0 = inside ? q.x[c0] : 0.0;
+    nb.qy0 = inside ? q.y[c0] : 0.0;
+    nb.qz0 = inside ? q.z[c0] : 0.0;
+    // u* of K+2, delta of K+3, p of K+1 have landed; projected K+1 complete;
+    // slots of K-1 free
+    if (!land_batch()) return;
+    if (K + 1 <= K1) {
+      if (K + 2 <= K1) {   // raw data of the next iteration's projection
+        issue_us(K + 3);
+        box(delta, K + 4, d[4]);
+      }
+      box(p_in, K + 2, p_nn);
+    }
+    issue_batch();
+    if (K + 1 <= K1) project_plane(us_slot(K + 2), d[2], d[3], un_new);
+    if (inside) {
+      const double *pk = p_cur + h, *pk1 = p_next + h;
+      const double *dk = d[0] + h, *dk1 = d[1] + h;
+      nb.p0 = pk[0] + dk[0] * radt;
+      nb.pE = pk[1] + dk[1] * radt;
+      nb.pN = pk[SY] + dk[SY] * radt;
+      nb.pT = pk1[0] + dk1[0] * radt;
+      const double *cx = un_cur + h, *tx_ = un_next + h;
+      const double *cy = cx + GP_N, *ty_ = tx_ + GP_N;
+      const double *cz = cx + 2 * GP_N, *tz_ = tx_ + 2 * GP_N;
+      nb.ux0 = cx[0]; nb.uxE = cx[1]; nb.uxW = cx[-1]; nb.uxN = cx[SY]; nb.uxS = cx[-SY];
+      nb.uxT = tx_[0]; nb.uxB = bx0; nb.uxWN = cx[SY - 1]; nb.uxWT = tx_[-1];
+      nb.uy0 = cy[0]; nb.uyE = cy[1]; nb.uyW = cy[-1]; nb.uyN = cy[SY]; nb.uyS = cy[-SY];
+      nb.uyT = ty_[0]; nb.uyB = by0; nb.uySE = cy[1 - SY]; nb.uyST = ty_[-SY];
+      nb.uz0 = cz[0]; nb.uzE = cz[1]; nb.uzW = cz[-1]; nb.uzN = cz[SY]; nb.uzS = cz[-SY];
+      nb.uzT = tz_[0]; nb.uzB = bz0; nb.uzEB = bzE; nb.uzNB = bzN;
+      bx0 = nb.ux0; by0 = nb.uy0; bz0 = nb.uz0; bzE = nb.uzE; bzN = nb.uzN;
+      const MomCell m = mom_compute<MOM_IMPLICIT>(g, J, nb, A, dt, B, adt, 1, ymet, theta);
+      mom_store<MOM_IMPLICIT>(g, I, J, K, m, q, out);
+      store_img(p_out, g, I, J, K, nb.p0, STAG_P);
+    }
+    double *t = un_cur;
+    un_cur = un_next;
+    un_next = un_new;
+    un_new = t;
+    t = p_cur;
+    p_cur = p_next;
+    p_next = p_nn;
+    p_nn = t;
+    t = d[0];
+    d[0] = d[1];
+    d[1] = d[2];
+    d[2] = d[3];
+    d[3] = d[4];
+    d[4] = t;
+  }
+  // the last batch lands before the CTA leaves
+  if (tid == 0) mbar_wait_n(&gbar, (uint32_t)((nbatch - 1) & 1), DNSB_WAIT_LIMIT);
 }
 
 // Dynamic shared memory of k_gradmom_pipe.

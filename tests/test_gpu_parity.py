@@ -219,6 +219,10 @@ PRODUCTION = {
     "nx384_nz384": dict(n=(384, 8, 384), lims=((0, 4 * math.pi), (-1, 1), (0, 4 * math.pi / 3)),
                         bc=("periodic", "wall", "periodic"), stretch=R.tanhstretch(1.5),
                         visc=1 / 395, bodyforce=(1.0, 0.0, 0.0), ydiffusion="implicit"),
+    # two x tiles with two wrap columns, several y tiles with both walls
+    "nx64_ny40": dict(n=(64, 40, 24), lims=((0, 4 * math.pi), (-1, 1), (0, 4 * math.pi / 3)),
+                      bc=("periodic", "wall", "periodic"), stretch=R.tanhstretch(1.5),
+                      visc=1 / 395, bodyforce=(1.0, 0.0, 0.0), ydiffusion="implicit"),
     # the fused z-FFT / y-solve / inverse z-FFT (one cluster of ny/32 CTAs per
     # kx plane): 8, 1 and 2 chunks, nz = 384 and 256
     "zyz_ny256_nz384": dict(n=(8, 256, 384), lims=((0, 4 * math.pi), (-1, 1), (0, 4 * math.pi / 3)),
@@ -310,14 +314,16 @@ def test_one_step_production_lengths(oracle_mod, D, cfg):
 
 
 @pytest.mark.parametrize("planes,pipe", [("5", "0"), ("40", "0"), ("5", "1"), ("7", "1"),
-                                         ("32", "1"), ("5", "2"), ("7", "2"), ("32", "2")])
-@pytest.mark.parametrize("cfg", ["channel_implicit", "nx384_nz384"])
+                                         ("32", "1"), ("5", "2"), ("7", "2"), ("32", "2"),
+                                         ("5", "3"), ("7", "3"), ("32", "3")])
+@pytest.mark.parametrize("cfg", ["channel_implicit", "nx384_nz384", "nx64_ny40"])
 def test_fused_projection_momentum_planes(oracle_mod, D, cfg, planes, pipe, monkeypatch):
     """The fused projection + momentum kernel with other z-planes per CTA
     (DNSB_GMZ; 5, 7 and 40 leave a shorter last column, 7 a single-plane one
-    at nz = 8), its one-barrier pipelined variant (DNSB_GMPIPE=1) and the
-    variant that stages two planes ahead (DNSB_GMPIPE=2): one semi-implicit
-    step agrees with the oracle."""
+    at nz = 8), its one-barrier pipelined variant (DNSB_GMPIPE=1), the
+    variant that stages two planes ahead (DNSB_GMPIPE=2) and the one staged
+    by TMA boxes (DNSB_GMPIPE=3; the 16-wide channel falls back to 1): one
+    semi-implicit step agrees with the oracle."""
     monkeypatch.setenv("DNSB_GMZ", planes)
     monkeypatch.setenv("DNSB_GMPIPE", pipe)
     kw = CONFIGS.get(cfg) or PRODUCTION[cfg]
