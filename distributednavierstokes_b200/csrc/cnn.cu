@@ -303,6 +303,7 @@ struct Volume {
   CUtensorMap fwd[NL], bwd[NL], flatA[NL], flatB[NL];
   int Rf = 0, Rb = 0;          // patch rows of forward / transposed reads
   int subf = 1, subb = 1;      // 126-output sub-tiles per plane load, forward / transposed
+  int Rw = 0, wstages = 0;     // weight gradient: rows per K-block, K-blocks in flight
 };
 
 struct Prof {
@@ -428,22 +429,6 @@ int make_map_patch(dnsb_cnn *c, CUtensorMap *m, void *base, int P, int chunks, i
   return 0;
 }
 
-// Weight-gradient runs: dims {2 P^2 (positions and 8 channels), P (z),
-// chunks * B}, box {2 WG_K, 1, chunks} -> shared memory [chunk][WG_K][16 B].
-int make_map_run(dnsb_cnn *c, CUtensorMap *m, void *base, int P, int chunks, int B) {
-  EncodeTiledFn enc = encode_fn();
-  if (!enc) return cfail(c, DNSB_ECUDA, "cuTensorMapEncodeTiled is not available");
-  const cuuint64_t dims[3] = {2ull * P * P, (cuuint64_t)P, (cuuint64_t)chunks * B};
-  const cuuint64_t strides[2] = {16ull * P * P, 16ull * P * P * P};
-  const cuuint32_t box[3] = {2 * WG_K, 1, (cuuint32_t)chunks};
-  const cuuint32_t es[3] = {1, 1, 1};
-  const CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_UINT64, 3, base, dims, strides, box, es,
-                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                         CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  if (r != CUDA_SUCCESS) return cfail(c, DNSB_ECUDA, "cuTensorMapEncodeTiled (run) failed: %d", (int)r);
-  return 0;
-}
-
 constexpr int RING_MAX = 12, RING_MIN = 4;
 constexpr size_t CONV_EXTRA = CONV_BARS + CONV_XBUF + 1024;  // barriers, exchange, alignment slack
 
@@ -507,11 +492,46 @@ int alloc_volume(dnsb_cnn *c, Volume &V, int side, int B, bool training) {
       return cfail(c, DNSB_EUNSUP, "side %d too large: a convolution's plane ring (%d slots of %u bytes) "
                    "does not fit in shared memory", side, RING_MIN, sl);
   }
+  if (training) {
+    // weight-gradient K-blocks of R whole rows (R P positions, a multiple of
+    // 16): the most rows with at least three blocks in flight (four when
+    // they fit), at most 16 rows and P; DNSB_WGROWS / DNSB_WGSTAGES override
+    int best = 0, bstages = 0;
+    for (int r = 1; r <= std::min(16, P); r++) {
+      if ((r * P) % 16) continue;
+      // 16 chunks of taps + 4 of g, 16 bytes each, per position
+      const size_t stage = ((size_t)320 * r * P + 1023) & ~(size_t)1023;
+      const int ns = (int)std::min<size_t>(WG_STAGES, ((size_t)MAX_SMEM - 1280) / stage);
+      if (ns >= 3) {
+        best = r;
+        bstages = ns;
+      }
+    }
+    const char *er = getenv("DNSB_WGROWS"), *es = getenv("DNSB_WGSTAGES");
+    if (er) {
+      const int r = atoi(er);
+      const size_t stage = (((size_t)320 * r * P) + 1023) & ~(size_t)1023;
+      if (r >= 1 && r <= std::min(16, P) && (r * P) % 16 == 0 && 2 * stage + 1280 <= (size_t)MAX_SMEM) {
+        best = r;
+        bstages = (int)std::min<size_t>(WG_STAGES, ((size_t)MAX_SMEM - 1280) / stage);
+      }
+    }
+    if (es && best) {
+      const size_t stage = (((size_t)320 * best * P) + 1023) & ~(size_t)1023;
+      const int ns = atoi(es);
+      if (ns >= 2 && ns <= WG_STAGES && ns * stage + 1280 <= (size_t)MAX_SMEM) bstages = ns;
+    }
+    if (!best)
+      return cfail(c, DNSB_EUNSUP, "crop side %d: no weight-gradient block of whole rows fits (side + 8 must "
+                   "allow r (side + 8) to be a multiple of 16 with r <= 16)", side);
+    V.Rw = best;
+    V.wstages = bstages;
+  }
   for (int L = 0; L < NL; L++) {
     if ((rc = make_map_patch(c, &V.fwd[L], V.in[L], P, CICH[L], B, V.Rf))) return rc;
     if (training) {
-      if ((rc = make_map_run(c, &V.flatA[L], V.in[L], P, CICH[L], B))) return rc;
-      if ((rc = make_map_run(c, &V.flatB[L], V.gz[L], P, COCH[L], B))) return rc;
+      if ((rc = make_map_patch(c, &V.flatA[L], V.in[L], P, CICH[L], B, V.Rw))) return rc;
+      if ((rc = make_map_patch(c, &V.flatB[L], V.gz[L], P, COCH[L], B, V.Rw))) return rc;
       if (L > 0 && (rc = make_map_patch(c, &V.bwd[L], V.gz[L], P, COCH[L], B, V.Rb))) return rc;
     }
   }
@@ -607,16 +627,19 @@ int run_wgrad(dnsb_cnn *c, Volume &V, int L) {
   a.Pz = V.P;
   a.B = V.B;
   a.Do = V.P - 2 * (L + 1);
-  a.kpp = (a.Do * a.P + WG_K - 1) / WG_K;
+  a.R = V.Rw;
+  a.KB = V.Rw * V.P;
+  a.stages = V.wstages;
+  a.kpp = (a.Do + a.R - 1) / a.R;
   a.nk = V.B * a.Do * a.kpp;
   constexpr int G = 16 / CI;
   a.ngroups = (NTAPS + G - 1) / G;
   a.ones_slot = NTAPS - (a.ngroups - 1) * G;
-  a.a_bytes = (uint32_t)G * CI * WG_K * 16;
-  a.stage_bytes = ((a.a_bytes + (uint32_t)CO * WG_K * 16) + 1023) & ~1023u;
+  a.a_bytes = (uint32_t)G * CI * a.KB * 16;
+  a.stage_bytes = ((a.a_bytes + (uint32_t)CO * a.KB * 16) + 1023) & ~1023u;
   a.wait_limit = WAIT_LIMIT;
   a.err = c->deverr;
-  const size_t smem = (size_t)WG_STAGES * a.stage_bytes + 256 + 1024;
+  const size_t smem = (size_t)a.stages * a.stage_bytes + 256 + 1024;
   if (smem > (size_t)MAX_SMEM) return cfail(c, DNSB_EUNSUP, "weight gradient needs %zu bytes", smem);
   CC(c, cudaFuncSetAttribute(k_wgrad<CI, CO>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per = 1;

@@ -38,8 +38,9 @@
 // Weight gradient (k_wgrad): D[(tap slot j, ci)][co] = sum_o h[o + t_j][ci]
 // g[o][co] over the output positions o (the GEMM's K).  Both operands are
 // MN-major canonical layouts without swizzle, straight from the chunked
-// activations: a K-block of 128 positions of one plane is one TMA box
-// [chunk][2 KB run] per tap; 128 / (8 CI) taps fill the 128 rows (the slot
+// activations: a K-block of R whole rows of one plane (R P positions) is one
+// TMA box [chunk][R rows][x] per tap, the tap's x shift running past the row
+// end into zeros where g is zero anyway; 128 / (8 CI) taps fill the 128 rows (the slot
 // after the last real tap holds ones, which makes that row the bias
 // gradient).  Split-K partials are reduced in a fixed order.
 //
@@ -69,7 +70,6 @@ constexpr int TILE_M = 128;      // GEMM rows (positions) of a convolution tile
 constexpr int TILE_OUT = 126;    // outputs of a convolution tile (rows m, m + 1, m + 2 feed output m)
 constexpr int CONV_BARS = 512;   // bytes of barriers and flags after the plane ring
 constexpr int CONV_XBUF = CONV_GROUPS * 2 * 3 * 3 * 32 * 4;  // lane-quarter boundary exchange, bytes
-constexpr int WG_K = 128;         // positions per weight-gradient K-block (one 2 KB TMA row per chunk)
 constexpr int WG_STAGES = 4;
 constexpr int CV_STAGES = 2;
 enum { DEVERR_CNN_TIMEOUT = 2 };
@@ -655,7 +655,9 @@ __global__ void __launch_bounds__(CONV_THREADS, 1)
 struct WgradArgs {
   int P, Pz, B;     // volume geometry
   int Do;           // output box side (of g)
-  int kpp;          // K-blocks per plane: ceil(Do * P / 64)
+  int R, KB;        // rows per K-block and its positions R * P (a multiple of 16)
+  int stages;       // K-blocks in flight (<= WG_STAGES)
+  int kpp;          // K-blocks per plane: ceil(Do / R)
   int nk;           // B * Do * kpp
   int ngroups;      // ceil(27 / G) tap groups
   int nsplit;       // K splits (grid = ngroups * nsplit)
@@ -674,10 +676,10 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   constexpr int N = 8 * CO;
   constexpr int G = 16 / CI;             // tap slots per group (M = 128 rows)
   constexpr uint32_t NCOLS = N < 32 ? 32 : N;
-  constexpr uint32_t SLOT = CI * WG_K * 16;  // bytes of one tap slot
+  const uint32_t SLOT = (uint32_t)CI * a.KB * 16;  // bytes of one tap slot
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char *smem = smem_raw + ((1024u - (saddr(smem_raw) & 1023u)) & 1023u);
-  uint64_t *bars = reinterpret_cast<uint64_t *>(smem + WG_STAGES * a.stage_bytes);
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem + a.stages * a.stage_bytes);
   uint64_t *full = bars, *empty = bars + WG_STAGES, *done = bars + 2 * WG_STAGES;
   uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + 2 * WG_STAGES + 1);
   volatile int *abort_flag = reinterpret_cast<volatile int *>(bars + 2 * WG_STAGES + 2);
@@ -690,7 +692,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   const int k1 = (int)((long long)a.nk * (split + 1) / a.nsplit);
 
   if (threadIdx.x == 0) {
-    for (int i = 0; i < WG_STAGES; i++) {
+    for (int i = 0; i < a.stages; i++) {
       mb_init(&full[i], 1);
       mb_init(&empty[i], 1);
     }
@@ -701,7 +703,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   if (ones) {
     // the slot after the last tap: BF16 ones, in every stage, never copied over
     const uint32_t one2 = 0x3F803F80u;
-    for (int st = 0; st < WG_STAGES; st++) {
+    for (int st = 0; st < a.stages; st++) {
       uint32_t *p = reinterpret_cast<uint32_t *>(smem + st * a.stage_bytes + a.ones_slot * SLOT);
       for (int i = threadIdx.x; i < (int)(SLOT / 4); i += NTHREADS) p[i] = one2;
     }
@@ -715,10 +717,10 @@ __global__ void __launch_bounds__(NTHREADS, 1)
 
   if (warp == 0) {
     if (lane == 0) {
-      const uint32_t bytes = (uint32_t)ntap * SLOT + (uint32_t)CO * WG_K * 16;
+      const uint32_t bytes = (uint32_t)ntap * SLOT + (uint32_t)CO * a.KB * 16;
       int i = 0, issued = 0;
       for (int k = k0; k < k1; k++, i++) {
-        const int s = i % WG_STAGES, ph = (i / WG_STAGES) & 1;
+        const int s = i % a.stages, ph = (i / a.stages) & 1;
         if (*abort_flag || !mb_wait(&empty[s], ph ^ 1, a.wait_limit, abort_flag)) {
           *abort_flag = 1;
           atomicExch(a.err, DEVERR_CNN_TIMEOUT);
@@ -726,20 +728,22 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         }
         const int jb = k % a.kpp, rest = k / a.kpp;
         const int z = rest % a.Do, b = rest / a.Do;
-        const int f0 = jb * WG_K;
+        const int y0 = jb * a.R;
         unsigned char *st = smem + s * a.stage_bytes;
         mb_expect(&full[s], bytes);
+        // R whole rows per box; a tap's x shift runs past the row end into
+        // zeros, where g (zero outside its output box) takes nothing
         for (int j = 0; j < ntap; j++) {
           const int tap = tap0 + j;
           const int dz = tap / 9, dy = (tap / 3) % 3, dx = tap % 3;
-          tma3(st + j * SLOT, &th, 2 * (f0 + dx + dy * a.P), z + dz, b * CI, &full[s]);
+          tma4(st + j * SLOT, &th, 2 * dx, y0 + dy, z + dz, b * CI, &full[s]);
         }
-        tma3(st + a.a_bytes, &tg, 2 * f0, z, b * CO, &full[s]);
+        tma4(st + a.a_bytes, &tg, 0, y0, z, b * CO, &full[s]);
         issued = i + 1;
       }
       // let the last copies of every stage land before leaving
-      for (int i2 = issued - WG_STAGES < 0 ? 0 : issued - WG_STAGES; i2 < issued; i2++)
-        mb_wait(&full[i2 % WG_STAGES], (i2 / WG_STAGES) & 1, a.wait_limit, abort_flag);
+      for (int i2 = issued - a.stages < 0 ? 0 : issued - a.stages; i2 < issued; i2++)
+        mb_wait(&full[i2 % a.stages], (i2 / a.stages) & 1, a.wait_limit, abort_flag);
     }
   } else if (warp == 1) {
     if (lane == 0) {
@@ -747,7 +751,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       int i = 0;
       bool ok = true, any = false;
       for (int k = k0; k < k1; k++, i++) {
-        const int s = i % WG_STAGES, ph = (i / WG_STAGES) & 1;
+        const int s = i % a.stages, ph = (i / a.stages) & 1;
         if (*abort_flag || !mb_wait(&full[s], ph, a.wait_limit, abort_flag)) {
           ok = false;
           break;
@@ -755,12 +759,12 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         tc_fence_after();
         const uint32_t sa = saddr(smem + s * a.stage_bytes);
         const uint32_t sb = sa + a.a_bytes;
-#pragma unroll
-        for (int kk = 0; kk < WG_K / 16; kk++) {
-          // MN-major, no swizzle: SBO = stride of 8-element MN groups (1 KB),
-          // LBO = stride of 8-row K groups (128 B)
-          const uint64_t ad = sdesc(sa + kk * 256, 128, WG_K * 16);
-          const uint64_t bd = sdesc(sb + kk * 256, 128, WG_K * 16);
+        const int nkk = a.KB / 16;
+        for (int kk = 0; kk < nkk; kk++) {
+          // MN-major, no swizzle: SBO = stride of 8-element MN groups (one
+          // chunk's K-block, 16 KB bytes), LBO = stride of 8-row K groups (128 B)
+          const uint64_t ad = sdesc(sa + kk * 256, 128, (uint32_t)a.KB * 16);
+          const uint64_t bd = sdesc(sb + kk * 256, 128, (uint32_t)a.KB * 16);
           mma_bf16(tbase, ad, bd, idesc, (i | kk) != 0);
         }
         mma_commit(&empty[s]);
