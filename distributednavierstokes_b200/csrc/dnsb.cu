@@ -104,6 +104,11 @@ struct dnsb_ctx {
   int gm_planes = 32;
   std::map<const void *, CUtensorMap> gm_maps;  // TMA maps of the fused kernel's staged fields
   int mom_planes = MC_Z;  // z planes per CTA of k_momentum_march
+  // while a CUDA graph of LES steps is captured: the device word holding
+  // the step size, read by the kernels that take dt (else nullptr)
+  const double *dtp = nullptr;
+  cudaStream_t les_cap = nullptr;  // capture stream of dnsb_les_advance's graph
+  double *les_state = nullptr;     // its device state: t, dt, steps
   // one-barrier pipelined variant of the fused kernel: 2.5 % faster than
   // the two-barrier k_gradmom_march at 384x256x384
   int gm_pipe = 1;
@@ -955,7 +960,7 @@ int do_step(dnsb_ctx *c, double *ux, double *uy, double *uz, double *p, double *
         LAUNCH(c, DNSB_KIND_MOMENTUM,
                k_momentum_march<MOM_EXPLICIT><<<c->tgrid, c->tblock, 0, c->stream>>>(
                    g, ff(qx, qy, qz), cf(ux, uy, uz), ff(c->W[0], c->W[1], c->W[2]), nullptr, A,
-                   dt, B, 0.0, readq, c->ymet, 0.0, c->mom_planes));
+                   dt, B, 0.0, readq, c->ymet, 0.0, c->mom_planes, c->dtp));
       else
         LAUNCH(c, DNSB_KIND_MOMENTUM,
                k_momentum<MOM_EXPLICIT><<<c->cgrid, c->cblock, 0, c->stream>>>(
@@ -975,7 +980,7 @@ int do_step(dnsb_ctx *c, double *ux, double *uy, double *uz, double *p, double *
         LAUNCH(c, DNSB_KIND_MOMENTUM,
                k_momentum_march<MOM_IMPLICIT><<<c->tgrid, c->tblock, 0, c->stream>>>(
                    g, ff(qx, qy, qz), cf(ux, uy, uz), ff(c->V[0], c->V[1], c->V[2]), p, A, dt, B,
-                   adt, readq, c->ymet, th, c->mom_planes));
+                   adt, readq, c->ymet, th, c->mom_planes, c->dtp));
       else
         LAUNCH(c, DNSB_KIND_MOMENTUM,
                k_momentum<MOM_IMPLICIT><<<c->cgrid, c->cblock, 0, c->stream>>>(
@@ -1560,6 +1565,7 @@ void dnsb_destroy(dnsb_ctx *c) {
   for (void *p : c->allocs) cudaFree(p);
   if (c->hostred) cudaFreeHost(c->hostred);
   if (c->hostumax) cudaFreeHost(c->hostumax);
+  if (c->les_cap) cudaStreamDestroy(c->les_cap);
   delete c;
 }
 
@@ -1619,7 +1625,7 @@ int dnsb_momentum(dnsb_ctx *c, double *qx, double *qy, double *qz, const double 
   if (use_tile(c, ux, uy, uz))
     k_momentum_march<MOM_ONLY><<<c->tgrid, c->tblock, 0, c->stream>>>(
         c->g, ff(qx, qy, qz), cf(ux, uy, uz), ff(nullptr, nullptr, nullptr), nullptr, A, dt, 0.0,
-        0.0, 1, c->ymet, 0.0, c->mom_planes);
+        0.0, 1, c->ymet, 0.0, c->mom_planes, c->dtp);
   else
     k_momentum<MOM_ONLY><<<cell_grid(c->g), cell_block, 0, c->stream>>>(
         c->g, ff(qx, qy, qz), cf(ux, uy, uz), ff(nullptr, nullptr, nullptr), nullptr, A, dt, 0.0,
@@ -1762,7 +1768,8 @@ int dnsb_project(dnsb_ctx *c, double *ux, double *uy, double *uz, double *psi) {
 // edges (four cells) and differenced across the face's cell in the
 // transverse direction.  tau == NULL: the plain stage update.
 __global__ void k_sfs_stage(Geo g, const double *__restrict__ tau, Fields3 q, Fields3 u, double dt,
-                            double B) {
+                            double B, const double *__restrict__ dtp) {
+  if (dtp) dt = *dtp;  // the step size from device memory (a step inside a CUDA graph)
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int k = blockIdx.z;
@@ -1824,7 +1831,7 @@ int dnsb_sfs_stage(dnsb_ctx *c, const double *tau, double *qx, double *qy, doubl
   if (c->g.wall && tau) return fail(c, DNSB_EINVAL, "the closure stage needs a periodic box");
   if (ensure_device(c)) return DNSB_ECUDA;
   k_sfs_stage<<<cell_grid(c->g), cell_block, 0, c->stream>>>(c->g, tau, ff(qx, qy, qz),
-                                                             ff(ux, uy, uz), dt, B);
+                                                             ff(ux, uy, uz), dt, B, c->dtp);
   CKL(c);
   c->launches++;
   c->umax_for[0] = c->umax_for[1] = c->umax_for[2] = nullptr;
@@ -1853,6 +1860,136 @@ int dnsb_les_step(dnsb_ctx *c, dnsb_cnn *cnn, double *ux, double *uy, double *uz
   return 0;
 }
 
+// The CFL step of cfl_from_max on the device (the same correctly rounded
+// operations in the same order, so the same bits as the host's), limited
+// to t1 - t: st = {t, dt, steps}; cfl_diff = cfl * the diffusive limit.
+__global__ void k_les_dt(const unsigned long long *bits, double *st, double dx, double dymin, double dz,
+                         double cfl, double cfl_diff, double t1) {
+  const double eps = 2.220446049250313e-16;
+  const double m0 = __longlong_as_double((long long)bits[0]);
+  const double m1 = __longlong_as_double((long long)bits[1]);
+  const double m2 = __longlong_as_double((long long)bits[2]);
+  const double c1 = __ddiv_rn(dx, __dadd_rn(m0, eps)), c2 = __ddiv_rn(dymin, __dadd_rn(m1, eps));
+  const double c3 = __ddiv_rn(dz, __dadd_rn(m2, eps));
+  const double conv = fmin(fmin(c1, c2), c3);
+  const double dt = fmin(__dmul_rn(cfl, conv), cfl_diff);
+  const double left = __dsub_rn(t1, st[0]);
+  st[1] = left < dt ? left : dt;
+}
+
+// t += dt, one more step, and the loop condition t < thr for the next pass
+__global__ void k_les_tick(double *st, cudaGraphConditionalHandle cond, double thr) {
+  const double t = __dadd_rn(st[0], st[1]);
+  st[0] = t;
+  st[2] += 1.0;
+  cudaGraphSetConditional(cond, t < thr ? 1u : 0u);
+}
+
+// dnsb_les_advance as one launch of a CUDA graph: a conditional WHILE node
+// whose body is one step (CFL maximum -> dt on the device -> the step with
+// the kernels reading dt from device memory -> shell clamp -> t += dt and
+// the loop condition); no host synchronisation until the end.
+int les_advance_graph(dnsb_ctx *c, dnsb_cnn *cnn, double *ux, double *uy, double *uz, double *p,
+                      double *qx, double *qy, double *qz, double *tau, double t0, double t1, double cfl,
+                      const double *eref, int nshells, double *t_out, long *n_out) {
+  const Geo &g = c->g;
+  int rc;
+  const double thr = t1 - 1e-12 * (std::fabs(t1) + 1);
+  if (!(t0 < thr)) {
+    if (t_out) *t_out = t1;
+    if (n_out) *n_out = 0;
+    return 0;
+  }
+  if (!c->les_cap) CK(c, cudaStreamCreateWithFlags(&c->les_cap, cudaStreamNonBlocking));
+  if (!c->les_state && (rc = dalloc(c, &c->les_state, 4))) return rc;
+  const int nb = eref && nshells > 0 ? std::min(nshells, c->nshell_max) : 0;
+  if (nb && (rc = upload_eref(c, eref, nb))) return rc;  // scratch and table before the capture
+  // the diffusive limit exactly as cfl_from_max forms it
+  const double eps = 2.220446049250313e-16;
+  const double invdy2 = c->implicit ? 0.0 : 1 / (c->dymin * c->dymin);
+  const double diff = 1 / (2 * g.visc * (1 / (g.dx * g.dx) + invdy2 + 1 / (g.dz * g.dz)) + eps);
+  const double cfl_diff = cfl * diff;
+  cudaGraph_t graph = nullptr, captured = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaGraphConditionalHandle cond;
+  CK(c, cudaGraphCreate(&graph, 0));
+  // (the captured graph is the WHILE node's body, owned by `graph`)
+  auto drop = [&](int code) {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    return code;
+  };
+  if (cudaGraphConditionalHandleCreate(&cond, graph, 1, cudaGraphCondAssignDefault) != cudaSuccess)
+    return drop(fail(c, DNSB_ECUDA, "conditional handle creation failed"));
+  cudaGraphNodeParams wp = {};
+  wp.type = cudaGraphNodeTypeConditional;
+  wp.conditional.handle = cond;
+  wp.conditional.type = cudaGraphCondTypeWhile;
+  wp.conditional.size = 1;
+  cudaGraphNode_t wnode;
+  if (cudaGraphAddNode(&wnode, graph, nullptr, 0, &wp) != cudaSuccess)
+    return drop(fail(c, DNSB_ECUDA, "conditional node creation failed"));
+  cudaGraph_t body = wp.conditional.phGraph_out[0];
+  cudaStream_t orig = c->stream;
+  {
+    const cudaError_t se = cudaGetLastError();
+    if (se != cudaSuccess) return drop(fail(c, DNSB_ECUDA, "error pending before the capture: %s", cudaGetErrorString(se)));
+  }
+  if (cudaStreamBeginCaptureToGraph(c->les_cap, body, nullptr, nullptr, 0,
+                                    cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+    return drop(fail(c, DNSB_ECUDA, "stream capture could not start"));
+  c->stream = c->les_cap;
+  c->dtp = c->les_state + 1;
+  unsigned long long *scratch = c->umax + 3 * UMAX_SLOTS;
+  rc = 0;
+  if (cudaMemsetAsync(scratch, 0, 3 * sizeof(unsigned long long), c->stream) != cudaSuccess)
+    rc = fail(c, DNSB_ECUDA, "capture: memset failed");
+  auto launched = [&](const char *what) {
+    const cudaError_t le = cudaGetLastError();
+    return le == cudaSuccess ? 0 : fail(c, DNSB_ECUDA, "capture: %s: %s", what, cudaGetErrorString(le));
+  };
+  if (!rc) {
+    k_maxabs3<<<RED_BLOCKS, 256, 0, c->stream>>>(g, cf(ux, uy, uz), scratch, nullptr);
+    rc = launched("velocity maxima");
+  }
+  if (!rc) {
+    k_les_dt<<<1, 1, 0, c->stream>>>(scratch, c->les_state, g.dx, c->dymin, g.dz, cfl, cfl_diff, t1);
+    rc = launched("step size");
+  }
+  // the dt argument only passes the host-side checks: the kernels read *dtp
+  if (!rc)
+    rc = cnn ? dnsb_les_step(c, cnn, ux, uy, uz, p, qx, qy, qz, tau, 1.0)
+             : dnsb_step(c, ux, uy, uz, p, qx, qy, qz, nullptr, 1.0);
+  if (!rc && nb) rc = dnsb_shell_clamp(c, ux, uy, uz, eref, nshells);
+  if (!rc) {
+    k_les_tick<<<1, 1, 0, c->stream>>>(c->les_state, cond, thr);
+    rc = launched("time advance");
+  }
+  const cudaError_t ce = cudaStreamEndCapture(c->les_cap, &captured);
+  c->stream = orig;
+  c->dtp = nullptr;
+  if (cnn) dnsb_cnn_set_stream(cnn, orig);
+  if (rc) return drop(rc);
+  if (ce != cudaSuccess) return drop(fail(c, DNSB_ECUDA, "stream capture failed: %s", cudaGetErrorString(ce)));
+  if (cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess)
+    return drop(fail(c, DNSB_ECUDA, "graph instantiation failed"));
+  double *h = c->hostred;
+  h[0] = t0;
+  h[1] = 0.0;
+  h[2] = 0.0;
+  if (cudaMemcpyAsync(c->les_state, h, 3 * sizeof(double), cudaMemcpyHostToDevice, orig) != cudaSuccess ||
+      cudaGraphLaunch(exec, orig) != cudaSuccess ||
+      cudaMemcpyAsync(h, c->les_state, 3 * sizeof(double), cudaMemcpyDeviceToHost, orig) != cudaSuccess ||
+      cudaStreamSynchronize(orig) != cudaSuccess)
+    return drop(fail(c, DNSB_ECUDA, "graph launch failed: %s", cudaGetErrorString(cudaGetLastError())));
+  drop(0);
+  if ((rc = check_deverr(c))) return rc;
+  c->umax_for[0] = c->umax_for[1] = c->umax_for[2] = nullptr;
+  if (t_out) *t_out = t1;
+  if (n_out) *n_out = (long)h[2];
+  return 0;
+}
+
 int dnsb_les_advance(dnsb_ctx *c, dnsb_cnn *cnn, double *ux, double *uy, double *uz, double *p,
                      double *qx, double *qy, double *qz, double *tau, double t0, double t1,
                      double cfl, const double *eref, int nshells, double *t_out, long *n_out) {
@@ -1860,6 +1997,16 @@ int dnsb_les_advance(dnsb_ctx *c, dnsb_cnn *cnn, double *ux, double *uy, double 
     return c ? fail(c, DNSB_EINVAL, "null field") : DNSB_EINVAL;
   if (!(cfl > 0) || !std::isfinite(t0) || !std::isfinite(t1))
     return fail(c, DNSB_EINVAL, "cfl must be positive and the times finite");
+  if (ensure_device(c)) return DNSB_ECUDA;
+  // one graph launch for the whole run where every kernel of the step can
+  // read dt from device memory (the z-marching momentum: aligned fields),
+  // no per-launch timing is on and the box is explicit; DNSB_LESGRAPH=0
+  // keeps the host loop
+  const bool direct_clamp = !eref || nshells <= 0 || (!c->g.wall && clamp_direct(c, std::min(nshells, c->nshell_max)));
+  if (envint("DNSB_LESGRAPH", 1) != 0 && !c->implicit && !c->prof_on && use_tile(c, ux, uy, uz) &&
+      direct_clamp)
+    return les_advance_graph(c, cnn, ux, uy, uz, p, qx, qy, qz, tau, t0, t1, cfl, eref, nshells, t_out,
+                             n_out);
   double t = t0;
   long n = 0;
   while (t < t1 - 1e-12 * (std::fabs(t1) + 1)) {

@@ -252,8 +252,10 @@ template <int MODE>
 __global__ void __launch_bounds__(MC_X *MC_Y, 3)
     k_momentum_march(Geo g, Fields3 q, CFields3 u, Fields3 out, const double *__restrict__ p,
                      double A, double dt, double B, double adt, int readq,
-                     const double2 *__restrict__ ymet, double theta, int planes) {
+                     const double2 *__restrict__ ymet, double theta, int planes,
+                     const double *__restrict__ dtp) {
   __shared__ __align__(16) double ring[4][3][MP_N];
+  if (dtp) dt = *dtp;  // the step size from device memory (a step inside a CUDA graph)
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int tid = tx + MC_X * ty;
   const int I0 = blockIdx.x * MC_X + 1, J0 = blockIdx.y * MC_Y + 1;

@@ -136,10 +136,14 @@ def test_small_study_closure_beats_unclosed(M):
     assert les["steps"]["les_cnn"] > 0 and les["steps"]["dns"] > 0
 
 
-def test_les_advance_matches_step_loop(M):
+@pytest.mark.parametrize("graph", ["1", "0"])
+def test_les_advance_matches_step_loop(M, graph, monkeypatch):
     """dnsb_les_advance (CFL steps, closure every stage, shell clamp after
     each step, the last step shortened onto t1) equals the same loop driven
-    step by step from Python; without a closure it runs dnsb_step."""
+    step by step from Python bit for bit; without a closure it runs
+    dnsb_step.  graph "1": the whole run as one CUDA-graph launch with the
+    step size computed on the device (the default); "0": the host loop."""
+    monkeypatch.setenv("DNSB_LESGRAPH", graph)
     dns, L = M
     from distributednavierstokes_b200.closure import Closure
 
