@@ -112,7 +112,14 @@ int dnsb_les_step(dnsb_ctx *ctx, dnsb_cnn *cnn, double *ux, double *uy, double *
  * or the library's fused dnsb_step when cnn is NULL (the unclosed
  * fallback); after each step the shell-energy clamp dnsb_shell_clamp with
  * the HOST table eref[0..nshells) when eref is not NULL.  Reports t1 and the
- * number of steps; synchronises once per step (the CFL maximum). */
+ * number of steps.  Where the fields are 16-byte aligned, the box explicit,
+ * the clamp the direct one (at most 4 shells) and per-launch timing off, the
+ * whole run is one launch of a CUDA graph (a conditional loop whose body
+ * computes the CFL step on the device, with the same operations as
+ * cfl_timestep here, and runs the step reading it from device memory):
+ * the call synchronises once, at the end; otherwise (or with the
+ * environment variable DNSB_LESGRAPH=0) a host loop synchronises once per
+ * step for the CFL maximum.  Both give the same bits. */
 int dnsb_les_advance(dnsb_ctx *ctx, dnsb_cnn *cnn, double *ux, double *uy, double *uz, double *p,
                      double *qx, double *qy, double *qz, double *tau, double t0, double t1,
                      double cfl, const double *eref, int nshells, double *t_out, long *n_out);
