@@ -568,9 +568,11 @@ def closure_arm(args, wl, world, rank, local):
                      "note": "algorithmic FLOPs (2 x 27 x cin x cout per output voxel and "
                              "pass) over the CUDA-event time of the training loop"},
         "e2e": {"value": les["speedup_cnn_vs_dns"], "unit": "x", "h2d_bytes_per_step": 0,
-                "d2h_bytes_per_step": 8,
-                "note": "device-resident state; the CFL step size (8 bytes) is read back every "
-                        "step, inside the timed region, for both the LES and the DNS"},
+                "d2h_bytes_per_step": 24.0 * kw["nsample"] / max(les["steps"]["les_cnn"], 1),
+                "note": "device-resident state; every advance between two sample times (one "
+                        "CUDA-graph launch, the CFL step computed on the device) reads back its "
+                        "time and step count (24 bytes) inside the timed region, for both the "
+                        "LES and the DNS"},
         "gpu_launches": res.get("closure_launches"),
         "wall_s": wall,
         "clocks": clk,
