@@ -629,17 +629,50 @@ def slab_arm(args, wl, world, rank, local):
     clocks = ClockSampler(local)
     clocks.start()
     stream = torch.cuda.current_stream(dev)
+    from distributednavierstokes_b200 import _lib
+
+    lib = _lib.load()
+    ctxs = [part.s._ctx, sg._ctx]
+    n0 = sum(lib.dnsb_launch_count(cx) for cx in ctxs)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
     for _ in range(args.steps):
         one_step()
     ev1.record(stream)
     torch.cuda.synchronize(dev)
+    launches = sum(lib.dnsb_launch_count(cx) for cx in ctxs) - n0
     ms = ev0.elapsed_time(ev1)
     clk = clocks.stop()
-    t = torch.tensor([ms], device=dev, dtype=torch.float64)
+    # end to end: the same K steps with this rank's slab of u copied in from
+    # pinned host memory first and its u and p copied back after, inside the
+    # timed region (the same collective sequence on every rank)
+    e2e_err, ms_e2e, slab_bytes = None, 0.0, 0
+    try:
+        hu = {c: st[0][c].detach().to("cpu").pin_memory() for c in "xyz"}
+        hp = st[1].detach().to("cpu").pin_memory()
+        slab_bytes = hu["x"].numel() * 8
+    except Exception as exc:  # reported in the line; the timing below keeps every rank in step
+        e2e_err = f"{type(exc).__name__}: {exc}"
+    torch.cuda.synchronize(dev)
+    dist.barrier()
+    torch.cuda.synchronize(dev)
+    ev2, ev3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev2.record(stream)
+    if e2e_err is None:
+        for c in "xyz":
+            st[0][c].copy_(hu[c], non_blocking=True)
+    for _ in range(args.steps):
+        one_step()
+    if e2e_err is None:
+        for c in "xyz":
+            hu[c].copy_(st[0][c], non_blocking=True)
+        hp.copy_(st[1], non_blocking=True)
+    ev3.record(stream)
+    torch.cuda.synchronize(dev)
+    ms_e2e = ev2.elapsed_time(ev3)
+    t = torch.tensor([ms, ms_e2e, 1.0 if e2e_err else 0.0], device=dev, dtype=torch.float64)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms = float(t.item())
+    ms, ms_e2e, e2e_failed = float(t[0].item()), float(t[1].item()), float(t[2].item()) > 0
     md = slab.maxdiv(parts, comm, lambda p: st[0])
     dist.barrier()
     if rank == 0:
@@ -657,7 +690,13 @@ def slab_arm(args, wl, world, rank, local):
             "step_roofline": {"bytes_per_cell_step": wl["bytes_per_cell_step"],
                               "achieved": wl["bytes_per_cell_step"] * value / 1e9 / world, "peak": peak,
                               "unit": "GB/s per GPU", "peak_source": peak_kind},
-            "e2e": None, "gpu_launches": None, "cpu_baseline": None}), flush=True)
+            "e2e": ({"unavailable": e2e_err or "the host copies failed on a rank"} if e2e_failed else
+                    {"value": cells * args.steps / (ms_e2e / 1e3), "unit": "cell-steps/s",
+                     "h2d_bytes_per_step": 3 * slab_bytes * world / args.steps,
+                     "d2h_bytes_per_step": 4 * slab_bytes * world / args.steps,
+                     "note": "each rank's slab of u from pinned host memory before the K steps, "
+                             "u and p back after, inside the timed region (max over ranks)"}),
+            "gpu_launches": launches, "cpu_baseline": None}), flush=True)
     for p in parts.values():
         p.close()
     sg.close()
