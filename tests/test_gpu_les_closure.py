@@ -182,3 +182,35 @@ def test_les_advance_matches_step_loop(M, graph, monkeypatch):
             assert torch.equal(ua[c], ub[c]), (closed, c)
     cl.close()
     s.close()
+
+
+def test_les_advance_edges(M):
+    """dnsb_les_advance: an interval shorter than the time tolerance takes no
+    step and leaves u alone; a closure without its tau buffer and the closed
+    step on a semi-implicit (channel) context are refused with an error."""
+    dns, L = M
+    from distributednavierstokes_b200 import _lib
+    from distributednavierstokes_b200.closure import Closure
+
+    n = 16
+    s = dns.setup(n=(n,) * 3, visc=0.01)
+    u = dns.random_field(dns.vectorfield(s), s, totalenergy=0.5, kpeak=3.0, seed=9)
+    u0 = {c: u[c].clone() for c in "xyz"}
+    p, q = dns.scalarfield(s), dns.vectorfield(s)
+    t_end, steps = L.advance(u, p, q, s, 0.3, 0.3, 0.5)
+    assert (t_end, steps) == (0.3, 0)
+    for c in "xyz":
+        assert torch.equal(u[c], u0[c]), c
+    cl = Closure(batch=0, crop=0, nfield=n, seed=1)
+    with pytest.raises(ValueError):
+        L.les_step(u, p, q, s, 0.01, cl, None)
+    ch = dns.setup(n=(16, 12, 16), lims=((0, 1.0), (-1, 1), (0, 1.0)),
+                   bc=("periodic", "wall", "periodic"), visc=0.01, ydiffusion="implicit")
+    uc = dns.vectorfield(ch)
+    pc, qc = dns.scalarfield(ch), dns.vectorfield(ch)
+    tau = torch.zeros((6, n, n, n), dtype=torch.float64, device="cuda")
+    with pytest.raises(_lib.DNSBError):
+        L.les_step(uc, pc, qc, ch, 0.01, cl, tau)
+    cl.close()
+    ch.close()
+    s.close()
