@@ -302,7 +302,7 @@ struct Volume {
   float4 *tgt = nullptr;       // targets (training)
   CUtensorMap fwd[NL], bwd[NL], flatA[NL], flatB[NL];
   int Rf = 0, Rb = 0;          // patch rows of forward / transposed reads
-  int subf = 1, subb = 1;      // 126-output sub-tiles per plane load, forward / transposed
+  int subf = 1, subb = 1;      // 126-output sub-tiles per plane load (1-4), forward / transposed
   int Rw = 0, wstages = 0;     // weight gradient: rows per K-block, K-blocks in flight
 };
 
@@ -470,14 +470,21 @@ int alloc_volume(dnsb_cnn *c, Volume &V, int side, int B, bool training) {
       if ((rc = dal(c, &V.gz[L], (size_t)B * COCH[L] * P3))) return rc;
     if ((rc = dal(c, &V.tgt, (size_t)B * P3 * 2))) return rc;
   }
-  // two sub-tiles per plane load (half the copies per output) where the
-  // wider patch fits the plane and a ring of at least RING_MIN planes
+  // up to four 126-output sub-tiles per plane load (fewer copies per
+  // output): the most whose wider patch fits the plane and a ring of at
+  // least RING_MIN planes
   {
-    int ns;
-    uint32_t sl, st, wb;
-    const int rf2 = patch_rows(P, 0, 0, 2), rb2 = patch_rows(P, -2, 1, 2);
-    V.subf = rf2 <= P && conv_smem(4, 4, P, rf2, &ns, &sl, &st, &wb) ? 2 : 1;
-    V.subb = rb2 <= P && conv_smem(4, 4, P, rb2, &ns, &sl, &st, &wb) ? 2 : 1;
+    auto most = [&](int s, int e) {
+      for (int sub = 4; sub > 1; sub--) {
+        int ns;
+        uint32_t sl, st, wb;
+        const int r = patch_rows(P, s, e, sub);
+        if (r <= P && conv_smem(4, 4, P, r, &ns, &sl, &st, &wb)) return sub;
+      }
+      return 1;
+    };
+    V.subf = most(0, 0);
+    V.subb = most(-2, 1);
   }
   V.Rf = patch_rows(P, 0, 0, V.subf);
   V.Rb = patch_rows(P, -2, 1, V.subb);

@@ -289,7 +289,7 @@ struct ConvArgs {
   int P, Pz, B;        // volume pitch (x, y), planes, samples
   int Do;              // output box side
   int s, e, R;         // input offset (0 / -2), extra patch row, patch rows
-  int sub;             // 126-output sub-tiles per tile (1 or 2), one plane load each tile
+  int sub;             // 126-output sub-tiles per tile (1 to 4), one plane load each tile
   int tpp;             // tiles per plane: ceil(Do * P / (126 sub))
   int ntiles;          // B * tpp * Do output tiles, z fastest
   int nslot;           // input planes held in the shared-memory ring
@@ -490,17 +490,12 @@ __global__ void __launch_bounds__(CONV_THREADS, 1)
     // the tile's (b, j, z) and this thread's positions in its sub-tiles,
     // updated as z marches
     int z = t0 % a.Do, j = (t0 / a.Do) % a.tpp, b = t0 / (a.Do * a.tpp);
-    int fA = 0, xA = 0, yA = 0, fB = 0, xB = 0, yB = 0;
+    int fA = 0;
     bool fresh = true, stop = false;
     int i = 0, own = 0;
     for (int t = t0; t < t1 && !stop; t++) {
       if (fresh) {
         fA = j * a.sub * TILE_OUT + m;
-        xA = fA % a.P;
-        yA = fA / a.P;
-        fB = fA + TILE_OUT;
-        xB = fB % a.P;
-        yB = fB / a.P;
         fresh = false;
       }
       const int zc = z, bc = b;
@@ -565,8 +560,10 @@ __global__ void __launch_bounds__(CONV_THREADS, 1)
           }
           own++;
         }
-        const int f = sb ? fB : fA, x = sb ? xB : xA, y = sb ? yB : yA;
-        if (!mine || m >= TILE_OUT || f >= P2) continue;
+        if (!mine || m >= TILE_OUT) continue;
+        const int f = fA + sb * TILE_OUT;
+        if (f >= P2) continue;
+        const int y = f / a.P, x = f - y * a.P;
         const bool valid = x < a.Do && y < a.Do;
         const long long vox = (long long)zc * P2 + f;
         if (MODE == FWD_GELU) {
