@@ -69,7 +69,7 @@ constexpr int NTAPS = 27;
 constexpr int TILE_M = 128;      // GEMM rows (positions) of a convolution tile
 constexpr int TILE_OUT = 126;    // outputs of a convolution tile (rows m, m + 1, m + 2 feed output m)
 constexpr int CONV_BARS = 512;   // bytes of barriers and flags after the plane ring
-constexpr int CONV_XBUF = CONV_GROUPS * 2 * 3 * 3 * 32 * 4;  // lane-quarter boundary exchange, bytes
+constexpr int CONV_XBUF = CONV_GROUPS * 2 * 3 * 2 * 32 * 4;  // lane-quarter boundary exchange, bytes
 constexpr int WG_STAGES = 4;
 constexpr int CV_STAGES = 2;
 enum { DEVERR_CNN_TIMEOUT = 2 };
@@ -335,7 +335,7 @@ __global__ void __launch_bounds__(CONV_THREADS, 1)
   constexpr uint32_t ACC_STRIDE = N <= 64 ? 64 : 128;   // TMEM columns per accumulator
   constexpr uint32_t NCOLS = NACC * ACC_STRIDE;         // 256 or 512 columns
   constexpr int MAXSLOT = 12;
-  constexpr int XB = 3 * 3 * NW;                        // exchange floats per group and buffer
+  constexpr int XB = 3 * 2 * NW;                        // exchange floats per group and buffer
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   // 1 KB-aligned base (TMA destinations; the host adds 1 KB of slack)
   unsigned char *smem = smem_raw + ((1024u - (saddr(smem_raw) & 1023u)) & 1023u);
@@ -349,7 +349,8 @@ __global__ void __launch_bounds__(CONV_THREADS, 1)
   float *lsum = reinterpret_cast<float *>(bars + 2 * MAXSLOT + 2 * NACC + 3);  // 16 floats
   float *bsm = reinterpret_cast<float *>(reinterpret_cast<unsigned char *>(bars) + 352);  // 32 biases
   // boundary rows handed between TMEM lane quarters: [group][buffer][quarter
-  // 1..3][3][NW] (row 32q: x-shift 1 and 2, row 32q + 1: x-shift 2)
+  // 1..3][2][NW] (row 32q's x-shift 2 for lane 30 of the quarter below; row
+  // 32q's x-shift 1 + row 32q + 1's x-shift 2 for its lane 31)
   float *xbuf = reinterpret_cast<float *>(reinterpret_cast<unsigned char *>(bars) + CONV_BARS);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   // this CTA's tiles
@@ -522,16 +523,13 @@ __global__ void __launch_bounds__(CONV_THREADS, 1)
             for (int c = 0; c < CO; c++) {
               float d[24];  // columns 8c.. of x-shift 0, 1, 2
               tmem_ld3x8(ta + 8 * c, ta + NW + 8 * c, ta + 2 * NW + 8 * c, d);
-              if (q > 0 && lane < 2) {
-                float *xs = xw + 3 * (q - 1) * NW + 8 * c;
+              float *xs = xw + 2 * (q > 0 ? q - 1 : 0) * NW + 8 * c;
 #pragma unroll
-                for (int k = 0; k < 8; k++) {
-                  if (lane == 0) {
-                    xs[k] = d[8 + k];
-                    xs[NW + k] = d[16 + k];
-                  } else {
-                    xs[2 * NW + k] = d[16 + k];
-                  }
+              for (int k = 0; k < 8; k++) {
+                const float up = __shfl_up_sync(0xffffffffu, d[8 + k], 1);  // lane 0's x-shift 1
+                if (q > 0 && lane < 2) {
+                  if (lane == 0) xs[k] = d[16 + k];
+                  else xs[NW + k] = up + d[16 + k];
                 }
               }
 #pragma unroll
@@ -554,9 +552,9 @@ __global__ void __launch_bounds__(CONV_THREADS, 1)
             break;
           }
           if (q < 3 && lane >= 30) {
-            const float *xr = xw + 3 * q * NW;  // quarter q + 1's rows
+            const float *xr = xw + 2 * q * NW + (lane - 30) * NW;  // quarter q + 1's rows
 #pragma unroll
-            for (int c = 0; c < NW; c++) v[c] += lane == 31 ? xr[c] + xr[2 * NW + c] : xr[NW + c];
+            for (int c = 0; c < NW; c++) v[c] += xr[c];
           }
           own++;
         }
