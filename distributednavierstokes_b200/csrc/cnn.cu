@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdarg>
 #include <cstdint>
@@ -22,6 +23,7 @@
 #include "../../include/dnsb.h"
 #include "../../include/dnsb_cnn.h"
 #include "cnn.cuh"
+#include "cnn_host.h"
 
 using namespace dnsb::cnn;
 
@@ -341,7 +343,15 @@ struct dnsb_cnn {
   std::vector<cudaEvent_t> evpool;
   double prof_ms[4] = {}, prof_flops[4] = {};
   long prof_n[4] = {};
+  unsigned long long serial = 0;  // creation number, unique in the process
 };
+
+namespace dnsb_internal {
+
+unsigned long long cnn_serial(const dnsb_cnn *c) { return c->serial; }
+bool cnn_profiling(const dnsb_cnn *c) { return c->prof_on; }
+
+}  // namespace dnsb_internal
 
 namespace {
 
@@ -750,6 +760,8 @@ int dnsb_cnn_create(int device, void *stream, int batch, int crop, int nfield, d
     return cfail(nullptr, DNSB_EUNSUP, "crop + 8 and nfield + 8 must be <= 256, batch <= 64");
   if (!encode_fn()) return cfail(nullptr, DNSB_ECUDA, "cuTensorMapEncodeTiled is not available");
   dnsb_cnn *c = new dnsb_cnn();
+  static std::atomic<unsigned long long> created{0};
+  c->serial = ++created;
   c->device = device;
   c->stream = (cudaStream_t)stream;
   auto bail = [&](int rc) {

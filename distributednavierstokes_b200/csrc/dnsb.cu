@@ -28,6 +28,7 @@
 
 #include "../../include/dnsb.h"
 #include "../../include/dnsb_cnn.h"
+#include "cnn_host.h"
 #include "common.cuh"
 #include "fft.cuh"
 #include "spectral.cuh"
@@ -108,7 +109,23 @@ struct dnsb_ctx {
   // the step size, read by the kernels that take dt (else nullptr)
   const double *dtp = nullptr;
   cudaStream_t les_cap = nullptr;  // capture stream of dnsb_les_advance's graph
-  double *les_state = nullptr;     // its device state: t, dt, steps
+  double *les_state = nullptr;     // its device state: t, dt, steps, t1, the loop threshold
+  // dnsb_les_advance's instantiated graphs, one per argument set (the eight
+  // fields, the closure and its creation serial, the CFL number, the shell
+  // count, graph_gen), reused by later calls with other intervals; least
+  // recently used out beyond LES_GRAPHS
+  struct LesGraph {
+    const void *ptr[9];
+    unsigned long long serial;
+    double cfl;
+    int nb;
+    unsigned gen;
+    unsigned long long used;
+    cudaGraphExec_t exec;
+  };
+  std::vector<LesGraph> les_graphs;
+  unsigned long long les_uses = 0;
+  unsigned graph_gen = 0;  // bumped by every setter whose value a captured kernel takes as an argument
   // one-barrier pipelined variant of the fused kernel: 2.5 % faster than
   // the two-barrier k_gradmom_march at 384x256x384
   int gm_pipe = 1;
@@ -1565,6 +1582,7 @@ void dnsb_destroy(dnsb_ctx *c) {
   for (void *p : c->allocs) cudaFree(p);
   if (c->hostred) cudaFreeHost(c->hostred);
   if (c->hostumax) cudaFreeHost(c->hostumax);
+  for (auto &e : c->les_graphs) cudaGraphExecDestroy(e.exec);
   if (c->les_cap) cudaStreamDestroy(c->les_cap);
   delete c;
 }
@@ -1590,6 +1608,7 @@ int dnsb_get_tuning(const dnsb_ctx *c, dnsb_tuning *t) {
 int dnsb_set_wait_limit(dnsb_ctx *c, unsigned long polls) {
   if (!c) return DNSB_EINVAL;
   c->wait_limit = polls == 0 ? 0u : (unsigned)std::min<unsigned long>(polls, 0xffffffffUL);
+  c->graph_gen++;
   return 0;
 }
 
@@ -1862,9 +1881,10 @@ int dnsb_les_step(dnsb_ctx *c, dnsb_cnn *cnn, double *ux, double *uy, double *uz
 
 // The CFL step of cfl_from_max on the device (the same correctly rounded
 // operations in the same order, so the same bits as the host's), limited
-// to t1 - t: st = {t, dt, steps}; cfl_diff = cfl * the diffusive limit.
+// to t1 - t: st = {t, dt, steps, t1, threshold}; cfl_diff = cfl * the
+// diffusive limit.
 __global__ void k_les_dt(const unsigned long long *bits, double *st, double dx, double dymin, double dz,
-                         double cfl, double cfl_diff, double t1) {
+                         double cfl, double cfl_diff) {
   const double eps = 2.220446049250313e-16;
   const double m0 = __longlong_as_double((long long)bits[0]);
   const double m1 = __longlong_as_double((long long)bits[1]);
@@ -1873,50 +1893,41 @@ __global__ void k_les_dt(const unsigned long long *bits, double *st, double dx, 
   const double c3 = __ddiv_rn(dz, __dadd_rn(m2, eps));
   const double conv = fmin(fmin(c1, c2), c3);
   const double dt = fmin(__dmul_rn(cfl, conv), cfl_diff);
-  const double left = __dsub_rn(t1, st[0]);
+  const double left = __dsub_rn(st[3], st[0]);
   st[1] = left < dt ? left : dt;
 }
 
-// t += dt, one more step, and the loop condition t < thr for the next pass
-__global__ void k_les_tick(double *st, cudaGraphConditionalHandle cond, double thr) {
+// t += dt, one more step, and the loop condition t < st[4] for the next pass
+__global__ void k_les_tick(double *st, cudaGraphConditionalHandle cond) {
   const double t = __dadd_rn(st[0], st[1]);
   st[0] = t;
   st[2] += 1.0;
-  cudaGraphSetConditional(cond, t < thr ? 1u : 0u);
+  cudaGraphSetConditional(cond, t < st[4] ? 1u : 0u);
 }
 
-// dnsb_les_advance as one launch of a CUDA graph: a conditional WHILE node
-// whose body is one step (CFL maximum -> dt on the device -> the step with
-// the kernels reading dt from device memory -> shell clamp -> t += dt and
-// the loop condition); no host synchronisation until the end.
-int les_advance_graph(dnsb_ctx *c, dnsb_cnn *cnn, double *ux, double *uy, double *uz, double *p,
-                      double *qx, double *qy, double *qz, double *tau, double t0, double t1, double cfl,
-                      const double *eref, int nshells, double *t_out, long *n_out) {
+constexpr size_t LES_GRAPHS = 4;
+
+// The graph of dnsb_les_advance: a conditional WHILE node whose body is one
+// step (CFL maximum -> dt on the device -> the step with the kernels
+// reading dt from device memory -> shell clamp -> t += dt and the loop
+// condition).  The interval (t, t1, threshold) is device state, so one
+// instantiation serves every later call with the same arguments.
+int les_capture(dnsb_ctx *c, dnsb_cnn *cnn, double *ux, double *uy, double *uz, double *p, double *qx,
+                double *qy, double *qz, double *tau, double cfl, const double *eref, int nshells, int nb,
+                cudaGraphExec_t *out) {
   const Geo &g = c->g;
   int rc;
-  const double thr = t1 - 1e-12 * (std::fabs(t1) + 1);
-  if (!(t0 < thr)) {
-    if (t_out) *t_out = t1;
-    if (n_out) *n_out = 0;
-    return 0;
-  }
-  if (!c->les_cap) CK(c, cudaStreamCreateWithFlags(&c->les_cap, cudaStreamNonBlocking));
-  if (!c->les_state && (rc = dalloc(c, &c->les_state, 4))) return rc;
-  const int nb = eref && nshells > 0 ? std::min(nshells, c->nshell_max) : 0;
-  if (nb && (rc = upload_eref(c, eref, nb))) return rc;  // scratch and table before the capture
   // the diffusive limit exactly as cfl_from_max forms it
   const double eps = 2.220446049250313e-16;
   const double invdy2 = c->implicit ? 0.0 : 1 / (c->dymin * c->dymin);
   const double diff = 1 / (2 * g.visc * (1 / (g.dx * g.dx) + invdy2 + 1 / (g.dz * g.dz)) + eps);
   const double cfl_diff = cfl * diff;
   cudaGraph_t graph = nullptr, captured = nullptr;
-  cudaGraphExec_t exec = nullptr;
   cudaGraphConditionalHandle cond;
   CK(c, cudaGraphCreate(&graph, 0));
   // (the captured graph is the WHILE node's body, owned by `graph`)
   auto drop = [&](int code) {
-    if (exec) cudaGraphExecDestroy(exec);
-    if (graph) cudaGraphDestroy(graph);
+    cudaGraphDestroy(graph);
     return code;
   };
   if (cudaGraphConditionalHandleCreate(&cond, graph, 1, cudaGraphCondAssignDefault) != cudaSuccess)
@@ -1953,7 +1964,7 @@ int les_advance_graph(dnsb_ctx *c, dnsb_cnn *cnn, double *ux, double *uy, double
     rc = launched("velocity maxima");
   }
   if (!rc) {
-    k_les_dt<<<1, 1, 0, c->stream>>>(scratch, c->les_state, g.dx, c->dymin, g.dz, cfl, cfl_diff, t1);
+    k_les_dt<<<1, 1, 0, c->stream>>>(scratch, c->les_state, g.dx, c->dymin, g.dz, cfl, cfl_diff);
     rc = launched("step size");
   }
   // the dt argument only passes the host-side checks: the kernels read *dtp
@@ -1962,7 +1973,7 @@ int les_advance_graph(dnsb_ctx *c, dnsb_cnn *cnn, double *ux, double *uy, double
              : dnsb_step(c, ux, uy, uz, p, qx, qy, qz, nullptr, 1.0);
   if (!rc && nb) rc = dnsb_shell_clamp(c, ux, uy, uz, eref, nshells);
   if (!rc) {
-    k_les_tick<<<1, 1, 0, c->stream>>>(c->les_state, cond, thr);
+    k_les_tick<<<1, 1, 0, c->stream>>>(c->les_state, cond);
     rc = launched("time advance");
   }
   const cudaError_t ce = cudaStreamEndCapture(c->les_cap, &captured);
@@ -1971,18 +1982,68 @@ int les_advance_graph(dnsb_ctx *c, dnsb_cnn *cnn, double *ux, double *uy, double
   if (cnn) dnsb_cnn_set_stream(cnn, orig);
   if (rc) return drop(rc);
   if (ce != cudaSuccess) return drop(fail(c, DNSB_ECUDA, "stream capture failed: %s", cudaGetErrorString(ce)));
-  if (cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess)
+  if (cudaGraphInstantiate(out, graph, 0) != cudaSuccess)
     return drop(fail(c, DNSB_ECUDA, "graph instantiation failed"));
+  return drop(0);
+}
+
+// dnsb_les_advance as one graph launch, with no host synchronisation until
+// the end; the graph is captured on the first call with these arguments.
+int les_advance_graph(dnsb_ctx *c, dnsb_cnn *cnn, double *ux, double *uy, double *uz, double *p,
+                      double *qx, double *qy, double *qz, double *tau, double t0, double t1, double cfl,
+                      const double *eref, int nshells, double *t_out, long *n_out) {
+  int rc;
+  const double thr = t1 - 1e-12 * (std::fabs(t1) + 1);
+  if (!(t0 < thr)) {
+    if (t_out) *t_out = t1;
+    if (n_out) *n_out = 0;
+    return 0;
+  }
+  if (!c->les_cap) CK(c, cudaStreamCreateWithFlags(&c->les_cap, cudaStreamNonBlocking));
+  if (!c->les_state && (rc = dalloc(c, &c->les_state, 8))) return rc;
+  const int nb = eref && nshells > 0 ? std::min(nshells, c->nshell_max) : 0;
+  if (nb && (rc = upload_eref(c, eref, nb))) return rc;  // the clamp's table (scratch before a capture)
+  const void *key[9] = {ux, uy, uz, p, qx, qy, qz, tau, cnn};
+  const unsigned long long serial = cnn ? dnsb_internal::cnn_serial(cnn) : 0;
+  cudaGraphExec_t exec = nullptr;
+  for (auto &e : c->les_graphs)
+    if (std::equal(key, key + 9, e.ptr) && e.serial == serial && e.cfl == cfl && e.nb == nb &&
+        e.gen == c->graph_gen) {
+      exec = e.exec;
+      e.used = ++c->les_uses;
+      break;
+    }
+  if (!exec) {
+    if ((rc = les_capture(c, cnn, ux, uy, uz, p, qx, qy, qz, tau, cfl, eref, nshells, nb, &exec))) return rc;
+    if (c->les_graphs.size() >= LES_GRAPHS) {
+      auto old = std::min_element(c->les_graphs.begin(), c->les_graphs.end(),
+                                  [](const dnsb_ctx::LesGraph &a, const dnsb_ctx::LesGraph &b) {
+                                    return a.used < b.used;
+                                  });
+      cudaGraphExecDestroy(old->exec);
+      c->les_graphs.erase(old);
+    }
+    dnsb_ctx::LesGraph e{};
+    std::copy(key, key + 9, e.ptr);
+    e.serial = serial;
+    e.cfl = cfl;
+    e.nb = nb;
+    e.gen = c->graph_gen;
+    e.used = ++c->les_uses;
+    e.exec = exec;
+    c->les_graphs.push_back(e);
+  }
   double *h = c->hostred;
   h[0] = t0;
   h[1] = 0.0;
   h[2] = 0.0;
-  if (cudaMemcpyAsync(c->les_state, h, 3 * sizeof(double), cudaMemcpyHostToDevice, orig) != cudaSuccess ||
-      cudaGraphLaunch(exec, orig) != cudaSuccess ||
-      cudaMemcpyAsync(h, c->les_state, 3 * sizeof(double), cudaMemcpyDeviceToHost, orig) != cudaSuccess ||
-      cudaStreamSynchronize(orig) != cudaSuccess)
-    return drop(fail(c, DNSB_ECUDA, "graph launch failed: %s", cudaGetErrorString(cudaGetLastError())));
-  drop(0);
+  h[3] = t1;
+  h[4] = thr;
+  if (cudaMemcpyAsync(c->les_state, h, 5 * sizeof(double), cudaMemcpyHostToDevice, c->stream) != cudaSuccess ||
+      cudaGraphLaunch(exec, c->stream) != cudaSuccess ||
+      cudaMemcpyAsync(h, c->les_state, 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
+      cudaStreamSynchronize(c->stream) != cudaSuccess)
+    return fail(c, DNSB_ECUDA, "graph launch failed: %s", cudaGetErrorString(cudaGetLastError()));
   if ((rc = check_deverr(c))) return rc;
   c->umax_for[0] = c->umax_for[1] = c->umax_for[2] = nullptr;
   if (t_out) *t_out = t1;
@@ -2000,11 +2061,11 @@ int dnsb_les_advance(dnsb_ctx *c, dnsb_cnn *cnn, double *ux, double *uy, double 
   if (ensure_device(c)) return DNSB_ECUDA;
   // one graph launch for the whole run where every kernel of the step can
   // read dt from device memory (the z-marching momentum: aligned fields),
-  // no per-launch timing is on and the box is explicit; DNSB_LESGRAPH=0
-  // keeps the host loop
+  // no per-launch timing is on (the context's or the closure's) and the box
+  // is explicit; DNSB_LESGRAPH=0 keeps the host loop
   const bool direct_clamp = !eref || nshells <= 0 || (!c->g.wall && clamp_direct(c, std::min(nshells, c->nshell_max)));
   if (envint("DNSB_LESGRAPH", 1) != 0 && !c->implicit && !c->prof_on && use_tile(c, ux, uy, uz) &&
-      direct_clamp)
+      direct_clamp && !(cnn && dnsb_internal::cnn_profiling(cnn)))
     return les_advance_graph(c, cnn, ux, uy, uz, p, qx, qy, qz, tau, t0, t1, cfl, eref, nshells, t_out,
                              n_out);
   double t = t0;

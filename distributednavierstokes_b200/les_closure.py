@@ -59,8 +59,10 @@ def advance(u, p, q, s, t, t_end, cfl, forcing=None, closure=None, tau=None, pla
     With a closure: dnsb_les_step; without (or plain): the library's fused
     step (dnsb_step), the unclosed fallback.  A shell forcing from
     api.shellforcing is applied after every step; the whole loop runs in
-    dnsb_les_advance (one call, one synchronisation per step for the CFL
-    maximum)."""
+    dnsb_les_advance: on explicit boxes one launch of a CUDA graph (the
+    step size computed on the device; captured on the first call with these
+    fields, closure and CFL number, relaunched by later ones), else a host
+    loop with one synchronisation per step for the CFL maximum."""
     if closure is not None and plain:
         raise ValueError("plain excludes a closure")
     table = getattr(forcing, "_table", None) if forcing is not None else None

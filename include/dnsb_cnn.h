@@ -117,9 +117,13 @@ int dnsb_les_step(dnsb_ctx *ctx, dnsb_cnn *cnn, double *ux, double *uy, double *
  * whole run is one launch of a CUDA graph (a conditional loop whose body
  * computes the CFL step on the device, with the same operations as
  * cfl_timestep here, and runs the step reading it from device memory):
- * the call synchronises once, at the end; otherwise (or with the
- * environment variable DNSB_LESGRAPH=0) a host loop synchronises once per
- * step for the CFL maximum.  Both give the same bits. */
+ * the call synchronises once, at the end.  The context keeps the graphs
+ * of its last four argument sets (fields, tau, closure, cfl, shell count)
+ * and relaunches one for any later interval (a closure created at a
+ * destroyed one's address is told apart; fields are matched by address
+ * and are the context's shape by contract).  Otherwise (or with the environment variable
+ * DNSB_LESGRAPH=0) a host loop synchronises once per step for the CFL
+ * maximum.  Both give the same bits. */
 int dnsb_les_advance(dnsb_ctx *ctx, dnsb_cnn *cnn, double *ux, double *uy, double *uz, double *p,
                      double *qx, double *qy, double *qz, double *tau, double t0, double t1,
                      double cfl, const double *eref, int nshells, double *t_out, long *n_out);

@@ -184,6 +184,64 @@ def test_les_advance_matches_step_loop(M, graph, monkeypatch):
     s.close()
 
 
+def test_les_advance_graph_reuse(M):
+    """The advance graph is captured once per argument set and relaunched
+    for later intervals: closed and unclosed runs alternating on one
+    context over three intervals, a wait-limit change between two of them
+    (a new capture) and a closure created after the first one was closed
+    (a new capture even where the new closure reuses the old one's
+    address) each equal the step-by-step loop bit for bit."""
+    dns, L = M
+    from distributednavierstokes_b200 import _lib
+    from distributednavierstokes_b200.closure import Closure
+
+    n = 16
+    s = dns.setup(n=(n,) * 3, visc=0.01)
+    u = dns.random_field(dns.vectorfield(s), s, totalenergy=0.5, kpeak=3.0, seed=11)
+    forcing = dns.shellforcing(u, s, shells=(1, 2))
+    copies = []
+    for _ in range(4):
+        v = dns.vectorfield(s)
+        for c in "xyz":
+            v[c].copy_(u[c])
+        copies.append((v, dns.scalarfield(s), dns.vectorfield(s)))
+    tau = torch.zeros((6, n, n, n), dtype=torch.float64, device="cuda")
+
+    def loop(ub, p, q, t, t1, cl):
+        k = 0
+        while t < t1 - 1e-12 * (abs(t1) + 1):
+            dt = min(dns.cfl_timestep(ub, s, 0.5), t1 - t)
+            if cl is not None:
+                L.les_step(ub, p, q, s, dt, cl, tau)
+            else:
+                dns.step(ub, p, q, None, s, dt)
+            forcing(ub, s)
+            t += dt
+            k += 1
+        return k
+
+    cl = Closure(batch=0, crop=0, nfield=n, seed=5)
+    cl.set_scales([2.0, 2.0, 2.0], [0.2] * 6)
+    times = (0.0, 0.15, 0.3, 0.45, 0.6)
+    for i in range(4):
+        t0, t1 = times[i], times[i + 1]
+        if i == 2:
+            assert _lib.load().dnsb_set_wait_limit(s.ctx, 1 << 26) == 0
+        if i == 3:
+            cl.close()
+            cl = Closure(batch=0, crop=0, nfield=n, seed=6)
+            cl.set_scales([2.0, 2.0, 2.0], [0.2] * 6)
+        for closed, (ga, ref) in ((True, (copies[0], copies[1])), (False, (copies[2], copies[3]))):
+            c = cl if closed else None
+            t_end, steps = L.advance(*ga, s, t0, t1, 0.5, forcing, c, tau if closed else None)
+            assert t_end == t1 and steps >= 1
+            assert loop(*ref, t0, t1, c) == steps, (i, closed)
+            for comp in "xyz":
+                assert torch.equal(ga[0][comp], ref[0][comp]), (i, closed, comp)
+    cl.close()
+    s.close()
+
+
 def test_les_advance_edges(M):
     """dnsb_les_advance: an interval shorter than the time tolerance takes no
     step and leaves u alone; a closure without its tau buffer and the closed
