@@ -22,8 +22,9 @@ INCLUDES = [os.path.join(ROOT, "include", h) for h in ("dnsb.h", "dnsb_cnn.h")]
 # headers each translation unit includes (a change rebuilds its object)
 HEADERS = {
     "dnsb.cu": ["common.cuh", "fft.cuh", "fft4.cuh", "spectral.cuh", "spectral4.cuh", "stencil.cuh",
-                "tma.cuh", "ysolve.cuh", "gradmom.cuh", "zyz.cuh", "spsolver.cuh", "lowshells.cuh"],
-    "cnn.cu": ["cnn.cuh"],
+                "tma.cuh", "ysolve.cuh", "gradmom.cuh", "zyz.cuh", "spsolver.cuh", "lowshells.cuh",
+                "cnn_host.h"],
+    "cnn.cu": ["cnn.cuh", "cnn_host.h"],
 }
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
