@@ -64,7 +64,7 @@ namespace cnn {
 
 constexpr int NTHREADS = 192;       // weight gradient: TMA, MMA, 4 epilogue warps
 constexpr int CONV_GROUPS = 4;      // convolution epilogue: groups of 4 warps taking tiles in turn
-constexpr int CONV_THREADS = 64 + 128 * CONV_GROUPS;  // TMA, MMA, epilogue warps
+constexpr int CONV_THREADS = 96 + 128 * CONV_GROUPS;  // TMA, two MMA, epilogue warps
 constexpr int NTAPS = 27;
 constexpr int TILE_M = 128;      // GEMM rows (positions) of a convolution tile
 constexpr int TILE_OUT = 126;    // outputs of a convolution tile (rows m, m + 1, m + 2 feed output m)
@@ -380,7 +380,7 @@ __global__ void __launch_bounds__(CONV_THREADS, 1)
   if (threadIdx.x == 0) {
     for (int i = 0; i < a.nslot; i++) {
       mb_init(&full[i], 1);
-      mb_init(&empty[i], 1);
+      mb_init(&empty[i], 2);  // released by both issuing lanes
     }
     for (int i = 0; i < NACC; i++) {
       mb_init(&tfull[i], 1);
@@ -435,8 +435,14 @@ __global__ void __launch_bounds__(CONV_THREADS, 1)
         mb_wait(&full[g2 % a.nslot], (g2 / a.nslot) & 1, a.wait_limit, abort_flag);
       mb_wait(wbar, 0, a.wait_limit, abort_flag);
     }
-  } else if (warp == 1) {
+  } else if (warp == 1 || warp == 2) {
     if (lane == 0) {
+      // Two issuing lanes (warps 1 and 2) take the sub-tiles in turn (sub-tile
+      // i on lane i % 2): while one does its waits and bookkeeping, the
+      // other's MMAs keep the tensor pipe fed.  Both wait for every plane and
+      // both release it (the empty barriers count two arrivals: a commit
+      // arrives once that lane's earlier MMAs are done).
+      const int r = warp - 1;
       constexpr uint32_t idesc = idesc_bf16(N, false, false);
       // Descriptors are built once; per MMA only the start-address field
       // (bits 0-13, 16-byte units) moves, by an offset added to the whole
@@ -448,19 +454,25 @@ __global__ void __launch_bounds__(CONV_THREADS, 1)
       uint32_t yrow[3];  // (dy + e) P, 16-byte units
 #pragma unroll
       for (int q = 0; q < 3; q++) yrow[q] = (uint32_t)((q + a.e) * a.P);
-      // one lane runs this loop serially: plane slots, tile coordinates and
+      // each lane runs this loop serially: plane slots, tile coordinates and
       // accumulators advance by increments (no division per tile)
       int i = 0, last_a = -1, last_aph = 0;
       int gs = 0, gph = 0;  // slot and phase of the next plane to arrive
-      int ac = 0, aph = 0;  // accumulator of sub-tile i and its phase
+      int ac = r, aph = 0;  // accumulator (i % NACC) of this lane's next sub-tile and its phase
       int z = t0 % a.Do, j = (t0 / a.Do) % a.tpp;
       int x0 = (j * a.sub * TILE_OUT) % a.P;  // the tile's first position in patch row y0
+      // phases seen complete ahead of their wait, by tests placed among the
+      // MMAs (the issue is throttled by the tensor pipe, so the tests cost
+      // nothing there): the next accumulator's release, the next plane
+      bool acc_ready = false, plane_ready = false;
       bool ok = mb_wait(wbar, 0, a.wait_limit, abort_flag);
       for (int t = t0; ok && t < t1; t++) {
         const bool fresh = t == t0 || z == 0;
         const bool last = t == t1 - 1 || z == a.Do - 1;
+        const bool more = t + 1 < t1;
         for (int q = fresh ? 0 : 2; q < 3 && ok; q++) {
-          ok = !*abort_flag && mb_wait(&full[gs], gph, a.wait_limit, abort_flag);
+          if (!plane_ready) ok = !*abort_flag && mb_wait(&full[gs], gph, a.wait_limit, abort_flag);
+          plane_ready = false;
           if (++gs == a.nslot) gs = 0, gph ^= 1;
         }
         if (!ok) break;
@@ -474,15 +486,21 @@ __global__ void __launch_bounds__(CONV_THREADS, 1)
         for (int dz = 0; dz < 3; dz++)
           ab[dz] = adesc_st + (uint64_t)(ring_u + (uint32_t)sz[dz] * stride_u + (uint32_t)(x0 + a.s));
         for (int sb = 0; sb < a.sub; sb++, i++) {
-          if (*abort_flag || !mb_wait(&tempty[ac], aph ^ 1, a.wait_limit, abort_flag)) {
+          if ((i & 1) != r) continue;
+          if (!acc_ready && (*abort_flag || !mb_wait(&tempty[ac], aph ^ 1, a.wait_limit, abort_flag))) {
             ok = false;
             break;
           }
           tc_fence_after();
           const uint32_t dacc = tbase + (uint32_t)ac * ACC_STRIDE;
           const uint64_t so = (uint64_t)(sb * TILE_OUT);  // the sub-tile's rows, 16-byte units
+          const int nac = ac + 2 >= NACC ? ac + 2 - NACC : ac + 2, naph = ac + 2 >= NACC ? aph ^ 1 : aph;
 #pragma unroll
           for (int zy = 0; zy < 9; zy++) {
+            if (zy == 5) {
+              acc_ready = mb_test(&tempty[nac], naph ^ 1);
+              if (sb + 2 >= a.sub && more) plane_ready = mb_test(&full[gs], gph);
+            }
             const uint64_t at = ab[zy / 3] + so + (uint64_t)yrow[zy % 3];
 #pragma unroll
             for (int k = 0; k < CI / 2; k++)
@@ -492,7 +510,8 @@ __global__ void __launch_bounds__(CONV_THREADS, 1)
           mma_commit(&tfull[ac]);
           last_a = ac;
           last_aph = aph;
-          if (++ac == NACC) ac = 0, aph ^= 1;
+          ac = nac;
+          aph = naph;
         }
         if (!ok) break;
         // release the planes this tile used for the last time
@@ -519,7 +538,7 @@ __global__ void __launch_bounds__(CONV_THREADS, 1)
     // e / 4 the tiles with local index i % CONV_GROUPS == e / 4); warp w
     // reads TMEM lanes 32 (w % 4) .. + 31 (rows m = 32 (w % 4) + lane of its
     // tile), 8 columns of each x-shift at a time
-    const int e = warp - 2, q = warp & 3, grp = e >> 2;
+    const int e = warp - 3, q = warp & 3, grp = e >> 2;
     const int m = q * 32 + lane;
     const float keep1 = lane < 31 ? 1.f : 0.f, keep2 = lane < 30 ? 1.f : 0.f;
     float osc[6];
