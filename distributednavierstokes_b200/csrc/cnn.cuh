@@ -550,12 +550,18 @@ __global__ void __launch_bounds__(CONV_THREADS, 1)
     // the tile's (b, j, z) and this thread's positions in its sub-tiles,
     // updated as z marches
     int z = t0 % a.Do, j = (t0 / a.Do) % a.tpp, b = t0 / (a.Do * a.tpp);
-    int fA = 0;
+    int fA = 0, xA = 0, yA = 0;  // this thread's row in sub-tile 0: offset, x, y
+    // a sub-tile further: TILE_OUT = q126 rows of P + r126
+    const int q126 = TILE_OUT / a.P, r126 = TILE_OUT - q126 * a.P;
+    const long long cstr = (long long)a.Pz * P2;  // one chunk of 8 channels further
+    const float4 *bias4 = reinterpret_cast<const float4 *>(bsm);
     bool fresh = true, stop = false;
     int i = 0, own = 0;
     for (int t = t0; t < t1 && !stop; t++) {
       if (fresh) {
         fA = j * a.sub * TILE_OUT + m;
+        yA = fA / a.P;
+        xA = fA - yA * a.P;
         fresh = false;
       }
       const int zc = z, bc = b;
@@ -567,7 +573,9 @@ __global__ void __launch_bounds__(CONV_THREADS, 1)
           b++;
         }
       }
-      for (int sb = 0; sb < a.sub; sb++, i++) {
+      int x = xA, y = yA;
+      for (int sb = 0; sb < a.sub; sb++, i++, x += r126, y += q126) {
+        if (x >= a.P) x -= a.P, y++;
         const bool mine = (i % CONV_GROUPS) == grp;
         const int ac = i % NACC, aph = (i / NACC) & 1;
         float v[NW];
@@ -582,14 +590,17 @@ __global__ void __launch_bounds__(CONV_THREADS, 1)
             for (int c = 0; c < CO; c++) {
               float d[24];  // columns 8c.. of x-shift 0, 1, 2
               tmem_ld3x8(ta + 8 * c, ta + NW + 8 * c, ta + 2 * NW + 8 * c, d);
-              float *xs = xw + 2 * (q > 0 ? q - 1 : 0) * NW + 8 * c;
+              // lane 0: its x-shift 2; lane 1: lane 0's x-shift 1 + its x-shift 2
+              float hx[8];
 #pragma unroll
               for (int k = 0; k < 8; k++) {
-                const float up = __shfl_up_sync(0xffffffffu, d[8 + k], 1);  // lane 0's x-shift 1
-                if (q > 0 && lane < 2) {
-                  if (lane == 0) xs[k] = d[16 + k];
-                  else xs[NW + k] = up + d[16 + k];
-                }
+                const float up = __shfl_up_sync(0xffffffffu, d[8 + k], 1);
+                hx[k] = lane == 0 ? d[16 + k] : up + d[16 + k];
+              }
+              if (q > 0 && lane < 2) {
+                float4 *xs = reinterpret_cast<float4 *>(xw + 2 * (q - 1) * NW + lane * NW + 8 * c);
+                xs[0] = make_float4(hx[0], hx[1], hx[2], hx[3]);
+                xs[1] = make_float4(hx[4], hx[5], hx[6], hx[7]);
               }
 #pragma unroll
               for (int k = 0; k < 8; k++) {
@@ -611,29 +622,37 @@ __global__ void __launch_bounds__(CONV_THREADS, 1)
             break;
           }
           if (q < 3 && lane >= 30) {
-            const float *xr = xw + 2 * q * NW + (lane - 30) * NW;  // quarter q + 1's rows
+            const float4 *xr = reinterpret_cast<const float4 *>(xw + 2 * q * NW + (lane - 30) * NW);
 #pragma unroll
-            for (int c = 0; c < NW; c++) v[c] += xr[c];
+            for (int c = 0; c < NW / 4; c++) {  // quarter q + 1's rows
+              const float4 h = xr[c];
+              v[4 * c] += h.x;
+              v[4 * c + 1] += h.y;
+              v[4 * c + 2] += h.z;
+              v[4 * c + 3] += h.w;
+            }
           }
           own++;
         }
         if (!mine || m >= TILE_OUT) continue;
         const int f = fA + sb * TILE_OUT;
         if (f >= P2) continue;
-        const int y = f / a.P, x = f - y * a.P;
         const bool valid = x < a.Do && y < a.Do;
         const long long vox = (long long)zc * P2 + f;
         if (MODE == FWD_GELU) {
+          const long long o0 = (long long)bc * CO * cstr + vox;
 #pragma unroll
           for (int c = 0; c < CO; c++) {
+            const float4 b0 = bias4[2 * c], b1 = bias4[2 * c + 1];
+            const float bb[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
             float zv[8], hv[8];
 #pragma unroll
             for (int k = 0; k < 8; k++) {
-              const float zz = valid ? v[8 * c + k] + bsm[8 * c + k] : 0.f;
+              const float zz = valid ? v[8 * c + k] + bb[k] : 0.f;
               zv[k] = zz;
               hv[k] = gelu_f(zz);
             }
-            const long long o = ((long long)(bc * CO + c) * a.Pz) * P2 + vox;
+            const long long o = o0 + c * cstr;
             if (store_z) a.zout[o] = pack8(zv);
             a.out[o] = pack8(hv);
           }
