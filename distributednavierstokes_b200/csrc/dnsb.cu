@@ -136,6 +136,7 @@ struct dnsb_ctx {
   double2 *S = nullptr;
   double2 *Sx[2] = {nullptr, nullptr};  // spectra of u.y, u.z during a shell clamp
   double2 *lsA = nullptr, *lsB = nullptr, *lsG = nullptr, *lsH = nullptr;  // low-shell clamp scratch
+  double2 *lsX = nullptr;  // e^{2 pi i x / nx}, x = 0..nx-1, for the clamp's x-sums
   double *work = nullptr;
   double *ycin = nullptr;  // c' entering each y-chunk, per (kx, kz) line
   double *r = nullptr;
@@ -316,25 +317,45 @@ int allow_smem(dnsb_ctx *c, K kernel, size_t bytes) {
 // out[0..2]: max |u_c| over the interior (as ordered bits); with deverr,
 // out[3] also receives the device error word (read after every earlier
 // kernel of the stream has finished), so that one copy brings both back.
-__global__ void k_maxabs3(Geo g, CFields3 u, unsigned long long *out, const int *deverr) {
+// max |u_c| over the interior cells (dbits order = value order for x >= 0).
+// Warps walk the (J, K) rows and their lanes stride along x: one 32-bit
+// division per row instead of 64-bit divisions per cell, coalesced loads;
+// the block's maxima meet in shared memory and leave in one atomic per
+// component (a maximum does not depend on the order).  Grid: maxabs_blocks.
+__global__ void __launch_bounds__(256) k_maxabs3(Geo g, CFields3 u, unsigned long long *out,
+                                                 const int *deverr) {
   if (deverr && blockIdx.x == 0 && threadIdx.x == 0) out[3] = (unsigned long long)(unsigned)*deverr;
-  double m[3] = {0, 0, 0};
-  const long long n = (long long)g.nx * g.ny * g.nz;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
-       t += (long long)gridDim.x * blockDim.x) {
-    const int I = (int)(t % g.nx) + 1;
-    const long long r = t / g.nx;
-    const int J = (int)(r % g.ny) + 1, K = (int)(r / g.ny) + 1;
-    const long long c0 = gidx(g, I, J, K);
-    m[0] = fmax(m[0], fabs(u.x[c0]));
-    m[1] = fmax(m[1], fabs(u.y[c0]));
-    m[2] = fmax(m[2], fabs(u.z[c0]));
+  __shared__ double wm[3][8];
+  double m0 = 0, m1 = 0, m2 = 0;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int rows = g.ny * g.nz;
+  for (int r = blockIdx.x * nw + w; r < rows; r += gridDim.x * nw) {
+    const int K = r / g.ny, J = r - K * g.ny;
+    const int row = gidx(g, 0, J + 1, K + 1);
+    for (int I = lane + 1; I <= g.nx; I += 32) {
+      m0 = fmax(m0, fabs(u.x[row + I]));
+      m1 = fmax(m1, fabs(u.y[row + I]));
+      m2 = fmax(m2, fabs(u.z[row + I]));
+    }
   }
-  for (int c = 0; c < 3; c++) {
-    double v = m[c];
-    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
-    if ((threadIdx.x & 31) == 0) atomicMax(out + c, dbits(v));
+  for (int o = 16; o > 0; o >>= 1) {
+    m0 = fmax(m0, __shfl_xor_sync(0xffffffffu, m0, o));
+    m1 = fmax(m1, __shfl_xor_sync(0xffffffffu, m1, o));
+    m2 = fmax(m2, __shfl_xor_sync(0xffffffffu, m2, o));
   }
+  if (lane == 0) wm[0][w] = m0, wm[1][w] = m1, wm[2][w] = m2;
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    double v = 0;
+    for (int k = 0; k < nw; k++) v = fmax(v, wm[threadIdx.x][k]);
+    atomicMax(out + threadIdx.x, dbits(v));
+  }
+}
+
+// blocks of k_maxabs3: four rows per warp, at most RED_BLOCKS
+inline unsigned maxabs_blocks(const Geo &g) {
+  const long long rows = (long long)g.ny * g.nz;
+  return (unsigned)std::max(1LL, std::min<long long>(RED_BLOCKS, (rows + 31) / 32));
 }
 
 __global__ void k_maxdiv(Geo g, CFields3 u, unsigned long long *out) {
@@ -1233,12 +1254,15 @@ int upload_eref(dnsb_ctx *c, const double *eref, int nb) {
   const Geo &g = c->g;
   int rc;
   if (clamp_direct(c, nb)) {
-    if (!c->lsA) {  // scratch for the largest direct case (first clamp only)
+    if (!c->lsA) {  // scratch for the largest direct case and the x-phases (first clamp only)
       if ((rc = dalloc(c, &c->lsA, (size_t)3 * LS_KX * g.ny * g.nz)) ||
           (rc = dalloc(c, &c->lsB, (size_t)3 * LS_KX * g.nz * LS_KY)) ||
           (rc = dalloc(c, &c->lsG, (size_t)3 * LS_KX * LS_KY * LS_KY)) ||
-          (rc = dalloc(c, &c->lsH, (size_t)3 * LS_KX * LS_KY * g.nz)))
+          (rc = dalloc(c, &c->lsH, (size_t)3 * LS_KX * LS_KY * g.nz)) ||
+          (rc = dalloc(c, &c->lsX, (size_t)g.nx)))
         return rc;
+      k_ls_xphase<<<(g.nx + 255) / 256, 256, 0, c->stream>>>(g.nx, c->lsX);
+      CKL(c);
     }
   } else if (!c->Sx[0]) {  // the transform clamp keeps all three spectra
     const size_t nspec = (size_t)g.nkx * g.ny * g.nz;
@@ -1797,38 +1821,39 @@ __global__ void k_sfs_stage(Geo g, const double *__restrict__ tau, Fields3 q, Fi
   const long long n3 = (long long)g.nx * g.ny * g.nz;
   double f[3] = {0.0, 0.0, 0.0};
   if (tau) {
-    auto T = [&](int c, int a, int b, int d) {  // component c at cell (a, b, d), periodic
-      a = (a + g.nx) % g.nx;
-      b = (b + g.ny) % g.ny;
-      d = (d + g.nz) % g.nz;
+    // periodic neighbours, wrapped once per cell
+    const int ip = i + 1 == g.nx ? 0 : i + 1, im = i == 0 ? g.nx - 1 : i - 1;
+    const int jp = j + 1 == g.ny ? 0 : j + 1, jm = j == 0 ? g.ny - 1 : j - 1;
+    const int kp = k + 1 == g.nz ? 0 : k + 1, km = k == 0 ? g.nz - 1 : k - 1;
+    auto T = [&](int c, int a, int b, int d) {  // component c at cell (a, b, d), wrapped
       return __ldg(tau + c * n3 + ((long long)d * g.ny + b) * g.nx + a);
     };
     const double rdy = g.rdy[J], rdyu = g.rdyu[J];
     // x-face between cells i, i+1
     {
-      const double dxx = (T(0, i + 1, j, k) - T(0, i, j, k)) * g.rdx;
-      const double en = 0.25 * (T(3, i, j, k) + T(3, i + 1, j, k) + T(3, i, j + 1, k) + T(3, i + 1, j + 1, k));
-      const double es = 0.25 * (T(3, i, j, k) + T(3, i + 1, j, k) + T(3, i, j - 1, k) + T(3, i + 1, j - 1, k));
-      const double eu = 0.25 * (T(5, i, j, k) + T(5, i + 1, j, k) + T(5, i, j, k + 1) + T(5, i + 1, j, k + 1));
-      const double ed = 0.25 * (T(5, i, j, k) + T(5, i + 1, j, k) + T(5, i, j, k - 1) + T(5, i + 1, j, k - 1));
+      const double dxx = (T(0, ip, j, k) - T(0, i, j, k)) * g.rdx;
+      const double en = 0.25 * (T(3, i, j, k) + T(3, ip, j, k) + T(3, i, jp, k) + T(3, ip, jp, k));
+      const double es = 0.25 * (T(3, i, j, k) + T(3, ip, j, k) + T(3, i, jm, k) + T(3, ip, jm, k));
+      const double eu = 0.25 * (T(5, i, j, k) + T(5, ip, j, k) + T(5, i, j, kp) + T(5, ip, j, kp));
+      const double ed = 0.25 * (T(5, i, j, k) + T(5, ip, j, k) + T(5, i, j, km) + T(5, ip, j, km));
       f[0] = -(dxx + (en - es) * rdy + (eu - ed) * g.rdz);
     }
     // y-face between cells j, j+1
     {
-      const double dyy = (T(1, i, j + 1, k) - T(1, i, j, k)) * rdyu;
-      const double ee = 0.25 * (T(3, i, j, k) + T(3, i, j + 1, k) + T(3, i + 1, j, k) + T(3, i + 1, j + 1, k));
-      const double ew = 0.25 * (T(3, i, j, k) + T(3, i, j + 1, k) + T(3, i - 1, j, k) + T(3, i - 1, j + 1, k));
-      const double eu = 0.25 * (T(4, i, j, k) + T(4, i, j + 1, k) + T(4, i, j, k + 1) + T(4, i, j + 1, k + 1));
-      const double ed = 0.25 * (T(4, i, j, k) + T(4, i, j + 1, k) + T(4, i, j, k - 1) + T(4, i, j + 1, k - 1));
+      const double dyy = (T(1, i, jp, k) - T(1, i, j, k)) * rdyu;
+      const double ee = 0.25 * (T(3, i, j, k) + T(3, i, jp, k) + T(3, ip, j, k) + T(3, ip, jp, k));
+      const double ew = 0.25 * (T(3, i, j, k) + T(3, i, jp, k) + T(3, im, j, k) + T(3, im, jp, k));
+      const double eu = 0.25 * (T(4, i, j, k) + T(4, i, jp, k) + T(4, i, j, kp) + T(4, i, jp, kp));
+      const double ed = 0.25 * (T(4, i, j, k) + T(4, i, jp, k) + T(4, i, j, km) + T(4, i, jp, km));
       f[1] = -((ee - ew) * g.rdx + dyy + (eu - ed) * g.rdz);
     }
     // z-face between cells k, k+1
     {
-      const double dzz = (T(2, i, j, k + 1) - T(2, i, j, k)) * g.rdz;
-      const double ee = 0.25 * (T(5, i, j, k) + T(5, i, j, k + 1) + T(5, i + 1, j, k) + T(5, i + 1, j, k + 1));
-      const double ew = 0.25 * (T(5, i, j, k) + T(5, i, j, k + 1) + T(5, i - 1, j, k) + T(5, i - 1, j, k + 1));
-      const double en = 0.25 * (T(4, i, j, k) + T(4, i, j, k + 1) + T(4, i, j + 1, k) + T(4, i, j + 1, k + 1));
-      const double es = 0.25 * (T(4, i, j, k) + T(4, i, j, k + 1) + T(4, i, j - 1, k) + T(4, i, j - 1, k + 1));
+      const double dzz = (T(2, i, j, kp) - T(2, i, j, k)) * g.rdz;
+      const double ee = 0.25 * (T(5, i, j, k) + T(5, i, j, kp) + T(5, ip, j, k) + T(5, ip, j, kp));
+      const double ew = 0.25 * (T(5, i, j, k) + T(5, i, j, kp) + T(5, im, j, k) + T(5, im, j, kp));
+      const double en = 0.25 * (T(4, i, j, k) + T(4, i, j, kp) + T(4, i, jp, k) + T(4, i, jp, kp));
+      const double es = 0.25 * (T(4, i, j, k) + T(4, i, j, kp) + T(4, i, jm, k) + T(4, i, jm, kp));
       f[2] = -((ee - ew) * g.rdx + (en - es) * rdy + dzz);
     }
   }
@@ -1960,7 +1985,7 @@ int les_capture(dnsb_ctx *c, dnsb_cnn *cnn, double *ux, double *uy, double *uz, 
     return le == cudaSuccess ? 0 : fail(c, DNSB_ECUDA, "capture: %s: %s", what, cudaGetErrorString(le));
   };
   if (!rc) {
-    k_maxabs3<<<RED_BLOCKS, 256, 0, c->stream>>>(g, cf(ux, uy, uz), scratch, nullptr);
+    k_maxabs3<<<maxabs_blocks(g), 256, 0, c->stream>>>(g, cf(ux, uy, uz), scratch, nullptr);
     rc = launched("velocity maxima");
   }
   if (!rc) {
@@ -2130,7 +2155,7 @@ int dnsb_cfl(dnsb_ctx *c, const double *ux, const double *uy, const double *uz, 
   unsigned long long *scratch = c->umax + 3 * UMAX_SLOTS;
   if (!cached) {
     CK(c, cudaMemsetAsync(scratch, 0, 3 * sizeof(unsigned long long), c->stream));
-    k_maxabs3<<<RED_BLOCKS, 256, 0, c->stream>>>(c->g, cf(ux, uy, uz), scratch, c->deverr);
+    k_maxabs3<<<maxabs_blocks(c->g), 256, 0, c->stream>>>(c->g, cf(ux, uy, uz), scratch, c->deverr);
     CKL(c);
     CK(c, cudaMemcpyAsync(c->hostred, scratch, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream));
     CK(c, cudaStreamSynchronize(c->stream));
@@ -2283,7 +2308,7 @@ int dnsb_shell_clamp(dnsb_ctx *c, double *ux, double *uy, double *uz, const doub
     const Geo &g = c->g;
     const int KM = nb - 1;
     const unsigned lines = (unsigned)(((long long)g.ny * g.nz + LS_LINES - 1) / LS_LINES);
-    k_ls_xsums<<<lines, 32 * LS_LINES, 0, c->stream>>>(g, cf(ux, uy, uz), KM, c->lsA);
+    k_ls_xsums<<<lines, 32 * LS_LINES, 0, c->stream>>>(g, cf(ux, uy, uz), KM, c->lsX, c->lsA);
     CKL(c);
     k_ls_ysums<<<(unsigned)(3 * (KM + 1) * g.nz), 128, 0, c->stream>>>(g, c->lsA, KM, c->lsB);
     CKL(c);
@@ -2291,7 +2316,7 @@ int dnsb_shell_clamp(dnsb_ctx *c, double *ux, double *uy, double *uz, const doub
     CKL(c);
     k_ls_modes<<<1, 1024, 0, c->stream>>>(g, KM, c->lsG, c->lsH, E, er, f, nb);
     CKL(c);
-    k_ls_correct<<<lines, 32 * LS_LINES, 0, c->stream>>>(g, ff(ux, uy, uz), KM, c->lsH);
+    k_ls_correct<<<lines, 32 * LS_LINES, 0, c->stream>>>(g, ff(ux, uy, uz), KM, c->lsH, c->lsX);
     CKL(c);
     c->umax_for[0] = c->umax_for[1] = c->umax_for[2] = nullptr;
     return 0;

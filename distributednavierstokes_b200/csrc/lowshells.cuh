@@ -37,8 +37,20 @@ __device__ __forceinline__ double2 ls_phase(int m, int n, double sign) {
   return make_double2(c, sign * s);
 }
 
+// the x-phases e^{+2 pi i x / nx} = (cos, sin) for x = 0..nx-1, formed once
+// per context (the expression the partial sums evaluated per point before)
+__global__ void k_ls_xphase(int nx, double2 *__restrict__ xph) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nx) {
+    double sn, cs;
+    sincospi(2.0 * (double)i / (double)nx, &sn, &cs);
+    xph[i] = make_double2(cs, sn);
+  }
+}
+
 // A[((c * (KM+1) + kx) * nz + (K-1)) * ny + (J-1)] = sum_i u_c(i, J, K) e^{-2 pi i kx i / nx}
-__global__ void __launch_bounds__(256) k_ls_xsums(Geo g, CFields3 u, int KM, double2 *__restrict__ A) {
+__global__ void __launch_bounds__(256) k_ls_xsums(Geo g, CFields3 u, int KM, const double2 *__restrict__ xph,
+                                                  double2 *__restrict__ A) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const long long line = (long long)blockIdx.x * LS_LINES + warp;
   if (line >= (long long)g.ny * g.nz) return;
@@ -50,9 +62,8 @@ __global__ void __launch_bounds__(256) k_ls_xsums(Geo g, CFields3 u, int KM, dou
     for (int kx = 0; kx < LS_KX; kx++) acc[c][kx] = make_double2(0.0, 0.0);
   const int row = gidx(g, 1, J, K);
   for (int i = lane; i < g.nx; i += 32) {
-    double sn, cs;
-    sincospi(2.0 * (double)i / (double)g.nx, &sn, &cs);
-    const double2 z1 = make_double2(cs, -sn);
+    const double2 e = xph[i];
+    const double2 z1 = make_double2(e.x, -e.y);
     const double v[3] = {u.x[row + i], u.y[row + i], u.z[row + i]};
     double2 zk = make_double2(1.0, 0.0);
 #pragma unroll
@@ -231,7 +242,8 @@ __global__ void __launch_bounds__(1024) k_ls_modes(Geo g, int KM, double2 *__res
 // u_c(i, J, K) += Re sum_{kx, ky, kz} w(kx) G e^{+2 pi i (kx i/nx + ky j/ny + kz k/nz)},
 // then the periodic ghost images of the updated cells
 __global__ void __launch_bounds__(256) k_ls_correct(Geo g, Fields3 u, int KM,
-                                                    const double2 *__restrict__ Hz) {
+                                                    const double2 *__restrict__ Hz,
+                                                    const double2 *__restrict__ xph) {
   const int W = 2 * KM + 1, H = KM + 1;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const long long line = (long long)blockIdx.x * LS_LINES + warp;
@@ -260,9 +272,7 @@ __global__ void __launch_bounds__(256) k_ls_correct(Geo g, Fields3 u, int KM,
   double *fc[3] = {u.x, u.y, u.z};
   const int row = gidx(g, 1, J, K);
   for (int i = lane; i < g.nx; i += 32) {
-    double sn, cs;
-    sincospi(2.0 * (double)i / (double)g.nx, &sn, &cs);
-    const double2 z1 = make_double2(cs, sn);
+    const double2 z1 = xph[i];
     double d[3] = {0.0, 0.0, 0.0};
     double2 zk = make_double2(1.0, 0.0);
 #pragma unroll
