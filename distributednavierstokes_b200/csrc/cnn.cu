@@ -251,13 +251,15 @@ __global__ void k_batch_in(const float *x, const float *t, int B, int crop, int 
 // the periodic field with a halo of 4: from cell-centred values v[3][n^3]
 // or from the staggered ghosted FV fields (the cell average of the two
 // faces, operators.jl:71-72); scaled by in_scale
+// grid (ceil(P / blockDim.x), P, P): x along the threads, y and z from the
+// block (no division per voxel); the halo (HALO < n) wraps by one correction
 __global__ void k_infer_in(const double *v, const double *ux, const double *uy, const double *uz,
                            int n, int P, const float *in_scale, uint4 *x0) {
-  const long P3 = (long)P * P * P;
-  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= P3) return;
-  const int x = (int)(i % P), y = (int)((i / P) % P), z = (int)(i / ((long)P * P));
-  const int cx = ((x - HALO) % n + n) % n, cy = ((y - HALO) % n + n) % n, cz = ((z - HALO) % n + n) % n;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y, z = blockIdx.z;
+  if (x >= P) return;
+  const long i = ((long)z * P + y) * P + x;
+  auto wrap = [n](int a) { return a < 0 ? a + n : (a >= n ? a - n : a); };
+  const int cx = wrap(x - HALO), cy = wrap(y - HALO), cz = wrap(z - HALO);
   double a, b, c;
   if (v) {
     const long n3 = (long)n * n * n, gi = ((long)cz * n + cy) * n + cx;
@@ -998,10 +1000,14 @@ static int infer_common(dnsb_cnn *c, const double *v, const double *ux, const do
   int rc;
   if ((rc = ensure_dev(c))) return rc;
   Volume &V = c->inf;
-  const long P3 = (long)V.P * V.P * V.P;
+  if (V.side <= HALO) return cfail(c, DNSB_EUNSUP, "inference side %d <= halo %d", V.side, HALO);
   Prof p;
   prof_begin(c, p, 3, 0);
-  k_infer_in<<<(unsigned)((P3 + 255) / 256), 256, 0, c->stream>>>(v, ux, uy, uz, V.side, V.P, c->scales, V.in[0]);
+  {
+    const unsigned bx = std::min(256u, (unsigned)(V.P + 31) / 32 * 32);
+    k_infer_in<<<dim3((V.P + bx - 1) / bx, V.P, V.P), bx, 0, c->stream>>>(v, ux, uy, uz, V.side, V.P, c->scales,
+                                                                         V.in[0]);
+  }
   prof_end(c, p);
   CC(c, cudaGetLastError());
   // inference keeps no pre-activations (zout = nullptr)
