@@ -352,6 +352,10 @@ __global__ void __launch_bounds__(CONV_THREADS, 1)
   constexpr int NW = 8 * CO;                            // outputs per position
   constexpr int N = 3 * NW;                             // MMA columns: 96 or 48
   constexpr int NACC = 4;                               // accumulators in flight
+  // one epilogue group per accumulator: a group then waits for its
+  // accumulator's phases in order, so a parity wait never meets a barrier
+  // two phases behind (with fewer groups than accumulators it can)
+  static_assert(CONV_GROUPS == NACC, "one epilogue group per accumulator");
   constexpr uint32_t ACC_STRIDE = N <= 64 ? 64 : 128;   // TMEM columns per accumulator
   constexpr uint32_t NCOLS = NACC * ACC_STRIDE;         // 256 or 512 columns
   constexpr int MAXSLOT = 12;
