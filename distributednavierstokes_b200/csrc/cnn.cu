@@ -15,6 +15,7 @@
 #include <cstdarg>
 #include <cstdint>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -346,6 +347,7 @@ struct dnsb_cnn {
   double prof_ms[4] = {}, prof_flops[4] = {};
   long prof_n[4] = {};
   unsigned long long serial = 0;  // creation number, unique in the process
+  bool pdl = true;  // convolutions launched as programmatic dependents (DNSB_CNN_PDL=0: ordinary)
 };
 
 namespace dnsb_internal {
@@ -635,7 +637,20 @@ int run_conv(dnsb_cnn *c, Volume &V, int L, const CUtensorMap &map, bool transpo
   const double flops = 2.0 * 27 * CIN[L] * COUT[L] * V.B * pow((double)(V.P - 2 * (L + 1)), 3);
   Prof p;
   prof_begin(c, p, kind, flops);
-  k_conv<CI, CO, MODE><<<grid, CONV_THREADS, smem, c->stream>>>(map, a);
+  {
+    // programmatic dependent launch (the kernel waits before any memory access)
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3(CONV_THREADS);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = c->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = c->pdl ? 1 : 0;
+    CC(c, cudaLaunchKernelEx(&cfg, k_conv<CI, CO, MODE>, map, a));
+  }
   prof_end(c, p);
   CC(c, cudaGetLastError());
   return 0;
@@ -766,6 +781,10 @@ int dnsb_cnn_create(int device, void *stream, int batch, int crop, int nfield, d
   c->serial = ++created;
   c->device = device;
   c->stream = (cudaStream_t)stream;
+  {
+    const char *e = getenv("DNSB_CNN_PDL");
+    if (e && atoi(e) == 0) c->pdl = false;
+  }
   auto bail = [&](int rc) {
     if (!c->err.empty()) cfail(nullptr, rc, "%s", c->err.c_str());
     dnsb_cnn_destroy(c);

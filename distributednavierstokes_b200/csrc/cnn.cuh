@@ -380,6 +380,10 @@ __global__ void __launch_bounds__(CONV_THREADS, 1)
   // this CTA's tiles
   const int t0 = (int)((long long)a.ntiles * blockIdx.x / gridDim.x);
   const int t1 = (int)((long long)a.ntiles * (blockIdx.x + 1) / gridDim.x);
+  // the next convolution may launch now: its blocks start once this grid's
+  // blocks have all started (this grid is one wave: grid_for) and wait for
+  // its completion before touching memory
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 
   if (threadIdx.x == 0) {
     for (int i = 0; i < a.nslot; i++) {
@@ -395,6 +399,11 @@ __global__ void __launch_bounds__(CONV_THREADS, 1)
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 1) tmem_alloc(tslot, NCOLS);
+  // programmatic dependent launch: the barrier set-up and the tensor-memory
+  // allocation above overlap the tail of the previous convolution; every
+  // read of global memory (biases, weights, input planes, zin, targets) and
+  // every write follows the wait (a no-op for an ordinary launch)
+  asm volatile("griddepcontrol.wait;" ::: "memory");
   if (warp == 2) bsm[lane] = MODE != DGRAD && lane < (CO == 4 ? 32 : 6) ? __ldg(a.bias + lane) : 0.f;
   tc_fence_before();
   __syncthreads();
