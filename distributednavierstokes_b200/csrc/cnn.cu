@@ -690,7 +690,20 @@ int run_wgrad(dnsb_cnn *c, Volume &V, int L) {
   const double flops = 2.0 * 27 * CIN[L] * COUT[L] * V.B * pow((double)a.Do, 3);
   Prof p;
   prof_begin(c, p, 2, flops);
-  k_wgrad<CI, CO><<<a.ngroups * a.nsplit, NTHREADS, smem, c->stream>>>(V.flatA[L], V.flatB[L], a);
+  {
+    // programmatic dependent launch (the kernel waits before any memory access)
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(a.ngroups * a.nsplit));
+    cfg.blockDim = dim3(NTHREADS);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = c->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = c->pdl ? 1 : 0;
+    CC(c, cudaLaunchKernelEx(&cfg, k_wgrad<CI, CO>, V.flatA[L], V.flatB[L], a));
+  }
   prof_end(c, p);
   CC(c, cudaGetLastError());
   const int N = 8 * CO;

@@ -776,6 +776,9 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   const bool ones = grp == a.ngroups - 1 && a.ones_slot < G;
   const int k0 = (int)((long long)a.nk * split / a.nsplit);
   const int k1 = (int)((long long)a.nk * (split + 1) / a.nsplit);
+  // programmatic dependent launch: dependents may launch once every block
+  // of this grid has started; they wait for its completion before memory
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 
   if (threadIdx.x == 0) {
     for (int i = 0; i < a.stages; i++) {
@@ -796,6 +799,9 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
   if (warp == 1) tmem_alloc(tslot, NCOLS);
+  // the previous kernel's outputs (activations, gradients) complete and
+  // visible past this (a no-op for an ordinary launch)
+  asm volatile("griddepcontrol.wait;" ::: "memory");
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
