@@ -136,7 +136,8 @@ struct dnsb_ctx {
   double2 *S = nullptr;
   double2 *Sx[2] = {nullptr, nullptr};  // spectra of u.y, u.z during a shell clamp
   double2 *lsA = nullptr, *lsB = nullptr, *lsG = nullptr, *lsH = nullptr;  // low-shell clamp scratch
-  double2 *lsX = nullptr;  // e^{2 pi i x / nx}, x = 0..nx-1, for the clamp's x-sums
+  // e^{2 pi i r / n}, r = 0..n-1, per direction, for the clamp's partial sums
+  double2 *lsX = nullptr, *lsY = nullptr, *lsZ = nullptr;
   double *work = nullptr;
   double *ycin = nullptr;  // c' entering each y-chunk, per (kx, kz) line
   double *r = nullptr;
@@ -1259,9 +1260,12 @@ int upload_eref(dnsb_ctx *c, const double *eref, int nb) {
           (rc = dalloc(c, &c->lsB, (size_t)3 * LS_KX * g.nz * LS_KY)) ||
           (rc = dalloc(c, &c->lsG, (size_t)3 * LS_KX * LS_KY * LS_KY)) ||
           (rc = dalloc(c, &c->lsH, (size_t)3 * LS_KX * LS_KY * g.nz)) ||
-          (rc = dalloc(c, &c->lsX, (size_t)g.nx)))
+          (rc = dalloc(c, &c->lsX, (size_t)g.nx)) || (rc = dalloc(c, &c->lsY, (size_t)g.ny)) ||
+          (rc = dalloc(c, &c->lsZ, (size_t)g.nz)))
         return rc;
-      k_ls_xphase<<<(g.nx + 255) / 256, 256, 0, c->stream>>>(g.nx, c->lsX);
+      k_ls_phases<<<(g.nx + 255) / 256, 256, 0, c->stream>>>(g.nx, c->lsX);
+      k_ls_phases<<<(g.ny + 255) / 256, 256, 0, c->stream>>>(g.ny, c->lsY);
+      k_ls_phases<<<(g.nz + 255) / 256, 256, 0, c->stream>>>(g.nz, c->lsZ);
       CKL(c);
     }
   } else if (!c->Sx[0]) {  // the transform clamp keeps all three spectra
@@ -2310,13 +2314,13 @@ int dnsb_shell_clamp(dnsb_ctx *c, double *ux, double *uy, double *uz, const doub
     const unsigned lines = (unsigned)(((long long)g.ny * g.nz + LS_LINES - 1) / LS_LINES);
     k_ls_xsums<<<lines, 32 * LS_LINES, 0, c->stream>>>(g, cf(ux, uy, uz), KM, c->lsX, c->lsA);
     CKL(c);
-    k_ls_ysums<<<(unsigned)(3 * (KM + 1) * g.nz), 128, 0, c->stream>>>(g, c->lsA, KM, c->lsB);
+    k_ls_ysums<<<(unsigned)(3 * (KM + 1) * g.nz), 128, 0, c->stream>>>(g, c->lsA, KM, c->lsY, c->lsB);
     CKL(c);
-    k_ls_zsums<<<(unsigned)(3 * (KM + 1) * (2 * KM + 1)), 128, 0, c->stream>>>(g, c->lsB, KM, c->lsG);
+    k_ls_zsums<<<(unsigned)(3 * (KM + 1) * (2 * KM + 1)), 128, 0, c->stream>>>(g, c->lsB, KM, c->lsZ, c->lsG);
     CKL(c);
-    k_ls_modes<<<1, 1024, 0, c->stream>>>(g, KM, c->lsG, c->lsH, E, er, f, nb);
+    k_ls_modes<<<1, 1024, 0, c->stream>>>(g, KM, c->lsG, c->lsH, E, er, f, nb, c->lsZ);
     CKL(c);
-    k_ls_correct<<<lines, 32 * LS_LINES, 0, c->stream>>>(g, ff(ux, uy, uz), KM, c->lsH, c->lsX);
+    k_ls_correct<<<lines, 32 * LS_LINES, 0, c->stream>>>(g, ff(ux, uy, uz), KM, c->lsH, c->lsX, c->lsY);
     CKL(c);
     c->umax_for[0] = c->umax_for[1] = c->umax_for[2] = nullptr;
     return 0;

@@ -27,25 +27,25 @@ constexpr int LS_KX = 4;             // kx = 0..3
 constexpr int LS_KY = 7;             // ky, kz = -3..3
 constexpr int LS_LINES = 8;          // (y, z) lines per CTA of 256 threads
 
-// e^{-2 pi i m / n} (sign -1) or e^{+2 pi i m / n} (sign +1) for integer m
-// (|m| < 2^31; 32-bit reduction, the 64-bit one costs far more)
-__device__ __forceinline__ double2 ls_phase(int m, int n, double sign) {
-  int r = m % n;
-  if (r < 0) r += n;
-  double s, c;
-  sincospi(2.0 * (double)r / (double)n, &s, &c);
-  return make_double2(c, sign * s);
+// the phases e^{+2 pi i r / n} = (cos, sin) for r = 0..n-1 of one direction,
+// formed once per context (the expression the partial sums evaluated per
+// point before)
+__global__ void k_ls_phases(int n, double2 *__restrict__ ph) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) {
+    double sn, cs;
+    sincospi(2.0 * (double)i / (double)n, &sn, &cs);
+    ph[i] = make_double2(cs, sn);
+  }
 }
 
-// the x-phases e^{+2 pi i x / nx} = (cos, sin) for x = 0..nx-1, formed once
-// per context (the expression the partial sums evaluated per point before)
-__global__ void k_ls_xphase(int nx, double2 *__restrict__ xph) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < nx) {
-    double sn, cs;
-    sincospi(2.0 * (double)i / (double)nx, &sn, &cs);
-    xph[i] = make_double2(cs, sn);
-  }
+// e^{-2 pi i m / n} (sign -1) or e^{+2 pi i m / n} (sign +1) for integer m
+// (|m| < 2^31, 32-bit reduction) from the direction's table
+__device__ __forceinline__ double2 ls_phase_tab(int m, int n, double sign, const double2 *__restrict__ ph) {
+  int r = m % n;
+  if (r < 0) r += n;
+  const double2 e = ph[r];
+  return make_double2(e.x, sign * e.y);
 }
 
 // A[((c * (KM+1) + kx) * nz + (K-1)) * ny + (J-1)] = sum_i u_c(i, J, K) e^{-2 pi i kx i / nx}
@@ -95,7 +95,7 @@ __global__ void __launch_bounds__(256) k_ls_xsums(Geo g, CFields3 u, int KM, con
 // = sum_j A[...][j] e^{-2 pi i ky j / ny}, each thread over a stride of j,
 // then a fixed-order tree reduction
 __global__ void __launch_bounds__(128) k_ls_ysums(Geo g, const double2 *__restrict__ A, int KM,
-                                                  double2 *__restrict__ B) {
+                                                  const double2 *__restrict__ yph, double2 *__restrict__ B) {
   const int W = 2 * KM + 1;
   const long long r = blockIdx.x;  // (c H + kx) nz + k
   const double2 *a = A + r * g.ny;
@@ -104,9 +104,8 @@ __global__ void __launch_bounds__(128) k_ls_ysums(Geo g, const double2 *__restri
   for (int q = 0; q < LS_KY; q++) acc[q] = make_double2(0.0, 0.0);
   for (int j = threadIdx.x; j < g.ny; j += blockDim.x) {
     const double2 v = a[j];
-    double sn, cs;
-    sincospi(2.0 * (double)j / (double)g.ny, &sn, &cs);
-    const double2 z1 = make_double2(cs, -sn);    // e^{-2 pi i j / ny}
+    const double2 e = yph[j];
+    const double2 z1 = make_double2(e.x, -e.y);  // e^{-2 pi i j / ny}
     double2 zp = v, zm = v;                      // v e^{-+2 pi i ky j / ny}, ky = 0, 1, ..
     acc[KM] = cadd(acc[KM], v);
 #pragma unroll
@@ -136,7 +135,7 @@ __global__ void __launch_bounds__(128) k_ls_ysums(Geo g, const double2 *__restri
 // z-sums, one block of 128 per (c, kx, ky): Gm[((c H + kx) W + ky + KM) W + kz + KM]
 // = sum_k B[...][k] e^{-2 pi i kz k / nz} (the modes u_hat), fixed-order tree
 __global__ void __launch_bounds__(128) k_ls_zsums(Geo g, const double2 *__restrict__ B, int KM,
-                                                  double2 *__restrict__ Gm) {
+                                                  const double2 *__restrict__ zph, double2 *__restrict__ Gm) {
   const int W = 2 * KM + 1;
   const int r = blockIdx.x;  // (c H + kx) W + ky + KM
   const int ckx = r / W, kyi = r % W;
@@ -145,9 +144,8 @@ __global__ void __launch_bounds__(128) k_ls_zsums(Geo g, const double2 *__restri
   for (int q = 0; q < LS_KY; q++) acc[q] = make_double2(0.0, 0.0);
   for (int k = threadIdx.x; k < g.nz; k += blockDim.x) {
     const double2 v = B[((long long)ckx * g.nz + k) * W + kyi];
-    double sn, cs;
-    sincospi(2.0 * (double)k / (double)g.nz, &sn, &cs);
-    const double2 z1 = make_double2(cs, -sn);  // e^{-2 pi i k / nz}
+    const double2 e = zph[k];
+    const double2 z1 = make_double2(e.x, -e.y);  // e^{-2 pi i k / nz}
     double2 zp = v, zm = v;
     acc[KM] = cadd(acc[KM], v);
 #pragma unroll
@@ -181,7 +179,8 @@ __global__ void __launch_bounds__(128) k_ls_zsums(Geo g, const double2 *__restri
 __global__ void __launch_bounds__(1024) k_ls_modes(Geo g, int KM, double2 *__restrict__ Gm,
                                                    double2 *__restrict__ Hz, double *__restrict__ E,
                                                    const double *__restrict__ eref,
-                                                   double *__restrict__ f, int nb) {
+                                                   double *__restrict__ f, int nb,
+                                                   const double2 *__restrict__ zph) {
   const int W = 2 * KM + 1, H = KM + 1;
   const double N = (double)g.nx * g.ny * g.nz;
   const int nM = 3 * H * W * W;
@@ -234,7 +233,7 @@ __global__ void __launch_bounds__(1024) k_ls_modes(Geo g, int KM, double2 *__res
     const int k = t % g.nz, r = t / g.nz;  // r = (c H + kx) W + ky + KM
     double2 sacc = make_double2(0.0, 0.0);
     for (int kzi = 0; kzi < W; kzi++)
-      sacc = cadd(sacc, cmul(Gm[r * W + kzi], ls_phase((kzi - KM) * k, g.nz, 1.0)));
+      sacc = cadd(sacc, cmul(Gm[r * W + kzi], ls_phase_tab((kzi - KM) * k, g.nz, 1.0, zph)));
     Hz[t] = sacc;
   }
 }
@@ -243,7 +242,8 @@ __global__ void __launch_bounds__(1024) k_ls_modes(Geo g, int KM, double2 *__res
 // then the periodic ghost images of the updated cells
 __global__ void __launch_bounds__(256) k_ls_correct(Geo g, Fields3 u, int KM,
                                                     const double2 *__restrict__ Hz,
-                                                    const double2 *__restrict__ xph) {
+                                                    const double2 *__restrict__ xph,
+                                                    const double2 *__restrict__ yph) {
   const int W = 2 * KM + 1, H = KM + 1;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const long long line = (long long)blockIdx.x * LS_LINES + warp;
@@ -256,7 +256,7 @@ __global__ void __launch_bounds__(256) k_ls_correct(Geo g, Fields3 u, int KM,
     const int c = lane / H, kx = lane % H;
     for (int kyi = 0; kyi < W; kyi++)
       P = cadd(P, cmul(Hz[((long long)(c * H + kx) * W + kyi) * g.nz + k],
-                       ls_phase((kyi - KM) * j, g.ny, 1.0)));
+                       ls_phase_tab((kyi - KM) * j, g.ny, 1.0, yph)));
     if (kx > 0) P = cscale(P, 2.0);
   }
   double2 Pc[3][LS_KX];
