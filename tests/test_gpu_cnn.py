@@ -163,3 +163,27 @@ def test_training_reduces_loss(C):
     print(f"training: loss {first:.4f} -> {last:.4f}")
     assert last < 0.5 * first
     cl.close()
+
+
+def test_dependent_launch_same_bits(C, monkeypatch):
+    """The convolutions and weight gradients launched as programmatic
+    dependents (the default) and as ordinary kernels (DNSB_CNN_PDL=0, read
+    when a closure is created) give the same bits: inference on a 24^3
+    field, and 20 Adam steps of a training batch (losses and parameters)."""
+    closure, O = C
+    rng = np.random.default_rng(21)
+    n = 24
+    v = torch.from_numpy(rng.standard_normal((3, n, n, n))).cuda()
+    data = torch.from_numpy(rng.standard_normal((3, 9, 16, 16, 16)).astype(np.float32)).cuda()
+    out = []
+    for flag in ("1", "0"):
+        monkeypatch.setenv("DNSB_CNN_PDL", flag)
+        cl = closure.Closure(batch=2, crop=8, nfield=n, seed=4)
+        cl.set_scales([1.0, 2.0, 0.5], [1.0] * 6)
+        tau = cl.infer_cells(v).cpu().numpy()
+        cl.set_dataset(data)
+        cl.train(20, lr=1e-3, seed=6)
+        out.append((tau, cl.losses().copy(), cl.get_params().copy()))
+        cl.close()
+    for a, b in zip(out[0], out[1]):
+        assert np.array_equal(a, b)
