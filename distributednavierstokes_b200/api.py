@@ -438,8 +438,7 @@ def step(u, p, q, delta, s, dt):
 
 class Ensemble:
     """A batched ensemble of independent setups (no counterpart in the
-    reference: the north star's ensemble of periodic boxes of uneven sizes and
-    viscosities).  run() advances every member nsteps RK3 steps of a fixed
+    reference: periodic boxes of uneven sizes and viscosities).  run() advances every member nsteps RK3 steps of a fixed
     step in one launch of a CUDA graph (a conditional while loop over one
     step of all members, member branches concurrent; captured once); the
     result equals stepping each member alone with step().  Members take the

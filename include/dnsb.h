@@ -159,8 +159,7 @@ int dnsb_project(dnsb_ctx *ctx, double *ux, double *uy, double *uz, double *psi)
  * edges), then u += B q with the ghost images of u rewritten.  tau: DEVICE
  * [6][nz][ny][nx] cell-centred components xx, yy, zz, xy, yz, zx (e.g.
  * from dnsb_cnn_infer; periodic boxes only); NULL gives the plain stage
- * update (any box).  The closure is the north star's addition; the
- * reference has no SFS model. */
+ * update (any box).  The reference has no SFS model. */
 int dnsb_sfs_stage(dnsb_ctx *ctx, const double *tau, double *qx, double *qy, double *qz,
                    double *ux, double *uy, double *uz, double dt, double B);
 
@@ -312,8 +311,8 @@ int dnsb_shell_clamp(dnsb_ctx *ctx, double *ux, double *uy, double *uz, const do
  * reported by dnsb_last_error(NULL). */
 int dnsb_poisson_noalloc(const dnsb_grid *grid, const double *r, double *p, void *stream);
 
-/* Ensembles (no counterpart in the reference; the batched periodic-box
- * ensemble of the north star): n independent members, each a context of its
+/* Ensembles (no counterpart in the reference; a batched ensemble of
+ * periodic boxes): n independent members, each a context of its
  * own grid and viscosity with its own stream.  dnsb_ensemble_run advances
  * every member nsteps RK3 steps with a fixed step dts[i] (dnsb_step on each
  * member) in ONE graph launch: the graph is a conditional while loop whose

@@ -4,7 +4,7 @@ Only the tests, the smoke check and the benchmark's CPU baseline use this
 module, as the checker of the device kernels; the product never imports it.
 
 The reference (DistributedNavierStokes) has no neural closure: the network
-is the north star's addition.  Its definition here is the one the device
+has no counterpart there.  Its definition here is the one the device
 kernels implement, restated in float64 numpy with the same storage
 roundings, so that the two can be compared:
 

@@ -1,7 +1,7 @@
 """The batched ensemble (dnsb_ensemble_*, api.Ensemble): members of uneven
 sizes and viscosities advanced through one CUDA graph must equal, bit for
-bit, each member stepped alone with dnsb_step (the north star's batched
-periodic-box ensemble; the reference has no ensemble path)."""
+bit, each member stepped alone with dnsb_step (a batched periodic-box
+ensemble; the reference has no ensemble path)."""
 import math
 
 import pytest

@@ -75,7 +75,7 @@ check_pressure = R.check_pressure
 
 
 
-CONFIGS = {
+GRID_CASES = {
     "periodic": dict(n=(16, 12, 8), visc=0.01, bodyforce=(0.3, 0.1, -0.2)),
     "channel": R.channel_kwargs(visc=0.05, bodyforce=(1.0, 0.0, 0.0)),
     "channel_implicit": R.channel_kwargs(visc=0.05, bodyforce=(1.0, 0.0, 0.0), ydiffusion="implicit"),
@@ -102,9 +102,9 @@ def test_halo_exact(oracle_mod, D, bcy, stag):
 
 # --------------------------------------------------------------- operators
 
-@pytest.mark.parametrize("cfg", list(CONFIGS))
+@pytest.mark.parametrize("cfg", list(GRID_CASES))
 def test_divergence_momentum_gradient(oracle_mod, D, cfg):
-    so, sd = both(oracle_mod, D, **CONFIGS[cfg])
+    so, sd = both(oracle_mod, D, **GRID_CASES[cfg])
     u = rand_fields(so)
     ud = to_dev(D, u)
     r = so.divergence(u)
@@ -133,7 +133,7 @@ def test_divergence_momentum_gradient(oracle_mod, D, cfg):
 
 @pytest.mark.parametrize("cfg", ["periodic", "channel", "ragged"])
 def test_poisson_and_project(oracle_mod, D, cfg):
-    so, sd = both(oracle_mod, D, **CONFIGS[cfg])
+    so, sd = both(oracle_mod, D, **GRID_CASES[cfg])
     u = rand_fields(so)
     ud = to_dev(D, u)
     r = so.divergence(u)
@@ -170,7 +170,7 @@ def test_poisson_recovers_pressure(oracle_mod, D, bcy):
 
 
 def test_imex_update(oracle_mod, D):
-    so, sd = both(oracle_mod, D, **CONFIGS["channel_implicit"])
+    so, sd = both(oracle_mod, D, **GRID_CASES["channel_implicit"])
     u = rand_fields(so)
     q = rand_fields(so, 5)
     p = so.scalarfield()
@@ -186,10 +186,10 @@ def test_imex_update(oracle_mod, D):
 
 # ----------------------------------------------------------------- stepping
 
-@pytest.mark.parametrize("cfg", list(CONFIGS))
+@pytest.mark.parametrize("cfg", list(GRID_CASES))
 def test_one_step(oracle_mod, D, cfg):
     """One RK3 step from the same projected random field: <= 1e-12 relative."""
-    so, sd = both(oracle_mod, D, **CONFIGS[cfg])
+    so, sd = both(oracle_mod, D, **GRID_CASES[cfg])
     u = rand_fields(so)
     p = so.scalarfield()
     so.project(u, p)
@@ -326,7 +326,7 @@ def test_fused_projection_momentum_planes(oracle_mod, D, cfg, planes, pipe, monk
     semi-implicit step agrees with the oracle."""
     monkeypatch.setenv("DNSB_GMZ", planes)
     monkeypatch.setenv("DNSB_GMPIPE", pipe)
-    kw = CONFIGS.get(cfg) or PRODUCTION[cfg]
+    kw = GRID_CASES.get(cfg) or PRODUCTION[cfg]
     so, sd = both(oracle_mod, D, **kw)
     u = rand_fields(so)
     p = so.scalarfield()
@@ -352,7 +352,7 @@ def test_momentum_march_planes(oracle_mod, D, cfg, planes, monkeypatch):
     nz = 8): one RK3 step agrees with the oracle (the production grids use
     16 planes, small boxes 2 to 8)."""
     monkeypatch.setenv("DNSB_MOMZ", planes)
-    kw = CONFIGS.get(cfg) or PRODUCTION[cfg]
+    kw = GRID_CASES.get(cfg) or PRODUCTION[cfg]
     so, sd = both(oracle_mod, D, **kw)
     u = rand_fields(so)
     p = so.scalarfield()
@@ -417,7 +417,7 @@ def T_offset(a):
 def test_one_step_unaligned_fields(oracle_mod, D, cfg):
     """Velocity fields that are not 16-byte aligned take the per-cell momentum
     kernel (the z-marching one copies 16-byte chunks): one RK3 step <= 1e-12."""
-    so, sd = both(oracle_mod, D, **CONFIGS[cfg])
+    so, sd = both(oracle_mod, D, **GRID_CASES[cfg])
     u = rand_fields(so)
     p = so.scalarfield()
     so.project(u, p)
@@ -635,7 +635,7 @@ def test_channel_flow_sanity(D):
 
 @pytest.mark.parametrize("cfg", ["periodic", "channel", "channel_implicit"])
 def test_reductions(oracle_mod, D, cfg):
-    so, sd = both(oracle_mod, D, **CONFIGS[cfg])
+    so, sd = both(oracle_mod, D, **GRID_CASES[cfg])
     u = rand_fields(so)
     ud = to_dev(D, u)
     assert D.cfl_timestep(ud, sd, 0.7) == so.cfl_timestep(u, 0.7)
