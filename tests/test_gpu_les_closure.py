@@ -187,10 +187,12 @@ def test_les_advance_matches_step_loop(M, graph, monkeypatch):
 def test_les_advance_graph_reuse(M):
     """The advance graph is captured once per argument set and relaunched
     for later intervals: closed and unclosed runs alternating on one
-    context over three intervals, a wait-limit change between two of them
-    (a new capture) and a closure created after the first one was closed
-    (a new capture even where the new closure reuses the old one's
-    address) each equal the step-by-step loop bit for bit."""
+    context over six intervals, a wait-limit change between two of them
+    (a new capture), the closure's per-launch timing on (the host loop) and
+    off again (the earlier graph relaunched), and a closure created after
+    the first one was closed (a new capture even where the new closure
+    reuses the old one's address) each equal the step-by-step loop bit for
+    bit."""
     dns, L = M
     from distributednavierstokes_b200 import _lib
     from distributednavierstokes_b200.closure import Closure
@@ -222,12 +224,17 @@ def test_les_advance_graph_reuse(M):
 
     cl = Closure(batch=0, crop=0, nfield=n, seed=5)
     cl.set_scales([2.0, 2.0, 2.0], [0.2] * 6)
-    times = (0.0, 0.15, 0.3, 0.45, 0.6)
-    for i in range(4):
+    times = (0.0, 0.15, 0.3, 0.45, 0.6, 0.75, 0.9)
+    for i in range(6):
         t0, t1 = times[i], times[i + 1]
         if i == 2:
             assert _lib.load().dnsb_set_wait_limit(s.ctx, 1 << 26) == 0
-        if i == 3:
+        if i == 3:  # the closure's per-launch timing on: the host loop
+            cl.profile(True)
+        if i == 4:  # off again: the graph captured at i == 2 is relaunched
+            cl.profile_read()
+            cl.profile(False)
+        if i == 5:
             cl.close()
             cl = Closure(batch=0, crop=0, nfield=n, seed=6)
             cl.set_scales([2.0, 2.0, 2.0], [0.2] * 6)
