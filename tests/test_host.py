@@ -24,6 +24,32 @@ def header_functions():
     return sorted(names)
 
 
+def header_arities():
+    """{name: number of parameters} of every prototype in include/*.h."""
+    out = {}
+    for h in sorted(os.listdir(os.path.join(ROOT, "include"))):
+        if not h.endswith(".h"):
+            continue
+        txt = open(os.path.join(ROOT, "include", h)).read()
+        txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+        txt = re.sub(r"//[^\n]*", "", txt)
+        for m in re.finditer(r"\b(dnsb_[a-z_0-9]+)\s*\(([^;{]*?)\)\s*;", txt):
+            params = " ".join(m.group(2).split())
+            out[m.group(1)] = 0 if params in ("", "void") else params.count(",") + 1
+    return out
+
+
+def test_binding_arities_match_headers():
+    """Every ctypes binding takes as many arguments as its C prototype (a
+    wrong count would shift the arguments of a call silently)."""
+    from distributednavierstokes_b200 import _lib
+
+    ar = header_arities()
+    assert sorted(ar) == sorted(_lib.SIGNATURES)
+    bad = {n: (ar[n], len(_lib.SIGNATURES[n][1])) for n in ar if ar[n] != len(_lib.SIGNATURES[n][1])}
+    assert not bad, bad
+
+
 def test_library_exports_every_header_symbol():
     from distributednavierstokes_b200 import _lib, build
 
